@@ -1,0 +1,92 @@
+/*
+ * pla_b200.h — additions of the B200 library that have no counterpart in the
+ * reference's headers.  Included by PLA.h.
+ */
+#ifndef PLA_B200_EXT_H
+#define PLA_B200_EXT_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Copy the message of the last fatal error into buf (NUL-terminated, at most
+ * len bytes).  Returns PLA_SUCCESS when no error has been recorded, else the
+ * PLA_ERROR code of that error.  The reference prints and exits instead
+ * (OBJ/PLA_Diagnostics.c:108-128). */
+int PLA_Last_error(char *buf, int len);
+int PLA_Clear_error(void);
+
+/* PLA_LU plus a LAPACK-style info: 0, or the 1-based index of the first exact
+ * zero pivot (the factorization still completes, as PLA_LU does). */
+int PLA_LU_info(PLA_Obj A, PLA_Obj pivots, int *info);
+
+/* The CUDA stream all library work is queued on (a cudaStream_t, passed as
+ * void*).  NULL selects the library's own stream.  Every PLA_* call returns
+ * after its work has completed on the device. */
+int PLA_B200_set_stream(void *stream);
+void *PLA_B200_get_stream(void);
+
+/* Fill or extract an object from a DEVICE buffer (column-major, ldim >= the
+ * object's length), for callers whose data is already in GPU memory.  The
+ * host-buffer forms are PLA_Obj_set/get_local_contents. */
+int PLA_Obj_set_local_contents_device(const void *dev_buf, int ldim, PLA_Obj obj);
+int PLA_Obj_get_local_contents_device(PLA_Obj obj, void *dev_buf, int ldim);
+
+/* Device time of the last solver call, in milliseconds, by phase. */
+typedef struct {
+  double total_ms;
+  double panel_ms;   /* panel factorization (iamax, swap, scale, rank-1)  */
+  double swap_ms;    /* row interchanges outside the panel                */
+  double trsm_ms;    /* triangular solves with the diagonal block         */
+  double update_ms;  /* trailing GEMM / SYRK                              */
+  double solve_ms;   /* triangular solves with the right-hand sides       */
+  double refine_ms;  /* residuals and corrections of iterative refinement */
+} PLA_Phase_times;
+int PLA_B200_phase_times(PLA_Phase_times *t);
+int PLA_B200_set_phase_timing(int on);
+
+/* ---- mixed-precision solve with FP64 iterative refinement ------------------
+ * Factor a low-precision copy of A (trailing updates on the tensor cores),
+ * then refine x in FP64 until the normwise backward error
+ *     ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf)
+ * reaches tol.  A is read, never overwritten; B (n x nrhs) is overwritten by
+ * X.  LU-IR corrects with the low-precision factors; GMRES-IR runs restarted
+ * GMRES on A preconditioned by them (FP64 residual, orthogonalisation and
+ * update).  The result is the same contract as PLA_General_solve /
+ * PLA_Pos_def_solve: X overwrites B. */
+#define PLA_B200_PREC_BF16   1   /* trailing update in bf16, fp32 accumulate */
+#define PLA_B200_PREC_FP16   2   /* trailing update in fp16, fp32 accumulate */
+#define PLA_B200_PREC_FP32   3   /* fp32 throughout                          */
+#define PLA_B200_IR_LU       1   /* classic iterative refinement             */
+#define PLA_B200_IR_GMRES    2   /* GMRES-IR                                 */
+
+typedef struct {
+  int precision;        /* PLA_B200_PREC_*                                  */
+  int refinement;       /* PLA_B200_IR_*                                    */
+  int max_iterations;   /* outer refinement steps (default 50)              */
+  int gmres_restart;    /* inner GMRES iterations per step (default 30)     */
+  int nb;               /* block size of the low-precision factorization; 0 = nb_alg */
+  double tol;           /* target backward error; <= 0 selects n * 2^-53    */
+} PLA_Mixed_params;
+
+typedef struct {
+  int converged;          /* 1 when backward_error <= tol for every column */
+  int iterations;         /* outer steps taken                              */
+  int inner_iterations;   /* total GMRES iterations                         */
+  int info;               /* LU: first zero pivot (1-based) or 0; Chol: failing column */
+  double backward_error;  /* max over columns                               */
+  double factor_ms;       /* device time of the factorization               */
+  double refine_ms;       /* device time of the refinement                  */
+} PLA_Mixed_report;
+
+void PLA_Mixed_params_default(PLA_Mixed_params *p);
+int PLA_General_solve_mixed(PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *params,
+                            PLA_Mixed_report *report);
+int PLA_Pos_def_solve_mixed(PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *params,
+                            PLA_Mixed_report *report);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

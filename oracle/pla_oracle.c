@@ -153,7 +153,7 @@ void oracle_fill_drand48(long seed, long count, double *out) {
         T t = (T)-1.0 * A[IDX(k, l, lda)];                                     \
         for (i = k; i < n; i++) A[IDX(i, k, lda)] += t * A[IDX(i, l, lda)];    \
       }                                                                        \
-      if (!(A[IDX(k, k, lda)] > 0)) return k + 1;                              \
+      if (A[IDX(k, k, lda)] <= 0) return k + 1;                                \
       A[IDX(k, k, lda)] = (T)sqrt(A[IDX(k, k, lda)]);                          \
       inv = (T)1.0 / A[IDX(k, k, lda)];                                        \
       for (i = k + 1; i < n; i++) A[IDX(i, k, lda)] = inv * A[IDX(i, k, lda)]; \

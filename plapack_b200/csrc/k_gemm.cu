@@ -1,0 +1,298 @@
+// GEMM for the trailing updates: C := alpha op(A) op(B) + beta C, optionally
+// restricted to the lower or upper triangle of C (the SYRK-shaped update of
+// SOLVERS/Cholesky/PLA_Chol.c:207-210).
+//
+// FP64: tensor-core DMMA (mma.sync m16n8k8 .f64; tcgen05 has no f64 kind).
+//   CTA tile 128 x 64, k-step 16, 8 warps as 4 (M) x 2 (N) with a 32 x 32
+//   warp tile; three cp.async stages; two CTAs per SM so one CTA's epilogue
+//   (the read-modify-write of C) overlaps the other's main loop.  Shared
+//   memory is padded so every f64 fragment load is bank-conflict free:
+//   A stage [16][128+4], B stage [64][16+4].
+// FP32: the same tiling with SIMT FFMA (used for float objects).
+#include <cstdint>
+
+#include "PLA.h"
+#include "pla_kernels.h"
+
+namespace {
+
+constexpr int BM = 128, BN = 64, BK = 16, STAGES = 3, THREADS = 256;
+constexpr int LDA_S = BM + 4;  // doubles per k-row of the A stage
+constexpr int LDB_S = BK + 4;  // doubles per n-row of the B stage
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool valid) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  int src_size = valid ? 8 : 0;  // 0 = fill the destination with zeros
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem),
+               "r"(src_size));
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem, bool valid) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  int src_size = valid ? 4 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem),
+               "r"(src_size));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *smem, const T *gmem, bool valid) {
+  if constexpr (sizeof(T) == 8) cp_async8(smem, gmem, valid);
+  else cp_async4(smem, gmem, valid);
+}
+
+// Stage one k-slab of op(A) (BM x BK) and op(B) (BK x BN) into shared memory.
+template <typename T, bool TA, bool TB>
+__device__ __forceinline__ void load_stage(T *As, T *Bs, const T *A, long lda, const T *B,
+                                           long ldb, int m, int n, int k, int m0, int n0,
+                                           int k0, int tid) {
+  // A: element (row, kk) of op(A) -> As[kk * LDA_S + row]
+#pragma unroll
+  for (int it = 0; it < (BM * BK) / THREADS; it++) {
+    int e = tid + it * THREADS;
+    int row, kk;
+    if (!TA) { row = e % BM; kk = e / BM; }   // A is m x k, rows contiguous
+    else     { kk = e % BK; row = e / BK; }   // A is k x m, k contiguous
+    int gi = m0 + row, gk = k0 + kk;
+    bool ok = gi < m && gk < k;
+    const T *src = ok ? (TA ? A + gk + (long)gi * lda : A + gi + (long)gk * lda) : A;
+    cp_async_elem(As + kk * LDA_S + row, src, ok);
+  }
+  // B: element (kk, col) of op(B) -> Bs[col * LDB_S + kk]
+#pragma unroll
+  for (int it = 0; it < (BK * BN) / THREADS; it++) {
+    int e = tid + it * THREADS;
+    int col, kk;
+    if (!TB) { kk = e % BK; col = e / BK; }   // B is k x n, k contiguous
+    else     { col = e % BN; kk = e / BN; }   // B is n x k, n contiguous
+    int gj = n0 + col, gk = k0 + kk;
+    bool ok = gj < n && gk < k;
+    const T *src = ok ? (TB ? B + gj + (long)gk * ldb : B + gk + (long)gj * ldb) : B;
+    cp_async_elem(Bs + col * LDB_S + kk, src, ok);
+  }
+}
+
+__device__ __forceinline__ void dmma_16x8x8(double (&d)[4], const double (&a)[4],
+                                            const double (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+__device__ __forceinline__ bool keep(int uplo, int i, int j) {
+  return uplo == 0 || (uplo == 'L' ? i >= j : i <= j);
+}
+
+// FP64 tensor-core GEMM
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(THREADS, 2)
+dgemm_k(int m, int n, int k, double alpha, const double *__restrict__ A, long lda,
+        const double *__restrict__ B, long ldb, double beta, double *C, long ldc, int uplo,
+        const int *status) {
+  extern __shared__ __align__(16) double smem[];
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  if (uplo == 'L' && m0 + BM - 1 < n0) return;  // tile strictly above the diagonal
+  if (uplo == 'U' && n0 + BN - 1 < m0) return;  // tile strictly below the diagonal
+  if (status && *status != PLA_K_OK) return;
+  double *As = smem;                          // [STAGES][BK][LDA_S]
+  double *Bs = smem + STAGES * BK * LDA_S;    // [STAGES][BN][LDB_S]
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
+  const int g = lane >> 2, t = lane & 3;
+
+  double acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[i][j][q] = 0.0;
+
+  const int nk = (k + BK - 1) / BK;
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; s++) {
+    if (s < nk)
+      load_stage<double, TA, TB>(As + s * BK * LDA_S, Bs + s * BN * LDB_S, A, lda, B, ldb, m, n,
+                                 k, m0, n0, s * BK, tid);
+    cp_commit();
+  }
+  for (int kt = 0; kt < nk; kt++) {
+    cp_wait<STAGES - 2>();
+    __syncthreads();
+    {  // prefetch stage kt + STAGES - 1 into the slot freed by stage kt - 1
+      int ks = kt + STAGES - 1;
+      if (ks < nk) {
+        int slot = ks % STAGES;
+        load_stage<double, TA, TB>(As + slot * BK * LDA_S, Bs + slot * BN * LDB_S, A, lda, B,
+                                   ldb, m, n, k, m0, n0, ks * BK, tid);
+      }
+      cp_commit();
+    }
+    const double *as = As + (kt % STAGES) * BK * LDA_S;
+    const double *bs = Bs + (kt % STAGES) * BN * LDB_S;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 8) {
+      double af[2][4], bf[4][2];
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+        const int r = wm + i * 16 + g;
+        af[i][0] = as[(kk + t) * LDA_S + r];
+        af[i][1] = as[(kk + t) * LDA_S + r + 8];
+        af[i][2] = as[(kk + t + 4) * LDA_S + r];
+        af[i][3] = as[(kk + t + 4) * LDA_S + r + 8];
+      }
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int c = wn + j * 8 + g;
+        bf[j][0] = bs[c * LDB_S + kk + t];
+        bf[j][1] = bs[c * LDB_S + kk + t + 4];
+      }
+#pragma unroll
+      for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) dmma_16x8x8(acc[i][j], af[i], bf[j]);
+    }
+  }
+  cp_wait<0>();
+
+  // epilogue: C = alpha * acc + beta * C, fragment (g, 2t), (g, 2t+1), (g+8, ...)
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int gi = m0 + wm + i * 16 + g + (q >> 1) * 8;
+        const int gj = n0 + wn + j * 8 + 2 * t + (q & 1);
+        if (gi < m && gj < n && keep(uplo, gi, gj)) {
+          double *cp = C + gi + (long)gj * ldc;
+          double v = alpha * acc[i][j][q];
+          *cp = beta == 0.0 ? v : fma(beta, *cp, v);
+        }
+      }
+}
+
+// FP32 SIMT GEMM with the same staging; each thread computes an 8 x 4 block
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(THREADS, 2)
+sgemm_k(int m, int n, int k, float alpha, const float *__restrict__ A, long lda,
+        const float *__restrict__ B, long ldb, float beta, float *C, long ldc, int uplo,
+        const int *status) {
+  extern __shared__ __align__(16) float fsm[];
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  if (uplo == 'L' && m0 + BM - 1 < n0) return;
+  if (uplo == 'U' && n0 + BN - 1 < m0) return;
+  if (status && *status != PLA_K_OK) return;
+  float *As = fsm;
+  float *Bs = fsm + STAGES * BK * LDA_S;
+  const int tid = threadIdx.x;
+  const int tm = (tid & 15) * 8, tn = (tid >> 4) * 4;  // 16 x 16 threads
+  float acc[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
+  const int nk = (k + BK - 1) / BK;
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; s++) {
+    if (s < nk)
+      load_stage<float, TA, TB>(As + s * BK * LDA_S, Bs + s * BN * LDB_S, A, lda, B, ldb, m, n,
+                                k, m0, n0, s * BK, tid);
+    cp_commit();
+  }
+  for (int kt = 0; kt < nk; kt++) {
+    cp_wait<STAGES - 2>();
+    __syncthreads();
+    int ks = kt + STAGES - 1;
+    if (ks < nk) {
+      int slot = ks % STAGES;
+      load_stage<float, TA, TB>(As + slot * BK * LDA_S, Bs + slot * BN * LDB_S, A, lda, B, ldb,
+                                m, n, k, m0, n0, ks * BK, tid);
+    }
+    cp_commit();
+    const float *as = As + (kt % STAGES) * BK * LDA_S;
+    const float *bs = Bs + (kt % STAGES) * BN * LDB_S;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk++) {
+      float a[8], b[4];
+#pragma unroll
+      for (int i = 0; i < 8; i++) a[i] = as[kk * LDA_S + tm + i];
+#pragma unroll
+      for (int j = 0; j < 4; j++) b[j] = bs[(tn + j) * LDB_S + kk];
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+  }
+  cp_wait<0>();
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      int gi = m0 + tm + i, gj = n0 + tn + j;
+      if (gi < m && gj < n && keep(uplo, gi, gj)) {
+        float *cp = C + gi + (long)gj * ldc;
+        float v = alpha * acc[i][j];
+        *cp = beta == 0.f ? v : fmaf(beta, *cp, v);
+      }
+    }
+}
+
+template <typename K>
+void set_smem(K kern, size_t bytes) {
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+}  // namespace
+
+extern "C" int pla_k_gemm(int dt, int transa, int transb, int m, int n, int k, double alpha,
+                          const void *A, long lda, const void *B, long ldb, double beta, void *C,
+                          long ldc, int uplo_c, const int *status, cudaStream_t s) {
+  if (m <= 0 || n <= 0) return 0;
+  if (k <= 0 || alpha == 0.0) {
+    if (beta == 1.0) return 0;
+    // C := beta C on the requested triangle: an empty main loop
+    k = 0;
+    alpha = 0.0;
+  }
+  const bool ta = transa != PLA_NO_TRANSPOSE, tb = transb != PLA_NO_TRANSPOSE;
+  dim3 grid((m + BM - 1) / BM, (n + BN - 1) / BN);
+  if (dt == MPI_DOUBLE) {
+    size_t sm = (size_t)STAGES * (BK * LDA_S + BN * LDB_S) * sizeof(double);
+    const double *a = (const double *)A, *b = (const double *)B;
+    double *c = (double *)C;
+#define L(TA_, TB_)                                                                          \
+  do {                                                                                       \
+    set_smem(dgemm_k<TA_, TB_>, sm);                                                         \
+    dgemm_k<TA_, TB_><<<grid, THREADS, sm, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, \
+                                                uplo_c, status);                             \
+  } while (0)
+    if (!ta && !tb) L(false, false);
+    else if (!ta && tb) L(false, true);
+    else if (ta && !tb) L(true, false);
+    else L(true, true);
+#undef L
+  } else if (dt == MPI_FLOAT) {
+    size_t sm = (size_t)STAGES * (BK * LDA_S + BN * LDB_S) * sizeof(float);
+    const float *a = (const float *)A, *b = (const float *)B;
+    float *c = (float *)C;
+#define L(TA_, TB_)                                                                            \
+  do {                                                                                         \
+    set_smem(sgemm_k<TA_, TB_>, sm);                                                           \
+    sgemm_k<TA_, TB_><<<grid, THREADS, sm, s>>>(m, n, k, (float)alpha, a, lda, b, ldb,          \
+                                                (float)beta, c, ldc, uplo_c, status);          \
+  } while (0)
+    if (!ta && !tb) L(false, false);
+    else if (!ta && tb) L(false, true);
+    else if (ta && !tb) L(true, false);
+    else L(true, true);
+#undef L
+  } else {
+    return (int)cudaErrorInvalidValue;
+  }
+  return (int)cudaGetLastError();
+}

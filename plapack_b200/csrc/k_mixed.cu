@@ -1,0 +1,158 @@
+// Kernels of the mixed-precision solvers:
+//   pack_rows   : fp32 column-major panel -> bf16/fp16 row-major (K-contiguous)
+//                 operand of the tensor-core trailing update, through a
+//                 32 x 32 shared tile so reads and writes stay coalesced;
+//   residual    : R = B - A X (or row sums of |A|) in FP64, split over column
+//                 slices so every SM streams A at full bandwidth; partial sums
+//                 land in a [slices][n] workspace and a second pass adds them
+//                 in a fixed order (deterministic).
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "PLA.h"
+#include "pla_kernels.h"
+
+namespace {
+
+template <typename D>
+__device__ inline D from_f32(float v);
+template <>
+__device__ inline __nv_bfloat16 from_f32<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+template <>
+__device__ inline __half from_f32<__half>(float v) { return __float2half_rn(v); }
+
+// dst[i * ldd + k] = src[i + k * lds] for i < m, k < kdim
+template <typename D>
+__global__ void pack_rows_k(int m, int kdim, const float *src, long lds, D *dst, long ldd) {
+  __shared__ float tile[32][33];
+  const int i0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    int i = i0 + threadIdx.x, k = k0 + r;
+    tile[r][threadIdx.x] = (i < m && k < kdim) ? src[i + (long)k * lds] : 0.f;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    int i = i0 + r, k = k0 + threadIdx.x;
+    if (i < m && k < kdim) dst[(long)i * ldd + k] = from_f32<D>(tile[threadIdx.x][r]);
+  }
+}
+
+constexpr int kRows = 256;
+
+// partial[s][i] = sum over j in slice s of op(A)(i, j) * X(j, r) for NR columns
+template <int NR, bool ABS>
+__global__ void __launch_bounds__(kRows)
+gemv_slices_k(int n, int ncols, int nrhs, int slice, const double *__restrict__ A, long lda,
+              const double *__restrict__ X, long ldx, double *__restrict__ partial) {
+  __shared__ double xs[NR][256];
+  const int i = blockIdx.x * kRows + threadIdx.x;
+  const int s = blockIdx.y;
+  const int j0 = s * slice, j1 = min(j0 + slice, ncols);
+  double acc[NR];
+#pragma unroll
+  for (int r = 0; r < NR; r++) acc[r] = 0.0;
+  for (int jb = j0; jb < j1; jb += 256) {
+    const int cnt = min(256, j1 - jb);
+    __syncthreads();
+    for (int t = threadIdx.x; t < cnt; t += kRows)
+#pragma unroll
+      for (int r = 0; r < NR; r++)
+        xs[r][t] = ABS ? 1.0 : (r < nrhs ? X[(jb + t) + (long)r * ldx] : 0.0);
+    __syncthreads();
+    if (i < n) {
+      const double *a = A + i + (long)jb * lda;
+#pragma unroll 8
+      for (int t = 0; t < cnt; t++) {
+        double v = a[(long)t * lda];
+        if (ABS) v = fabs(v);
+#pragma unroll
+        for (int r = 0; r < NR; r++) acc[r] = fma(v, xs[r][t], acc[r]);
+      }
+    }
+  }
+  if (i < n)
+#pragma unroll
+    for (int r = 0; r < NR; r++) partial[((long)s * NR + r) * n + i] = acc[r];
+}
+
+// R(i, r) = B(i, r) - sum_s partial[s][r][i]   (or the plain sum when B == 0)
+template <int NR>
+__global__ void gemv_reduce_k(int n, int nrhs, int slices, const double *partial, const double *B,
+                              long ldb, double *R, long ldr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+#pragma unroll
+  for (int r = 0; r < NR; r++) {
+    if (r >= nrhs) break;
+    double s = 0.0;
+    for (int q = 0; q < slices; q++) s += partial[((long)q * NR + r) * n + i];
+    R[i + (long)r * ldr] = B ? B[i + (long)r * ldb] - s : s;
+  }
+}
+
+int g_sms = 0;
+
+}  // namespace
+
+extern "C" int pla_k_pack_rows(int prec, int m, int kdim, const float *src, long lds, void *dst,
+                               long ldd, cudaStream_t s) {
+  if (m <= 0 || kdim <= 0) return 0;
+  dim3 grid((m + 31) / 32, (kdim + 31) / 32), block(32, 8);
+  if (prec == PLA_K_BF16)
+    pack_rows_k<__nv_bfloat16><<<grid, block, 0, s>>>(m, kdim, src, lds, (__nv_bfloat16 *)dst, ldd);
+  else
+    pack_rows_k<__half><<<grid, block, 0, s>>>(m, kdim, src, lds, (__half *)dst, ldd);
+  return (int)cudaGetLastError();
+}
+
+// R := B - A X for n x ncols A (FP64) and up to 16 columns of X; with abs_rows
+// set, R(:,0) := row sums of |A| (X and B unused).  `work` must hold
+// slices * nr * n doubles; pla_k_residual_work() gives the size.
+extern "C" size_t pla_k_residual_work(int n, int ncols, int nrhs) {
+  if (!g_sms) {
+    int d;
+    cudaGetDevice(&d);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, d);
+  }
+  int rb = (n + kRows - 1) / kRows;
+  int slices = (4 * g_sms + rb - 1) / rb;
+  if (slices < 1) slices = 1;
+  if (slices > 64) slices = 64;
+  int nr = nrhs <= 1 ? 1 : nrhs <= 2 ? 2 : nrhs <= 4 ? 4 : nrhs <= 8 ? 8 : 16;
+  (void)ncols;
+  return (size_t)slices * nr * n * sizeof(double);
+}
+
+extern "C" int pla_k_residual(int n, int ncols, int nrhs, const double *A, long lda,
+                              const double *X, long ldx, const double *B, long ldb, double *R,
+                              long ldr, int abs_rows, double *work, cudaStream_t s) {
+  if (n <= 0) return 0;
+  if (nrhs > 16) return (int)cudaErrorInvalidValue;
+  pla_k_residual_work(n, ncols, nrhs);
+  int rb = (n + kRows - 1) / kRows;
+  int slices = (4 * g_sms + rb - 1) / rb;
+  if (slices < 1) slices = 1;
+  if (slices > 64) slices = 64;
+  int slice = (ncols + slices - 1) / slices;
+  slices = (ncols + slice - 1) / slice;
+  if (slices < 1) slices = 1;
+  dim3 grid(rb, slices);
+  int rg = (n + 255) / 256;
+#define RUN(NR)                                                                               \
+  do {                                                                                        \
+    if (abs_rows)                                                                             \
+      gemv_slices_k<NR, true><<<grid, kRows, 0, s>>>(n, ncols, 1, slice, A, lda, X, ldx, work); \
+    else                                                                                      \
+      gemv_slices_k<NR, false><<<grid, kRows, 0, s>>>(n, ncols, nrhs, slice, A, lda, X, ldx,    \
+                                                      work);                                  \
+    gemv_reduce_k<NR><<<rg, 256, 0, s>>>(n, abs_rows ? 1 : nrhs, slices, work,                \
+                                         abs_rows ? nullptr : B, ldb, R, ldr);                \
+  } while (0)
+  if (abs_rows || nrhs <= 1) RUN(1);
+  else if (nrhs <= 2) RUN(2);
+  else if (nrhs <= 4) RUN(4);
+  else if (nrhs <= 8) RUN(8);
+  else RUN(16);
+#undef RUN
+  return (int)cudaGetLastError();
+}

@@ -1,0 +1,791 @@
+// Library state, templates, block sizes, diagnostics, objects, views and
+// their inquiry functions: the object layer of the reference (OBJ/, TEMPLATE/,
+// INCLUDE/PLA_Obj.h) on a 1x1 template with device-resident buffers.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "pla_internal.h"
+#include "pla_kernels.h"
+
+namespace pla {
+
+State &state() {
+  static State s;
+  return s;
+}
+
+int esize_of(MPI_Datatype dt) {
+  switch (dt) {
+    case MPI_CHAR: return 1;
+    case MPI_INT: return 4;
+    case MPI_FLOAT: return 4;
+    case MPI_DOUBLE: return 8;
+    case MPI_COMPLEX: return 8;
+    case MPI_DOUBLE_COMPLEX: return 16;
+    default: return 0;
+  }
+}
+
+bool valid(PLA_Obj o) { return o != nullptr && o->magic == kObjMagic && o->base != nullptr; }
+bool valid(PLA_Template t) { return t != nullptr && t->magic == kTempMagic; }
+
+cudaStream_t stream() {
+  State &s = state();
+  if (s.stream) return s.stream;
+  if (!s.own_stream) cudaStreamCreateWithFlags(&s.own_stream, cudaStreamNonBlocking);
+  return s.own_stream;
+}
+
+int fail(const char *message, int line, const char *file) {
+  State &s = state();
+  char buf[512];
+  snprintf(buf, sizeof buf, "PLAPACK error: %s (line %d of %s)", message, line, file);
+  s.last_message = buf;
+  s.last_error = PLA_ERROR;
+  if (getenv("PLA_B200_VERBOSE")) fprintf(stderr, "%s\n", buf);
+  return PLA_ERROR;
+}
+
+int cuda_fail(cudaError_t e, int line, const char *file) {
+  char buf[256];
+  snprintf(buf, sizeof buf, "CUDA error %d: %s", (int)e, cudaGetErrorString(e));
+  return fail(buf, line, file);
+}
+
+void warn(const char *message) {
+  if (getenv("PLA_B200_VERBOSE")) fprintf(stderr, "PLAPACK warning: %s\n", message);
+}
+
+double scalar_value(PLA_Obj s) {
+  double v = 0.0;
+  char tmp[16];
+  const char *p = at(s, 0, 0);
+  if (!s->base->on_host) {
+    cudaMemcpy(tmp, p, s->base->esize, cudaMemcpyDeviceToHost);
+    p = tmp;
+  }
+  switch (s->base->datatype) {
+    case MPI_DOUBLE: v = *(const double *)p; break;
+    case MPI_FLOAT: v = *(const float *)p; break;
+    case MPI_INT: v = *(const int *)p; break;
+    default: v = 0.0;
+  }
+  return v;
+}
+
+namespace {
+struct Scratch {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+};
+Scratch g_scratch[16];
+}  // namespace
+
+void *scratch(int slot, size_t bytes) {
+  Scratch &s = g_scratch[slot];
+  if (s.bytes >= bytes && s.ptr) return s.ptr;
+  if (s.ptr) {
+    cudaStreamSynchronize(stream());
+    cudaFree(s.ptr);
+    s.ptr = nullptr;
+    s.bytes = 0;
+  }
+  size_t want = bytes < 256 ? 256 : bytes;
+  if (cudaMalloc(&s.ptr, want) != cudaSuccess) {
+    s.ptr = nullptr;
+    return nullptr;
+  }
+  s.bytes = want;
+  return s.ptr;
+}
+
+void release_scratch() {
+  for (auto &s : g_scratch) {
+    if (s.ptr) cudaFree(s.ptr);
+    s.ptr = nullptr;
+    s.bytes = 0;
+  }
+}
+
+PhaseTimer::PhaseTimer(double *target) : acc(target), on(state().phase_timing != 0) {
+  if (!on) return;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, stream());
+}
+
+PhaseTimer::~PhaseTimer() {
+  if (!on) return;
+  cudaEventRecord(e1, stream());
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  *acc += ms;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+}
+
+}  // namespace pla
+
+using namespace pla;
+
+// ---------------------------------------------------------------- objects --
+static pla_base *new_base(MPI_Datatype dt, int length, int width, bool on_host, int *err) {
+  *err = PLA_SUCCESS;
+  int es = esize_of(dt);
+  if (es == 0) {
+    *err = fail("unsupported datatype", __LINE__, __FILE__);
+    return nullptr;
+  }
+  if (length < 0 || width < 0) {
+    *err = fail("negative object dimension", __LINE__, __FILE__);
+    return nullptr;
+  }
+  pla_base *b = new pla_base();
+  b->datatype = dt;
+  b->esize = es;
+  b->length = length;
+  b->width = width;
+  // leading dimension = global length, as OBJ/PLA_Obj.c:368 attaches it
+  b->ldim = length > 0 ? length : 1;
+  b->views = 0;
+  b->user_buffer = 0;
+  b->on_host = on_host ? 1 : 0;
+  size_t bytes = (size_t)b->ldim * (size_t)(width > 0 ? width : 1) * es;
+  cudaError_t e;
+  if (on_host)
+    e = cudaHostAlloc((void **)&b->buf, bytes, cudaHostAllocMapped | cudaHostAllocPortable);
+  else
+    e = cudaMalloc((void **)&b->buf, bytes);
+  if (e != cudaSuccess) {
+    delete b;
+    *err = cuda_fail(e, __LINE__, __FILE__);
+    return nullptr;
+  }
+  // objects start as zero (OBJ/PLA_Obj.c:370)
+  if (on_host)
+    memset(b->buf, 0, bytes);
+  else
+    cudaMemsetAsync(b->buf, 0, bytes, stream());
+  return b;
+}
+
+static PLA_Obj new_view(pla_base *b, int objtype, PLA_Template templ) {
+  PLA_Obj v = new PLA_Obj_view_struct();
+  v->magic = kObjMagic;
+  v->objtype = objtype;
+  v->fixed = 0;
+  v->length = b->length;
+  v->width = b->width;
+  v->row0 = v->col0 = 0;
+  v->align_row = v->align_col = 0;
+  v->owner_row = v->owner_col = 0;
+  v->proj_onto = PLA_PROJ_ONTO_COL;
+  v->templ = templ;
+  v->base = b;
+  b->views++;
+  return v;
+}
+
+static PLA_Obj copy_view(PLA_Obj src) {
+  PLA_Obj v = new PLA_Obj_view_struct(*src);
+  v->base->views++;
+  return v;
+}
+
+static void drop_view(PLA_Obj v) {
+  if (!v) return;
+  pla_base *b = v->base;
+  v->magic = 0;
+  delete v;
+  if (b && --b->views == 0) {
+    if (!b->user_buffer && b->buf) {
+      if (b->on_host) {
+        cudaFreeHost(b->buf);
+      } else {
+        cudaStreamSynchronize(stream());
+        cudaFree(b->buf);
+      }
+    }
+    delete b;
+  }
+}
+
+static int create(MPI_Datatype dt, int objtype, int length, int width, PLA_Template templ,
+                  bool on_host, PLA_Obj *out) {
+  if (!out) PLA_FAIL("null output handle");
+  if (state().check_parameters && !valid(templ)) PLA_FAIL("invalid template");
+  int err;
+  pla_base *b = new_base(dt, length, width, on_host, &err);
+  if (!b) return err;
+  PLA_Obj v = new_view(b, objtype, templ);
+  if (*out && valid(*out)) drop_view(*out);
+  *out = v;
+  return PLA_SUCCESS;
+}
+
+extern "C" {
+
+// ------------------------------------------------------ init and templates --
+int PLA_Init(MPI_Comm comm) {
+  State &s = state();
+  if (s.initialized) PLA_FAIL("PLA_Init called more than once");
+  if (comm == MPI_COMM_NULL) PLA_FAIL("Null communicator");
+  int dev = 0;
+  PLA_CUDA(cudaGetDevice(&dev));
+  PLA_CUDA(cudaFree(nullptr));  // create the context now
+  s.initialized = 1;
+  (void)stream();
+  return PLA_SUCCESS;
+}
+
+int PLA_Finalize(void) {
+  State &s = state();
+  if (!s.initialized) PLA_FAIL("PLAPACK not yet initialized");
+  cudaStreamSynchronize(stream());
+  release_scratch();
+  pla_kernels_release();
+  if (s.own_stream) {
+    cudaStreamDestroy(s.own_stream);
+    s.own_stream = nullptr;
+  }
+  s.initialized = 0;
+  return PLA_SUCCESS;
+}
+
+int PLA_Initialized(int *initialized) {
+  if (initialized) *initialized = state().initialized;
+  return state().initialized;
+}
+
+int PLA_Comm_1D_to_2D(MPI_Comm comm1d, int nprows, int npcols, MPI_Comm *comm2d) {
+  if (nprows * npcols != 1) PLA_FAIL("only a 1 x 1 mesh drives one GPU");
+  if (comm2d) *comm2d = comm1d;
+  return PLA_SUCCESS;
+}
+
+int PLA_Comm_1D_to_2D_ratio(MPI_Comm comm1d, float ratio, MPI_Comm *comm2d) {
+  (void)ratio;
+  if (comm2d) *comm2d = comm1d;
+  return PLA_SUCCESS;
+}
+
+int PLA_Temp_create(int nb, int zero_or_one, PLA_Template *templ) {
+  if (!templ) PLA_FAIL("null template handle");
+  if (nb <= 0) PLA_FAIL("template block size must be positive");
+  if (zero_or_one != 0 && zero_or_one != 1) PLA_FAIL("zero_or_one must be 0 or 1");
+  PLA_Template t = new PLA_Template_struct();
+  t->magic = kTempMagic;
+  t->nb = nb;
+  t->zero_or_one = zero_or_one;
+  t->refs = 1;
+  *templ = t;
+  return PLA_SUCCESS;
+}
+
+int PLA_Temp_free(PLA_Template *templ) {
+  if (!templ || !*templ) return PLA_SUCCESS;
+  if (!valid(*templ)) PLA_FAIL("invalid template");
+  (*templ)->magic = 0;
+  delete *templ;
+  *templ = nullptr;
+  return PLA_SUCCESS;
+}
+
+int PLA_Temp_nb(PLA_Template t, int *nb) {
+  if (!valid(t)) PLA_FAIL("invalid template");
+  *nb = t->nb;
+  return PLA_SUCCESS;
+}
+int PLA_Temp_zero_or_one(PLA_Template t, int *z) {
+  if (!valid(t)) PLA_FAIL("invalid template");
+  *z = t->zero_or_one;
+  return PLA_SUCCESS;
+}
+int PLA_Temp_comm_all_size(PLA_Template t, int *n) {
+  (void)t;
+  *n = 1;
+  return PLA_SUCCESS;
+}
+int PLA_Temp_comm_all_rank(PLA_Template t, int *r) {
+  (void)t;
+  *r = 0;
+  return PLA_SUCCESS;
+}
+
+// TEMPLATE/PLA_Environ.c:54-127: one algorithmic block size per operation class
+static int op_slot(int op) {
+  int k = op - PLA_OP_OFFSET - 1;
+  return (k >= 0 && k < 6) ? k : -1;
+}
+
+int pla_Environ_set_nb_alg(int op, int nb_alg) {
+  if (nb_alg <= 0) PLA_FAIL("nb_alg must be positive");
+  State &s = state();
+  if (op == PLA_OP_ALL_ALG) {
+    for (int &v : s.nb_alg) v = nb_alg;
+    return PLA_SUCCESS;
+  }
+  int k = op_slot(op);
+  if (k < 0) PLA_FAIL("unknown operation class");
+  s.nb_alg[k] = nb_alg;
+  return PLA_SUCCESS;
+}
+
+int PLA_Environ_nb_alg(int op, PLA_Template templ, int *nb_alg) {
+  (void)templ;
+  int k = op_slot(op);
+  *nb_alg = state().nb_alg[k < 0 ? 2 : k];
+  return PLA_SUCCESS;
+}
+
+// ------------------------------------------------------------- diagnostics --
+int PLA_Set_error_checking(int error, int parameters, int sequential, int r12) {
+  State &s = state();
+  s.error_checking = error;
+  // with error checking off every other check is off (PLA_Diagnostics.c:413)
+  s.check_parameters = error ? parameters : 0;
+  s.check_sequential = error ? sequential : 0;
+  s.check_r12 = error ? r12 : 0;
+  return PLA_SUCCESS;
+}
+
+int PLA_Get_error_checking(int *error, int *parameters, int *sequential, int *r12) {
+  State &s = state();
+  if (error) *error = s.error_checking;
+  if (parameters) *parameters = s.check_parameters;
+  if (sequential) *sequential = s.check_sequential;
+  if (r12) *r12 = s.check_r12;
+  return PLA_SUCCESS;
+}
+
+int PLA_Abort(char *message, int line, char *file) { return fail(message, line, file); }
+
+int PLA_Warning(char *message) {
+  warn(message);
+  return PLA_SUCCESS;
+}
+
+int PLA_Last_error(char *buf, int len) {
+  State &s = state();
+  if (buf && len > 0) {
+    strncpy(buf, s.last_message.c_str(), (size_t)len - 1);
+    buf[len - 1] = 0;
+  }
+  return s.last_error;
+}
+
+int PLA_Clear_error(void) {
+  state().last_error = 0;
+  state().last_message.clear();
+  return PLA_SUCCESS;
+}
+
+int PLA_B200_set_stream(void *s) {
+  state().stream = (cudaStream_t)s;
+  return PLA_SUCCESS;
+}
+void *PLA_B200_get_stream(void) { return (void *)stream(); }
+
+int PLA_B200_phase_times(PLA_Phase_times *t) {
+  if (t) *t = state().phases;
+  return PLA_SUCCESS;
+}
+int PLA_B200_set_phase_timing(int on) {
+  state().phase_timing = on;
+  return PLA_SUCCESS;
+}
+
+// ---------------------------------------------------------------- creation --
+int PLA_Matrix_create(MPI_Datatype dt, int length, int width, PLA_Template templ,
+                      int align_row, int align_col, PLA_Obj *obj) {
+  int r = create(dt, PLA_MATRIX, length, width, templ, false, obj);
+  if (r == PLA_SUCCESS) {
+    (*obj)->align_row = align_row == PLA_ALIGN_FIRST ? 0 : align_row;
+    (*obj)->align_col = align_col == PLA_ALIGN_FIRST ? 0 : align_col;
+  }
+  return r;
+}
+
+int PLA_Mvector_create(MPI_Datatype dt, int length, int width, PLA_Template templ, int align,
+                       PLA_Obj *obj) {
+  int r = create(dt, PLA_MVECTOR, length, width, templ, false, obj);
+  if (r == PLA_SUCCESS) (*obj)->align_row = align == PLA_ALIGN_FIRST ? 0 : align;
+  return r;
+}
+
+int PLA_Mscalar_create(MPI_Datatype dt, int owner_row, int owner_col, int length, int width,
+                       PLA_Template templ, PLA_Obj *obj) {
+  // duplicated multiscalars hold small host-side data (constants, pivot
+  // blocks): keep them in pinned, device-mapped host memory
+  bool small = (long)length * (long)width <= 4096;
+  int r = create(dt, PLA_MSCALAR, length, width, templ, small, obj);
+  if (r == PLA_SUCCESS) {
+    (*obj)->owner_row = owner_row;
+    (*obj)->owner_col = owner_col;
+  }
+  return r;
+}
+
+int PLA_Pmvector_create(MPI_Datatype dt, int project_onto, int owner, int length, int width,
+                        PLA_Template templ, int align, PLA_Obj *obj) {
+  // a projected multivector of a 1x1 mesh is an ordinary column-major block
+  int r = create(dt, PLA_PMVECTOR, length, width, templ, false, obj);
+  if (r == PLA_SUCCESS) {
+    (*obj)->proj_onto = project_onto;
+    (*obj)->owner_row = owner;
+    (*obj)->align_row = align == PLA_ALIGN_FIRST ? 0 : align;
+  }
+  return r;
+}
+
+int PLA_Matrix_create_conf_to(PLA_Obj o, PLA_Obj *obj) {
+  if (!valid(o)) PLA_FAIL("invalid object");
+  return PLA_Matrix_create(o->base->datatype, o->length, o->width, o->templ, o->align_row,
+                           o->align_col, obj);
+}
+
+int PLA_Mvector_create_conf_to(PLA_Obj o, int width, PLA_Obj *obj) {
+  if (!valid(o)) PLA_FAIL("invalid object");
+  // conformal to the object's length (a row projection already stores the
+  // matrix's row dimension as its length)
+  return PLA_Mvector_create(o->base->datatype, o->length, width, o->templ, o->align_row, obj);
+}
+
+int PLA_Mscalar_create_conf_to(PLA_Obj o, int owner_row, int owner_col, PLA_Obj *obj) {
+  if (!valid(o)) PLA_FAIL("invalid object");
+  return PLA_Mscalar_create(o->base->datatype, owner_row, owner_col, o->length, o->width,
+                            o->templ, obj);
+}
+
+int PLA_Pmvector_create_conf_to(PLA_Obj o, int project_onto, int owner, int width,
+                                PLA_Obj *obj) {
+  if (!valid(o)) PLA_FAIL("invalid object");
+  int length = project_onto == PLA_PROJ_ONTO_COL ? o->length : o->width;
+  int r = PLA_Pmvector_create(o->base->datatype, project_onto, owner, length, width, o->templ,
+                              o->align_row, obj);
+  return r;
+}
+
+int PLA_Create_constants_conf_to(PLA_Obj o, PLA_Obj *minus_one, PLA_Obj *zero,
+                                 PLA_Obj *one) {
+  if (!valid(o)) PLA_FAIL("invalid object");
+  MPI_Datatype dt = o->base->datatype;
+  if (dt == MPI_INT) dt = MPI_DOUBLE;
+  const double vals[3] = {-1.0, 0.0, 1.0};
+  PLA_Obj *outs[3] = {minus_one, zero, one};
+  for (int k = 0; k < 3; k++) {
+    if (!outs[k]) continue;
+    int r = PLA_Mscalar_create(dt, PLA_ALL_ROWS, PLA_ALL_COLS, 1, 1, o->templ, outs[k]);
+    if (r != PLA_SUCCESS) return r;
+    r = PLA_Obj_set(*outs[k], MPI_DOUBLE, (void *)&vals[k]);
+    if (r != PLA_SUCCESS) return r;
+    (*outs[k])->fixed = 1;
+  }
+  return PLA_SUCCESS;
+}
+
+int PLA_Obj_free(PLA_Obj *obj) {
+  if (!obj || !*obj) return PLA_SUCCESS;
+  if (!valid(*obj)) PLA_FAIL("invalid object");
+  drop_view(*obj);
+  *obj = nullptr;
+  return PLA_SUCCESS;
+}
+
+// ------------------------------------------------------------------- views --
+static void assign(PLA_Obj *out, PLA_Obj v) {
+  if (!out) {
+    drop_view(v);
+    return;
+  }
+  PLA_Obj old = *out;
+  *out = v;
+  if (old && valid(old)) drop_view(old);
+}
+
+int PLA_Obj_view(PLA_Obj o, int length, int width, int disp_row, int disp_col, PLA_Obj *view) {
+  if (!valid(o)) PLA_FAIL("invalid object");
+  if (length == PLA_DIM_ALL) length = o->length - disp_row;
+  if (width == PLA_DIM_ALL) width = o->width - disp_col;
+  if (disp_row < 0 || disp_col < 0 || length < 0 || width < 0 ||
+      disp_row + length > o->length || disp_col + width > o->width)
+    PLA_FAIL("view out of range");
+  PLA_Obj v = copy_view(o);
+  v->row0 += disp_row;
+  v->col0 += disp_col;
+  v->length = length;
+  v->width = width;
+  v->align_row += disp_row;
+  v->align_col += disp_col;
+  v->fixed = 0;
+  assign(view, v);
+  return PLA_SUCCESS;
+}
+
+int PLA_Obj_view_all(PLA_Obj o, PLA_Obj *view) {
+  if (!valid(o)) PLA_FAIL("invalid object");
+  PLA_Obj v = copy_view(o);
+  v->fixed = 0;
+  assign(view, v);
+  return PLA_SUCCESS;
+}
+
+int PLA_Obj_split_4(PLA_Obj o, int length, int width, PLA_Obj *tl, PLA_Obj *tr, PLA_Obj *bl,
+                    PLA_Obj *br) {
+  if (!valid(o)) PLA_FAIL("invalid object");
+  // sign selects which block the size describes (OBJ/PLA_Obj.c:2078-2088)
+  int top = length >= 0 ? length : o->length + length;
+  int left = width >= 0 ? width : o->width + width;
+  if (top < 0) top = 0;
+  if (top > o->length) top = o->length;
+  if (left < 0) left = 0;
+  if (left > o->width) left = o->width;
+  const int rows[2] = {top, o->length - top}, cols[2] = {left, o->width - left};
+  const int r0[2] = {0, top}, c0[2] = {0, left};
+  PLA_Obj *outs[4] = {tl, tr, bl, br};
+  PLA_Obj made[4] = {nullptr, nullptr, nullptr, nullptr};
+  for (int q = 0; q < 4; q++) {
+    if (!outs[q]) continue;
+    int i = q / 2, j = q % 2;
+    PLA_Obj v = copy_view(o);
+    v->row0 += r0[i];
+    v->col0 += c0[j];
+    v->align_row += r0[i];
+    v->align_col += c0[j];
+    v->length = rows[i];
+    v->width = cols[j];
+    v->fixed = 0;
+    made[q] = v;
+  }
+  for (int q = 0; q < 4; q++)
+    if (outs[q]) assign(outs[q], made[q]);
+  return PLA_SUCCESS;
+}
+
+int PLA_Obj_horz_split_2(PLA_Obj o, int length, PLA_Obj *top, PLA_Obj *bottom) {
+  if (!valid(o)) PLA_FAIL("invalid object");
+  return PLA_Obj_split_4(o, length, o->width, top, nullptr, bottom, nullptr);
+}
+
+int PLA_Obj_vert_split_2(PLA_Obj o, int width, PLA_Obj *left, PLA_Obj *right) {
+  if (!valid(o)) PLA_FAIL("invalid object");
+  return PLA_Obj_split_4(o, o->length, width, left, right, nullptr, nullptr);
+}
+
+// positive moves a boundary down / right (OBJ/PLA_Obj.c:3189-3201)
+int PLA_Obj_view_shift(PLA_Obj o, int shift_top, int shift_left, int shift_right,
+                       int shift_bottom) {
+  if (!valid(o)) PLA_FAIL("invalid object");
+  int row0 = o->row0 + shift_top, col0 = o->col0 + shift_left;
+  int length = o->length - shift_top + shift_bottom;
+  int width = o->width - shift_left + shift_right;
+  if (row0 < 0 || col0 < 0 || length < 0 || width < 0 || row0 + length > o->base->length ||
+      col0 + width > o->base->width)
+    PLA_FAIL("view shift leaves the base object");
+  o->row0 = row0;
+  o->col0 = col0;
+  o->align_row += shift_top;
+  o->align_col += shift_left;
+  o->length = length;
+  o->width = width;
+  return PLA_SUCCESS;
+}
+
+int PLA_Obj_view_swap(PLA_Obj *a, PLA_Obj *b) {
+  PLA_Obj t = *a;
+  *a = *b;
+  *b = t;
+  return PLA_SUCCESS;
+}
+
+// ----------------------------------------------------------------- inquiry --
+#define INQ(name, expr)                          \
+  int name(PLA_Obj o, int *out) {                \
+    if (!valid(o)) PLA_FAIL("invalid object");   \
+    *out = (expr);                               \
+    return PLA_SUCCESS;                          \
+  }
+INQ(PLA_Obj_objtype, o->objtype)
+INQ(PLA_Obj_global_length, o->length)
+INQ(PLA_Obj_global_width, o->width)
+INQ(PLA_Obj_global_name, 0)
+INQ(PLA_Obj_global_align_row, o->align_row)
+INQ(PLA_Obj_global_align_col, o->align_col)
+INQ(PLA_Obj_local_length, o->length)
+INQ(PLA_Obj_local_width, o->width)
+INQ(PLA_Obj_local_ldim, (int)o->base->ldim)
+INQ(PLA_Obj_local_stride, 1)
+INQ(PLA_Obj_owner_row, o->owner_row)
+INQ(PLA_Obj_owner_col, o->owner_col)
+INQ(PLA_Obj_project_onto, o->proj_onto)
+#undef INQ
+
+int PLA_Obj_datatype(PLA_Obj o, MPI_Datatype *dt) {
+  if (!valid(o)) PLA_FAIL("invalid object");
+  *dt = o->base->datatype;
+  return PLA_SUCCESS;
+}
+
+int PLA_Obj_template(PLA_Obj o, PLA_Template *t) {
+  if (!valid(o)) PLA_FAIL("invalid object");
+  *t = o->templ;
+  return PLA_SUCCESS;
+}
+
+int PLA_Obj_local_buffer(PLA_Obj o, void **buffer) {
+  if (!valid(o)) PLA_FAIL("invalid object");
+  *buffer = at(o, 0, 0);
+  return PLA_SUCCESS;
+}
+
+int PLA_Obj_set_orientation(PLA_Obj o, int project_onto) {
+  if (!valid(o)) PLA_FAIL("invalid object");
+  o->proj_onto = project_onto;
+  return PLA_SUCCESS;
+}
+
+// ---------------------------------------------------------------- contents --
+int PLA_Obj_set(PLA_Obj o, MPI_Datatype dt, void *value) {
+  if (!valid(o)) PLA_FAIL("invalid object");
+  double v;
+  if (dt == MPI_DOUBLE) v = *(double *)value;
+  else if (dt == MPI_FLOAT) v = *(float *)value;
+  else if (dt == MPI_INT) v = *(int *)value;
+  else PLA_FAIL("unsupported datatype of value");
+  if (o->length == 0 || o->width == 0) return PLA_SUCCESS;
+  if (o->base->on_host) {
+    for (int j = 0; j < o->width; j++)
+      for (int i = 0; i < o->length; i++) {
+        char *p = at(o, i, j);
+        switch (o->base->datatype) {
+          case MPI_DOUBLE: *(double *)p = v; break;
+          case MPI_FLOAT: *(float *)p = (float)v; break;
+          case MPI_INT: *(int *)p = (int)v; break;
+          default: break;
+        }
+      }
+    return PLA_SUCCESS;
+  }
+  int r = pla_k_fill(o->base->datatype, o->length, o->width, at(o, 0, 0), ld(o), v, stream());
+  if (r) PLA_FAIL("fill kernel failed");
+  PLA_CUDA(cudaStreamSynchronize(stream()));
+  return PLA_SUCCESS;
+}
+
+int PLA_Obj_set_to_zero(PLA_Obj o) {
+  double z = 0.0;
+  return PLA_Obj_set(o, MPI_DOUBLE, &z);
+}
+int PLA_Obj_set_to_one(PLA_Obj o) {
+  double z = 1.0;
+  return PLA_Obj_set(o, MPI_DOUBLE, &z);
+}
+int PLA_Obj_set_to_minus_one(PLA_Obj o) {
+  double z = -1.0;
+  return PLA_Obj_set(o, MPI_DOUBLE, &z);
+}
+
+int PLA_Obj_set_to_identity(PLA_Obj o) {
+  int r = PLA_Obj_set_to_zero(o);
+  if (r) return r;
+  int k = o->length < o->width ? o->length : o->width;
+  double one = 1.0;
+  for (int i = 0; i < k; i++) {
+    PLA_Obj e = nullptr;
+    PLA_Obj_view(o, 1, 1, i, i, &e);
+    PLA_Obj_set(e, MPI_DOUBLE, &one);
+    PLA_Obj_free(&e);
+  }
+  return PLA_SUCCESS;
+}
+
+// copy between a host buffer (column-major, ldim_buf, element stride) and the
+// object; trans = PLA_TRANSPOSE stores the transpose (OBJ/PLA_Obj.c)
+static int local_contents(bool to_obj, PLA_Obj o, int trans, void *buf, int ldim_buf,
+                          int stride_buf) {
+  const int m = o->length, n = o->width, es = o->base->esize;
+  if (m == 0 || n == 0) return PLA_SUCCESS;
+  if (stride_buf != 1) PLA_FAIL("only unit stride host buffers are supported");
+  if (trans == PLA_NO_TRANSPOSE) {
+    if (ldim_buf < m) PLA_FAIL("host leading dimension too small");
+    if (o->base->on_host) {
+      for (int j = 0; j < n; j++) {
+        char *d = at(o, 0, j), *h = (char *)buf + (size_t)j * ldim_buf * es;
+        if (to_obj) memcpy(d, h, (size_t)m * es);
+        else memcpy(h, d, (size_t)m * es);
+      }
+      return PLA_SUCCESS;
+    }
+    if (to_obj)
+      PLA_CUDA(cudaMemcpy2DAsync(at(o, 0, 0), ld(o) * es, buf, (size_t)ldim_buf * es,
+                                 (size_t)m * es, n, cudaMemcpyHostToDevice, stream()));
+    else
+      PLA_CUDA(cudaMemcpy2DAsync(buf, (size_t)ldim_buf * es, at(o, 0, 0), ld(o) * es,
+                                 (size_t)m * es, n, cudaMemcpyDeviceToHost, stream()));
+    PLA_CUDA(cudaStreamSynchronize(stream()));
+    return PLA_SUCCESS;
+  }
+  // transposed: element (i, j) of the object <-> buf[j + i * ldim_buf]
+  if (ldim_buf < n) PLA_FAIL("host leading dimension too small");
+  std::vector<char> tmp((size_t)m * n * es);
+  if (to_obj) {
+    for (int j = 0; j < n; j++)
+      for (int i = 0; i < m; i++)
+        memcpy(&tmp[((size_t)i + (size_t)j * m) * es],
+               (char *)buf + ((size_t)j + (size_t)i * ldim_buf) * es, es);
+    return local_contents(true, o, PLA_NO_TRANSPOSE, tmp.data(), m, 1);
+  }
+  int r = local_contents(false, o, PLA_NO_TRANSPOSE, tmp.data(), m, 1);
+  if (r) return r;
+  for (int j = 0; j < n; j++)
+    for (int i = 0; i < m; i++)
+      memcpy((char *)buf + ((size_t)j + (size_t)i * ldim_buf) * es,
+             &tmp[((size_t)i + (size_t)j * m) * es], es);
+  return PLA_SUCCESS;
+}
+
+int PLA_Obj_get_local_contents(PLA_Obj o, int trans, int *rows_in_buf, int *cols_in_buf,
+                               void *buf, int ldim_buf, int stride_buf) {
+  if (!valid(o)) PLA_FAIL("invalid object");
+  if (rows_in_buf) *rows_in_buf = trans == PLA_NO_TRANSPOSE ? o->length : o->width;
+  if (cols_in_buf) *cols_in_buf = trans == PLA_NO_TRANSPOSE ? o->width : o->length;
+  return local_contents(false, o, trans, buf, ldim_buf, stride_buf);
+}
+
+static int device_contents(bool to_obj, PLA_Obj o, void *dev, int ldim) {
+  if (!valid(o)) PLA_FAIL("invalid object");
+  const int m = o->length, n = o->width, es = o->base->esize;
+  if (m == 0 || n == 0) return PLA_SUCCESS;
+  if (ldim < m) PLA_FAIL("device leading dimension too small");
+  if (to_obj)
+    PLA_CUDA(cudaMemcpy2DAsync(at(o, 0, 0), ld(o) * es, dev, (size_t)ldim * es, (size_t)m * es, n,
+                               cudaMemcpyDefault, stream()));
+  else
+    PLA_CUDA(cudaMemcpy2DAsync(dev, (size_t)ldim * es, at(o, 0, 0), ld(o) * es, (size_t)m * es, n,
+                               cudaMemcpyDefault, stream()));
+  PLA_CUDA(cudaStreamSynchronize(stream()));
+  return PLA_SUCCESS;
+}
+
+int PLA_Obj_set_local_contents_device(const void *dev_buf, int ldim, PLA_Obj obj) {
+  return device_contents(true, obj, const_cast<void *>(dev_buf), ldim);
+}
+
+int PLA_Obj_get_local_contents_device(PLA_Obj obj, void *dev_buf, int ldim) {
+  return device_contents(false, obj, dev_buf, ldim);
+}
+
+int PLA_Obj_set_local_contents(int trans, int rows_in_buf, int cols_in_buf, void *buf,
+                               int ldim_buf, int stride_buf, PLA_Obj o) {
+  if (!valid(o)) PLA_FAIL("invalid object");
+  int m = trans == PLA_NO_TRANSPOSE ? rows_in_buf : cols_in_buf;
+  int n = trans == PLA_NO_TRANSPOSE ? cols_in_buf : rows_in_buf;
+  if (m != o->length || n != o->width) PLA_FAIL("buffer does not conform to the object");
+  return local_contents(true, o, trans, buf, ldim_buf, stride_buf);
+}
+
+}  // extern "C"

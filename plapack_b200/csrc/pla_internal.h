@@ -1,0 +1,116 @@
+// Internal declarations shared by the host-side translation units of
+// libplapack_b200.  Not installed; the public surface is include/PLA.h.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "PLA.h"
+
+// A base object owns one device (or, for multiscalars, pinned host) buffer;
+// views share it and count references, like PLA_Obj_base_struct in the
+// reference (INCLUDE/PLA_Obj.h:15-44, OBJ/PLA_Obj_management.c:63-110).
+struct pla_base {
+  MPI_Datatype datatype;
+  int esize;           // bytes per element
+  char *buf;           // device pointer (host pinned for PLA_MSCALAR)
+  long ldim;           // leading dimension in elements (column-major)
+  int length, width;   // size of the base object
+  int views;           // number of live views
+  int user_buffer;     // buffer not owned by the library
+  int on_host;         // buf is pinned host memory (duplicated multiscalars)
+};
+
+// A view: a rectangular window into a base object (INCLUDE/PLA_Obj.h:49-82).
+// On a 1x1 template every view is entirely local.
+struct PLA_Obj_view_struct {
+  unsigned magic;
+  int objtype;
+  int fixed;           // constants created by PLA_Create_constants_conf_to
+  int length, width;   // global (== local) size
+  int row0, col0;      // displacement inside the base
+  int align_row, align_col;
+  int owner_row, owner_col;
+  int proj_onto;
+  PLA_Template templ;
+  pla_base *base;
+};
+
+struct PLA_Template_struct {
+  unsigned magic;
+  int nb;
+  int zero_or_one;
+  int refs;
+};
+
+namespace pla {
+
+constexpr unsigned kObjMagic = 0x504c414fu;   // "PLAO"
+constexpr unsigned kTempMagic = 0x504c4154u;  // "PLAT"
+
+// library state (TEMPLATE/PLA_Init.c, TEMPLATE/PLA_Environ.c:46-52,
+// OBJ/PLA_Diagnostics.c:16-19)
+struct State {
+  int initialized = 0;
+  int nb_alg[8] = {128, 128, 128, 128, 128, 128, 128, 128};
+  int error_checking = 1;
+  int check_parameters = 1;
+  int check_sequential = 0;
+  int check_r12 = 0;
+  int api_active = 0;
+  int last_error = 0;
+  std::string last_message;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  int phase_timing = 0;
+  PLA_Phase_times phases{};
+};
+State &state();
+
+int esize_of(MPI_Datatype dt);
+bool valid(PLA_Obj obj);
+bool valid(PLA_Template t);
+cudaStream_t stream();
+
+// typed pointer to element (i, j) of a view (device pointer unless on_host)
+inline char *at(PLA_Obj v, long i, long j) {
+  return v->base->buf + ((long)(v->row0 + i) + (long)(v->col0 + j) * v->base->ldim) *
+                            v->base->esize;
+}
+inline long ld(PLA_Obj v) { return v->base->ldim; }
+inline bool is_double(PLA_Obj v) { return v->base->datatype == MPI_DOUBLE; }
+inline bool is_float(PLA_Obj v) { return v->base->datatype == MPI_FLOAT; }
+
+// value of a 1x1 scalar object as double (reads host or device memory)
+double scalar_value(PLA_Obj s);
+
+// error handling: records the message, returns PLA_ERROR; never exits
+int fail(const char *message, int line, const char *file);
+int cuda_fail(cudaError_t e, int line, const char *file);
+void warn(const char *message);
+
+// device scratch owned by the library (grown on demand, freed at PLA_Finalize)
+void *scratch(int slot, size_t bytes);
+void release_scratch();
+
+// phase timing helpers
+struct PhaseTimer {
+  cudaEvent_t e0{}, e1{};
+  double *acc;
+  bool on;
+  explicit PhaseTimer(double *target);
+  ~PhaseTimer();
+};
+
+}  // namespace pla
+
+#define PLA_CUDA(call)                                                   \
+  do {                                                                   \
+    cudaError_t e_ = (call);                                             \
+    if (e_ != cudaSuccess) return pla::cuda_fail(e_, __LINE__, __FILE__); \
+  } while (0)
+
+#define PLA_FAIL(msg) return pla::fail((msg), __LINE__, __FILE__)

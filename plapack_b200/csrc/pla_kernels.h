@@ -1,0 +1,116 @@
+// Thin C ABI between the host library and the CUDA kernels (sm_100a).
+// Every matrix is column-major with an explicit leading dimension (elements);
+// every launch goes on the given stream and returns 0 on success, else a
+// cudaError_t value.  `dt` is MPI_DOUBLE or MPI_FLOAT unless noted.
+#pragma once
+
+#include <cstddef>
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status word: kernels report failures here instead of trapping ---- */
+#define PLA_K_OK 0
+#define PLA_K_TIMEOUT 1        /* a bounded wait gave up (grid barrier)   */
+#define PLA_K_NOT_SPD 2        /* Cholesky met a non-positive pivot       */
+
+void pla_kernels_release(void);
+
+int pla_k_fill(int dt, int m, int n, void *A, long lda, double value, cudaStream_t s);
+/* Y := alpha * X + beta * Y (beta == 0 ignores Y's contents) */
+int pla_k_axpby(int dt, int m, int n, double alpha, const void *X, long ldx, double beta,
+                void *Y, long ldy, cudaStream_t s);
+/* Y := X or X' (m x n result) */
+int pla_k_copy(int dt, int trans, int m, int n, const void *X, long ldx, void *Y, long ldy,
+               cudaStream_t s);
+/* convert between precisions: dst(m x n, dt_dst) := src(m x n, dt_src).
+ * dt codes: MPI_DOUBLE, MPI_FLOAT, PLA_K_BF16, PLA_K_FP16 */
+#define PLA_K_BF16 1001
+#define PLA_K_FP16 1002
+int pla_k_convert(int dt_src, const void *src, long lds, int dt_dst, void *dst, long ldd, int m,
+                  int n, cudaStream_t s);
+
+/* ---- panel LU: factor the r x w panel at A in place with partial pivoting.
+ * piv[j] = offset from row j to the pivot row (reference encoding).
+ * zero_info (optional): set to the 1-based first exact zero pivot + row_base. */
+int pla_k_lu_panel(int dt, int r, int w, void *A, long lda, int *piv, int *status,
+                   int *zero_info, int row_base, cudaStream_t s);
+
+/* ---- row interchanges: for i in [0, npiv): swap rows i and i + piv[i] of the
+ * block whose row 0 is A (rows relative to A), in columns [c0, c1) and
+ * [c2, c3). */
+int pla_k_laswp(int dt, void *A, long lda, int npiv, const int *piv, int c0, int c1, int c2,
+                int c3, cudaStream_t s);
+/* apply a host pivot vector to m x n B in sequence (device pivots) */
+int pla_k_laswp_rows(int dt, void *B, long ldb, int ncols, int npiv, const int *piv,
+                     cudaStream_t s);
+
+/* ---- GEMM: C := alpha op(A) op(B) + beta C; uplo_c = 0 full, 'L' lower only,
+ * 'U' upper only (SYRK-shaped updates). */
+int pla_k_gemm(int dt, int transa, int transb, int m, int n, int k, double alpha,
+               const void *A, long lda, const void *B, long ldb, double beta, void *C,
+               long ldc, int uplo_c, const int *status, cudaStream_t s);
+
+/* ---- small triangular solves (the triangle is b x b with b <= 128):
+ * side 'L': B := alpha inv(op(T)) B  (B is b x ncols)
+ * side 'R': B := alpha B inv(op(T))  (B is nrows x b)
+ * uplo 'L'/'U', trans 'N'/'T', diag 'U'/'N'. */
+int pla_k_trsm_small(int dt, char side, char uplo, char trans, char diag, int b, int other,
+                     double alpha, const void *T, long ldt, void *B, long ldb,
+                     const int *status, cudaStream_t s);
+
+/* ---- unblocked lower Cholesky of the b x b block at A (b <= 128); on a
+ * non-positive pivot sets *status = PLA_K_NOT_SPD and *info = base + k + 1. */
+int pla_k_potrf_lower(int dt, int b, void *A, long lda, int *status, int *info, int base,
+                      cudaStream_t s);
+
+/* ---- level-1/2 helpers ---- */
+int pla_k_scal(int dt, int m, int n, double alpha, void *X, long ldx, cudaStream_t s);
+int pla_k_inv_scal(int dt, int m, int n, double alpha, void *X, long ldx, cudaStream_t s);
+int pla_k_swap(int dt, int m, int n, void *X, long ldx, void *Y, long ldy, cudaStream_t s);
+int pla_k_ger(int dt, int m, int n, double alpha, const void *x, long incx, const void *y,
+              long incy, void *A, long lda, cudaStream_t s);
+/* y := alpha op(A) x + beta y ; x, y with unit stride */
+int pla_k_gemv(int dt, int trans, int m, int n, double alpha, const void *A, long lda,
+               const void *x, double beta, void *y, cudaStream_t s);
+/* first index of max |x| (0-based) and the signed value there */
+int pla_k_iamax(int dt, int n, const void *x, long incx, int *index_out, void *value_out,
+                cudaStream_t s);
+
+/* ---- triangular solve with one or more right-hand sides (n x nrhs, ldb),
+ * blocked: diagonal blocks by substitution, off-diagonal by GEMM/GEMV. */
+int pla_k_trsv_blocked(int dt, char uplo, char trans, char diag, int n, int nrhs,
+                       const void *A, long lda, void *B, long ldb, cudaStream_t s);
+
+/* ---- norms and refinement helpers (FP64 unless noted) ---- */
+/* row sums of |A| (m x n): rs[i] = sum_j |A(i,j)| */
+int pla_k_row_abs_sums(int dt, int m, int n, const void *A, long lda, double *rs,
+                       cudaStream_t s);
+/* out[j] = max_i |X(i,j)| for each column j */
+int pla_k_col_abs_max(int dt, int m, int n, const void *X, long ldx, double *out,
+                      cudaStream_t s);
+
+/* ---- mixed precision ---- */
+/* C(row0 + i, col0 + j) += alpha * sum_k L(i,k) U(j,k) on the tensor cores:
+ * L (M x K, l_rows allocated) and U (N x K, u_rows allocated) in bf16/fp16
+ * with K contiguous (leading dimensions ldl, ldu in elements, multiples of 8);
+ * C fp32 column-major with ldc (multiple of 4), c_rows x c_cols allocated.
+ * K must be a multiple of 64 and at most 256. */
+int pla_k_tc_update(int prec, int M, int N, int K, float alpha, const void *L, long ldl,
+                    long l_rows, const void *U, long ldu, long u_rows, float *C, long ldc,
+                    long c_rows, long c_cols, int row0, int col0, int *status, cudaStream_t s);
+/* dst (bf16/fp16, row-major, ldd) := src (fp32, m x kdim column-major, lds) */
+int pla_k_pack_rows(int prec, int m, int kdim, const float *src, long lds, void *dst, long ldd,
+                    cudaStream_t s);
+/* R := B - A X in FP64 (A n x ncols, X ncols x nrhs, nrhs <= 16); with
+ * abs_rows, R(:,0) := row sums of |A|.  work: pla_k_residual_work() bytes. */
+size_t pla_k_residual_work(int n, int ncols, int nrhs);
+int pla_k_residual(int n, int ncols, int nrhs, const double *A, long lda, const double *X,
+                   long ldx, const double *B, long ldb, double *R, long ldr, int abs_rows,
+                   double *work, cudaStream_t s);
+
+#ifdef __cplusplus
+}
+#endif

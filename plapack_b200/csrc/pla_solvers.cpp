@@ -1,0 +1,616 @@
+// Solvers and parallel/local BLAS of the dense direct-solve path on a 1x1
+// template: the view loops of SOLVERS/LU, SOLVERS/Cholesky, BLAS2/PLA_Trsv*,
+// BLAS3/PLA_Trsm*, BLAS3/PLA_Gemm* and Local_BLAS/ become sequences of
+// device kernels on the library stream.  Every redistribution the reference
+// performs with PLA_Copy (panels to multivectors, transposed projections) is
+// a view into the same device buffer here, so no copy is made.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "pla_internal.h"
+#include "pla_kernels.h"
+
+using namespace pla;
+
+namespace {
+
+constexpr int kTri = 128;  // largest diagonal block solved in shared memory
+
+struct Status {
+  int status;     // PLA_K_* of the kernels
+  int info;       // Cholesky: failing global column (1-based)
+  int zero_info;  // LU: first exact zero pivot (1-based)
+};
+
+Status *device_status() {
+  return (Status *)scratch(0, sizeof(Status));
+}
+
+int finish(const char *what) {
+  cudaError_t e = cudaStreamSynchronize(stream());
+  if (e != cudaSuccess) return cuda_fail(e, __LINE__, what);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, __LINE__, what);
+  return PLA_SUCCESS;
+}
+
+#define K(call)                                                    \
+  do {                                                             \
+    int r_ = (call);                                               \
+    if (r_) return cuda_fail((cudaError_t)r_, __LINE__, __FILE__); \
+  } while (0)
+
+bool numeric(PLA_Obj o) { return is_double(o) || is_float(o); }
+
+char uplo_c(int uplo) { return uplo == PLA_LOWER_TRIANGULAR ? 'L' : 'U'; }
+char trans_c(int t) { return t == PLA_NO_TRANSPOSE ? 'N' : 'T'; }
+char diag_c(int d) { return d == PLA_UNIT_DIAG ? 'U' : 'N'; }
+int gemm_t(int t) { return t == PLA_NO_TRANSPOSE ? PLA_NO_TRANSPOSE : PLA_TRANSPOSE; }
+
+// op(T) X = alpha B (side L) or X op(T) = alpha B (side R) for a triangle of
+// any size: diagonal blocks of <= 128 by substitution, the coupling blocks by
+// GEMM, ordered like BLAS3/PLA_Trsm_left_lower.c:33-78.
+int trsm_blocked(int dt, char side, char uplo, char trans, char diag, int nt, int other,
+                 double alpha, const char *T, long ldt, char *B, long ldb, const int *status) {
+  if (nt <= 0 || other <= 0) return 0;
+  const int es = dt == MPI_DOUBLE ? 8 : 4;
+  const bool tr = trans != 'N';
+  auto t_at = [&](long i, long j) { return T + (i + j * ldt) * es; };
+  if (nt <= kTri)
+    return pla_k_trsm_small(dt, side, uplo, trans, diag, nt, other, alpha, T, ldt, B, ldb,
+                            status, stream());
+  const int nblk = (nt + kTri - 1) / kTri;
+  if (side == 'L') {
+    // op(T) lower: forward over row blocks; upper: backward
+    const bool forward = (uplo == 'L') != tr;
+    auto b_at = [&](long i) { return B + i * es; };
+    for (int q = 0; q < nblk; q++) {
+      const int blk = forward ? q : nblk - 1 - q;
+      const int k0 = blk * kTri, kb = std::min(kTri, nt - k0);
+      // alpha scales the first block here and every other row in the first
+      // GEMM below (its beta), so later steps use 1
+      const double a = q == 0 ? alpha : 1.0;
+      int r = pla_k_trsm_small(dt, 'L', uplo, trans, diag, kb, other, a, t_at(k0, k0), ldt,
+                               b_at(k0), ldb, status, stream());
+      if (r) return r;
+      int r0 = forward ? k0 + kb : 0, rn = forward ? nt - r0 : k0;
+      if (rn <= 0) continue;
+      const char *Ablk = tr ? t_at(k0, r0) : t_at(r0, k0);
+      // B_rest := a_rest * B_rest - op(T)(rest, blk) X_blk, where the rest
+      // rows still carry their original scale on the first step
+      r = pla_k_gemm(dt, tr ? PLA_TRANSPOSE : PLA_NO_TRANSPOSE, PLA_NO_TRANSPOSE, rn, other, kb,
+                     -1.0, Ablk, ldt, b_at(k0), ldb, q == 0 ? alpha : 1.0, b_at(r0), ldb, 0,
+                     status, stream());
+      if (r) return r;
+    }
+    return 0;
+  }
+  // side R: X op(T) = alpha B; op(T) upper: forward over column blocks
+  const bool forward = (uplo == 'U') != tr;
+  auto b_col = [&](long j) { return B + j * ldb * es; };
+  for (int q = 0; q < nblk; q++) {
+    const int blk = forward ? q : nblk - 1 - q;
+    const int k0 = blk * kTri, kb = std::min(kTri, nt - k0);
+    int r = pla_k_trsm_small(dt, 'R', uplo, trans, diag, kb, other, q == 0 ? alpha : 1.0,
+                             t_at(k0, k0), ldt, b_col(k0), ldb, status, stream());
+    if (r) return r;
+    int c0 = forward ? k0 + kb : 0, cn = forward ? nt - c0 : k0;
+    if (cn <= 0) continue;
+    // B(:, rest) := a B(:, rest) - X_blk op(T)(blk, rest)
+    const char *Tblk = tr ? t_at(c0, k0) : t_at(k0, c0);
+    r = pla_k_gemm(dt, PLA_NO_TRANSPOSE, tr ? PLA_TRANSPOSE : PLA_NO_TRANSPOSE, other, cn, kb,
+                   -1.0, b_col(k0), ldb, Tblk, ldt, q == 0 ? alpha : 1.0, b_col(c0), ldb, 0,
+                   status, stream());
+    if (r) return r;
+  }
+  return 0;
+}
+
+// Blocked right-looking LU (SOLVERS/LU/PLA_LU.c:103-192) on device memory.
+int lu_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, Status *st) {
+  const int es = dt == MPI_DOUBLE ? 8 : 4;
+  auto at = [&](long i, long j) { return A + (i + j * lda) * es; };
+  const int kmax = std::min(m, n);
+  PLA_Phase_times &ph = state().phases;
+  for (int k = 0; k < kmax; k += nb) {
+    const int b = std::min(nb, kmax - k), r = m - k;
+    {
+      PhaseTimer t(&ph.panel_ms);
+      K(pla_k_lu_panel(dt, r, b, at(k, k), lda, piv + k, &st->status, &st->zero_info, k,
+                       stream()));
+    }
+    {
+      PhaseTimer t(&ph.swap_ms);
+      K(pla_k_laswp(dt, at(k, 0), lda, b, piv + k, 0, k, k + b, n, stream()));
+    }
+    if (k + b < n) {
+      {
+        PhaseTimer t(&ph.trsm_ms);
+        K(trsm_blocked(dt, 'L', 'L', 'N', 'U', b, n - k - b, 1.0, at(k, k), lda, at(k, k + b),
+                       lda, &st->status));
+      }
+      if (m - k - b > 0) {
+        PhaseTimer t(&ph.update_ms);
+        K(pla_k_gemm(dt, PLA_NO_TRANSPOSE, PLA_NO_TRANSPOSE, m - k - b, n - k - b, b, -1.0,
+                     at(k + b, k), lda, at(k, k + b), lda, 1.0, at(k + b, k + b), lda, 0,
+                     &st->status, stream()));
+      }
+    }
+  }
+  return 0;
+}
+
+// Blocked right-looking lower Cholesky (SOLVERS/Cholesky/PLA_Chol.c:159-224).
+int chol_device(int dt, int n, char *A, long lda, int nb, Status *st) {
+  const int es = dt == MPI_DOUBLE ? 8 : 4;
+  auto at = [&](long i, long j) { return A + (i + j * lda) * es; };
+  nb = std::min(nb, kTri);
+  PLA_Phase_times &ph = state().phases;
+  for (int k = 0; k < n; k += nb) {
+    const int b = std::min(nb, n - k), rest = n - k - b;
+    {
+      PhaseTimer t(&ph.panel_ms);
+      K(pla_k_potrf_lower(dt, b, at(k, k), lda, &st->status, &st->info, k, stream()));
+    }
+    if (rest <= 0) continue;
+    {
+      PhaseTimer t(&ph.trsm_ms);
+      K(pla_k_trsm_small(dt, 'R', 'L', 'T', 'N', b, rest, 1.0, at(k, k), lda, at(k + b, k), lda,
+                         &st->status, stream()));
+    }
+    {
+      PhaseTimer t(&ph.update_ms);
+      K(pla_k_gemm(dt, PLA_NO_TRANSPOSE, PLA_TRANSPOSE, rest, rest, b, -1.0, at(k + b, k), lda,
+                   at(k + b, k), lda, 1.0, at(k + b, k + b), lda, 'L', &st->status, stream()));
+    }
+  }
+  return 0;
+}
+
+void reset_phases() {
+  if (state().phase_timing) state().phases = PLA_Phase_times{};
+}
+
+// vector increment of a 1-row or 1-column view
+long vinc(PLA_Obj v) { return (v->length == 1 && v->width > 1) ? ld(v) : 1; }
+int vlen(PLA_Obj v) { return (v->length == 1) ? v->width : v->length; }
+
+}  // namespace
+
+namespace pla {
+int lu_on_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, int *zero_info_host) {
+  Status *st = device_status();
+  if (!st) PLA_FAIL("cannot allocate the status word");
+  PLA_CUDA(cudaMemsetAsync(st, 0, sizeof(Status), stream()));
+  int r = lu_device(dt, m, n, A, lda, piv, nb, st);
+  if (r) return r;
+  Status h{};
+  PLA_CUDA(cudaMemcpyAsync(&h, st, sizeof h, cudaMemcpyDeviceToHost, stream()));
+  r = finish("lu");
+  if (r) return r;
+  if (h.status == PLA_K_TIMEOUT) PLA_FAIL("panel factorization: grid barrier timed out");
+  if (zero_info_host) *zero_info_host = h.zero_info;
+  return PLA_SUCCESS;
+}
+int trsm_device(int dt, char side, char uplo, char trans, char diag, int nt, int other,
+                double alpha, const char *T, long ldt, char *B, long ldb) {
+  return trsm_blocked(dt, side, uplo, trans, diag, nt, other, alpha, T, ldt, B, ldb, nullptr);
+}
+int chol_on_device(int dt, int n, char *A, long lda, int nb, int *info_host) {
+  Status *st = device_status();
+  if (!st) PLA_FAIL("cannot allocate the status word");
+  PLA_CUDA(cudaMemsetAsync(st, 0, sizeof(Status), stream()));
+  int r = chol_device(dt, n, A, lda, nb, st);
+  if (r) return r;
+  Status h{};
+  PLA_CUDA(cudaMemcpyAsync(&h, st, sizeof h, cudaMemcpyDeviceToHost, stream()));
+  r = finish("chol");
+  if (r) return r;
+  *info_host = h.status == PLA_K_NOT_SPD ? h.info : 0;
+  return PLA_SUCCESS;
+}
+}  // namespace pla
+
+extern "C" {
+
+// ------------------------------------------------------------------- LU ----
+int PLA_LU_info(PLA_Obj A, PLA_Obj pivots, int *info) {
+  State &s = state();
+  if (s.check_parameters) {
+    int value = PLA_SUCCESS;
+    // SOLVERS/LU/PLA_LU_enter_exit.c:17-103
+    if (!valid(A) || A->objtype != PLA_MATRIX) { warn("Invalid object A"); value--; }
+    else if (!numeric(A)) { warn("datatype not yet supported"); value--; }
+    if (!valid(pivots) || pivots->objtype != PLA_MVECTOR) {
+      return fail("Invalid objtype for pivots: pivots must be a multivector of size n x 1",
+                  __LINE__, __FILE__);
+    }
+    if (pivots->base->datatype != MPI_INT) { warn("pivots must be of type MPI_INT"); value--; }
+    if (valid(A) && pivots->length != std::min(A->length, A->width)) {
+      warn("length of pivots must match min( length of A, width of A )");
+      value--;
+    }
+    if (value != PLA_SUCCESS) return value;
+  }
+  if (!valid(A) || !numeric(A)) PLA_FAIL("PLA_LU needs a float or double matrix");
+  int nb;
+  PLA_Environ_nb_alg(PLA_OP_PAN_PAN, A->templ, &nb);
+  reset_phases();
+  int zi = 0;
+  int r = lu_on_device(A->base->datatype, A->length, A->width, at(A, 0, 0), ld(A),
+                       (int *)at(pivots, 0, 0), nb, &zi);
+  if (r) return r;
+  if (info) *info = zi;
+  return PLA_SUCCESS;  // the reference never reports singularity (PLA_LU.c:29)
+}
+
+int PLA_LU(PLA_Obj A, PLA_Obj pivots) { return PLA_LU_info(A, pivots, nullptr); }
+
+// SOLVERS/LU/PLA_Apply_pivots_new.c:13-179: the interchanges in sequence
+int PLA_Apply_pivots_to_rows(PLA_Obj A, PLA_Obj ipiv) {
+  if (!valid(A) || !valid(ipiv)) PLA_FAIL("invalid object");
+  if (ipiv->base->datatype != MPI_INT) PLA_FAIL("pivots must be of type MPI_INT");
+  if (!numeric(A)) PLA_FAIL("datatype not yet supported");
+  int npiv = vlen(ipiv);
+  if (npiv > A->length) PLA_FAIL("more pivots than rows");
+  if (vinc(ipiv) != 1) PLA_FAIL("pivots must be a column");
+  K(pla_k_laswp_rows(A->base->datatype, at(A, 0, 0), ld(A), A->width, npiv,
+                     (const int *)at(ipiv, 0, 0), stream()));
+  return finish("apply pivots");
+}
+
+// columns j = n-1 .. 0: swap column j with column j + piv[j] (:309-451)
+int PLA_Apply_pivots_to_columns_in_reverse(PLA_Obj A, PLA_Obj ipiv) {
+  if (!valid(A) || !valid(ipiv)) PLA_FAIL("invalid object");
+  if (ipiv->objtype != PLA_MVECTOR) PLA_FAIL("not yet implemented");
+  int npiv = std::min(vlen(ipiv), A->width);
+  std::vector<int> h(npiv);
+  PLA_CUDA(cudaMemcpy(h.data(), at(ipiv, 0, 0), npiv * sizeof(int), cudaMemcpyDeviceToHost));
+  for (int j = npiv - 1; j >= 0; j--) {
+    int p = j + h[j];
+    if (p == j) continue;
+    if (p >= A->width) PLA_FAIL("pivot out of range");
+    K(pla_k_swap(A->base->datatype, A->length, 1, at(A, 0, j), ld(A), at(A, 0, p), ld(A),
+                 stream()));
+  }
+  return finish("apply pivots to columns");
+}
+
+// -------------------------------------------------------------- Cholesky ----
+int PLA_Chol(int uplo, PLA_Obj A) {
+  State &s = state();
+  if (s.check_parameters) {
+    // SOLVERS/Cholesky/PLA_Chol_enter_exit.c:17-60
+    if (uplo != PLA_LOWER_TRIANGULAR && uplo != PLA_UPPER_TRIANGULAR) warn("Invalid parameter uplo");
+    if (uplo != PLA_LOWER_TRIANGULAR) PLA_FAIL("Only lower triangular factorization supported");
+    if (!valid(A) || A->objtype != PLA_MATRIX) { warn("Invalid objtype for A"); return -1; }
+    if (A->length != A->width) { warn("A must be square"); return -1; }
+  }
+  if (!valid(A) || !numeric(A)) PLA_FAIL("PLA_Chol needs a float or double matrix");
+  if (uplo != PLA_LOWER_TRIANGULAR) PLA_FAIL("Only lower triangular factorization supported");
+  int nb;
+  PLA_Environ_nb_alg(PLA_OP_PAN_PAN, A->templ, &nb);
+  reset_phases();
+  int info = 0;
+  int r = chol_on_device(A->base->datatype, A->length, at(A, 0, 0), ld(A), nb, &info);
+  if (r) return r;
+  return info;  // global 1-based failing column, as PLA_Chol.c:181-185 computes
+}
+
+int PLA_Local_chol(int uplo, PLA_Obj A) {
+  if (uplo != PLA_LOWER_TRIANGULAR) PLA_FAIL("Only lower triangular factorization supported");
+  if (!valid(A) || !numeric(A)) PLA_FAIL("invalid object");
+  int info = 0;
+  int r = chol_on_device(A->base->datatype, A->length, at(A, 0, 0), ld(A), kTri, &info);
+  return r ? r : info;
+}
+
+// --------------------------------------------------------------- solves ----
+int PLA_Trsv(int uplo, int trans, int diag, PLA_Obj A, PLA_Obj x) {
+  if (!valid(A) || !valid(x)) PLA_FAIL("invalid object");
+  if (!numeric(A) || A->base->datatype != x->base->datatype) PLA_FAIL("datatype mismatch");
+  if (A->length != A->width || vlen(x) != A->length) PLA_FAIL("nonconformal objects");
+  if (vinc(x) != 1) PLA_FAIL("x must be a column vector");
+  reset_phases();
+  PhaseTimer t(&state().phases.solve_ms);
+  K(pla_k_trsv_blocked(A->base->datatype, uplo_c(uplo), trans_c(trans), diag_c(diag), A->length,
+                       1, at(A, 0, 0), ld(A), at(x, 0, 0), ld(x), stream()));
+  return finish("trsv");
+}
+
+int PLA_Local_trsv(int uplo, int trans, int diag, PLA_Obj A, PLA_Obj x) {
+  return PLA_Trsv(uplo, trans, diag, A, x);
+}
+
+int PLA_Trsm(int side, int uplo, int trans, int diag, PLA_Obj alpha, PLA_Obj A, PLA_Obj B) {
+  if (!valid(A) || !valid(B) || !valid(alpha)) PLA_FAIL("invalid object");
+  if (!numeric(A) || A->base->datatype != B->base->datatype) PLA_FAIL("datatype mismatch");
+  const int nt = side == PLA_SIDE_LEFT ? B->length : B->width;
+  const int other = side == PLA_SIDE_LEFT ? B->width : B->length;
+  if (A->length != nt || A->width != nt) PLA_FAIL("nonconformal objects");
+  reset_phases();
+  PhaseTimer t(&state().phases.solve_ms);
+  K(trsm_blocked(A->base->datatype, side == PLA_SIDE_LEFT ? 'L' : 'R', uplo_c(uplo),
+                 trans_c(trans), diag_c(diag), nt, other, scalar_value(alpha), at(A, 0, 0), ld(A),
+                 at(B, 0, 0), ld(B), nullptr));
+  return finish("trsm");
+}
+
+int PLA_Local_trsm(int side, int uplo, int trans, int diag, PLA_Obj alpha, PLA_Obj A,
+                   PLA_Obj B) {
+  return PLA_Trsm(side, uplo, trans, diag, alpha, A, B);
+}
+
+static int gemm_objs(int transa, int transb, PLA_Obj alpha, PLA_Obj A, PLA_Obj B, PLA_Obj beta,
+                     PLA_Obj C, int uplo_c) {
+  if (!valid(A) || !valid(B) || !valid(C) || !valid(alpha) || !valid(beta))
+    PLA_FAIL("invalid object");
+  if (!numeric(C) || A->base->datatype != C->base->datatype ||
+      B->base->datatype != C->base->datatype)
+    PLA_FAIL("datatype mismatch");
+  const bool ta = transa != PLA_NO_TRANSPOSE, tb = transb != PLA_NO_TRANSPOSE;
+  const int m = C->length, n = C->width;
+  const int k = ta ? A->length : A->width;
+  if ((ta ? A->width : A->length) != m || (tb ? B->length : B->width) != n ||
+      (tb ? B->width : B->length) != k)
+    PLA_FAIL("nonconformal objects");
+  PhaseTimer t(&state().phases.update_ms);
+  K(pla_k_gemm(C->base->datatype, gemm_t(transa), gemm_t(transb), m, n, k, scalar_value(alpha),
+               at(A, 0, 0), ld(A), at(B, 0, 0), ld(B), scalar_value(beta), at(C, 0, 0), ld(C),
+               uplo_c, nullptr, stream()));
+  return finish("gemm");
+}
+
+int PLA_Gemm(int transa, int transb, PLA_Obj alpha, PLA_Obj A, PLA_Obj B, PLA_Obj beta,
+             PLA_Obj C) {
+  reset_phases();
+  return gemm_objs(transa, transb, alpha, A, B, beta, C, 0);
+}
+
+int PLA_Local_gemm(int transa, int transb, PLA_Obj alpha, PLA_Obj A, PLA_Obj B, PLA_Obj beta,
+                   PLA_Obj C) {
+  return gemm_objs(transa, transb, alpha, A, B, beta, C, 0);
+}
+
+// C := beta C + alpha X X_trans restricted to one triangle; X_trans holds X'
+// (BLAS3/PLA_Syrk_perform_local_part.c:13-78)
+int PLA_Syrk_perform_local_part(int uplo, PLA_Obj alpha, PLA_Obj X, PLA_Obj X_trans,
+                                PLA_Obj beta, PLA_Obj A) {
+  return gemm_objs(PLA_NO_TRANSPOSE, PLA_NO_TRANSPOSE, alpha, X, X_trans, beta, A, uplo_c(uplo));
+}
+
+// C := beta C + alpha op(A) op(A)' on one triangle (Local_BLAS/PLA_Local_syrk.c)
+int PLA_Local_syrk(int uplo, int trans, PLA_Obj alpha, PLA_Obj A, PLA_Obj beta, PLA_Obj C) {
+  int t2 = trans == PLA_NO_TRANSPOSE ? PLA_TRANSPOSE : PLA_NO_TRANSPOSE;
+  return gemm_objs(trans, t2, alpha, A, A, beta, C, uplo_c(uplo));
+}
+
+int PLA_General_solve(PLA_Obj A, PLA_Obj ipiv, PLA_Obj B) {
+  // SOLVERS/LU/PLA_General.c:67-119
+  int error = PLA_LU(A, ipiv);
+  if (error != PLA_SUCCESS) return error;
+  if (!valid(B)) PLA_FAIL("invalid object B");
+  if (B->width > 0) {
+    int r = PLA_Apply_pivots_to_rows(B, ipiv);
+    if (r) return r;
+    const int dt = A->base->datatype, n = A->length;
+    PhaseTimer t(&state().phases.solve_ms);
+    // Trsm for several right-hand sides, Trsv for one: the same blocked kernel
+    K(pla_k_trsv_blocked(dt, 'L', 'N', 'U', n, B->width, at(A, 0, 0), ld(A), at(B, 0, 0), ld(B),
+                         stream()));
+    K(pla_k_trsv_blocked(dt, 'U', 'N', 'N', n, B->width, at(A, 0, 0), ld(A), at(B, 0, 0), ld(B),
+                         stream()));
+    r = finish("general solve");
+    if (r) return r;
+  }
+  return PLA_SUCCESS;
+}
+
+int PLA_Pos_def_solve(PLA_Obj A, PLA_Obj B) {
+  // SOLVERS/Cholesky/PLA_Pos_def.c:44-99: warn on failure, solve regardless
+  int value = PLA_Chol(PLA_LOWER_TRIANGULAR, A);
+  if (value < 0) return value;
+  if (value != PLA_SUCCESS) warn("irregular return from PLA_Chol");
+  if (!valid(B)) PLA_FAIL("invalid object B");
+  const int dt = A->base->datatype, n = A->length;
+  PhaseTimer t(&state().phases.solve_ms);
+  K(pla_k_trsv_blocked(dt, 'L', 'N', 'N', n, B->width, at(A, 0, 0), ld(A), at(B, 0, 0), ld(B),
+                       stream()));
+  K(pla_k_trsv_blocked(dt, 'L', 'T', 'N', n, B->width, at(A, 0, 0), ld(A), at(B, 0, 0), ld(B),
+                       stream()));
+  int r = finish("pos def solve");
+  return r ? r : value;
+}
+
+// --------------------------------------------------------- level 1 / 2 -----
+int PLA_Gemv(int trans, PLA_Obj alpha, PLA_Obj A, PLA_Obj x, PLA_Obj beta, PLA_Obj y) {
+  if (!valid(A) || !valid(x) || !valid(y)) PLA_FAIL("invalid object");
+  if (vinc(x) != 1 || vinc(y) != 1) PLA_FAIL("x and y must be column vectors");
+  K(pla_k_gemv(A->base->datatype, gemm_t(trans), A->length, A->width, scalar_value(alpha),
+               at(A, 0, 0), ld(A), at(x, 0, 0), scalar_value(beta), at(y, 0, 0), stream()));
+  return finish("gemv");
+}
+
+int PLA_Local_gemv(int trans, PLA_Obj alpha, PLA_Obj A, PLA_Obj x, PLA_Obj beta, PLA_Obj y) {
+  return PLA_Gemv(trans, alpha, A, x, beta, y);
+}
+
+int PLA_Iamax(PLA_Obj x, PLA_Obj k, PLA_Obj xmax) {
+  // BLAS1/PLA_Iamax.c:37-124: value and global index of the first max |x_i|
+  if (!valid(x) || !valid(k) || !valid(xmax)) PLA_FAIL("invalid object");
+  if (x->base->datatype != xmax->base->datatype) PLA_FAIL("datatype mismatch");
+  int *di = (int *)scratch(1, 64);
+  char *dv = (char *)di + 16;
+  K(pla_k_iamax(x->base->datatype, vlen(x), at(x, 0, 0), vinc(x), di, dv, stream()));
+  int hi;
+  double hv[1];
+  PLA_CUDA(cudaMemcpyAsync(&hi, di, sizeof hi, cudaMemcpyDeviceToHost, stream()));
+  PLA_CUDA(cudaMemcpyAsync(hv, dv, x->base->esize, cudaMemcpyDeviceToHost, stream()));
+  int r = finish("iamax");
+  if (r) return r;
+  if (vlen(x) == 0) hi = 0;
+  PLA_Obj_set(k, MPI_INT, &hi);
+  if (is_double(x)) PLA_Obj_set(xmax, MPI_DOUBLE, hv);
+  else PLA_Obj_set(xmax, MPI_FLOAT, hv);
+  return PLA_SUCCESS;
+}
+
+int PLA_Local_iamax(PLA_Obj x, int *index, void *value) {
+  if (!valid(x)) PLA_FAIL("invalid object");
+  int *di = (int *)scratch(1, 64);
+  char *dv = (char *)di + 16;
+  K(pla_k_iamax(x->base->datatype, vlen(x), at(x, 0, 0), vinc(x), di, dv, stream()));
+  PLA_CUDA(cudaMemcpyAsync(index, di, sizeof(int), cudaMemcpyDeviceToHost, stream()));
+  PLA_CUDA(cudaMemcpyAsync(value, dv, x->base->esize, cudaMemcpyDeviceToHost, stream()));
+  return finish("local iamax");
+}
+
+int PLA_Local_scal(PLA_Obj alpha, PLA_Obj x) {
+  if (!valid(alpha) || !valid(x)) PLA_FAIL("invalid object");
+  K(pla_k_scal(x->base->datatype, x->length, x->width, scalar_value(alpha), at(x, 0, 0), ld(x),
+               stream()));
+  return finish("scal");
+}
+
+int PLA_Local_inv_scal(PLA_Obj alpha, PLA_Obj x) {
+  if (!valid(alpha) || !valid(x)) PLA_FAIL("invalid object");
+  K(pla_k_inv_scal(x->base->datatype, x->length, x->width, scalar_value(alpha), at(x, 0, 0),
+                   ld(x), stream()));
+  return finish("inv_scal");
+}
+
+int PLA_Local_swap(PLA_Obj x, PLA_Obj y) {
+  if (!valid(x) || !valid(y)) PLA_FAIL("invalid object");
+  if (x->length != y->length || x->width != y->width) PLA_FAIL("nonconformal objects");
+  K(pla_k_swap(x->base->datatype, x->length, x->width, at(x, 0, 0), ld(x), at(y, 0, 0), ld(y),
+               stream()));
+  return finish("swap");
+}
+
+int PLA_Local_ger(PLA_Obj alpha, PLA_Obj x, PLA_Obj y, PLA_Obj A) {
+  if (!valid(alpha) || !valid(x) || !valid(y) || !valid(A)) PLA_FAIL("invalid object");
+  if (vlen(x) != A->length || vlen(y) != A->width) PLA_FAIL("nonconformal objects");
+  K(pla_k_ger(A->base->datatype, A->length, A->width, scalar_value(alpha), at(x, 0, 0), vinc(x),
+              at(y, 0, 0), vinc(y), at(A, 0, 0), ld(A), stream()));
+  return finish("ger");
+}
+
+// ----------------------------------------------------------------- copies ---
+static int copy_objs(PLA_Obj from, PLA_Obj to) {
+  if (!valid(from) || !valid(to)) PLA_FAIL("invalid object");
+  if (from->base->datatype != to->base->datatype) PLA_FAIL("datatype mismatch");
+  const int dt = from->base->datatype;
+  const int es = from->base->esize;
+  bool same = from->length == to->length && from->width == to->width;
+  bool transposed = from->length == to->width && from->width == to->length;
+  // a row projection stores the rows of the matrix it is conformal to as its
+  // columns, so a copy between it and a matrix transposes (COPY/PLA_Copy.c)
+  bool proj_from = from->objtype == PLA_PMVECTOR && from->proj_onto == PLA_PROJ_ONTO_ROW;
+  bool proj_to = to->objtype == PLA_PMVECTOR && to->proj_onto == PLA_PROJ_ONTO_ROW;
+  bool trans = proj_from != proj_to;
+  if (trans ? !transposed : !same) PLA_FAIL("objects do not conform");
+  if (from->length == 0 || from->width == 0) return PLA_SUCCESS;
+  if (from->base->on_host || to->base->on_host) {
+    cudaMemcpyKind kind = cudaMemcpyDefault;
+    if (trans) PLA_FAIL("transposed copy involving a host multiscalar");
+    PLA_CUDA(cudaMemcpy2DAsync(at(to, 0, 0), ld(to) * es, at(from, 0, 0), ld(from) * es,
+                               (size_t)from->length * es, from->width, kind, stream()));
+    return finish("copy");
+  }
+  if (dt == MPI_INT && trans) PLA_FAIL("transposed integer copy");
+  K(pla_k_copy(dt == MPI_INT ? MPI_FLOAT : dt, trans ? PLA_TRANSPOSE : PLA_NO_TRANSPOSE,
+               to->length, to->width, at(from, 0, 0), ld(from), at(to, 0, 0), ld(to), stream()));
+  return finish("copy");
+}
+
+int PLA_Copy(PLA_Obj from, PLA_Obj to) { return copy_objs(from, to); }
+int PLA_Local_copy(PLA_Obj from, PLA_Obj to) { return copy_objs(from, to); }
+
+// -------------------------------------------------- application interface ---
+int PLA_API_begin(void) {
+  if (state().api_active) PLA_FAIL("PLA_API_begin called twice");
+  state().api_active = 1;
+  return PLA_SUCCESS;
+}
+int PLA_API_end(void) {
+  state().api_active = 0;
+  return finish("api end");
+}
+int PLA_Obj_API_open(PLA_Obj obj) { return valid(obj) ? PLA_SUCCESS : fail("invalid object", __LINE__, __FILE__); }
+int PLA_Obj_API_close(PLA_Obj obj) {
+  if (!valid(obj)) PLA_FAIL("invalid object");
+  return finish("api close");
+}
+int PLA_Obj_API_sync(PLA_Obj obj) { return PLA_Obj_API_close(obj); }
+
+// obj(i0:i0+m, j0:j0+n) += alpha * host(m x n, ldim): staged through the
+// library's device scratch in column chunks (API/PLA_API.c:390-590)
+static int axpy_to_global(int m, int n, void *alpha, const void *host, long ldh, long inch,
+                          PLA_Obj obj, int i0, int j0) {
+  if (!valid(obj)) PLA_FAIL("invalid object");
+  if (m == 0 || n == 0) return PLA_SUCCESS;
+  if (i0 < 0 || j0 < 0 || i0 + m > obj->length || j0 + n > obj->width)
+    PLA_FAIL("API axpy outside the object");
+  const int dt = obj->base->datatype, es = obj->base->esize;
+  double a = dt == MPI_DOUBLE ? *(double *)alpha : dt == MPI_FLOAT ? *(float *)alpha : *(int *)alpha;
+  if (inch != 1) PLA_FAIL("only unit-stride local vectors are supported");
+  const size_t chunk_bytes = (size_t)256 << 20;
+  int cols = (int)std::max<size_t>(1, chunk_bytes / ((size_t)m * es));
+  cols = std::min(cols, n);
+  char *stage = (char *)scratch(2, (size_t)m * cols * es);
+  if (!stage) PLA_FAIL("cannot allocate the staging buffer");
+  for (int j = 0; j < n; j += cols) {
+    int c = std::min(cols, n - j);
+    PLA_CUDA(cudaMemcpy2DAsync(stage, (size_t)m * es, (const char *)host + (size_t)j * ldh * es,
+                               (size_t)ldh * es, (size_t)m * es, c, cudaMemcpyHostToDevice,
+                               stream()));
+    K(pla_k_axpby(dt, m, c, a, stage, m, 1.0, at(obj, i0, j0 + j), ld(obj), stream()));
+  }
+  return finish("api axpy to global");
+}
+
+// host(m x n) += alpha * obj(i0.., j0..)
+static int axpy_from_global(int m, int n, void *alpha, PLA_Obj obj, int i0, int j0, void *host,
+                            long ldh) {
+  if (!valid(obj)) PLA_FAIL("invalid object");
+  if (m == 0 || n == 0) return PLA_SUCCESS;
+  if (i0 < 0 || j0 < 0 || i0 + m > obj->length || j0 + n > obj->width)
+    PLA_FAIL("API axpy outside the object");
+  const int dt = obj->base->datatype, es = obj->base->esize;
+  std::vector<char> tmp((size_t)m * n * es);
+  PLA_CUDA(cudaMemcpy2DAsync(tmp.data(), (size_t)m * es, at(obj, i0, j0), ld(obj) * es,
+                             (size_t)m * es, n, cudaMemcpyDefault, stream()));
+  int r = finish("api axpy from global");
+  if (r) return r;
+  for (int j = 0; j < n; j++)
+    for (int i = 0; i < m; i++) {
+      size_t src = (size_t)i + (size_t)j * m, dst = (size_t)i + (size_t)j * ldh;
+      if (dt == MPI_DOUBLE) ((double *)host)[dst] += *(double *)alpha * ((double *)tmp.data())[src];
+      else if (dt == MPI_FLOAT) ((float *)host)[dst] += *(float *)alpha * ((float *)tmp.data())[src];
+      else if (dt == MPI_INT) ((int *)host)[dst] += *(int *)alpha * ((int *)tmp.data())[src];
+    }
+  return PLA_SUCCESS;
+}
+
+int PLA_API_axpy_matrix_to_global(int m, int n, void *alpha, void *local, int ldim, PLA_Obj obj,
+                                  int disp_row, int disp_col) {
+  return axpy_to_global(m, n, alpha, local, ldim, 1, obj, disp_row, disp_col);
+}
+int PLA_API_axpy_global_to_matrix(int m, int n, void *alpha, PLA_Obj obj, int disp_row,
+                                  int disp_col, void *local, int ldim) {
+  return axpy_from_global(m, n, alpha, obj, disp_row, disp_col, local, ldim);
+}
+int PLA_API_axpy_vector_to_global(int size, void *alpha, void *local, int stride, PLA_Obj obj,
+                                  int disp) {
+  if (!valid(obj)) PLA_FAIL("invalid object");
+  return axpy_to_global(size, 1, alpha, local, size, stride, obj, disp, 0);
+}
+int PLA_API_axpy_global_to_vector(int size, void *alpha, PLA_Obj obj, int disp, void *local,
+                                  int stride) {
+  if (stride != 1) PLA_FAIL("only unit-stride local vectors are supported");
+  return axpy_from_global(size, 1, alpha, obj, disp, 0, local, size);
+}
+
+}  // extern "C"
