@@ -1,0 +1,445 @@
+#!/usr/bin/env python
+"""Dense direct solve on one B200: n = 32768 solve time, mixed-precision
+(fp16 factors, FP64 GMRES-IR) versus FP64 LU, both to FP64 backward error.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one solve A x = b of the n = 32768 system (A = U diag(sigma) V' with
+sigma geometric from 1 to 1/kappa, U and V products of 8 Householder
+reflectors with seeded Gaussian vectors; kappa = 1e6; x_true ~ N(0,1)),
+called through the library's C ABI (PLA_General_solve_mixed; the FP64 arm is
+PLA_General_solve).  Inputs are resident in HBM and larger than L2 (8.6 GB).
+`e2e` repeats the mixed solve with the matrix and right-hand side in pinned
+host memory, copied in through PLA_Obj_set_local_contents and the solution
+read back through PLA_Obj_get_local_contents, every step.
+
+--impl reference times the upstream PLAPACK (compiled from its sources into
+oracle/_ref, linked to a threaded OpenBLAS) on the host cores: PLA_General_solve
+on a bounded sample of the same matrix family, scaled to n = 32768 by n^3.
+
+Under torchrun (--gpus N > 1) every rank solves its own system (replicas; the
+path has no data exchange) and rank 0 prints the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "n=32768 solve time: mixed-prec LU-IR vs FP64 LU, same B200, both at FP64 bkwd err"
+# DRAM bytes per tensor-core update launch as a fraction of its algorithmic
+# bytes, from the ncu capture summarised in profiles/ (None until captured)
+TC_UPDATE_TRAFFIC_RATIO = None
+
+
+def parse():
+    p = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--n", type=int, default=32768)
+    p.add_argument("--kappa", type=float, default=1e6)
+    p.add_argument("--precision", choices=["fp16", "bf16", "fp32"], default="fp16")
+    p.add_argument("--refinement", choices=["gmres", "lu"], default="gmres")
+    p.add_argument("--nb", type=int, default=256, help="block size of the mixed factorization")
+    p.add_argument("--nb-fp64", type=int, default=128, help="nb_alg of the FP64 LU")
+    p.add_argument("--skip-fp64", action="store_true")
+    p.add_argument("--skip-e2e", action="store_true")
+    p.add_argument("--skip-cpu", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=12.0,
+                   help="target length of one reference sample on the host")
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------- inputs ---
+def c3_device(n, kappa, seed, torch, device):
+    """Column-major A = U diag(sigma) V' as the memory of a row-major tensor T
+    (T = A'), built by 16 seeded Householder reflections of diag(sigma)."""
+    g = torch.Generator(device=device).manual_seed(seed)
+    sigma = kappa ** (-torch.arange(n, dtype=torch.float64, device=device) / max(n - 1, 1))
+    T = torch.diag(sigma)
+    for _ in range(8):                      # T <- H T
+        v = torch.randn(n, dtype=torch.float64, device=device, generator=g)
+        w = v @ T
+        T.addr_(v, w, alpha=-2.0 / float(v @ v))
+    for _ in range(8):                      # T <- T H
+        v = torch.randn(n, dtype=torch.float64, device=device, generator=g)
+        w = T @ v
+        T.addr_(w, v, alpha=-2.0 / float(v @ v))
+    x = torch.randn(n, 1, dtype=torch.float64, device=device, generator=g)
+    b = T.t() @ x                            # b = A x_true
+    return T, x, b
+
+
+def c3_host(n, kappa, seed):
+    rng = np.random.default_rng(seed)
+    sigma = kappa ** (-np.arange(n) / max(n - 1, 1))
+    A = np.diag(sigma)
+    for _ in range(8):
+        v = rng.standard_normal(n)
+        A -= (2.0 / (v @ v)) * np.outer(v, v @ A)
+    for _ in range(8):
+        v = rng.standard_normal(n)
+        A -= (2.0 / (v @ v)) * np.outer(A @ v, v)
+    x = rng.standard_normal((n, 1))
+    return np.asfortranarray(A), x, A @ x
+
+
+# --------------------------------------------------------------- helpers ---
+class Clocks:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        if self.path and os.path.exists(self.path):
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        busy = [v for v in sm if mx and v > 0.5 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(busy) if busy else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ----------------------------------------------------- reference (CPU) arm ---
+def reference_sample(n_full, kappa, target_s, steps=1, warmup=0):
+    """Time the upstream PLA_General_solve on the host cores on a bounded sample
+    and scale its time to n_full by n^3.  Returns (seconds at n_full, info)."""
+    cores = cpu_cores()
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", str(cores))
+    from oracle import oracle as orc
+    ref = orc.Reference("openblas", nb_distr=128, nb_alg=128, error_checking=0)
+    # probe the rate on a small case, then size the sample to ~target_s
+    A, _, b = c3_host(2048, kappa, 11)
+    t0 = time.perf_counter()
+    ref.general_solve(A, b)
+    rate = (2 / 3 * 2048 ** 3) / max(time.perf_counter() - t0, 1e-3)
+    n_s = int((target_s * rate * 1.5) ** (1 / 3)) // 512 * 512
+    n_s = max(2048, min(n_s, n_full))
+    A, x_true, b = c3_host(n_s, kappa, 12)
+    times = []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        _, X, _, ret, t_inner = ref.general_solve(A, b)
+        wall = time.perf_counter() - t0
+        if i >= warmup:
+            times.append(t_inner if t_inner > 0 else wall)
+    t = statistics.median(times)
+    scaled = t * (n_full / n_s) ** 3
+    resid = b - A @ X
+    eta = float(np.abs(resid).max() / (np.abs(A).sum(axis=1).max() * np.abs(X).max() + np.abs(b).max()))
+    info = {"value": scaled, "unit": "s", "cores": int(os.environ["OPENBLAS_NUM_THREADS"]),
+            "kind": "reference",
+            "sample": (f"upstream PLA_General_solve (PLA_LU nb_alg=128 + PLA_Trsv, FP64, 1x1 "
+                       f"template, OpenBLAS 0.3.15, {os.environ['OPENBLAS_NUM_THREADS']} threads) "
+                       f"on the same matrix family at n={n_s}: {t:.3f} s, scaled by "
+                       f"(32768/{n_s})^3; backward error {eta:.2e}")}
+    return scaled, info
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    lib = os.path.join(ROOT, "oracle", "_ref", "libplapack_ref_openblas.so")
+    if not os.path.exists(lib):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/libplapack_ref_openblas.so is not built"}))
+        return 0
+    per_step = max(3.0, args.cpu_seconds / 2)
+    value, info = reference_sample(args.n, args.kappa, per_step, steps=args.steps,
+                                   warmup=min(args.warmup, 1))
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s",
+           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded C3 family)",
+           "config": {"workload": f"general solve n={args.n}, kappa={args.kappa:g}, 1 rhs",
+                      "n": args.n, "kappa": args.kappa, "nrhs": 1, "parallelism": "host cores"},
+           "cpu_baseline": info,
+           "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+# ---------------------------------------------------------------- our arm ---
+def run_ours(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    device = torch.device("cuda", torch.cuda.current_device())
+    torch.backends.cuda.matmul.allow_tf32 = False
+
+    from plapack_b200 import pla
+    s = pla.Session(nb_distr=128, nb_alg=args.nb_fp64, error_checking=0)
+    lib = s.lib
+    stream = torch.cuda.current_stream()
+    lib.PLA_B200_set_stream(ctypes.c_void_p(stream.cuda_stream))
+    n = args.n
+
+    T, x_true, b = c3_device(n, args.kappa, 1000 + rank, torch, device)
+    torch.cuda.synchronize()
+    a = s.matrix(n, n)
+    bo = s.matrix(n, 1)
+    check = pla.check
+    check(lib.PLA_Obj_set_local_contents_device(ctypes.c_void_p(T.data_ptr()), n, a), "fill A")
+
+    prec = {"fp16": pla.PLA_B200_PREC_FP16, "bf16": pla.PLA_B200_PREC_BF16,
+            "fp32": pla.PLA_B200_PREC_FP32}[args.precision]
+    params = pla.MixedParams()
+    lib.PLA_Mixed_params_default(ctypes.byref(params))
+    params.precision = prec
+    params.refinement = pla.PLA_B200_IR_GMRES if args.refinement == "gmres" else pla.PLA_B200_IR_LU
+    params.nb = args.nb
+    report = pla.MixedReport()
+
+    def mixed_step():
+        check(lib.PLA_Obj_set_local_contents_device(ctypes.c_void_p(b.data_ptr()), n, bo), "fill b")
+        check(lib.PLA_General_solve_mixed(a, bo, ctypes.byref(params), ctypes.byref(report)),
+              "PLA_General_solve_mixed")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        mixed_step()
+    lib.PLA_B200_set_phase_timing(1)
+    lib.PLA_B200_reset_phase_times()
+    launches0 = lib.PLA_B200_kernel_launches()
+    barrier()
+    with Clocks(device.index) as clocks:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            mixed_step()
+        e1.record(stream)
+        barrier()
+    launches = lib.PLA_B200_kernel_launches() - launches0
+    ph = pla.PhaseTimes()
+    lib.PLA_B200_phase_times(ctypes.byref(ph))
+    lib.PLA_B200_set_phase_timing(0)
+    mixed_s = max_over_ranks(e0.elapsed_time(e1) / 1e3 / args.steps)
+    clock_summary = clocks.summary()
+
+    # accuracy of the last solve, checked independently with torch
+    x = torch.empty(n, 1, dtype=torch.float64, device=device)
+    check(lib.PLA_Obj_get_local_contents_device(bo, ctypes.c_void_p(x.data_ptr()), n), "get x")
+    r = b - T.t() @ x
+    a_inf = T.abs().sum(dim=0).max().item()        # ||A||_inf = max row sum of A = max col sum of T
+    eta = (r.abs().max() / (a_inf * x.abs().max() + b.abs().max())).item()
+    fwd = ((x - x_true).abs().max() / x_true.abs().max()).item()
+
+    # tensor-core update roofline: algorithmic bytes (fp32 C read + write,
+    # fp16 L and U read) over the update kernels' own event-timed duration
+    nb = args.nb
+    steps_bytes = 0.0
+    for k in range(0, n, nb):
+        rest = n - k - min(nb, n - k)
+        if rest > 0:
+            steps_bytes += rest * rest * 8.0 + 2.0 * rest * nb * 2.0
+    algo_bytes = steps_bytes * args.steps
+    peak, peak_src = measured_peaks()
+    achieved = algo_bytes / (ph.update_ms / 1e3) / 1e9 if ph.update_ms > 0 else None
+    per_launch = steps_bytes / max(1, ph.update_launches // max(1, args.steps))
+    roofline = {"bound": "hbm", "kernel": "tc_update_k (tcgen05 fp16 trailing update)",
+                "achieved": achieved, "peak": peak, "peak_source": peak_src, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None,
+                "traffic": (per_launch * TC_UPDATE_TRAFFIC_RATIO) if TC_UPDATE_TRAFFIC_RATIO else None,
+                "algorithmic_bytes_per_launch": per_launch,
+                "update_ms_per_step": ph.update_ms / args.steps,
+                "update_launches_per_step": ph.update_launches / args.steps,
+                "phase_ms_per_step": {k: getattr(ph, k) / args.steps for k in
+                                      ("panel_ms", "swap_ms", "trsm_ms", "convert_ms", "update_ms")}}
+
+    # ---- FP64 LU arm (PLA_General_solve), restoring A every step ----
+    fp64_s = None
+    fp64_eta = None
+    if not args.skip_fp64:
+        s.set_nb_alg(args.nb_fp64)
+        piv = s.mvector(n, 1, np.int32)
+
+        def fp64_step():
+            check(lib.PLA_Obj_set_local_contents_device(ctypes.c_void_p(T.data_ptr()), n, a), "A")
+            check(lib.PLA_Obj_set_local_contents_device(ctypes.c_void_p(b.data_ptr()), n, bo), "b")
+            check(lib.PLA_General_solve(a, piv, bo), "PLA_General_solve")
+
+        for _ in range(args.warmup):
+            fp64_step()
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            fp64_step()
+        f1.record(stream)
+        barrier()
+        fp64_s = max_over_ranks(f0.elapsed_time(f1) / 1e3 / args.steps)
+        check(lib.PLA_Obj_get_local_contents_device(bo, ctypes.c_void_p(x.data_ptr()), n), "x")
+        r = b - T.t() @ x
+        fp64_eta = (r.abs().max() / (a_inf * x.abs().max() + b.abs().max())).item()
+        s.free(piv)
+        # leave A as it was for the end-to-end arm
+        check(lib.PLA_Obj_set_local_contents_device(ctypes.c_void_p(T.data_ptr()), n, a), "A")
+
+    # ---- end to end: host buffers in, host solution out ----
+    e2e = None
+    if not args.skip_e2e:
+        Th = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+        Th.copy_(T)
+        bh = torch.empty((n, 1), dtype=torch.float64, pin_memory=True)
+        bh.copy_(b)
+        xh = torch.empty((n, 1), dtype=torch.float64, pin_memory=True)
+        NT = pla.PLA_NO_TRANSPOSE
+
+        def e2e_step():
+            check(lib.PLA_Obj_set_local_contents(NT, n, n, ctypes.c_void_p(Th.data_ptr()), n, 1, a),
+                  "set A")
+            check(lib.PLA_Obj_set_local_contents(NT, n, 1, ctypes.c_void_p(bh.data_ptr()), n, 1, bo),
+                  "set b")
+            check(lib.PLA_General_solve_mixed(a, bo, ctypes.byref(params), ctypes.byref(report)),
+                  "solve")
+            check(lib.PLA_Obj_get_local_contents(bo, NT, None, None, ctypes.c_void_p(xh.data_ptr()),
+                                                 n, 1), "get x")
+
+        e2e_step()
+        barrier()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        g1.record(stream)
+        barrier()
+        e2e = {"value": max_over_ranks(g0.elapsed_time(g1) / 1e3 / args.steps), "unit": "s",
+               "h2d_bytes_per_step": n * n * 8 + n * 8, "d2h_bytes_per_step": n * 8,
+               "path": "PLA_Obj_set_local_contents (pinned host) -> PLA_General_solve_mixed -> "
+                       "PLA_Obj_get_local_contents"}
+        del Th
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        try:
+            _, cpu = reference_sample(n, args.kappa, args.cpu_seconds)
+        except Exception as exc:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "s", "cores": cpu_cores(), "kind": "reference",
+                   "sample": f"unavailable: {exc}"}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": mixed_s, "unit": "s", "n_gpus": world,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": mixed_s * 1e3,
+               "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+               "dtype": "f16 tensor-core factors, f32 panels, f64 refinement",
+               "data": "synthetic: seeded A = U diag(sigma) V', U,V = 8 Householder reflectors each",
+               "config": {"workload": f"general solve n={n}, kappa={args.kappa:g}, 1 rhs, "
+                                      f"{args.precision} factors + {args.refinement.upper()}-IR",
+                          "n": n, "nrhs": 1, "kappa": args.kappa, "precision": args.precision,
+                          "refinement": args.refinement, "nb": args.nb, "nb_fp64": args.nb_fp64,
+                          "l2": "inputs larger than L2 (8.6 GB FP64 matrix)",
+                          "parallelism": f"replicas x{world}"},
+               "fp64_lu_solve_s": fp64_s,
+               "speedup_vs_fp64": (fp64_s / mixed_s) if fp64_s else None,
+               "backward_error": eta, "backward_error_fp64": fp64_eta,
+               "backward_error_target": n * 2.0 ** -53, "forward_error": fwd,
+               "refinement_iterations": report.iterations,
+               "gmres_iterations": report.inner_iterations,
+               "factor_ms": report.factor_ms, "refine_ms": report.refine_ms,
+               "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+               "clocks": clock_summary, "gpu_launches": launches}
+        print(json.dumps(out))
+    s.free(a, bo)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

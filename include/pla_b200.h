@@ -41,9 +41,19 @@ typedef struct {
   double update_ms;  /* trailing GEMM / SYRK                              */
   double solve_ms;   /* triangular solves with the right-hand sides       */
   double refine_ms;  /* residuals and corrections of iterative refinement */
+  double convert_ms; /* precision conversions and operand packing         */
+  int update_launches; /* trailing-update kernels timed in update_ms      */
 } PLA_Phase_times;
+/* Phase timing uses CUDA events recorded on the library stream without
+ * synchronizing; the times are collected when PLA_B200_phase_times is
+ * called.  Timing stays on until switched off and accumulates across calls
+ * until PLA_B200_reset_phase_times. */
 int PLA_B200_phase_times(PLA_Phase_times *t);
 int PLA_B200_set_phase_timing(int on);
+int PLA_B200_reset_phase_times(void);
+
+/* Number of CUDA kernels the library has launched since it was loaded. */
+long PLA_B200_kernel_launches(void);
 
 /* ---- mixed-precision solve with FP64 iterative refinement ------------------
  * Factor a low-precision copy of A (trailing updates on the tensor cores),

@@ -118,6 +118,20 @@ class Restated:
         return out
 
 
+def _preload_openblas_deps() -> None:
+    """The OpenBLAS build used for timing ships beside its own libgfortran and
+    libquadmath; load those first so the dynamic linker finds them."""
+    import glob
+    import sys
+    for d in sys.path:
+        libs = os.path.join(d, "opencv_python_headless.libs")
+        if os.path.isdir(libs):
+            for pat in ("libquadmath-*.so*", "libgfortran-*.so*"):
+                for f in sorted(glob.glob(os.path.join(libs, pat))):
+                    ctypes.CDLL(f, mode=ctypes.RTLD_GLOBAL)
+            return
+
+
 class Reference:
     """ctypes view of the upstream PLAPACK compiled from its sources."""
 
@@ -127,6 +141,8 @@ class Reference:
         path = os.path.join(REF_DIR, name)
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} is not built (make -C oracle ref)")
+        if blas != "netlib":
+            _preload_openblas_deps()
         self.lib = ctypes.CDLL(path)
         self.lib.ref_trsm.argtypes = [_i] * 6 + [ctypes.c_double, _i, _vp, _i, _vp, _i]
         self.lib.ref_gemm.argtypes = [_i] * 5 + [ctypes.c_double, _i, _vp, _i, _vp, _i,

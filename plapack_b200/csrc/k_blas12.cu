@@ -1,6 +1,8 @@
 // Level-1/2 kernels, copies, conversions, row interchanges and norms.
 // All bandwidth-bound: grid-stride loops over column-major data with the row
 // index fastest across threads so that warps read contiguous memory.
+#include <atomic>
+
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -214,11 +216,20 @@ __global__ void col_abs_max_k(int m, int n, const T *X, long ldx, double *out) {
   }
 }
 
-inline int status() { return (int)cudaGetLastError(); }
+std::atomic<long> g_launches{0};
+
+// every launcher below issues exactly one kernel before calling this
+inline int status() {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return (int)cudaGetLastError();
+}
 
 }  // namespace
 
 extern "C" {
+
+void pla_k_count(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long pla_k_launches(void) { return g_launches.load(std::memory_order_relaxed); }
 
 int pla_k_fill(int dt, int m, int n, void *A, long lda, double value, cudaStream_t s) {
   if (m <= 0 || n <= 0) return 0;

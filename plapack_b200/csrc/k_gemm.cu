@@ -294,5 +294,6 @@ extern "C" int pla_k_gemm(int dt, int transa, int transb, int m, int n, int k, d
   } else {
     return (int)cudaErrorInvalidValue;
   }
+  pla_k_count(1);
   return (int)cudaGetLastError();
 }

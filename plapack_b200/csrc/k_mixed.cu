@@ -102,6 +102,7 @@ extern "C" int pla_k_pack_rows(int prec, int m, int kdim, const float *src, long
     pack_rows_k<__nv_bfloat16><<<grid, block, 0, s>>>(m, kdim, src, lds, (__nv_bfloat16 *)dst, ldd);
   else
     pack_rows_k<__half><<<grid, block, 0, s>>>(m, kdim, src, lds, (__half *)dst, ldd);
+  pla_k_count(1);
   return (int)cudaGetLastError();
 }
 
@@ -154,5 +155,6 @@ extern "C" int pla_k_residual(int n, int ncols, int nrhs, const double *A, long 
   else if (nrhs <= 8) RUN(8);
   else RUN(16);
 #undef RUN
+  pla_k_count(2);
   return (int)cudaGetLastError();
 }

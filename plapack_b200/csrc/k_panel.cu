@@ -260,6 +260,7 @@ int launch(int r, int w, void *A, long lda, int *piv, int *status, int *zero_inf
   void *args[] = {&Ap, &lda, &r, &w, &R, &use_smem, &piv, &status, &zero_info, &row_base, &bar,
                   &cand_abs, &cand_idx, &cand_row, &top_row};
   e = cudaLaunchCooperativeKernel((void *)panel_lu_k<T>, dim3(P), dim3(kThreads), args, dyn, s);
+  pla_k_count(1);
   return (int)e;
 }
 

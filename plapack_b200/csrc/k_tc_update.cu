@@ -147,7 +147,7 @@ template <int KB>
 __global__ void __launch_bounds__(THREADS, 1)
 tc_update_k(const __grid_constant__ CUtensorMap mapL, const __grid_constant__ CUtensorMap mapU,
             const __grid_constant__ CUtensorMap mapC, int row0, int col0, float alpha,
-            uint32_t idesc, int *status) {
+            uint32_t idesc, int lower, int *status) {
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t bar_full, bar_mma;
   __shared__ uint32_t tmem_s;
@@ -158,6 +158,9 @@ tc_update_k(const __grid_constant__ CUtensorMap mapL, const __grid_constant__ CU
   float *sC = reinterpret_cast<float *>(base);  // reused once the MMAs are done
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
+  // SYRK-shaped update: tiles strictly above the diagonal are not needed
+  if (lower && m0 + TM - 1 < n0) return;
+  if (*(volatile int *)status != PLA_K_OK) return;
 
   if (warp == 0) tmem_alloc(&tmem_s, TN);
   if (threadIdx.x == 32) {
@@ -257,13 +260,15 @@ int encode(CUtensorMap *map, CUtensorMapDataType dt, int esize, const void *ptr,
 
 template <int KB>
 int launch(const CUtensorMap &mL, const CUtensorMap &mU, const CUtensorMap &mC, int M, int N,
-           int row0, int col0, float alpha, uint32_t idesc, int *status, cudaStream_t s) {
+           int row0, int col0, float alpha, uint32_t idesc, int lower, int *status,
+           cudaStream_t s) {
   // operand tiles, reused afterwards as the 128 x 128 fp32 staging tile
   size_t ops = (size_t)2 * KB * BOX_BYTES, stage = (size_t)TM * TN * sizeof(float);
   size_t sm = (ops > stage ? ops : stage) + 1024;
   cudaFuncSetAttribute(tc_update_k<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   dim3 grid((M + TM - 1) / TM, (N + TN - 1) / TN);
-  tc_update_k<KB><<<grid, THREADS, sm, s>>>(mL, mU, mC, row0, col0, alpha, idesc, status);
+  tc_update_k<KB><<<grid, THREADS, sm, s>>>(mL, mU, mC, row0, col0, alpha, idesc, lower, status);
+  pla_k_count(1);
   return (int)cudaGetLastError();
 }
 
@@ -272,7 +277,7 @@ int launch(const CUtensorMap &mL, const CUtensorMap &mU, const CUtensorMap &mC, 
 extern "C" int pla_k_tc_update(int prec, int M, int N, int K, float alpha, const void *L,
                                long ldl, long l_rows, const void *U, long ldu, long u_rows,
                                float *C, long ldc, long c_rows, long c_cols, int row0, int col0,
-                               int *status, cudaStream_t s) {
+                               int lower, int *status, cudaStream_t s) {
   if (M <= 0 || N <= 0 || K <= 0) return 0;
   if (K % KBOX != 0 || K > 4 * KBOX) return (int)cudaErrorInvalidValue;
   if (ldl % 8 || ldu % 8 || ldc % 4 || (row0 % 4) || ((uintptr_t)C % 16) || ((uintptr_t)L % 16) ||
@@ -297,9 +302,9 @@ extern "C" int pla_k_tc_update(int prec, int M, int N, int K, float alpha, const
   const uint32_t idesc = (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)(TN >> 3) << 17) |
                          ((uint32_t)(TM >> 4) << 24);
   switch (K / KBOX) {
-    case 1: return launch<1>(mL, mU, mC, M, N, row0, col0, alpha, idesc, status, s);
-    case 2: return launch<2>(mL, mU, mC, M, N, row0, col0, alpha, idesc, status, s);
-    case 3: return launch<3>(mL, mU, mC, M, N, row0, col0, alpha, idesc, status, s);
-    default: return launch<4>(mL, mU, mC, M, N, row0, col0, alpha, idesc, status, s);
+    case 1: return launch<1>(mL, mU, mC, M, N, row0, col0, alpha, idesc, lower, status, s);
+    case 2: return launch<2>(mL, mU, mC, M, N, row0, col0, alpha, idesc, lower, status, s);
+    case 3: return launch<3>(mL, mU, mC, M, N, row0, col0, alpha, idesc, lower, status, s);
+    default: return launch<4>(mL, mU, mC, M, N, row0, col0, alpha, idesc, lower, status, s);
   }
 }

@@ -209,6 +209,7 @@ int trsm_small_t(char side, char uplo, char trans, char diag, int b, int other, 
     trsm_right_k<T, RB><<<grid, kThreads, sm, s>>>(b, other, (T)alpha, (const T *)Tm, ldt, (T *)B,
                                                    ldb, upper_op, tr, unit, status);
   }
+  pla_k_count(1);
   return (int)cudaGetLastError();
 }
 
@@ -239,6 +240,7 @@ extern "C" int pla_k_potrf_lower(int dt, int b, void *A, long lda, int *status, 
   } else {
     return (int)cudaErrorInvalidValue;
   }
+  pla_k_count(1);
   return (int)cudaGetLastError();
 }
 

@@ -1,0 +1,221 @@
+// Triangular solve with one right-hand side in a single launch.
+//
+//   tri_inv_blocks_k : inverse of every TB x TB diagonal block of op(A)
+//                      (computed once per factor, reused by every solve);
+//   trsv_ticket_k    : x := inv(op(A)) b.  CTAs take block rows through an
+//                      atomic ticket in dependency order, so a block row only
+//                      ever waits for rows whose owners are already running
+//                      (no co-residency assumption).  For block row i a CTA
+//                      accumulates op(A)(i, j) x_j over every finished block j
+//                      (waiting on j's flag with a bounded spin), multiplies by
+//                      the inverse diagonal block, publishes x_i and raises
+//                      flag i.  The triangle is read exactly once, so the solve
+//                      is HBM-bound apart from the per-block latency chain.
+//                      b and x may be the same array.
+#include "PLA.h"
+#include "pla_kernels.h"
+
+namespace {
+
+constexpr int TB = 128, THREADS = 256;
+constexpr long kSpin = 20000000;
+
+template <typename T>
+__device__ __forceinline__ T opA(const T *A, long lda, bool trans, long i, long j) {
+  return trans ? A[j + i * lda] : A[i + j * lda];
+}
+
+// inverse of the TB x TB diagonal block `blockIdx.x` of op(A) into Dinv
+// (element (r, c) of block i at Dinv[i*TB + r + c*ldd])
+template <typename T>
+__global__ void __launch_bounds__(THREADS)
+tri_inv_blocks_k(int n, const T *A, long lda, bool lower_op, bool trans, bool unit, T *Dinv,
+                 long ldd) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  T *D = (T *)sm;                 // TB x TB, ld TB + 1
+  T *X = D + TB * (TB + 1);       // TB x TB, ld TB + 1
+  constexpr int L = TB + 1;
+  const int blk = blockIdx.x, r0 = blk * TB, nb = min(TB, n - r0);
+  for (int t = threadIdx.x; t < TB * TB; t += THREADS) {
+    int i = t % TB, j = t / TB;
+    T v = T(0);
+    if (i < nb && j < nb) v = opA(A, lda, trans, (long)r0 + i, (long)r0 + j);
+    if (i == j && (unit || i >= nb)) v = T(1);
+    D[i + j * L] = v;
+    X[i + j * L] = i == j ? T(1) : T(0);
+  }
+  __syncthreads();
+  // solve D X = I; column c is handled by the two threads with c = tid % TB
+  const int c = threadIdx.x % TB, half = threadIdx.x / TB;
+  for (int step = 0; step < TB; step++) {
+    const int l = lower_op ? step : TB - 1 - step;
+    if (half == 0) X[l + c * L] = X[l + c * L] / D[l + l * L];
+    __syncthreads();
+    const T xl = X[l + c * L];
+    if (lower_op)
+      for (int i = l + 1 + half; i < TB; i += 2) X[i + c * L] -= D[i + l * L] * xl;
+    else
+      for (int i = half; i < l; i += 2) X[i + c * L] -= D[i + l * L] * xl;
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < TB * TB; t += THREADS) {
+    int i = t % TB, j = t / TB;
+    Dinv[(long)(r0 + i) + (long)j * ldd] = X[i + j * L];
+  }
+}
+
+__device__ __forceinline__ int ld_acquire(const int *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int *p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+template <typename T>
+__global__ void __launch_bounds__(THREADS)
+trsv_ticket_k(int n, int nblk, const T *A, long lda, bool lower_op, bool trans, const T *Dinv,
+              long ldd, const T *b, T *x, int *ticket, int *flags, int *status) {
+  __shared__ T xs[TB];
+  __shared__ T part[2][TB];
+  __shared__ int s_blk, s_bad;
+  const int r = threadIdx.x % TB, half = threadIdx.x / TB;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_blk = atomicAdd(ticket, 1);
+      s_bad = 0;
+    }
+    __syncthreads();
+    const int q = s_blk;
+    if (q >= nblk) return;
+    const int i = lower_op ? q : nblk - 1 - q;
+    const long r0 = (long)i * TB;
+    const int nbi = min(TB, n - (int)r0);
+    T acc = T(0);
+    for (int s = 0; s < q; s++) {
+      const int j = lower_op ? s : nblk - 1 - s;
+      const long c0 = (long)j * TB;
+      const int nbj = min(TB, n - (int)c0);
+      if (threadIdx.x == 0) {
+        long spins = 0;
+        while (ld_acquire(&flags[j]) == 0) {
+          if (++spins > kSpin || *(volatile int *)status != PLA_K_OK) {
+            atomicCAS(status, PLA_K_OK, PLA_K_TIMEOUT);
+            s_bad = 1;
+            break;
+          }
+          __nanosleep(32);
+        }
+      }
+      __syncthreads();
+      if (s_bad) return;
+      if (threadIdx.x < nbj) xs[threadIdx.x] = __ldcg(&x[c0 + threadIdx.x]);
+      __syncthreads();
+      if (r < nbi) {
+        if (!trans) {
+          // warps read down the columns of A: coalesced
+          for (int c = half; c < nbj; c += 2) acc += A[(r0 + r) + (c0 + c) * lda] * xs[c];
+        } else {
+          // op(A)(r, c) = A(c, r): each thread walks a contiguous stretch of column r
+          const int cb = half * (TB / 2), ce = min(cb + TB / 2, nbj);
+          const T *col = A + (r0 + r) * lda + c0;
+          for (int c = cb; c < ce; c++) acc += col[c] * xs[c];
+        }
+      }
+      __syncthreads();
+    }
+    part[half][r] = acc;
+    __syncthreads();
+    if (threadIdx.x < TB) xs[threadIdx.x] = r < nbi ? b[r0 + r] - (part[0][r] + part[1][r]) : T(0);
+    __syncthreads();
+    // x_i = inv(D_i) y
+    T y = T(0);
+    for (int c = half; c < TB; c += 2) y += Dinv[(r0 + r) + (long)c * ldd] * xs[c];
+    part[half][r] = y;
+    __syncthreads();
+    if (threadIdx.x < nbi) x[r0 + threadIdx.x] = part[0][threadIdx.x] + part[1][threadIdx.x];
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) st_release(&flags[i], 1);
+  }
+}
+
+void *g_flags = nullptr;
+size_t g_flags_bytes = 0;
+
+int *flags_for(int nblk) {
+  size_t need = (size_t)(nblk + 8) * sizeof(int);
+  if (g_flags_bytes < need) {
+    if (g_flags) cudaFree(g_flags);
+    g_flags = nullptr;
+    g_flags_bytes = 0;
+    if (cudaMalloc(&g_flags, need) != cudaSuccess) return nullptr;
+    g_flags_bytes = need;
+  }
+  return (int *)g_flags;
+}
+
+int g_sms = 0;
+
+template <typename T>
+int inv_blocks(char uplo, char trans, char diag, int n, const void *A, long lda, void *Dinv,
+               long ldd, cudaStream_t s) {
+  const bool tr = trans != 'N', lower_op = (uplo == 'L') != tr, unit = diag == 'U';
+  const int nblk = (n + TB - 1) / TB;
+  size_t sm = (size_t)2 * TB * (TB + 1) * sizeof(T);
+  cudaFuncSetAttribute(tri_inv_blocks_k<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  tri_inv_blocks_k<T><<<nblk, THREADS, sm, s>>>(n, (const T *)A, lda, lower_op, tr, unit,
+                                                (T *)Dinv, ldd);
+  pla_k_count(1);
+  return (int)cudaGetLastError();
+}
+
+template <typename T>
+int ticket_solve(char uplo, char trans, int n, const void *A, long lda, const void *Dinv,
+                 long ldd, const void *b, void *x, int *status, cudaStream_t s) {
+  const bool tr = trans != 'N', lower_op = (uplo == 'L') != tr;
+  const int nblk = (n + TB - 1) / TB;
+  int *fl = flags_for(nblk);
+  if (!fl) return (int)cudaErrorMemoryAllocation;
+  cudaError_t e = cudaMemsetAsync(fl, 0, (size_t)(nblk + 8) * sizeof(int), s);
+  if (e) return (int)e;
+  if (!g_sms) {
+    int d;
+    cudaGetDevice(&d);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, d);
+  }
+  int grid = nblk < 4 * g_sms ? nblk : 4 * g_sms;
+  trsv_ticket_k<T><<<grid, THREADS, 0, s>>>(n, nblk, (const T *)A, lda, lower_op, tr,
+                                            (const T *)Dinv, ldd, (const T *)b, (T *)x,
+                                            fl + nblk, fl, status);
+  pla_k_count(1);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace
+
+// Dinv must hold ldd x 128 elements with ldd >= n rounded up to 128.
+extern "C" int pla_k_trsv_inv_blocks(int dt, char uplo, char trans, char diag, int n,
+                                     const void *A, long lda, void *Dinv, long ldd,
+                                     cudaStream_t s) {
+  if (n <= 0) return 0;
+  // fp32 only: two 128 x 129 fp64 blocks would not fit in shared memory
+  if (dt == MPI_FLOAT) return inv_blocks<float>(uplo, trans, diag, n, A, lda, Dinv, ldd, s);
+  return (int)cudaErrorInvalidValue;
+}
+
+extern "C" int pla_k_trsv_ticket(int dt, char uplo, char trans, int n, const void *A, long lda,
+                                 const void *Dinv, long ldd, const void *b, void *x, int *status,
+                                 cudaStream_t s) {
+  if (n <= 0) return 0;
+  if (dt == MPI_FLOAT)
+    return ticket_solve<float>(uplo, trans, n, A, lda, Dinv, ldd, b, x, status, s);
+  return (int)cudaErrorInvalidValue;
+}
+
+extern "C" void pla_trsv_release(void) {
+  if (g_flags) cudaFree(g_flags);
+  g_flags = nullptr;
+  g_flags_bytes = 0;
+}

@@ -110,22 +110,49 @@ void release_scratch() {
   }
 }
 
+namespace {
+struct Pending {
+  double *acc;
+  cudaEvent_t a, b;
+};
+std::vector<Pending> g_pending;
+std::vector<cudaEvent_t> g_event_pool;
+
+cudaEvent_t take_event() {
+  if (!g_event_pool.empty()) {
+    cudaEvent_t e = g_event_pool.back();
+    g_event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+}  // namespace
+
 PhaseTimer::PhaseTimer(double *target) : acc(target), on(state().phase_timing != 0) {
   if (!on) return;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
+  e0 = take_event();
+  e1 = take_event();
   cudaEventRecord(e0, stream());
 }
 
 PhaseTimer::~PhaseTimer() {
   if (!on) return;
   cudaEventRecord(e1, stream());
-  cudaEventSynchronize(e1);
-  float ms = 0.f;
-  cudaEventElapsedTime(&ms, e0, e1);
-  *acc += ms;
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  g_pending.push_back({acc, e0, e1});
+}
+
+void resolve_phases() {
+  for (Pending &p : g_pending) {
+    cudaEventSynchronize(p.b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, p.a, p.b);
+    *p.acc += ms;
+    g_event_pool.push_back(p.a);
+    g_event_pool.push_back(p.b);
+  }
+  g_pending.clear();
 }
 
 }  // namespace pla
@@ -391,13 +418,23 @@ int PLA_B200_set_stream(void *s) {
 void *PLA_B200_get_stream(void) { return (void *)stream(); }
 
 int PLA_B200_phase_times(PLA_Phase_times *t) {
-  if (t) *t = state().phases;
+  resolve_phases();
+  PLA_Phase_times &p = state().phases;
+  p.total_ms = p.panel_ms + p.swap_ms + p.trsm_ms + p.update_ms + p.solve_ms + p.refine_ms +
+               p.convert_ms;
+  if (t) *t = p;
   return PLA_SUCCESS;
 }
 int PLA_B200_set_phase_timing(int on) {
   state().phase_timing = on;
   return PLA_SUCCESS;
 }
+int PLA_B200_reset_phase_times(void) {
+  resolve_phases();
+  state().phases = PLA_Phase_times{};
+  return PLA_SUCCESS;
+}
+long PLA_B200_kernel_launches(void) { return pla_k_launches(); }
 
 // ---------------------------------------------------------------- creation --
 int PLA_Matrix_create(MPI_Datatype dt, int length, int width, PLA_Template templ,

@@ -96,7 +96,7 @@ void warn(const char *message);
 void *scratch(int slot, size_t bytes);
 void release_scratch();
 
-// phase timing helpers
+// phase timing: events recorded on the library stream, resolved later
 struct PhaseTimer {
   cudaEvent_t e0{}, e1{};
   double *acc;
@@ -104,6 +104,7 @@ struct PhaseTimer {
   explicit PhaseTimer(double *target);
   ~PhaseTimer();
 };
+void resolve_phases();
 
 }  // namespace pla
 

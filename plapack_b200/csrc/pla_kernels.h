@@ -17,6 +17,9 @@ extern "C" {
 #define PLA_K_NOT_SPD 2        /* Cholesky met a non-positive pivot       */
 
 void pla_kernels_release(void);
+/* number of kernels the library has launched (all streams, since load) */
+void pla_k_count(int n);
+long pla_k_launches(void);
 
 int pla_k_fill(int dt, int m, int n, void *A, long lda, double value, cudaStream_t s);
 /* Y := alpha * X + beta * Y (beta == 0 ignores Y's contents) */
@@ -97,15 +100,26 @@ int pla_k_col_abs_max(int dt, int m, int n, const void *X, long ldx, double *out
  * L (M x K, l_rows allocated) and U (N x K, u_rows allocated) in bf16/fp16
  * with K contiguous (leading dimensions ldl, ldu in elements, multiples of 8);
  * C fp32 column-major with ldc (multiple of 4), c_rows x c_cols allocated.
- * K must be a multiple of 64 and at most 256. */
+ * K must be a multiple of 64 and at most 256.  lower != 0 skips the tiles
+ * strictly above the diagonal (SYRK-shaped updates). */
 int pla_k_tc_update(int prec, int M, int N, int K, float alpha, const void *L, long ldl,
                     long l_rows, const void *U, long ldu, long u_rows, float *C, long ldc,
-                    long c_rows, long c_cols, int row0, int col0, int *status, cudaStream_t s);
+                    long c_rows, long c_cols, int row0, int col0, int lower, int *status,
+                    cudaStream_t s);
 /* dst (bf16/fp16, row-major, ldd) := src (fp32, m x kdim column-major, lds) */
 int pla_k_pack_rows(int prec, int m, int kdim, const float *src, long lds, void *dst, long ldd,
                     cudaStream_t s);
 /* R := B - A X in FP64 (A n x ncols, X ncols x nrhs, nrhs <= 16); with
  * abs_rows, R(:,0) := row sums of |A|.  work: pla_k_residual_work() bytes. */
+/* single-launch fp32 triangular solve with one right-hand side: the inverses
+ * of the 128 x 128 diagonal blocks of op(A) go to Dinv (ldd >= n rounded up to
+ * 128, 128 columns) once per factor; then x := inv(op(A)) b (x may alias b). */
+int pla_k_trsv_inv_blocks(int dt, char uplo, char trans, char diag, int n, const void *A,
+                          long lda, void *Dinv, long ldd, cudaStream_t s);
+int pla_k_trsv_ticket(int dt, char uplo, char trans, int n, const void *A, long lda,
+                      const void *Dinv, long ldd, const void *b, void *x, int *status,
+                      cudaStream_t s);
+void pla_trsv_release(void);
 size_t pla_k_residual_work(int n, int ncols, int nrhs);
 int pla_k_residual(int n, int ncols, int nrhs, const double *A, long lda, const double *X,
                    long ldx, const double *B, long ldb, double *R, long ldr, int abs_rows,

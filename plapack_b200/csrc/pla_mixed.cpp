@@ -1,0 +1,435 @@
+// Mixed-precision direct solves with FP64 iterative refinement.
+//
+// Factorization: an fp32 working copy of A is factored with the same blocked
+// right-looking loops as PLA_LU / PLA_Chol (fp32 panel, pivots, triangular
+// solves); only the trailing update -- the O(n^3) part -- runs in bf16 or
+// fp16 on the tensor cores with fp32 accumulation (k_tc_update.cu).  A itself
+// is never modified.
+//
+// Refinement, both in FP64 with the fp32 factors as the preconditioner M:
+//   LU-IR    : x <- x + M^{-1} (b - A x)
+//   GMRES-IR : x <- x + d, d from restarted GMRES on M^{-1} A d = M^{-1} r with
+//              classical Gram-Schmidt applied twice (CGS2)
+// until  ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= tol  for every
+// right-hand side.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "pla_internal.h"
+#include "pla_kernels.h"
+
+using namespace pla;
+
+namespace pla {
+int trsm_device(int dt, char side, char uplo, char trans, char diag, int nt, int other,
+                double alpha, const char *T, long ldt, char *B, long ldb);
+}
+
+namespace {
+
+#define K(call)                                                    \
+  do {                                                             \
+    int r_ = (call);                                               \
+    if (r_) return cuda_fail((cudaError_t)r_, __LINE__, __FILE__); \
+  } while (0)
+
+enum Slots { kSlotA32 = 4, kSlotL = 5, kSlotU = 6, kSlotPiv = 7, kSlotVec = 8, kSlotWork = 9,
+             kSlotV = 10, kSlotSt = 11 };
+
+long round_up(long v, long m) { return (v + m - 1) / m * m; }
+
+struct Factor {
+  int n = 0, ld = 0, prec = 0, kind = 0;  // kind 0 = LU, 1 = Cholesky
+  float *a = nullptr;
+  int *piv = nullptr;
+  int *status = nullptr;  // [status, info, zero_info]
+  // inverses of the 128 x 128 diagonal blocks of the two triangular factors
+  float *dinv1 = nullptr, *dinv2 = nullptr;
+  long ldd = 0;
+};
+
+constexpr int kSlotDinv = 13;
+
+// the per-factor data of the single-launch triangular solves
+int prepare_solves(Factor &F) {
+  F.ldd = round_up(F.n, 128);
+  float *d = (float *)scratch(kSlotDinv, (size_t)2 * F.ldd * 128 * sizeof(float));
+  if (!d) PLA_FAIL("cannot allocate the inverse diagonal blocks");
+  F.dinv1 = d;
+  F.dinv2 = d + F.ldd * 128;
+  if (F.kind == 0) {
+    K(pla_k_trsv_inv_blocks(MPI_FLOAT, 'L', 'N', 'U', F.n, F.a, F.ld, F.dinv1, F.ldd, stream()));
+    K(pla_k_trsv_inv_blocks(MPI_FLOAT, 'U', 'N', 'N', F.n, F.a, F.ld, F.dinv2, F.ldd, stream()));
+  } else {
+    K(pla_k_trsv_inv_blocks(MPI_FLOAT, 'L', 'N', 'N', F.n, F.a, F.ld, F.dinv1, F.ldd, stream()));
+    K(pla_k_trsv_inv_blocks(MPI_FLOAT, 'L', 'T', 'N', F.n, F.a, F.ld, F.dinv2, F.ldd, stream()));
+  }
+  return PLA_SUCCESS;
+}
+
+struct EventTimer {
+  cudaEvent_t a, b;
+  EventTimer() {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, stream());
+  }
+  double stop() {
+    cudaEventRecord(b, stream());
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+  }
+  ~EventTimer() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+};
+
+// fp32 factorization with low-precision trailing updates
+int factor_mixed(Factor &F, const double *A, long lda, int nb) {
+  const int n = F.n;
+  const long ld = F.ld;
+  auto at = [&](long i, long j) { return F.a + i + j * ld; };
+  K(pla_k_convert(MPI_DOUBLE, A, lda, MPI_FLOAT, F.a, ld, n, n, stream()));
+  const bool lowp = F.prec != PLA_B200_PREC_FP32;
+  const int kprec = F.prec == PLA_B200_PREC_BF16 ? PLA_K_BF16 : PLA_K_FP16;
+  void *Lp = nullptr, *Up = nullptr;
+  if (lowp) {
+    Lp = scratch(kSlotL, (size_t)n * nb * 2 + 256);
+    Up = scratch(kSlotU, (size_t)n * nb * 2 + 256);
+    if (!Lp || !Up) PLA_FAIL("cannot allocate the low-precision panels");
+  }
+  int *st = F.status;
+  PLA_Phase_times &ph = state().phases;
+  for (int k = 0; k < n; k += nb) {
+    const int b = std::min(nb, n - k), rest = n - k - b;
+    if (F.kind == 0) {
+      {
+        PhaseTimer t(&ph.panel_ms);
+        K(pla_k_lu_panel(MPI_FLOAT, n - k, b, at(k, k), ld, F.piv + k, &st[0], &st[2], k,
+                         stream()));
+      }
+      {
+        PhaseTimer t(&ph.swap_ms);
+        K(pla_k_laswp(MPI_FLOAT, at(k, 0), ld, b, F.piv + k, 0, k, k + b, n, stream()));
+      }
+      if (rest <= 0) continue;
+      PhaseTimer t(&ph.trsm_ms);
+      K(trsm_device(MPI_FLOAT, 'L', 'L', 'N', 'U', b, rest, 1.0, (const char *)at(k, k), ld,
+                    (char *)at(k, k + b), ld));
+    } else {
+      {
+        PhaseTimer t(&ph.panel_ms);
+        K(pla_k_potrf_lower(MPI_FLOAT, b, at(k, k), ld, &st[0], &st[1], k, stream()));
+      }
+      if (rest <= 0) continue;
+      PhaseTimer t(&ph.trsm_ms);
+      K(pla_k_trsm_small(MPI_FLOAT, 'R', 'L', 'T', 'N', b, rest, 1.0, at(k, k), ld, at(k + b, k),
+                         ld, &st[0], stream()));
+    }
+    if (lowp && b % 64 == 0) {
+      const void *Uop = Lp;
+      {
+        PhaseTimer t(&ph.convert_ms);
+        K(pla_k_pack_rows(kprec, rest, b, at(k + b, k), ld, Lp, nb, stream()));
+        if (F.kind == 0) {
+          K(pla_k_convert(MPI_FLOAT, at(k, k + b), ld, kprec, Up, nb, b, rest, stream()));
+          Uop = Up;
+        }
+      }
+      PhaseTimer t(&ph.update_ms);
+      K(pla_k_tc_update(kprec, rest, rest, b, -1.0f, Lp, nb, n, Uop, nb, n, F.a, ld, ld, n, k + b,
+                        k + b, F.kind == 1, &st[0], stream()));
+      if (t.on) ph.update_launches++;
+    } else if (F.kind == 0) {
+      K(pla_k_gemm(MPI_FLOAT, PLA_NO_TRANSPOSE, PLA_NO_TRANSPOSE, rest, rest, b, -1.0, at(k + b, k),
+                   ld, at(k, k + b), ld, 1.0, at(k + b, k + b), ld, 0, &st[0], stream()));
+    } else {
+      K(pla_k_gemm(MPI_FLOAT, PLA_NO_TRANSPOSE, PLA_TRANSPOSE, rest, rest, b, -1.0, at(k + b, k),
+                   ld, at(k + b, k), ld, 1.0, at(k + b, k + b), ld, 'L', &st[0], stream()));
+    }
+  }
+  return PLA_SUCCESS;
+}
+
+// out (fp64, n x nrhs, ldo) := M^{-1} v (fp64, ldv) with the fp32 factors
+int precond(const Factor &F, const double *v, long ldv, double *out, long ldo, int nrhs,
+            float *t32) {
+  const int n = F.n;
+  K(pla_k_convert(MPI_DOUBLE, v, ldv, MPI_FLOAT, t32, n, n, nrhs, stream()));
+  if (F.kind == 0) K(pla_k_laswp_rows(MPI_FLOAT, t32, n, nrhs, n, F.piv, stream()));
+  const char u1 = 'L', t1 = 'N', d1 = F.kind == 0 ? 'U' : 'N';
+  const char u2 = F.kind == 0 ? 'U' : 'L', t2 = F.kind == 0 ? 'N' : 'T', d2 = 'N';
+  if (nrhs <= 2 && F.dinv1) {
+    for (int j = 0; j < nrhs; j++) {
+      float *col = t32 + (long)j * n;
+      K(pla_k_trsv_ticket(MPI_FLOAT, u1, t1, n, F.a, F.ld, F.dinv1, F.ldd, col, col, F.status,
+                          stream()));
+      K(pla_k_trsv_ticket(MPI_FLOAT, u2, t2, n, F.a, F.ld, F.dinv2, F.ldd, col, col, F.status,
+                          stream()));
+    }
+  } else {
+    K(pla_k_trsv_blocked(MPI_FLOAT, u1, t1, d1, n, nrhs, F.a, F.ld, t32, n, stream()));
+    K(pla_k_trsv_blocked(MPI_FLOAT, u2, t2, d2, n, nrhs, F.a, F.ld, t32, n, stream()));
+  }
+  K(pla_k_convert(MPI_FLOAT, t32, n, MPI_DOUBLE, out, ldo, n, nrhs, stream()));
+  return PLA_SUCCESS;
+}
+
+double host_max(const double *dev, int count) {
+  std::vector<double> h(count);
+  cudaMemcpyAsync(h.data(), dev, count * sizeof(double), cudaMemcpyDeviceToHost, stream());
+  cudaStreamSynchronize(stream());
+  double m = 0;
+  for (double v : h) m = std::max(m, v);
+  return m;
+}
+
+struct Norms {
+  double a_inf = 0;
+  std::vector<double> b_inf;
+};
+
+// per-column backward error of x given r = b - A x
+int backward_errors(int n, int nrhs, const double *R, long ldr, const double *X, long ldx,
+                    const Norms &nm, double *tmp, std::vector<double> &eta) {
+  K(pla_k_col_abs_max(MPI_DOUBLE, n, nrhs, R, ldr, tmp, stream()));
+  K(pla_k_col_abs_max(MPI_DOUBLE, n, nrhs, X, ldx, tmp + nrhs, stream()));
+  std::vector<double> h(2 * nrhs);
+  PLA_CUDA(cudaMemcpyAsync(h.data(), tmp, 2 * nrhs * sizeof(double), cudaMemcpyDeviceToHost,
+                           stream()));
+  PLA_CUDA(cudaStreamSynchronize(stream()));
+  eta.resize(nrhs);
+  for (int j = 0; j < nrhs; j++) {
+    double den = nm.a_inf * h[nrhs + j] + nm.b_inf[j];
+    eta[j] = den > 0 ? h[j] / den : h[j];
+  }
+  return PLA_SUCCESS;
+}
+
+double dot(int n, const double *x, const double *y, double *tmp) {
+  pla_k_gemv(MPI_DOUBLE, PLA_TRANSPOSE, n, 1, 1.0, x, n, y, 0.0, tmp, stream());
+  double h = 0;
+  cudaMemcpyAsync(&h, tmp, sizeof h, cudaMemcpyDeviceToHost, stream());
+  cudaStreamSynchronize(stream());
+  return h;
+}
+
+// one restarted-GMRES correction: d ~= A^{-1} r (d, r fp64 columns)
+int gmres(const Factor &F, const double *A, long lda, const double *r, double *d, int restart,
+          double tau, double *V, double *w, double *tmp, float *t32, double *work, int *iters) {
+  const int n = F.n, m = restart;
+  // z = M^{-1} r, beta = ||z||
+  int rc = precond(F, r, n, V, n, 1, t32);
+  if (rc) return rc;
+  double beta = std::sqrt(dot(n, V, V, tmp));
+  K(pla_k_fill(MPI_DOUBLE, n, 1, d, n, 0.0, stream()));
+  if (!(beta > 0)) return PLA_SUCCESS;
+  K(pla_k_scal(MPI_DOUBLE, n, 1, 1.0 / beta, V, n, stream()));
+  std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1, 0.0);
+  g[0] = beta;
+  int j = 0;
+  for (; j < m; j++) {
+    double *vj = V + (long)j * n, *vn = V + (long)(j + 1) * n;
+    // w = M^{-1} (A v_j)
+    K(pla_k_residual(n, n, 1, A, lda, vj, n, nullptr, n, w, n, 0, work, stream()));
+    rc = precond(F, w, n, vn, n, 1, t32);
+    if (rc) return rc;
+    // CGS2 against v_0 .. v_j
+    std::vector<double> h(j + 1, 0.0);
+    for (int pass = 0; pass < 2; pass++) {
+      K(pla_k_gemv(MPI_DOUBLE, PLA_TRANSPOSE, n, j + 1, 1.0, V, n, vn, 0.0, tmp, stream()));
+      std::vector<double> hp(j + 1);
+      PLA_CUDA(cudaMemcpyAsync(hp.data(), tmp, (j + 1) * sizeof(double), cudaMemcpyDeviceToHost,
+                               stream()));
+      PLA_CUDA(cudaStreamSynchronize(stream()));
+      // tmp still holds the coefficients on the device
+      K(pla_k_gemv(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, j + 1, -1.0, V, n, tmp, 1.0, vn, stream()));
+      for (int i = 0; i <= j; i++) h[i] += hp[i];
+    }
+    double hn = std::sqrt(dot(n, vn, vn, tmp));
+    for (int i = 0; i <= j; i++) H[i + (size_t)j * (m + 1)] = h[i];
+    H[j + 1 + (size_t)j * (m + 1)] = hn;
+    if (hn > 0) K(pla_k_scal(MPI_DOUBLE, n, 1, 1.0 / hn, vn, n, stream()));
+    // Givens rotations on column j
+    for (int i = 0; i < j; i++) {
+      double a = H[i + (size_t)j * (m + 1)], b = H[i + 1 + (size_t)j * (m + 1)];
+      H[i + (size_t)j * (m + 1)] = cs[i] * a + sn[i] * b;
+      H[i + 1 + (size_t)j * (m + 1)] = -sn[i] * a + cs[i] * b;
+    }
+    double a = H[j + (size_t)j * (m + 1)], b = H[j + 1 + (size_t)j * (m + 1)];
+    double rr = std::hypot(a, b);
+    cs[j] = rr > 0 ? a / rr : 1.0;
+    sn[j] = rr > 0 ? b / rr : 0.0;
+    H[j + (size_t)j * (m + 1)] = rr;
+    H[j + 1 + (size_t)j * (m + 1)] = 0.0;
+    g[j + 1] = -sn[j] * g[j];
+    g[j] = cs[j] * g[j];
+    if (std::fabs(g[j + 1]) <= tau * beta || hn == 0) {
+      j++;
+      break;
+    }
+  }
+  // y = H(0:j,0:j) \ g(0:j); d = V y
+  std::vector<double> y(j, 0.0);
+  for (int i = j - 1; i >= 0; i--) {
+    double s = g[i];
+    for (int c = i + 1; c < j; c++) s -= H[i + (size_t)c * (m + 1)] * y[c];
+    y[i] = s / H[i + (size_t)i * (m + 1)];
+  }
+  if (j > 0) {
+    PLA_CUDA(cudaMemcpyAsync(tmp, y.data(), j * sizeof(double), cudaMemcpyHostToDevice, stream()));
+    K(pla_k_gemv(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, j, 1.0, V, n, tmp, 0.0, d, stream()));
+  }
+  *iters += j;
+  return PLA_SUCCESS;
+}
+
+int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
+                PLA_Mixed_report *rep) {
+  if (!valid(A) || !valid(B)) PLA_FAIL("invalid object");
+  if (!is_double(A) || !is_double(B)) PLA_FAIL("the mixed-precision solvers take FP64 objects");
+  if (A->length != A->width || B->length != A->length) PLA_FAIL("nonconformal objects");
+  PLA_Mixed_params p;
+  PLA_Mixed_params_default(&p);
+  if (pin) p = *pin;
+  if (p.max_iterations <= 0) p.max_iterations = 50;
+  if (p.gmres_restart <= 0) p.gmres_restart = 30;
+  const int n = A->length, nrhs = B->width;
+  if (n == 0 || nrhs == 0) {
+    if (rep) *rep = PLA_Mixed_report{1, 0, 0, 0, 0.0, 0.0, 0.0};
+    return PLA_SUCCESS;
+  }
+  if (nrhs > 16) PLA_FAIL("at most 16 right-hand sides per mixed-precision solve");
+  int nb = p.nb;
+  if (nb <= 0) PLA_Environ_nb_alg(PLA_OP_PAN_PAN, A->templ, &nb);
+  if (p.precision != PLA_B200_PREC_FP32) {
+    nb = std::max(64, nb / 64 * 64);
+    nb = std::min(nb, kind == 0 ? 256 : 128);
+  } else if (kind == 1) {
+    nb = std::min(nb, 128);
+  }
+  const double tol = p.tol > 0 ? p.tol : n * std::ldexp(1.0, -53);
+  const double *Ad = (const double *)at(A, 0, 0);
+  const long lda = ld(A);
+  double *Bd = (double *)at(B, 0, 0);
+  const long ldb = ld(B);
+
+  Factor F;
+  F.n = n;
+  F.ld = (int)round_up(n, 32);
+  F.prec = p.precision;
+  F.kind = kind;
+  F.a = (float *)scratch(kSlotA32, (size_t)F.ld * n * sizeof(float));
+  F.piv = (int *)scratch(kSlotPiv, (size_t)n * sizeof(int) + 64);
+  F.status = (int *)scratch(kSlotSt, 64);
+  const size_t vec = (size_t)n * 16;
+  double *X = (double *)scratch(kSlotVec, (5 * vec + 64) * sizeof(double));
+  if (!F.a || !F.piv || !F.status || !X) PLA_FAIL("cannot allocate the mixed-precision workspace");
+  double *R = X + vec, *Dv = R + vec, *Bsave = Dv + vec, *tmp = Bsave + vec;
+  float *t32b = (float *)scratch(kSlotWork + 3, vec * sizeof(float) + 256);
+  double *work = (double *)scratch(kSlotWork, std::max(pla_k_residual_work(n, n, nrhs),
+                                                       (size_t)n * sizeof(double)) + 256);
+  double *V = nullptr, *w = nullptr;
+  if (p.refinement == PLA_B200_IR_GMRES) {
+    V = (double *)scratch(kSlotV, (size_t)n * (p.gmres_restart + 2) * sizeof(double));
+    w = V + (size_t)n * (p.gmres_restart + 1);
+  }
+  if (!t32b || !work || (p.refinement == PLA_B200_IR_GMRES && !V))
+    PLA_FAIL("cannot allocate the refinement workspace");
+  PLA_CUDA(cudaMemsetAsync(F.status, 0, 64, stream()));
+
+  PLA_Mixed_report r{};
+  // ---- factorization ----
+  {
+    EventTimer t;
+    int rc = factor_mixed(F, Ad, lda, nb);
+    if (rc) return rc;
+    r.factor_ms = t.stop();
+  }
+  int hst[3];
+  PLA_CUDA(cudaMemcpy(hst, F.status, sizeof hst, cudaMemcpyDeviceToHost));
+  if (hst[0] == PLA_K_TIMEOUT) PLA_FAIL("factorization: a bounded wait timed out");
+  r.info = kind == 0 ? hst[2] : (hst[0] == PLA_K_NOT_SPD ? hst[1] : 0);
+  if (kind == 1 && r.info) {
+    if (rep) *rep = r;
+    return r.info;  // not positive definite in low precision
+  }
+
+  // ---- refinement ----
+  EventTimer t;
+
+  {
+    int rc0 = prepare_solves(F);
+    if (rc0) return rc0;
+  }
+  Norms nm;
+  K(pla_k_residual(n, n, 1, Ad, lda, nullptr, n, nullptr, n, tmp, n, 1, work, stream()));
+  nm.a_inf = host_max(tmp, n);
+  K(pla_k_col_abs_max(MPI_DOUBLE, n, nrhs, Bd, ldb, tmp, stream()));
+  nm.b_inf.resize(nrhs);
+  PLA_CUDA(cudaMemcpy(nm.b_inf.data(), tmp, nrhs * sizeof(double), cudaMemcpyDeviceToHost));
+  // keep b, start from x = M^{-1} b
+  K(pla_k_copy(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, nrhs, Bd, ldb, Bsave, n, stream()));
+  int rc = precond(F, Bsave, n, X, n, nrhs, t32b);
+  if (rc) return rc;
+  std::vector<double> eta;
+  int it = 0;
+  for (;; it++) {
+    K(pla_k_residual(n, n, nrhs, Ad, lda, X, n, Bsave, n, R, n, 0, work, stream()));
+    rc = backward_errors(n, nrhs, R, n, X, n, nm, tmp, eta);
+    if (rc) return rc;
+    double worst = *std::max_element(eta.begin(), eta.end());
+    r.backward_error = worst;
+    if (worst <= tol || !(worst == worst)) break;
+    if (it >= p.max_iterations) break;
+    if (p.refinement == PLA_B200_IR_GMRES) {
+      for (int j = 0; j < nrhs; j++) {
+        rc = gmres(F, Ad, lda, R + (long)j * n, Dv + (long)j * n, p.gmres_restart, 1e-8, V, w,
+                   tmp, t32b, work, &r.inner_iterations);
+        if (rc) return rc;
+      }
+    } else {
+      rc = precond(F, R, n, Dv, n, nrhs, t32b);
+      if (rc) return rc;
+    }
+    K(pla_k_axpby(MPI_DOUBLE, n, nrhs, 1.0, Dv, n, 1.0, X, n, stream()));
+  }
+  r.iterations = it;
+  r.converged = r.backward_error <= tol;
+  K(pla_k_copy(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, nrhs, X, n, Bd, ldb, stream()));
+  r.refine_ms = t.stop();
+  PLA_CUDA(cudaStreamSynchronize(stream()));
+  if (rep) *rep = r;
+  return PLA_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" {
+
+void PLA_Mixed_params_default(PLA_Mixed_params *p) {
+  if (!p) return;
+  p->precision = PLA_B200_PREC_FP16;
+  p->refinement = PLA_B200_IR_GMRES;
+  p->max_iterations = 50;
+  p->gmres_restart = 30;
+  p->nb = 0;
+  p->tol = 0.0;
+}
+
+int PLA_General_solve_mixed(PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *params,
+                            PLA_Mixed_report *report) {
+  return solve_mixed(0, A, B, params, report);
+}
+
+int PLA_Pos_def_solve_mixed(PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *params,
+                            PLA_Mixed_report *report) {
+  return solve_mixed(1, A, B, params, report);
+}
+
+}  // extern "C"

@@ -136,6 +136,7 @@ int lu_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, Status 
         K(pla_k_gemm(dt, PLA_NO_TRANSPOSE, PLA_NO_TRANSPOSE, m - k - b, n - k - b, b, -1.0,
                      at(k + b, k), lda, at(k, k + b), lda, 1.0, at(k + b, k + b), lda, 0,
                      &st->status, stream()));
+        if (t.on) ph.update_launches++;
       }
     }
   }
@@ -164,14 +165,12 @@ int chol_device(int dt, int n, char *A, long lda, int nb, Status *st) {
       PhaseTimer t(&ph.update_ms);
       K(pla_k_gemm(dt, PLA_NO_TRANSPOSE, PLA_TRANSPOSE, rest, rest, b, -1.0, at(k + b, k), lda,
                    at(k + b, k), lda, 1.0, at(k + b, k + b), lda, 'L', &st->status, stream()));
+      if (t.on) ph.update_launches++;
     }
   }
   return 0;
 }
 
-void reset_phases() {
-  if (state().phase_timing) state().phases = PLA_Phase_times{};
-}
 
 // vector increment of a 1-row or 1-column view
 long vinc(PLA_Obj v) { return (v->length == 1 && v->width > 1) ? ld(v) : 1; }
@@ -237,7 +236,6 @@ int PLA_LU_info(PLA_Obj A, PLA_Obj pivots, int *info) {
   if (!valid(A) || !numeric(A)) PLA_FAIL("PLA_LU needs a float or double matrix");
   int nb;
   PLA_Environ_nb_alg(PLA_OP_PAN_PAN, A->templ, &nb);
-  reset_phases();
   int zi = 0;
   int r = lu_on_device(A->base->datatype, A->length, A->width, at(A, 0, 0), ld(A),
                        (int *)at(pivots, 0, 0), nb, &zi);
@@ -292,7 +290,6 @@ int PLA_Chol(int uplo, PLA_Obj A) {
   if (uplo != PLA_LOWER_TRIANGULAR) PLA_FAIL("Only lower triangular factorization supported");
   int nb;
   PLA_Environ_nb_alg(PLA_OP_PAN_PAN, A->templ, &nb);
-  reset_phases();
   int info = 0;
   int r = chol_on_device(A->base->datatype, A->length, at(A, 0, 0), ld(A), nb, &info);
   if (r) return r;
@@ -313,7 +310,6 @@ int PLA_Trsv(int uplo, int trans, int diag, PLA_Obj A, PLA_Obj x) {
   if (!numeric(A) || A->base->datatype != x->base->datatype) PLA_FAIL("datatype mismatch");
   if (A->length != A->width || vlen(x) != A->length) PLA_FAIL("nonconformal objects");
   if (vinc(x) != 1) PLA_FAIL("x must be a column vector");
-  reset_phases();
   PhaseTimer t(&state().phases.solve_ms);
   K(pla_k_trsv_blocked(A->base->datatype, uplo_c(uplo), trans_c(trans), diag_c(diag), A->length,
                        1, at(A, 0, 0), ld(A), at(x, 0, 0), ld(x), stream()));
@@ -330,7 +326,6 @@ int PLA_Trsm(int side, int uplo, int trans, int diag, PLA_Obj alpha, PLA_Obj A, 
   const int nt = side == PLA_SIDE_LEFT ? B->length : B->width;
   const int other = side == PLA_SIDE_LEFT ? B->width : B->length;
   if (A->length != nt || A->width != nt) PLA_FAIL("nonconformal objects");
-  reset_phases();
   PhaseTimer t(&state().phases.solve_ms);
   K(trsm_blocked(A->base->datatype, side == PLA_SIDE_LEFT ? 'L' : 'R', uplo_c(uplo),
                  trans_c(trans), diag_c(diag), nt, other, scalar_value(alpha), at(A, 0, 0), ld(A),
@@ -365,7 +360,6 @@ static int gemm_objs(int transa, int transb, PLA_Obj alpha, PLA_Obj A, PLA_Obj B
 
 int PLA_Gemm(int transa, int transb, PLA_Obj alpha, PLA_Obj A, PLA_Obj B, PLA_Obj beta,
              PLA_Obj C) {
-  reset_phases();
   return gemm_objs(transa, transb, alpha, A, B, beta, C, 0);
 }
 

@@ -48,7 +48,8 @@ _pi, _pobj = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_void_p)
 
 class PhaseTimes(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in
-                ("total_ms", "panel_ms", "swap_ms", "trsm_ms", "update_ms", "solve_ms", "refine_ms")]
+                ("total_ms", "panel_ms", "swap_ms", "trsm_ms", "update_ms", "solve_ms", "refine_ms",
+                 "convert_ms")] + [("update_launches", ctypes.c_int)]
 
 
 class MixedParams(ctypes.Structure):
@@ -113,13 +114,15 @@ _SIGS = {
     "PLA_Last_error": [ctypes.c_char_p, _i], "PLA_Clear_error": [],
     "PLA_B200_set_stream": [_vp], "PLA_B200_get_stream": [],
     "PLA_B200_phase_times": [ctypes.POINTER(PhaseTimes)], "PLA_B200_set_phase_timing": [_i],
+    "PLA_B200_reset_phase_times": [], "PLA_B200_kernel_launches": [],
     "PLA_Mixed_params_default": [ctypes.POINTER(MixedParams)],
     "PLA_General_solve_mixed": [Obj, Obj, ctypes.POINTER(MixedParams), ctypes.POINTER(MixedReport)],
     "PLA_Pos_def_solve_mixed": [Obj, Obj, ctypes.POINTER(MixedParams), ctypes.POINTER(MixedReport)],
     "PLA_Obj_set_local_contents_device": [_vp, _i, Obj],
     "PLA_Obj_get_local_contents_device": [Obj, _vp, _i],
 }
-_RESTYPE = {"PLA_B200_get_stream": _vp, "PLA_Mixed_params_default": None}
+_RESTYPE = {"PLA_B200_get_stream": _vp, "PLA_Mixed_params_default": None,
+            "PLA_B200_kernel_launches": ctypes.c_long}
 
 
 class PLAError(RuntimeError):

@@ -1,0 +1,218 @@
+"""Mixed-precision path on the B200, through the C ABI.
+
+ - the tensor-core trailing update (tcgen05, bf16/fp16 operands, fp32
+   accumulation, TMA reduce-add into fp32 C) against a plain PyTorch fp32
+   product of the same rounded operands;
+ - PLA_General_solve_mixed / PLA_Pos_def_solve_mixed reach FP64 backward
+   error (<= n * 2^-53) and agree with an FP64 LAPACK solve.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def env():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from plapack_b200 import pla
+    s = pla.Session(nb_distr=128, nb_alg=128)
+    yield s, torch, pla
+    s.close()
+
+
+def tc_update(lib, torch, prec, M, N, K, L, U, C, row0, col0, lower=0):
+    fn = lib.pla_k_tc_update
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_int] * 4 + [ctypes.c_float, ctypes.c_void_p, ctypes.c_long,
+                                        ctypes.c_long, ctypes.c_void_p, ctypes.c_long,
+                                        ctypes.c_long, ctypes.c_void_p, ctypes.c_long,
+                                        ctypes.c_long, ctypes.c_long, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    status = torch.zeros(4, dtype=torch.int32, device="cuda")
+    ldc, ccols = C.shape[1], C.shape[0]   # C stored as a transposed torch tensor (column-major)
+    rc = fn(prec, M, N, K, -1.0, L.data_ptr(), L.shape[1], L.shape[0], U.data_ptr(), U.shape[1],
+            U.shape[0], C.data_ptr(), ldc, ldc, ccols, row0, col0, lower, status.data_ptr(), None)
+    torch.cuda.synchronize()
+    assert rc == 0
+    assert status[0].item() == 0
+
+
+@pytest.mark.parametrize("prec,dt", [(1001, "bfloat16"), (1002, "float16")])
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (300, 257, 128), (1000, 777, 256), (64, 200, 192)])
+def test_tc_update_matches_fp32_product(env, prec, dt, M, N, K):
+    s, torch, pla = env
+    g = torch.Generator(device="cuda").manual_seed(M + N + K)
+    tdt = getattr(torch, dt)
+    rows, cols = M + 8, N + 12
+    L = torch.randn(M, K, device="cuda", generator=g).to(tdt).contiguous()
+    U = torch.randn(N, K, device="cuda", generator=g).to(tdt).contiguous()
+    ld = (rows + 31) // 32 * 32
+    Cc = torch.randn(cols, ld, device="cuda", generator=g)   # column-major rows x cols, ld
+    ref = Cc.clone()
+    r0, c0 = 4, 12
+    tc_update(s.lib, torch, prec, M, N, K, L, U, Cc, r0, c0)
+    prod = (L.float() @ U.float().T)          # M x N
+    ref[c0:c0 + N, r0:r0 + M] -= prod.T
+    err = (Cc - ref).abs().max().item()
+    assert err <= 1e-5 * K * max(1.0, prod.abs().max().item())
+    # everything outside the updated block is untouched
+    mask = torch.ones_like(Cc, dtype=torch.bool)
+    mask[c0:c0 + N, r0:r0 + M] = False
+    assert torch.equal(Cc[mask], ref[mask])
+
+
+def test_tc_update_lower_tiles(env):
+    s, torch, pla = env
+    M = N = 512
+    K = 128
+    g = torch.Generator(device="cuda").manual_seed(3)
+    L = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16).contiguous()
+    Cc = torch.zeros(N, M, device="cuda")
+    tc_update(s.lib, torch, 1001, M, N, K, L, L, Cc, 0, 0, lower=1)
+    full = -(L.float() @ L.float().T)
+    got = Cc.T
+    low = torch.tril(torch.ones(M, N, device="cuda", dtype=torch.bool))
+    assert (got[low] - full[low]).abs().max().item() <= 1e-4 * K
+
+
+@pytest.mark.parametrize("uplo,trans,diag", [("L", "N", "U"), ("U", "N", "N"), ("L", "N", "N"),
+                                             ("L", "T", "N")])
+@pytest.mark.parametrize("n", [1, 100, 128, 1000, 3001])
+def test_single_launch_trsv(env, uplo, trans, diag, n):
+    """Ticket-ordered single-kernel solve vs a plain FP64 PyTorch triangular solve."""
+    s, torch, pla = env
+    lib = s.lib
+    g = torch.Generator(device="cuda").manual_seed(n)
+    ld = (n + 31) // 32 * 32
+    M = torch.randn(n, ld, device="cuda", generator=g) * (0.5 / max(n, 1) ** 0.5)
+    M[:, :n] += 2.0 * torch.eye(n, device="cuda")   # well conditioned; memory: column-major A = M'
+    Acm = M[:, :n].t()                               # the column-major matrix A as a torch view
+    ldd = (n + 127) // 128 * 128
+    Dinv = torch.zeros(128, ldd, device="cuda")
+    b = torch.randn(n, device="cuda", generator=g)
+    x = b.clone()
+    status = torch.zeros(4, dtype=torch.int32, device="cuda")
+    c = ctypes.c_char
+    vp = ctypes.c_void_p
+    lib.pla_k_trsv_inv_blocks.argtypes = [ctypes.c_int, c, c, c, ctypes.c_int, vp, ctypes.c_long,
+                                          vp, ctypes.c_long, vp]
+    lib.pla_k_trsv_ticket.argtypes = [ctypes.c_int, c, c, ctypes.c_int, vp, ctypes.c_long, vp,
+                                      ctypes.c_long, vp, vp, vp, vp]
+    assert lib.pla_k_trsv_inv_blocks(pla.MPI_FLOAT, uplo.encode(), trans.encode(), diag.encode(),
+                                     n, M.data_ptr(), ld, Dinv.data_ptr(), ldd, None) == 0
+    assert lib.pla_k_trsv_ticket(pla.MPI_FLOAT, uplo.encode(), trans.encode(), n, M.data_ptr(),
+                                 ld, Dinv.data_ptr(), ldd, x.data_ptr(), x.data_ptr(),
+                                 status.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    assert status[0].item() == 0
+    T = torch.tril(Acm) if uplo == "L" else torch.triu(Acm)
+    if diag == "U":
+        T = T - torch.diag(torch.diag(T)) + torch.eye(n, device="cuda")
+    if trans == "T":
+        T = T.t()
+    ref = torch.linalg.solve_triangular(T.double(), b.double()[:, None],
+                                        upper=(uplo == "U") != (trans == "T"))[:, 0]
+    err = (x.double() - ref).abs().max().item()
+    assert err <= 1e-4 * max(1.0, ref.abs().max().item())
+
+
+def solve_mixed(s, pla, A, B, kind, prec, ref, nb=0):
+    n = A.shape[0]
+    a = s.matrix(n, n)
+    s.set(a, A)
+    b = s.matrix(*B.shape)
+    s.set(b, B)
+    p = pla.MixedParams()
+    s.lib.PLA_Mixed_params_default(ctypes.byref(p))
+    p.precision, p.refinement, p.nb = prec, ref, nb
+    rep = pla.MixedReport()
+    fn = s.lib.PLA_General_solve_mixed if kind == "lu" else s.lib.PLA_Pos_def_solve_mixed
+    rc = pla.check(fn(a, b, ctypes.byref(p), ctypes.byref(rep)), "solve_mixed")
+    X = s.get(b)
+    A_after = s.get(a)
+    s.free(a, b)
+    return rc, X, rep, A_after
+
+
+def backward_error(A, X, B):
+    R = B - A @ X
+    return (np.abs(R).max(axis=0) /
+            (np.abs(A).sum(axis=1).max() * np.abs(X).max(axis=0) + np.abs(B).max(axis=0))).max()
+
+
+@pytest.mark.parametrize("prec", [1, 2, 3])
+@pytest.mark.parametrize("ref", [1, 2])
+def test_general_solve_mixed(env, prec, ref):
+    """GMRES-IR on a Gaussian matrix (kappa ~ 1e4); classic LU-IR needs
+    kappa * u_factor < 1, so it gets a kappa = 10 matrix of the C3 family."""
+    s, torch, pla = env
+    n = 1536
+    rng = np.random.default_rng(prec * 10 + ref)
+    if ref == 2:
+        A = np.asfortranarray(rng.standard_normal((n, n)))
+    else:
+        A = c3_matrix(n, 10.0, prec)
+    B = np.asfortranarray(rng.standard_normal((n, 3)))
+    rc, X, rep, A_after = solve_mixed(s, pla, A, B, "lu", prec, ref)
+    assert rc == 0 and rep.converged == 1, (rep.iterations, rep.backward_error)
+    assert np.array_equal(A_after, A)              # A is read, never overwritten
+    eta = backward_error(A, X, B)
+    assert eta <= n * 2.0 ** -53
+    assert abs(eta - rep.backward_error) <= 0.5 * max(eta, rep.backward_error) + 1e-18
+    Xr = np.linalg.solve(A, B)
+    assert np.abs(X - Xr).max() <= 1e-10 * np.abs(Xr).max() * np.linalg.cond(A) ** 0.5
+
+
+def c3_matrix(n, kappa, seed):
+    """A = U diag(sigma) V' with sigma geometric 1 -> 1/kappa and U, V products of
+    8 Householder reflectors with seeded Gaussian vectors."""
+    rng = np.random.default_rng(seed)
+    sigma = kappa ** (-np.arange(n) / (n - 1))
+    A = np.diag(sigma)
+    for _ in range(8):
+        v = rng.standard_normal(n)
+        A -= (2.0 / (v @ v)) * np.outer(v, v @ A)
+    for _ in range(8):
+        v = rng.standard_normal(n)
+        A -= (2.0 / (v @ v)) * np.outer(A @ v, v)
+    return np.asfortranarray(A)
+
+
+@pytest.mark.parametrize("kappa", [1e2, 1e6])
+def test_gmres_ir_c3_family(env, kappa):
+    s, torch, pla = env
+    n = 2048
+    A = c3_matrix(n, kappa, 7)
+    x_true = np.random.default_rng(8).standard_normal((n, 1))
+    B = A @ x_true
+    rc, X, rep, _ = solve_mixed(s, pla, A, B, "lu", 2, 2)
+    assert rep.converged == 1, (rep.iterations, rep.backward_error)
+    assert backward_error(A, X, B) <= n * 2.0 ** -53
+
+
+@pytest.mark.parametrize("prec", [1, 2])
+def test_pos_def_solve_mixed(env, prec):
+    s, torch, pla = env
+    n = 1280
+    rng = np.random.default_rng(prec)
+    G = rng.standard_normal((n, n))
+    A = np.asfortranarray(G @ G.T / n + np.eye(n))
+    B = np.asfortranarray(rng.standard_normal((n, 2)))
+    rc, X, rep, _ = solve_mixed(s, pla, A, B, "chol", prec, 2)
+    assert rc == 0 and rep.converged == 1, (rep.iterations, rep.backward_error)
+    assert backward_error(A, X, B) <= n * 2.0 ** -53
+
+
+def test_pos_def_mixed_reports_not_spd(env):
+    s, torch, pla = env
+    n = 256
+    A = np.asfortranarray(np.eye(n))
+    A[100, 100] = -1.0
+    B = np.ones((n, 1), order="F")
+    rc, X, rep, _ = solve_mixed(s, pla, A, B, "chol", 2, 1)
+    assert rc == 101 and rep.info == 101
