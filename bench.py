@@ -337,6 +337,7 @@ def run_ours(args):
     # ---- FP64 LU arm (PLA_General_solve), restoring A every step ----
     fp64_s = None
     fp64_eta = None
+    fp64_detail = None
     if not args.skip_fp64:
         s.set_nb_alg(args.nb_fp64)
         piv = s.mvector(n, 1, np.int32)
@@ -348,6 +349,8 @@ def run_ours(args):
 
         for _ in range(args.warmup):
             fp64_step()
+        lib.PLA_B200_set_phase_timing(1)
+        lib.PLA_B200_reset_phase_times()
         barrier()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         f0.record(stream)
@@ -356,6 +359,16 @@ def run_ours(args):
         f1.record(stream)
         barrier()
         fp64_s = max_over_ranks(f0.elapsed_time(f1) / 1e3 / args.steps)
+        ph64 = pla.PhaseTimes()
+        lib.PLA_B200_phase_times(ctypes.byref(ph64))
+        lib.PLA_B200_set_phase_timing(0)
+        nbf = args.nb_fp64
+        gemm_flops = sum(2.0 * (n - k - nbf) ** 2 * nbf for k in range(0, n, nbf) if n - k - nbf > 0)
+        fp64_detail = {k: getattr(ph64, k) / args.steps for k in
+                       ("panel_ms", "swap_ms", "trsm_ms", "update_ms", "solve_ms")}
+        fp64_detail["dgemm_tflops"] = (gemm_flops * args.steps / (ph64.update_ms / 1e3) / 1e12
+                                       if ph64.update_ms > 0 else None)
+        fp64_detail["lu_tflops_effective"] = (2.0 / 3.0 * n ** 3) / fp64_s / 1e12
         check(lib.PLA_Obj_get_local_contents_device(bo, ctypes.c_void_p(x.data_ptr()), n), "x")
         r = b - T.t() @ x
         fp64_eta = (r.abs().max() / (a_inf * x.abs().max() + b.abs().max())).item()
@@ -417,7 +430,7 @@ def run_ours(args):
                           "refinement": args.refinement, "nb": args.nb, "nb_fp64": args.nb_fp64,
                           "l2": "inputs larger than L2 (8.6 GB FP64 matrix)",
                           "parallelism": f"replicas x{world}"},
-               "fp64_lu_solve_s": fp64_s,
+               "fp64_lu_solve_s": fp64_s, "fp64_phase_ms_per_step": fp64_detail,
                "speedup_vs_fp64": (fp64_s / mixed_s) if fp64_s else None,
                "backward_error": eta, "backward_error_fp64": fp64_eta,
                "backward_error_target": n * 2.0 ** -53, "forward_error": fwd,

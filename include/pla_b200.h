@@ -95,6 +95,38 @@ int PLA_General_solve_mixed(PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *params
 int PLA_Pos_def_solve_mixed(PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *params,
                             PLA_Mixed_report *report);
 
+/* ---- batched factor-and-solve ------------------------------------------------
+ * Many independent systems of uneven order, each factored in place (LU with
+ * partial pivoting, or lower Cholesky) and solved for its right-hand sides, in
+ * ONE persistent kernel launch replayed from a CUDA graph.  All pointers are
+ * device pointers; A is n x n and B n x nrhs, column-major with leading
+ * dimension n.  info (device, one int per instance) receives 0, the first
+ * exact zero pivot (LU) or the failing column (Cholesky), 1-based. */
+typedef struct {
+  int n;
+  int nrhs;
+  int kind;       /* 0 = LU with partial pivoting, 1 = Cholesky (lower) */
+  void *A;
+  void *B;
+  int *pivots;    /* LU only: n offsets in the reference's encoding */
+} PLA_Batch_instance;
+
+typedef struct PLA_Batch_plan_struct *PLA_Batch_plan;
+/* Sort and bucket the instances, optionally autotune the schedule on a
+ * synthetic sample of the same sizes, upload the descriptors and capture the
+ * launch in a CUDA graph.  The instances' buffers must stay valid. */
+int PLA_Batch_plan_create(MPI_Datatype datatype, int count, const PLA_Batch_instance *instances,
+                          int *info, int autotune, PLA_Batch_plan *plan);
+int PLA_Batch_plan_execute(PLA_Batch_plan plan);
+int PLA_Batch_plan_free(PLA_Batch_plan *plan);
+/* create + execute + free, without autotuning */
+int PLA_Batched_factor_solve(MPI_Datatype datatype, int count,
+                             const PLA_Batch_instance *instances, int *info);
+/* the same work as a loop of per-instance launches of the single-matrix
+ * kernels (the baseline the batched launch is measured against) */
+int PLA_Batched_factor_solve_loop(MPI_Datatype datatype, int count,
+                                  const PLA_Batch_instance *instances);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,367 @@
+// Batched factor-and-solve: thousands of independent LU (partial pivoting)
+// and Cholesky systems of uneven order in ONE persistent launch.
+//
+// The host sorts the instances by decreasing order and cuts them into tasks:
+//   mode 0 ("warp")   : up to 8 instances with n <= 32, one warp each, the
+//                       matrix in shared memory, warp-synchronous;
+//   mode 1 ("smem")   : one instance per CTA, matrix and right-hand sides in
+//                       shared memory;
+//   mode 2 ("global") : one instance per CTA working in place in global memory
+//                       (an instance of order <= 512 stays resident in L2).
+// CTAs pull tasks from an atomic queue, largest first, so the long instances
+// start early and the short ones fill the tail.  Each instance runs the same
+// column algorithms as the reference's sequential kernels: LU as PLA_dlu
+// (SOLVERS/LU/PLA_seq_lu.c:21-46: first-index argmax, full-row swap,
+// reciprocal scaling, rank-1 update), Cholesky right-looking with the
+// reciprocal scaling of PLA_dchol (SOLVERS/Cholesky/PLA_Local_chol.c:124-137),
+// then the forward and backward substitutions.  Status per instance is a
+// LAPACK-style info: LU the first exact zero pivot, Cholesky the failing
+// column (1-based), 0 otherwise.
+#include <climits>
+
+#include "PLA.h"
+#include "pla_kernels.h"
+
+namespace {
+
+constexpr int THREADS = 256;
+
+template <typename T>
+struct Inst {
+  int n, nrhs, kind, pad;
+  T *A;
+  T *B;
+  int *piv;
+};
+
+struct Task {
+  int first, count, mode, pad;
+};
+
+// ---------------------------------------------------------------- warp ----
+template <typename T>
+__device__ void warp_instance(const Inst<T> &in, T *S, int *info) {
+  const int lane = threadIdx.x & 31, n = in.n, ld = 33;
+  T *Bs = S + 32 * ld;  // 32 x 4 right-hand sides, ld 33
+  for (int c = 0; c < n; c++)
+    if (lane < n) S[lane + c * ld] = in.A[lane + (long)c * n];
+  for (int r = 0; r < in.nrhs; r++)
+    if (lane < n) Bs[lane + r * ld] = in.B[lane + (long)r * n];
+  __syncwarp();
+  int bad = 0;
+  if (in.kind == 0) {
+    for (int j = 0; j < n; j++) {
+      T v = (lane >= j && lane < n) ? fabs(S[lane + j * ld]) : T(-1);
+      int idx = lane >= j && lane < n ? lane : INT_MAX;
+      for (int o = 16; o; o >>= 1) {
+        T ov = __shfl_down_sync(0xffffffffu, v, o);
+        int oi = __shfl_down_sync(0xffffffffu, idx, o);
+        if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
+      }
+      const int p = __shfl_sync(0xffffffffu, idx, 0);
+      if (lane == 0) in.piv[j] = p - j;
+      if (p != j && lane < n) {
+        T a = S[j + lane * ld];
+        S[j + lane * ld] = S[p + lane * ld];
+        S[p + lane * ld] = a;
+      }
+      __syncwarp();
+      const T piv = S[j + j * ld];
+      if (piv == T(0) && !bad) bad = j + 1;
+      const T inv = T(1) / piv;
+      if (lane > j && lane < n) {
+        const T l = S[lane + j * ld] * inv;
+        S[lane + j * ld] = l;
+        for (int c = j + 1; c < n; c++) S[lane + c * ld] = fma(l, -S[j + c * ld], S[lane + c * ld]);
+      }
+      __syncwarp();
+    }
+    // P b, then L (unit) and U solves
+    for (int r = 0; r < in.nrhs; r++) {
+      if (lane == 0)
+        for (int j = 0; j < n; j++) {
+          int p = j + in.piv[j];
+          if (p != j) {
+            T a = Bs[j + r * ld];
+            Bs[j + r * ld] = Bs[p + r * ld];
+            Bs[p + r * ld] = a;
+          }
+        }
+      __syncwarp();
+      for (int j = 0; j < n; j++) {
+        const T x = Bs[j + r * ld];
+        if (lane > j && lane < n) Bs[lane + r * ld] -= S[lane + j * ld] * x;
+        __syncwarp();
+      }
+      for (int j = n - 1; j >= 0; j--) {
+        if (lane == 0) Bs[j + r * ld] = Bs[j + r * ld] / S[j + j * ld];
+        __syncwarp();
+        const T x = Bs[j + r * ld];
+        if (lane < j) Bs[lane + r * ld] -= S[lane + j * ld] * x;
+        __syncwarp();
+      }
+    }
+  } else {
+    for (int j = 0; j < n; j++) {
+      const T d = S[j + j * ld];
+      if (d <= T(0)) {
+        bad = j + 1;
+        break;
+      }
+      const T s = sqrt(d);
+      const T inv = T(1) / s;
+      __syncwarp();
+      if (lane == j) S[j + j * ld] = s;
+      if (lane > j && lane < n) S[lane + j * ld] *= inv;
+      __syncwarp();
+      if (lane > j && lane < n) {
+        const T l = S[lane + j * ld];
+        for (int c = j + 1; c <= lane; c++) S[lane + c * ld] = fma(-l, S[c + j * ld], S[lane + c * ld]);
+      }
+      __syncwarp();
+    }
+    if (!bad)
+      for (int r = 0; r < in.nrhs; r++) {
+        for (int j = 0; j < n; j++) {
+          if (lane == 0) Bs[j + r * ld] = Bs[j + r * ld] / S[j + j * ld];
+          __syncwarp();
+          const T x = Bs[j + r * ld];
+          if (lane > j && lane < n) Bs[lane + r * ld] -= S[lane + j * ld] * x;
+          __syncwarp();
+        }
+        for (int j = n - 1; j >= 0; j--) {
+          if (lane == 0) Bs[j + r * ld] = Bs[j + r * ld] / S[j + j * ld];
+          __syncwarp();
+          const T x = Bs[j + r * ld];
+          if (lane < j) Bs[lane + r * ld] -= S[j + lane * ld] * x;  // L' column = L row
+          __syncwarp();
+        }
+      }
+  }
+  __syncwarp();
+  for (int c = 0; c < n; c++)
+    if (lane < n && (in.kind == 0 || lane >= c)) in.A[lane + (long)c * n] = S[lane + c * ld];
+  if (!(in.kind == 1 && bad))
+    for (int r = 0; r < in.nrhs; r++)
+      if (lane < n) in.B[lane + (long)r * n] = Bs[lane + r * ld];
+  if (lane == 0) *info = bad;
+}
+
+// ----------------------------------------------------------------- CTA ----
+template <typename T>
+__device__ void block_argmax(T &v, int &i, T *sv, int *si) {
+  for (int o = 16; o; o >>= 1) {
+    T ov = __shfl_down_sync(0xffffffffu, v, o);
+    int oi = __shfl_down_sync(0xffffffffu, i, o);
+    if (ov > v || (ov == v && oi < i)) { v = ov; i = oi; }
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { sv[w] = v; si[w] = i; }
+  __syncthreads();
+  if (w == 0) {
+    v = l < THREADS / 32 ? sv[l] : T(-1);
+    i = l < THREADS / 32 ? si[l] : INT_MAX;
+    for (int o = 16; o; o >>= 1) {
+      T ov = __shfl_down_sync(0xffffffffu, v, o);
+      int oi = __shfl_down_sync(0xffffffffu, i, o);
+      if (ov > v || (ov == v && oi < i)) { v = ov; i = oi; }
+    }
+    if (l == 0) { sv[0] = v; si[0] = i; }
+  }
+  __syncthreads();
+  v = sv[0];
+  i = si[0];
+  __syncthreads();
+}
+
+// the instance's matrix at M (ld lm) and right-hand sides at X (ld lx):
+// shared memory in mode 1, the instance's own global buffers in mode 2
+template <typename T>
+__device__ void cta_instance(const Inst<T> &in, T *M, long lm, T *X, long lx, int *info) {
+  __shared__ T sv[32];
+  __shared__ int si[32];
+  __shared__ int s_bad;
+  const int n = in.n, tid = threadIdx.x;
+  if (tid == 0) s_bad = 0;
+  __syncthreads();
+  if (in.kind == 0) {
+    for (int j = 0; j < n; j++) {
+      T v = T(-1);
+      int idx = INT_MAX;
+      for (int i = j + tid; i < n; i += THREADS) {
+        T a = fabs(M[i + j * lm]);
+        if (a > v) { v = a; idx = i; }
+      }
+      block_argmax(v, idx, sv, si);
+      const int p = idx;
+      if (tid == 0) in.piv[j] = p - j;
+      if (p != j)
+        for (int c = tid; c < n; c += THREADS) {
+          T a = M[j + c * lm];
+          M[j + c * lm] = M[p + c * lm];
+          M[p + c * lm] = a;
+        }
+      __syncthreads();
+      const T piv = M[j + j * lm];
+      if (tid == 0 && piv == T(0) && !s_bad) s_bad = j + 1;
+      const T inv = T(1) / piv;
+      for (int i = j + 1 + tid; i < n; i += THREADS) M[i + j * lm] *= inv;
+      __syncthreads();
+      const int rows = n - j - 1;
+      const long tot = (long)rows * rows;
+      for (long e = tid; e < tot; e += THREADS) {
+        const int i = j + 1 + (int)(e % rows), c = j + 1 + (int)(e / rows);
+        M[i + c * lm] = fma(M[i + j * lm], -M[j + c * lm], M[i + c * lm]);
+      }
+      __syncthreads();
+    }
+    for (int r = tid; r < in.nrhs; r += THREADS)
+      for (int j = 0; j < n; j++) {
+        int p = j + in.piv[j];
+        if (p != j) {
+          T a = X[j + r * lx];
+          X[j + r * lx] = X[p + r * lx];
+          X[p + r * lx] = a;
+        }
+      }
+    __syncthreads();
+    for (int j = 0; j < n; j++) {
+      for (long e = tid; e < (long)(n - j - 1) * in.nrhs; e += THREADS) {
+        const int i = j + 1 + (int)(e % (n - j - 1)), r = (int)(e / (n - j - 1));
+        X[i + r * lx] -= M[i + j * lm] * X[j + r * lx];
+      }
+      __syncthreads();
+    }
+    for (int j = n - 1; j >= 0; j--) {
+      if (tid < in.nrhs) X[j + tid * lx] = X[j + tid * lx] / M[j + j * lm];
+      __syncthreads();
+      for (long e = tid; e < (long)j * in.nrhs; e += THREADS) {
+        const int i = (int)(e % j), r = (int)(e / j);
+        X[i + r * lx] -= M[i + j * lm] * X[j + r * lx];
+      }
+      __syncthreads();
+    }
+  } else {
+    for (int j = 0; j < n; j++) {
+      const T d = M[j + j * lm];
+      if (d <= T(0)) {
+        if (tid == 0) s_bad = j + 1;
+        break;
+      }
+      const T s = sqrt(d), inv = T(1) / s;
+      __syncthreads();
+      if (tid == 0) M[j + j * lm] = s;
+      for (int i = j + 1 + tid; i < n; i += THREADS) M[i + j * lm] *= inv;
+      __syncthreads();
+      const int rows = n - j - 1;
+      const long tot = (long)rows * rows;
+      for (long e = tid; e < tot; e += THREADS) {
+        const int i = j + 1 + (int)(e % rows), c = j + 1 + (int)(e / rows);
+        if (i >= c) M[i + c * lm] = fma(-M[i + j * lm], M[c + j * lm], M[i + c * lm]);
+      }
+      __syncthreads();
+    }
+    __syncthreads();
+    if (!s_bad) {
+      for (int j = 0; j < n; j++) {
+        if (tid < in.nrhs) X[j + tid * lx] = X[j + tid * lx] / M[j + j * lm];
+        __syncthreads();
+        for (long e = tid; e < (long)(n - j - 1) * in.nrhs; e += THREADS) {
+          const int i = j + 1 + (int)(e % (n - j - 1)), r = (int)(e / (n - j - 1));
+          X[i + r * lx] -= M[i + j * lm] * X[j + r * lx];
+        }
+        __syncthreads();
+      }
+      for (int j = n - 1; j >= 0; j--) {
+        if (tid < in.nrhs) X[j + tid * lx] = X[j + tid * lx] / M[j + j * lm];
+        __syncthreads();
+        for (long e = tid; e < (long)j * in.nrhs; e += THREADS) {
+          const int i = (int)(e % j), r = (int)(e / j);
+          X[i + r * lx] -= M[j + i * lm] * X[j + r * lx];
+        }
+        __syncthreads();
+      }
+    }
+  }
+  __syncthreads();
+  if (tid == 0) *info = s_bad;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(THREADS)
+batched_k(const Inst<T> *inst, const int *order, const Task *tasks, int ntasks, int *queue,
+          int *info) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *S = (T *)smem_raw;
+  __shared__ int s_task;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_task = atomicAdd(queue, 1);
+    __syncthreads();
+    const int t = s_task;
+    if (t >= ntasks) return;
+    const Task tk = tasks[t];
+    if (tk.mode == 0) {
+      const int w = threadIdx.x >> 5;
+      if (w < tk.count) {
+        const int id = order[tk.first + w];
+        warp_instance(inst[id], S + (long)w * (32 * 33 + 32 * 33), &info[id]);
+      }
+    } else {
+      const int id = order[tk.first];
+      const Inst<T> in = inst[id];
+      if (tk.mode == 1) {
+        const int n = in.n;
+        const long lm = n + 1, lx = n + 1;
+        T *M = S, *X = S + lm * n;
+        for (long e = threadIdx.x; e < (long)n * n; e += THREADS)
+          M[(e % n) + (e / n) * lm] = in.A[e];
+        for (long e = threadIdx.x; e < (long)n * in.nrhs; e += THREADS)
+          X[(e % n) + (e / n) * lx] = in.B[e];
+        __syncthreads();
+        cta_instance(in, M, lm, X, lx, &info[id]);
+        __syncthreads();
+        const bool keep_b = !(in.kind == 1 && info[id]);
+        for (long e = threadIdx.x; e < (long)n * n; e += THREADS) {
+          const int i = (int)(e % n), c = (int)(e / n);
+          if (in.kind == 0 || i >= c) in.A[e] = M[i + c * lm];
+        }
+        if (keep_b)
+          for (long e = threadIdx.x; e < (long)n * in.nrhs; e += THREADS)
+            in.B[e] = X[(e % n) + (e / n) * lx];
+      } else {
+        cta_instance(in, in.A, in.n, in.B, in.n, &info[id]);
+      }
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" size_t pla_k_batched_smem(int dt, int n_smem_max) {
+  const size_t es = dt == MPI_DOUBLE ? 8 : 4;
+  size_t warp = (size_t)8 * 2 * 32 * 33 * es;
+  size_t cta = ((size_t)(n_smem_max + 1) * n_smem_max + (size_t)(n_smem_max + 1) * 4) * es;
+  return warp > cta ? warp : cta;
+}
+
+// inst: device array of {n, nrhs, kind, pad, A, B, piv}; order: instance ids
+// by task; tasks: device {first, count, mode}; queue: zeroed int.
+extern "C" int pla_k_batched(int dt, const void *inst, const int *order, const void *tasks,
+                             int ntasks, int *queue, int *info, int grid, size_t smem,
+                             cudaStream_t s) {
+  if (ntasks <= 0) return 0;
+  if (dt == MPI_DOUBLE) {
+    cudaFuncSetAttribute(batched_k<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    batched_k<double><<<grid, THREADS, smem, s>>>((const Inst<double> *)inst, order,
+                                                  (const Task *)tasks, ntasks, queue, info);
+  } else if (dt == MPI_FLOAT) {
+    cudaFuncSetAttribute(batched_k<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    batched_k<float><<<grid, THREADS, smem, s>>>((const Inst<float> *)inst, order,
+                                                 (const Task *)tasks, ntasks, queue, info);
+  } else {
+    return (int)cudaErrorInvalidValue;
+  }
+  pla_k_count(1);
+  return (int)cudaGetLastError();
+}

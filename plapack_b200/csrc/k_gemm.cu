@@ -5,9 +5,10 @@
 // FP64: tensor-core DMMA (mma.sync m16n8k8 .f64; tcgen05 has no f64 kind).
 //   CTA tile 128 x 64, k-step 16, 8 warps as 4 (M) x 2 (N) with a 32 x 32
 //   warp tile; three cp.async stages; two CTAs per SM so one CTA's epilogue
-//   (the read-modify-write of C) overlaps the other's main loop.  Shared
-//   memory is padded so every f64 fragment load is bank-conflict free:
-//   A stage [16][128+4], B stage [64][16+4].
+//   (the read-modify-write of C) overlaps the other's main loop.  The stages
+//   are stored permuted (rows g and g+8, k and k+4 side by side) so that
+//   each thread's fragment pairs are single 16-byte loads, and padded so
+//   those loads are bank-conflict free: A stage [16][128+4], B stage [64][16+8].
 // FP32: the same tiling with SIMT FFMA (used for float objects).
 #include <cstdint>
 
@@ -18,7 +19,7 @@ namespace {
 
 constexpr int BM = 128, BN = 64, BK = 16, STAGES = 3, THREADS = 256;
 constexpr int LDA_S = BM + 4;  // doubles per k-row of the A stage
-constexpr int LDB_S = BK + 4;  // doubles per n-row of the B stage
+constexpr int LDB_S = BK + 8;  // per n-row of the B stage (16-byte loads conflict free)
 
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool valid) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -42,8 +43,21 @@ __device__ __forceinline__ void cp_async_elem(T *smem, const T *gmem, bool valid
   else cp_async4(smem, gmem, valid);
 }
 
+// Positions inside a stage.  With PERM (the FP64 tensor-core kernel) rows g
+// and g + 8 of every 16-row group are stored next to each other, and so are k
+// and k + 4 of every 8-wide k group, so that each pair of f64 fragment
+// elements the m16n8k8 MMA wants from one thread is one 16-byte load.
+template <bool PERM>
+__device__ __forceinline__ int pos_m(int row) {
+  return PERM ? (row & ~15) | ((row & 7) << 1) | ((row >> 3) & 1) : row;
+}
+template <bool PERM>
+__device__ __forceinline__ int pos_k(int kk) {
+  return PERM ? (kk & ~7) | ((kk & 3) << 1) | ((kk >> 2) & 1) : kk;
+}
+
 // Stage one k-slab of op(A) (BM x BK) and op(B) (BK x BN) into shared memory.
-template <typename T, bool TA, bool TB>
+template <typename T, bool TA, bool TB, bool PERM = false>
 __device__ __forceinline__ void load_stage(T *As, T *Bs, const T *A, long lda, const T *B,
                                            long ldb, int m, int n, int k, int m0, int n0,
                                            int k0, int tid) {
@@ -57,7 +71,7 @@ __device__ __forceinline__ void load_stage(T *As, T *Bs, const T *A, long lda, c
     int gi = m0 + row, gk = k0 + kk;
     bool ok = gi < m && gk < k;
     const T *src = ok ? (TA ? A + gk + (long)gi * lda : A + gi + (long)gk * lda) : A;
-    cp_async_elem(As + kk * LDA_S + row, src, ok);
+    cp_async_elem(As + kk * LDA_S + pos_m<PERM>(row), src, ok);
   }
   // B: element (kk, col) of op(B) -> Bs[col * LDB_S + kk]
 #pragma unroll
@@ -69,7 +83,7 @@ __device__ __forceinline__ void load_stage(T *As, T *Bs, const T *A, long lda, c
     int gj = n0 + col, gk = k0 + kk;
     bool ok = gj < n && gk < k;
     const T *src = ok ? (TB ? B + gj + (long)gk * ldb : B + gk + (long)gj * ldb) : B;
-    cp_async_elem(Bs + col * LDB_S + kk, src, ok);
+    cp_async_elem(Bs + col * LDB_S + pos_k<PERM>(kk), src, ok);
   }
 }
 
@@ -115,8 +129,8 @@ dgemm_k(int m, int n, int k, double alpha, const double *__restrict__ A, long ld
 #pragma unroll
   for (int s = 0; s < STAGES - 1; s++) {
     if (s < nk)
-      load_stage<double, TA, TB>(As + s * BK * LDA_S, Bs + s * BN * LDB_S, A, lda, B, ldb, m, n,
-                                 k, m0, n0, s * BK, tid);
+      load_stage<double, TA, TB, true>(As + s * BK * LDA_S, Bs + s * BN * LDB_S, A, lda, B, ldb,
+                                       m, n, k, m0, n0, s * BK, tid);
     cp_commit();
   }
   for (int kt = 0; kt < nk; kt++) {
@@ -126,8 +140,8 @@ dgemm_k(int m, int n, int k, double alpha, const double *__restrict__ A, long ld
       int ks = kt + STAGES - 1;
       if (ks < nk) {
         int slot = ks % STAGES;
-        load_stage<double, TA, TB>(As + slot * BK * LDA_S, Bs + slot * BN * LDB_S, A, lda, B,
-                                   ldb, m, n, k, m0, n0, ks * BK, tid);
+        load_stage<double, TA, TB, true>(As + slot * BK * LDA_S, Bs + slot * BN * LDB_S, A, lda,
+                                         B, ldb, m, n, k, m0, n0, ks * BK, tid);
       }
       cp_commit();
     }
@@ -136,19 +150,24 @@ dgemm_k(int m, int n, int k, double alpha, const double *__restrict__ A, long ld
 #pragma unroll
     for (int kk = 0; kk < BK; kk += 8) {
       double af[2][4], bf[4][2];
+      // (a0, a1) = rows g, g+8 at k = kk+t; (a2, a3) the same rows at kk+t+4;
+      // (b0, b1) = k = kk+t, kk+t+4 of column g: one 16-byte load each
 #pragma unroll
       for (int i = 0; i < 2; i++) {
-        const int r = wm + i * 16 + g;
-        af[i][0] = as[(kk + t) * LDA_S + r];
-        af[i][1] = as[(kk + t) * LDA_S + r + 8];
-        af[i][2] = as[(kk + t + 4) * LDA_S + r];
-        af[i][3] = as[(kk + t + 4) * LDA_S + r + 8];
+        const int r = wm + i * 16 + 2 * g;
+        const double2 lo = *reinterpret_cast<const double2 *>(&as[(kk + t) * LDA_S + r]);
+        const double2 hi = *reinterpret_cast<const double2 *>(&as[(kk + t + 4) * LDA_S + r]);
+        af[i][0] = lo.x;
+        af[i][1] = lo.y;
+        af[i][2] = hi.x;
+        af[i][3] = hi.y;
       }
 #pragma unroll
       for (int j = 0; j < 4; j++) {
         const int c = wn + j * 8 + g;
-        bf[j][0] = bs[c * LDB_S + kk + t];
-        bf[j][1] = bs[c * LDB_S + kk + t + 4];
+        const double2 bb = *reinterpret_cast<const double2 *>(&bs[c * LDB_S + kk + 2 * t]);
+        bf[j][0] = bb.x;
+        bf[j][1] = bb.y;
       }
 #pragma unroll
       for (int i = 0; i < 2; i++)

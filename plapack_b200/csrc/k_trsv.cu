@@ -12,6 +12,8 @@
 //                      flag i.  The triangle is read exactly once, so the solve
 //                      is HBM-bound apart from the per-block latency chain.
 //                      b and x may be the same array.
+#include <cstdint>
+
 #include "PLA.h"
 #include "pla_kernels.h"
 
@@ -76,7 +78,7 @@ __device__ __forceinline__ void st_release(int *p, int v) {
 template <typename T>
 __global__ void __launch_bounds__(THREADS)
 trsv_ticket_k(int n, int nblk, const T *A, long lda, bool lower_op, bool trans, const T *Dinv,
-              long ldd, const T *b, T *x, int *ticket, int *flags, int *status) {
+              long ldd, const T *b, T *x, int *ticket, int *flags, int *status, bool vec_ok) {
   __shared__ T xs[TB];
   __shared__ T part[2][TB];
   __shared__ int s_blk, s_bad;
@@ -92,6 +94,14 @@ trsv_ticket_k(int n, int nblk, const T *A, long lda, bool lower_op, bool trans, 
     const int i = lower_op ? q : nblk - 1 - q;
     const long r0 = (long)i * TB;
     const int nbi = min(TB, n - (int)r0);
+    // Each full 128 x 128 tile is read with 16 independent 16-byte loads per
+    // thread (64 KB in flight per CTA).  No transpose: thread (rg, cg) owns
+    // rows 4rg..4rg+3 and columns 16cg..16cg+15, so a warp reads 512
+    // contiguous bytes of a column.  Transpose: op(A)(r, c) = A(c, r), thread
+    // (r, half) reads 64 contiguous values of column r of A.  Ragged edge
+    // tiles take a scalar path.
+    const int rg = threadIdx.x & 31, cg = threadIdx.x >> 5;
+    T acc4[4] = {T(0), T(0), T(0), T(0)};
     T acc = T(0);
     for (int s = 0; s < q; s++) {
       const int j = lower_op ? s : nblk - 1 - s;
@@ -112,12 +122,34 @@ trsv_ticket_k(int n, int nblk, const T *A, long lda, bool lower_op, bool trans, 
       if (s_bad) return;
       if (threadIdx.x < nbj) xs[threadIdx.x] = __ldcg(&x[c0 + threadIdx.x]);
       __syncthreads();
-      if (r < nbi) {
+      const bool full = nbi == TB && nbj == TB && vec_ok;
+      if (full && !trans) {
+        float4 v[16];
+        const T *base = A + (r0 + 4 * rg) + (c0 + 16 * cg) * lda;
+#pragma unroll
+        for (int u = 0; u < 16; u++) v[u] = *reinterpret_cast<const float4 *>(base + u * lda);
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+          const T xv = xs[16 * cg + u];
+          acc4[0] += v[u].x * xv;
+          acc4[1] += v[u].y * xv;
+          acc4[2] += v[u].z * xv;
+          acc4[3] += v[u].w * xv;
+        }
+      } else if (full) {
+        float4 v[16];
+        const T *base = A + (r0 + r) * lda + c0 + 64 * half;
+#pragma unroll
+        for (int u = 0; u < 16; u++) v[u] = *reinterpret_cast<const float4 *>(base + 4 * u);
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+          const int c = 64 * half + 4 * u;
+          acc += v[u].x * xs[c] + v[u].y * xs[c + 1] + v[u].z * xs[c + 2] + v[u].w * xs[c + 3];
+        }
+      } else if (r < nbi) {
         if (!trans) {
-          // warps read down the columns of A: coalesced
           for (int c = half; c < nbj; c += 2) acc += A[(r0 + r) + (c0 + c) * lda] * xs[c];
         } else {
-          // op(A)(r, c) = A(c, r): each thread walks a contiguous stretch of column r
           const int cb = half * (TB / 2), ce = min(cb + TB / 2, nbj);
           const T *col = A + (r0 + r) * lda + c0;
           for (int c = cb; c < ce; c++) acc += col[c] * xs[c];
@@ -125,16 +157,45 @@ trsv_ticket_k(int n, int nblk, const T *A, long lda, bool lower_op, bool trans, 
       }
       __syncthreads();
     }
+    // reduce: acc4 from the 8 column groups (no-transpose full tiles) plus acc
+    // from the two halves (transpose or ragged tiles)
+    __shared__ T red[8][TB];
+#pragma unroll
+    for (int e = 0; e < 4; e++) red[cg][4 * rg + e] = acc4[e];
     part[half][r] = acc;
     __syncthreads();
-    if (threadIdx.x < TB) xs[threadIdx.x] = r < nbi ? b[r0 + r] - (part[0][r] + part[1][r]) : T(0);
+    if (threadIdx.x < TB) {
+      T sacc = part[0][r] + part[1][r];
+#pragma unroll
+      for (int g = 0; g < 8; g++) sacc += red[g][r];
+      xs[threadIdx.x] = r < nbi ? b[r0 + r] - sacc : T(0);
+    }
     __syncthreads();
-    // x_i = inv(D_i) y
-    T y = T(0);
-    for (int c = half; c < TB; c += 2) y += Dinv[(r0 + r) + (long)c * ldd] * xs[c];
-    part[half][r] = y;
+    // x_i = inv(D_i) y, the same 16-loads-per-thread pattern over Dinv
+    {
+      float4 v[16];
+      const T *base = Dinv + (r0 + 4 * rg) + (long)(16 * cg) * ldd;
+#pragma unroll
+      for (int u = 0; u < 16; u++) v[u] = *reinterpret_cast<const float4 *>(base + u * ldd);
+      T y4[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll
+      for (int u = 0; u < 16; u++) {
+        const T xv = xs[16 * cg + u];
+        y4[0] += v[u].x * xv;
+        y4[1] += v[u].y * xv;
+        y4[2] += v[u].z * xv;
+        y4[3] += v[u].w * xv;
+      }
+#pragma unroll
+      for (int e = 0; e < 4; e++) red[cg][4 * rg + e] = y4[e];
+    }
     __syncthreads();
-    if (threadIdx.x < nbi) x[r0 + threadIdx.x] = part[0][threadIdx.x] + part[1][threadIdx.x];
+    if (threadIdx.x < nbi) {
+      T y = T(0);
+#pragma unroll
+      for (int g = 0; g < 8; g++) y += red[g][threadIdx.x];
+      x[r0 + threadIdx.x] = y;
+    }
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) st_release(&flags[i], 1);
@@ -185,10 +246,12 @@ int ticket_solve(char uplo, char trans, int n, const void *A, long lda, const vo
     cudaGetDevice(&d);
     cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, d);
   }
+  if (ldd % TB || (uintptr_t)Dinv % 16) return (int)cudaErrorMisalignedAddress;
+  const bool vec_ok = lda % 4 == 0 && (uintptr_t)A % 16 == 0;
   int grid = nblk < 4 * g_sms ? nblk : 4 * g_sms;
   trsv_ticket_k<T><<<grid, THREADS, 0, s>>>(n, nblk, (const T *)A, lda, lower_op, tr,
                                             (const T *)Dinv, ldd, (const T *)b, (T *)x,
-                                            fl + nblk, fl, status);
+                                            fl + nblk, fl, status, vec_ok);
   pla_k_count(1);
   return (int)cudaGetLastError();
 }

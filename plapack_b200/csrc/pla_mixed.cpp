@@ -25,6 +25,8 @@ using namespace pla;
 namespace pla {
 int trsm_device(int dt, char side, char uplo, char trans, char diag, int nt, int other,
                 double alpha, const char *T, long ldt, char *B, long ldb);
+int panel_lu(int dt, int r, int b, char *P, long lda, int *piv, int *status, int *zero_info,
+             int row_base);
 }
 
 namespace {
@@ -110,8 +112,7 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
     if (F.kind == 0) {
       {
         PhaseTimer t(&ph.panel_ms);
-        K(pla_k_lu_panel(MPI_FLOAT, n - k, b, at(k, k), ld, F.piv + k, &st[0], &st[2], k,
-                         stream()));
+        K(panel_lu(MPI_FLOAT, n - k, b, (char *)at(k, k), ld, F.piv + k, &st[0], &st[2], k));
       }
       {
         PhaseTimer t(&ph.swap_ms);

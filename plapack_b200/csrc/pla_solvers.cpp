@@ -49,15 +49,39 @@ char trans_c(int t) { return t == PLA_NO_TRANSPOSE ? 'N' : 'T'; }
 char diag_c(int d) { return d == PLA_UNIT_DIAG ? 'U' : 'N'; }
 int gemm_t(int t) { return t == PLA_NO_TRANSPOSE ? PLA_NO_TRANSPOSE : PLA_TRANSPOSE; }
 
+// Left-side solve with one diagonal block of order kb <= 128 against `other`
+// columns.  For many columns the block is inverted once (substitution against
+// the identity) and applied as a GEMM, B := alpha inv(op(T)) B; the GEMM may
+// run in place because its M extent (kb) is a single 128-row tile, so every
+// column tile of B is read and written by one CTA only.
+int trsm_left_block(int dt, char uplo, char trans, char diag, int kb, int other, double alpha,
+                    const char *T, long ldt, char *B, long ldb, const int *status) {
+  if (other < 1024)
+    return pla_k_trsm_small(dt, 'L', uplo, trans, diag, kb, other, alpha, T, ldt, B, ldb, status,
+                            stream());
+  const int es = dt == MPI_DOUBLE ? 8 : 4;
+  char *inv = (char *)scratch(3, (size_t)kTri * kTri * es);
+  if (!inv) return (int)cudaErrorMemoryAllocation;
+  int r = pla_k_fill(dt, kb, kb, inv, kb, 0.0, stream());
+  if (!r) r = pla_k_fill(dt, 1, kb, inv, kb + 1, 1.0, stream());  // the diagonal
+  if (!r) r = pla_k_trsm_small(dt, 'L', uplo, trans, diag, kb, kb, 1.0, T, ldt, inv, kb, status,
+                               stream());
+  if (!r) r = pla_k_gemm(dt, PLA_NO_TRANSPOSE, PLA_NO_TRANSPOSE, kb, other, kb, alpha, inv, kb, B,
+                         ldb, 0.0, B, ldb, 0, status, stream());
+  return r;
+}
+
 // op(T) X = alpha B (side L) or X op(T) = alpha B (side R) for a triangle of
-// any size: diagonal blocks of <= 128 by substitution, the coupling blocks by
-// GEMM, ordered like BLAS3/PLA_Trsm_left_lower.c:33-78.
+// any size: diagonal blocks of <= 128 (inverse-diagonal + GEMM on the left),
+// the coupling blocks by GEMM, ordered like BLAS3/PLA_Trsm_left_lower.c:33-78.
 int trsm_blocked(int dt, char side, char uplo, char trans, char diag, int nt, int other,
                  double alpha, const char *T, long ldt, char *B, long ldb, const int *status) {
   if (nt <= 0 || other <= 0) return 0;
   const int es = dt == MPI_DOUBLE ? 8 : 4;
   const bool tr = trans != 'N';
   auto t_at = [&](long i, long j) { return T + (i + j * ldt) * es; };
+  if (nt <= kTri && side == 'L')
+    return trsm_left_block(dt, uplo, trans, diag, nt, other, alpha, T, ldt, B, ldb, status);
   if (nt <= kTri)
     return pla_k_trsm_small(dt, side, uplo, trans, diag, nt, other, alpha, T, ldt, B, ldb,
                             status, stream());
@@ -72,8 +96,8 @@ int trsm_blocked(int dt, char side, char uplo, char trans, char diag, int nt, in
       // alpha scales the first block here and every other row in the first
       // GEMM below (its beta), so later steps use 1
       const double a = q == 0 ? alpha : 1.0;
-      int r = pla_k_trsm_small(dt, 'L', uplo, trans, diag, kb, other, a, t_at(k0, k0), ldt,
-                               b_at(k0), ldb, status, stream());
+      int r = trsm_left_block(dt, uplo, trans, diag, kb, other, a, t_at(k0, k0), ldt, b_at(k0),
+                              ldb, status);
       if (r) return r;
       int r0 = forward ? k0 + kb : 0, rn = forward ? nt - r0 : k0;
       if (rn <= 0) continue;
@@ -108,6 +132,47 @@ int trsm_blocked(int dt, char side, char uplo, char trans, char diag, int nt, in
   return 0;
 }
 
+}  // namespace
+
+namespace pla {
+// The r x b panel at `P` (row k of the matrix) with partial pivoting.  The
+// column loop of PLA_LU_right_mv (SOLVERS/LU/PLA_LU_mv.c:52-82) runs in the
+// cooperative kernel on sub-panels of kSub columns, whose rows stay in shared
+// memory; after each sub-panel its pivots are applied to the panel's other
+// columns and the columns to its right get the unit-lower solve and the
+// rank-kSub update.  Pivot choices are those of the column-by-column loop;
+// only the rounding order of the panel's trailing columns differs.
+int panel_lu(int dt, int r, int b, char *P, long lda, int *piv, int *status, int *zero_info,
+             int row_base) {
+  constexpr int kSub = 32;
+  const int es = dt == MPI_DOUBLE ? 8 : 4;
+  auto at = [&](long i, long j) { return P + (i + j * lda) * es; };
+  if (b <= kSub)
+    return pla_k_lu_panel(dt, r, b, P, lda, piv, status, zero_info, row_base, stream());
+  for (int s = 0; s < b; s += kSub) {
+    const int sb = std::min(kSub, b - s), rest = b - s - sb;
+    int e = pla_k_lu_panel(dt, r - s, sb, at(s, s), lda, piv + s, status, zero_info,
+                           row_base + s, stream());
+    if (e) return e;
+    e = pla_k_laswp(dt, at(s, 0), lda, sb, piv + s, 0, s, s + sb, b, stream());
+    if (e) return e;
+    if (rest <= 0) continue;
+    e = pla_k_trsm_small(dt, 'L', 'L', 'N', 'U', sb, rest, 1.0, at(s, s), lda, at(s, s + sb), lda,
+                         status, stream());
+    if (e) return e;
+    if (r - s - sb > 0) {
+      e = pla_k_gemm(dt, PLA_NO_TRANSPOSE, PLA_NO_TRANSPOSE, r - s - sb, rest, sb, -1.0,
+                     at(s + sb, s), lda, at(s, s + sb), lda, 1.0, at(s + sb, s + sb), lda, 0,
+                     status, stream());
+      if (e) return e;
+    }
+  }
+  return 0;
+}
+}  // namespace pla
+
+namespace {
+
 // Blocked right-looking LU (SOLVERS/LU/PLA_LU.c:103-192) on device memory.
 int lu_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, Status *st) {
   const int es = dt == MPI_DOUBLE ? 8 : 4;
@@ -118,8 +183,7 @@ int lu_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, Status 
     const int b = std::min(nb, kmax - k), r = m - k;
     {
       PhaseTimer t(&ph.panel_ms);
-      K(pla_k_lu_panel(dt, r, b, at(k, k), lda, piv + k, &st->status, &st->zero_info, k,
-                       stream()));
+      K(panel_lu(dt, r, b, at(k, k), lda, piv + k, &st->status, &st->zero_info, k));
     }
     {
       PhaseTimer t(&ph.swap_ms);
@@ -179,6 +243,20 @@ int vlen(PLA_Obj v) { return (v->length == 1) ? v->width : v->length; }
 }  // namespace
 
 namespace pla {
+// the factorization loops without the final status read-back (callers that
+// queue many factorizations and synchronize once)
+int lu_async(int dt, int m, int n, char *A, long lda, int *piv, int nb) {
+  Status *st = device_status();
+  if (!st) PLA_FAIL("cannot allocate the status word");
+  PLA_CUDA(cudaMemsetAsync(st, 0, sizeof(Status), stream()));
+  return lu_device(dt, m, n, A, lda, piv, nb, st);
+}
+int chol_async(int dt, int n, char *A, long lda, int nb) {
+  Status *st = device_status();
+  if (!st) PLA_FAIL("cannot allocate the status word");
+  PLA_CUDA(cudaMemsetAsync(st, 0, sizeof(Status), stream()));
+  return chol_device(dt, n, A, lda, nb, st);
+}
 int lu_on_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, int *zero_info_host) {
   Status *st = device_status();
   if (!st) PLA_FAIL("cannot allocate the status word");

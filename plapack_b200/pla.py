@@ -62,6 +62,11 @@ class MixedReport(ctypes.Structure):
                 ("backward_error", _d), ("factor_ms", _d), ("refine_ms", _d)]
 
 
+class BatchInstance(ctypes.Structure):
+    _fields_ = [("n", _i), ("nrhs", _i), ("kind", _i), ("A", _vp), ("B", _vp),
+                ("pivots", ctypes.POINTER(ctypes.c_int))]
+
+
 # name -> argtypes (restype int unless listed in _RESTYPE)
 _SIGS = {
     "PLA_Init": [_i], "PLA_Finalize": [], "PLA_Initialized": [_pi],
@@ -118,6 +123,10 @@ _SIGS = {
     "PLA_Mixed_params_default": [ctypes.POINTER(MixedParams)],
     "PLA_General_solve_mixed": [Obj, Obj, ctypes.POINTER(MixedParams), ctypes.POINTER(MixedReport)],
     "PLA_Pos_def_solve_mixed": [Obj, Obj, ctypes.POINTER(MixedParams), ctypes.POINTER(MixedReport)],
+    "PLA_Batch_plan_create": [_i, _i, ctypes.POINTER(BatchInstance), _vp, _i, _pobj],
+    "PLA_Batch_plan_execute": [_vp], "PLA_Batch_plan_free": [_pobj],
+    "PLA_Batched_factor_solve": [_i, _i, ctypes.POINTER(BatchInstance), _vp],
+    "PLA_Batched_factor_solve_loop": [_i, _i, ctypes.POINTER(BatchInstance)],
     "PLA_Obj_set_local_contents_device": [_vp, _i, Obj],
     "PLA_Obj_get_local_contents_device": [Obj, _vp, _i],
 }
