@@ -25,6 +25,8 @@
 namespace {
 
 constexpr int THREADS = 256;
+// shared memory of one warp-mode instance: a 32 x 33 matrix and 4 x 33 RHS
+constexpr int kWarpSmem = 32 * 33 + 4 * 33;
 
 template <typename T>
 struct Inst {
@@ -42,7 +44,7 @@ struct Task {
 template <typename T>
 __device__ void warp_instance(const Inst<T> &in, T *S, int *info) {
   const int lane = threadIdx.x & 31, n = in.n, ld = 33;
-  T *Bs = S + 32 * ld;  // 32 x 4 right-hand sides, ld 33
+  T *Bs = S + 32 * ld;  // up to 4 right-hand sides, ld 33
   for (int c = 0; c < n; c++)
     if (lane < n) S[lane + c * ld] = in.A[lane + (long)c * n];
   for (int r = 0; r < in.nrhs; r++)
@@ -58,7 +60,8 @@ __device__ void warp_instance(const Inst<T> &in, T *S, int *info) {
         int oi = __shfl_down_sync(0xffffffffu, idx, o);
         if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
       }
-      const int p = __shfl_sync(0xffffffffu, idx, 0);
+      const int best = __shfl_sync(0xffffffffu, idx, 0);
+      const int p = best == INT_MAX ? j : best;  // all-NaN column: no interchange
       if (lane == 0) in.piv[j] = p - j;
       if (p != j && lane < n) {
         T a = S[j + lane * ld];
@@ -193,7 +196,7 @@ __device__ void cta_instance(const Inst<T> &in, T *M, long lm, T *X, long lx, in
         if (a > v) { v = a; idx = i; }
       }
       block_argmax(v, idx, sv, si);
-      const int p = idx;
+      const int p = idx == INT_MAX ? j : idx;  // all-NaN column: no interchange
       if (tid == 0) in.piv[j] = p - j;
       if (p != j)
         for (int c = tid; c < n; c += THREADS) {
@@ -305,7 +308,7 @@ batched_k(const Inst<T> *inst, const int *order, const Task *tasks, int ntasks, 
       const int w = threadIdx.x >> 5;
       if (w < tk.count) {
         const int id = order[tk.first + w];
-        warp_instance(inst[id], S + (long)w * (32 * 33 + 32 * 33), &info[id]);
+        warp_instance(inst[id], S + (long)w * kWarpSmem, &info[id]);
       }
     } else {
       const int id = order[tk.first];
@@ -340,7 +343,7 @@ batched_k(const Inst<T> *inst, const int *order, const Task *tasks, int ntasks, 
 
 extern "C" size_t pla_k_batched_smem(int dt, int n_smem_max) {
   const size_t es = dt == MPI_DOUBLE ? 8 : 4;
-  size_t warp = (size_t)8 * 2 * 32 * 33 * es;
+  size_t warp = (size_t)8 * kWarpSmem * es;
   size_t cta = ((size_t)(n_smem_max + 1) * n_smem_max + (size_t)(n_smem_max + 1) * 4) * es;
   return warp > cta ? warp : cta;
 }

@@ -19,8 +19,9 @@
 // with a bounded spin; on timeout the kernel records PLA_K_TIMEOUT and exits.
 #include <climits>
 #include <cstdio>
+#include <mutex>
 
-#include "PLA.h"
+#include "pla_internal.h"
 #include "pla_kernels.h"
 
 namespace {
@@ -164,8 +165,13 @@ panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *sta
       if (tid == 0) { s_p = bi; s_i[0] = bb; }
     }
     __syncthreads();
-    const int p = s_p, wb = s_i[0];
-    for (int c = tid; c < w; c += kThreads) u[c] = __ldcg(&cand_row[((long)par * P + wb) * w + c]);
+    // A column of NaNs has no candidate (NaN never compares greater): keep
+    // row j as its own pivot, whose contents the owner of row j published.
+    const bool none = s_p == INT_MAX;
+    const int p = none ? j : s_p, wb = s_i[0];
+    for (int c = tid; c < w; c += kThreads)
+      u[c] = none ? __ldcg(&top_row[(long)par * w + c])
+                  : __ldcg(&cand_row[((long)par * P + wb) * w + c]);
     __syncthreads();
     // the interchange of rows j and p over the panel width
     if (j >= row0 && j < row1)

@@ -72,9 +72,9 @@ void build_tasks(const std::vector<PLA_Batch_instance> &v, int n_smem, std::vect
   size_t i = 0;
   while (i < order.size()) {
     const PLA_Batch_instance &in = v[order[i]];
-    if (in.n <= 32 && in.nrhs <= 32) {
+    if (in.n <= 32 && in.nrhs <= 4) {
       TaskRec t{(int)i, 0, 0, 0};
-      while (i < order.size() && t.count < 8 && v[order[i]].n <= 32 && v[order[i]].nrhs <= 32) {
+      while (i < order.size() && t.count < 8 && v[order[i]].n <= 32 && v[order[i]].nrhs <= 4) {
         t.count++;
         i++;
       }

@@ -332,6 +332,13 @@ int PLA_Apply_pivots_to_rows(PLA_Obj A, PLA_Obj ipiv) {
   int npiv = vlen(ipiv);
   if (npiv > A->length) PLA_FAIL("more pivots than rows");
   if (vinc(ipiv) != 1) PLA_FAIL("pivots must be a column");
+  {
+    // a pivot vector from the caller must name rows of A (the kernel trusts it)
+    std::vector<int> h(npiv);
+    PLA_CUDA(cudaMemcpy(h.data(), at(ipiv, 0, 0), npiv * sizeof(int), cudaMemcpyDefault));
+    for (int i = 0; i < npiv; i++)
+      if (h[i] < 0 || i + h[i] >= A->length) PLA_FAIL("pivot entry outside the rows of A");
+  }
   K(pla_k_laswp_rows(A->base->datatype, at(A, 0, 0), ld(A), A->width, npiv,
                      (const int *)at(ipiv, 0, 0), stream()));
   return finish("apply pivots");

@@ -78,6 +78,20 @@ def test_lu_ties_first_index(pla_session, golden, restated):
     assert np.array_equal(piv, arrays["lu_ties_48_nb16__piv"])
 
 
+def test_lu_zero_column_nan_fill(pla_session):
+    """An exact zero pivot early on turns the rest of the matrix into NaN (as
+    the reference does: no detection, 1/0 scaling).  Pivot searches over NaN
+    columns must still name rows of the matrix, and info reports the column."""
+    rng = np.random.default_rng(4)
+    for n, nb in [(100, 32), (300, 128)]:
+        A = np.asfortranarray(rng.standard_normal((n, n)))
+        A[:, 5] = 0.0
+        LU, piv, info = pla_lu(pla_session, A, nb)
+        assert info == 6
+        assert np.all(piv >= 0) and np.all(piv + np.arange(n) < n)
+        assert np.isnan(LU[10:, 10:]).all()
+
+
 @pytest.mark.parametrize("n,nb", [(1000, 64), (2048, 128), (1537, 96)])
 def test_lu_vs_oracle_random(pla_session, restated, n, nb):
     rng = np.random.default_rng(n)
