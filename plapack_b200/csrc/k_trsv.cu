@@ -66,6 +66,17 @@ tri_inv_blocks_k(int n, const T *A, long lda, bool lower_op, bool trans, bool un
   }
 }
 
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
 __device__ __forceinline__ int ld_acquire(const int *p) {
   int v;
   asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -79,6 +90,8 @@ template <typename T>
 __global__ void __launch_bounds__(THREADS)
 trsv_ticket_k(int n, int nblk, const T *A, long lda, bool lower_op, bool trans, const T *Dinv,
               long ldd, const T *b, T *x, int *ticket, int *flags, int *status, bool vec_ok) {
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  T *Ds = reinterpret_cast<T *>(dyn_smem);  // TB x TB inverse diagonal block
   __shared__ T xs[TB];
   __shared__ T part[2][TB];
   __shared__ int s_blk, s_bad;
@@ -103,10 +116,27 @@ trsv_ticket_k(int n, int nblk, const T *A, long lda, bool lower_op, bool trans, 
     const int rg = threadIdx.x & 31, cg = threadIdx.x >> 5;
     T acc4[4] = {T(0), T(0), T(0), T(0)};
     T acc = T(0);
+    // the inverse diagonal block streams into shared memory while the row's
+    // tiles are processed
+    for (int u = threadIdx.x; u < TB * TB / 4; u += THREADS) {
+      const int c = u / (TB / 4), r4 = (u % (TB / 4)) * 4;
+      cp_async16(&Ds[c * TB + r4], Dinv + (r0 + r4) + (long)c * ldd);
+    }
+    cp_async_commit();
     for (int s = 0; s < q; s++) {
       const int j = lower_op ? s : nblk - 1 - s;
       const long c0 = (long)j * TB;
       const int nbj = min(TB, n - (int)c0);
+      const bool full = nbi == TB && nbj == TB && vec_ok;
+      // the tile does not depend on x_j: its loads are issued before waiting
+      float4 v[16];
+      if (full) {
+        const T *base = trans ? A + (r0 + r) * lda + c0 + 64 * half
+                              : A + (r0 + 4 * rg) + (c0 + 16 * cg) * lda;
+        const long step = trans ? 4 : lda;
+#pragma unroll
+        for (int u = 0; u < 16; u++) v[u] = *reinterpret_cast<const float4 *>(base + u * step);
+      }
       if (threadIdx.x == 0) {
         long spins = 0;
         while (ld_acquire(&flags[j]) == 0) {
@@ -122,12 +152,7 @@ trsv_ticket_k(int n, int nblk, const T *A, long lda, bool lower_op, bool trans, 
       if (s_bad) return;
       if (threadIdx.x < nbj) xs[threadIdx.x] = __ldcg(&x[c0 + threadIdx.x]);
       __syncthreads();
-      const bool full = nbi == TB && nbj == TB && vec_ok;
       if (full && !trans) {
-        float4 v[16];
-        const T *base = A + (r0 + 4 * rg) + (c0 + 16 * cg) * lda;
-#pragma unroll
-        for (int u = 0; u < 16; u++) v[u] = *reinterpret_cast<const float4 *>(base + u * lda);
 #pragma unroll
         for (int u = 0; u < 16; u++) {
           const T xv = xs[16 * cg + u];
@@ -137,10 +162,6 @@ trsv_ticket_k(int n, int nblk, const T *A, long lda, bool lower_op, bool trans, 
           acc4[3] += v[u].w * xv;
         }
       } else if (full) {
-        float4 v[16];
-        const T *base = A + (r0 + r) * lda + c0 + 64 * half;
-#pragma unroll
-        for (int u = 0; u < 16; u++) v[u] = *reinterpret_cast<const float4 *>(base + 4 * u);
 #pragma unroll
         for (int u = 0; u < 16; u++) {
           const int c = 64 * half + 4 * u;
@@ -171,20 +192,19 @@ trsv_ticket_k(int n, int nblk, const T *A, long lda, bool lower_op, bool trans, 
       xs[threadIdx.x] = r < nbi ? b[r0 + r] - sacc : T(0);
     }
     __syncthreads();
-    // x_i = inv(D_i) y, the same 16-loads-per-thread pattern over Dinv
+    // x_i = inv(D_i) y with the inverse block from shared memory
+    cp_async_wait_all();
+    __syncthreads();
     {
-      float4 v[16];
-      const T *base = Dinv + (r0 + 4 * rg) + (long)(16 * cg) * ldd;
-#pragma unroll
-      for (int u = 0; u < 16; u++) v[u] = *reinterpret_cast<const float4 *>(base + u * ldd);
       T y4[4] = {T(0), T(0), T(0), T(0)};
 #pragma unroll
       for (int u = 0; u < 16; u++) {
+        const float4 d = *reinterpret_cast<const float4 *>(&Ds[(16 * cg + u) * TB + 4 * rg]);
         const T xv = xs[16 * cg + u];
-        y4[0] += v[u].x * xv;
-        y4[1] += v[u].y * xv;
-        y4[2] += v[u].z * xv;
-        y4[3] += v[u].w * xv;
+        y4[0] += d.x * xv;
+        y4[1] += d.y * xv;
+        y4[2] += d.z * xv;
+        y4[3] += d.w * xv;
       }
 #pragma unroll
       for (int e = 0; e < 4; e++) red[cg][4 * rg + e] = y4[e];
@@ -248,8 +268,10 @@ int ticket_solve(char uplo, char trans, int n, const void *A, long lda, const vo
   }
   if (ldd % TB || (uintptr_t)Dinv % 16) return (int)cudaErrorMisalignedAddress;
   const bool vec_ok = lda % 4 == 0 && (uintptr_t)A % 16 == 0;
-  int grid = nblk < 4 * g_sms ? nblk : 4 * g_sms;
-  trsv_ticket_k<T><<<grid, THREADS, 0, s>>>(n, nblk, (const T *)A, lda, lower_op, tr,
+  int grid = nblk < 3 * g_sms ? nblk : 3 * g_sms;
+  const size_t dyn = (size_t)TB * TB * sizeof(T);
+  cudaFuncSetAttribute(trsv_ticket_k<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+  trsv_ticket_k<T><<<grid, THREADS, dyn, s>>>(n, nblk, (const T *)A, lda, lower_op, tr,
                                             (const T *)Dinv, ldd, (const T *)b, (T *)x,
                                             fl + nblk, fl, status, vec_ok);
   pla_k_count(1);
