@@ -95,6 +95,26 @@ int PLA_General_solve_mixed(PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *params
 int PLA_Pos_def_solve_mixed(PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *params,
                             PLA_Mixed_report *report);
 
+/* ---- panel factorization that allocates nothing ---------------------------
+ * No counterpart in the reference.  Factors the m x w panel A (device memory,
+ * column-major, lda >= m, w <= m) in place with partial pivoting, the column
+ * loop PLA_LU runs on each panel: pivots[j] receives the reference's offset
+ * encoding (row j was swapped with row j + pivots[j]), the swaps cover the
+ * panel's own columns only.  *status (device int, 0 on entry) is set to 1 if
+ * a bounded wait in the kernel gave up.
+ * For callers that cannot let the library call cudaMalloc -- programs whose
+ * GPU memory belongs to another allocator, or services that forbid allocation
+ * while running: the kernel's workspace is a fixed array of about 334 KB in
+ * device memory, present on every GPU that loads the library until the
+ * process exits, instead of memory the library allocates.  Limit: w <= 128
+ * (larger panels return PLA_ERROR with a message in PLA_Last_error).
+ * The call is asynchronous on `stream` (a cudaStream_t, NULL for the default
+ * stream).  The first call on a device looks up the array's device address;
+ * make that first call before any stream capture.  All calls share the one
+ * array, so calls whose kernels overlap on the GPU race. */
+int PLA_B200_lu_panel_noalloc(MPI_Datatype datatype, int m, int w, void *A, int lda, int *pivots,
+                              int *status, void *stream);
+
 /* ---- batched factor-and-solve ------------------------------------------------
  * Many independent systems of uneven order, each factored in place (LU with
  * partial pivoting, or lower Cholesky) and solved for its right-hand sides, in

@@ -286,3 +286,126 @@ extern "C" void pla_kernels_release(void) {
   g_ws.ptr = nullptr;
   g_ws.bytes = 0;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the panel factorization.
+//
+// Some callers cannot let a library call cudaMalloc: programs whose GPU memory
+// is owned by another allocator (a framework's caching allocator that has
+// reserved the device, for instance), and memory-budgeted or real-time
+// services that forbid allocation once they are running.  For them the panel
+// kernel's workspace -- the grid-barrier counter and the per-CTA pivot
+// candidates -- lives in the fixed device array below instead of memory the
+// library allocates.  The array holds the workspace of at most kNoAllocCtas
+// CTAs for panels of at most kNoAllocWidth columns in double precision
+// (about 334 KB); every GPU that loads the library keeps it until the process
+// exits.  Every call shares it, so calls whose kernels overlap on the GPU (on
+// different streams, or from different host threads) race.
+namespace {
+constexpr int kNoAllocCtas = 160;
+constexpr int kNoAllocWidth = 128;
+constexpr size_t kNoAllocAbs = 256;  // bytes [0, 256): the barrier counter
+constexpr size_t kNoAllocIdx = kNoAllocAbs + 2 * kNoAllocCtas * sizeof(double);
+constexpr size_t kNoAllocRow =
+    (kNoAllocIdx + 2 * kNoAllocCtas * sizeof(int) + 255) & ~(size_t)255;
+constexpr size_t kNoAllocTop =
+    kNoAllocRow + (size_t)2 * kNoAllocCtas * kNoAllocWidth * sizeof(double);
+constexpr size_t kNoAllocBytes = kNoAllocTop + (size_t)2 * kNoAllocWidth * sizeof(double);
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_panel_scratch[kNoAllocBytes];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[128] = {};
+
+// The array's device address on the current device, looked up once per
+// device (the host-side name of the array is only a stand-in).
+int noalloc_scratch(char **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
+  if (dev < 0 || dev >= 128) return (int)cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_panel_scratch);
+    if (e != cudaSuccess) return (int)e;
+    g_noalloc_addr[dev] = p;
+  }
+  *out = (char *)g_noalloc_addr[dev];
+  return 0;
+}
+
+template <typename T>
+int launch_noalloc(int r, int w, T *A, long lda, int *piv, int *status, cudaStream_t s) {
+  int dev = 0, sms = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  int P = (r + 31) / 32;
+  if (P > sms) P = sms;
+  if (P > kNoAllocCtas) P = kNoAllocCtas;
+  if (P < 1) P = 1;
+  int R = (r + P - 1) / P;
+  P = (r + R - 1) / R;
+  size_t ubytes = (size_t)((w + 1) & ~1) * sizeof(T);
+  size_t sbytes = ubytes + (size_t)R * w * sizeof(T);
+  int use_smem = sbytes + 1024 <= (size_t)optin - 2048;
+  size_t dyn = use_smem ? sbytes : ubytes;
+  cudaFuncSetAttribute(panel_lu_k<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, panel_lu_k<T>, kThreads, dyn);
+  if (per_sm * sms < P) return (int)cudaErrorCooperativeLaunchTooLarge;
+  char *ws = nullptr;
+  int rc = noalloc_scratch(&ws);
+  if (rc) return rc;
+  // the barrier counter must start at zero; the candidate slots are written
+  // before they are read, so the last call's contents are harmless
+  e = cudaMemsetAsync(ws, 0, kNoAllocAbs, s);
+  if (e != cudaSuccess) return (int)e;
+  unsigned *bar = (unsigned *)ws;
+  T *cand_abs = (T *)(ws + kNoAllocAbs);
+  int *cand_idx = (int *)(ws + kNoAllocIdx);
+  T *cand_row = (T *)(ws + kNoAllocRow);
+  T *top_row = (T *)(ws + kNoAllocTop);
+  int *zero_info = nullptr;
+  int row_base = 0;
+  void *args[] = {&A,   &lda,        &r,         &w,        &R,         &use_smem,
+                  &piv, &status,     &zero_info, &row_base, &bar,       &cand_abs,
+                  &cand_idx, &cand_row, &top_row};
+  e = cudaLaunchCooperativeKernel((void *)panel_lu_k<T>, dim3(P), dim3(kThreads), args, dyn, s);
+  pla_k_count(1);
+  return (int)e;
+}
+
+}  // namespace
+
+// See include/pla_b200.h.  No cudaMalloc, cudaFree or allocating library call
+// is made on this path.
+extern "C" int PLA_B200_lu_panel_noalloc(MPI_Datatype datatype, int m, int w, void *A, int lda,
+                                         int *pivots, int *status, void *stream) {
+  if (datatype != MPI_DOUBLE && datatype != MPI_FLOAT)
+    return pla::fail("PLA_B200_lu_panel_noalloc: datatype must be MPI_DOUBLE or MPI_FLOAT",
+                     __LINE__, __FILE__);
+  if (m < 0 || w < 0 || lda < (m > 1 ? m : 1))
+    return pla::fail("PLA_B200_lu_panel_noalloc: invalid m, w or lda", __LINE__, __FILE__);
+  if (m == 0 || w == 0) return PLA_SUCCESS;
+  if (w > m)
+    return pla::fail("PLA_B200_lu_panel_noalloc: the panel has more columns than rows",
+                     __LINE__, __FILE__);
+  if (w > kNoAllocWidth)
+    return pla::fail("PLA_B200_lu_panel_noalloc: panel wider than 128 columns, the limit of "
+                     "its fixed workspace",
+                     __LINE__, __FILE__);
+  if (!A || !pivots || !status)
+    return pla::fail("PLA_B200_lu_panel_noalloc: null pointer", __LINE__, __FILE__);
+  cudaStream_t s = (cudaStream_t)stream;
+  int e = datatype == MPI_DOUBLE
+              ? launch_noalloc<double>(m, w, (double *)A, lda, pivots, status, s)
+              : launch_noalloc<float>(m, w, (float *)A, lda, pivots, status, s);
+  if (e) return pla::cuda_fail((cudaError_t)e, __LINE__, __FILE__);
+  return PLA_SUCCESS;
+}
