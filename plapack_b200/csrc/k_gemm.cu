@@ -5,7 +5,7 @@
 // FP64: tensor-core DMMA (mma.sync m16n8k8 .f64; tcgen05 has no f64 kind).
 //   CTA tile 128 x 64, k-step 16, 8 warps as 4 (M) x 2 (N) with a 32 x 32
 //   warp tile; three cp.async stages; two CTAs per SM so one CTA's epilogue
-//   (the read-modify-write of C) overlaps the other's main loop.  The stages
+//   (the stores of C) overlaps the other's main loop.  The stages
 //   are stored permuted (rows g and g+8, k and k+4 side by side) so that
 //   each thread's fragment pairs are single 16-byte loads, and padded so
 //   those loads are bank-conflict free: A stage [16][128+4], B stage [64][16+8].
@@ -100,8 +100,11 @@ __device__ __forceinline__ bool keep(int uplo, int i, int j) {
   return uplo == 0 || (uplo == 'L' ? i >= j : i <= j);
 }
 
-// FP64 tensor-core GEMM
-template <bool TA, bool TB>
+// FP64 tensor-core GEMM.  FOLD (alpha = +-1, every trailing update): the
+// accumulators start as alpha * beta * C and the result is alpha * acc, so the
+// reads of C are issued before the main loop, under the pipeline fill, and the
+// epilogue only stores.  Without FOLD the epilogue reads C.
+template <bool TA, bool TB, bool FOLD>
 __global__ void __launch_bounds__(THREADS, 2)
 dgemm_k(int m, int n, int k, double alpha, const double *__restrict__ A, long lda,
         const double *__restrict__ B, long ldb, double beta, double *C, long ldc, int uplo,
@@ -117,13 +120,22 @@ dgemm_k(int m, int n, int k, double alpha, const double *__restrict__ A, long ld
   const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
   const int g = lane >> 2, t = lane & 3;
 
+  const double ab = FOLD && beta != 0.0 ? alpha * beta : 0.0;
   double acc[2][4][4];
-#pragma unroll
-  for (int i = 0; i < 2; i++)
+  {
+    const int ri = m0 + wm + g, cj = n0 + wn + 2 * t;
+    const double *cb = C + ri + (long)cj * ldc;
 #pragma unroll
     for (int j = 0; j < 4; j++)
 #pragma unroll
-      for (int q = 0; q < 4; q++) acc[i][j][q] = 0.0;
+      for (int q = 0; q < 4; q++)
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+          const int di = i * 16 + (q >> 1) * 8, dj = j * 8 + (q & 1);
+          acc[i][j][q] = ab != 0.0 && ri + di < m && cj + dj < n ? ab * cb[di + (long)dj * ldc]
+                                                                  : 0.0;
+        }
+  }
 
   const int nk = (k + BK - 1) / BK;
 #pragma unroll
@@ -189,13 +201,13 @@ dgemm_k(int m, int n, int k, double alpha, const double *__restrict__ A, long ld
         if (gi < m && gj < n && keep(uplo, gi, gj)) {
           double *cp = C + gi + (long)gj * ldc;
           double v = alpha * acc[i][j][q];
-          *cp = beta == 0.0 ? v : fma(beta, *cp, v);
+          *cp = FOLD || beta == 0.0 ? v : fma(beta, *cp, v);
         }
       }
 }
 
 // FP32 SIMT GEMM with the same staging; each thread computes an 8 x 4 block
-template <bool TA, bool TB>
+template <bool TA, bool TB, bool FOLD>
 __global__ void __launch_bounds__(THREADS, 2)
 sgemm_k(int m, int n, int k, float alpha, const float *__restrict__ A, long lda,
         const float *__restrict__ B, long ldb, float beta, float *C, long ldc, int uplo,
@@ -210,10 +222,14 @@ sgemm_k(int m, int n, int k, float alpha, const float *__restrict__ A, long lda,
   const int tid = threadIdx.x;
   const int tm = (tid & 15) * 8, tn = (tid >> 4) * 4;  // 16 x 16 threads
   float acc[8][4];
+  const float ab = FOLD && beta != 0.f ? alpha * beta : 0.f;  // as in dgemm_k
 #pragma unroll
   for (int i = 0; i < 8; i++)
 #pragma unroll
-    for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
+    for (int j = 0; j < 4; j++) {
+      const int gi = m0 + tm + i, gj = n0 + tn + j;
+      acc[i][j] = ab != 0.f && gi < m && gj < n ? ab * C[gi + (long)gj * ldc] : 0.f;
+    }
   const int nk = (k + BK - 1) / BK;
 #pragma unroll
   for (int s = 0; s < STAGES - 1; s++) {
@@ -256,7 +272,7 @@ sgemm_k(int m, int n, int k, float alpha, const float *__restrict__ A, long lda,
       if (gi < m && gj < n && keep(uplo, gi, gj)) {
         float *cp = C + gi + (long)gj * ldc;
         float v = alpha * acc[i][j];
-        *cp = beta == 0.f ? v : fmaf(beta, *cp, v);
+        *cp = FOLD || beta == 0.f ? v : fmaf(beta, *cp, v);
       }
     }
 }
@@ -279,6 +295,7 @@ extern "C" int pla_k_gemm(int dt, int transa, int transb, int m, int n, int k, d
     alpha = 0.0;
   }
   const bool ta = transa != PLA_NO_TRANSPOSE, tb = transb != PLA_NO_TRANSPOSE;
+  const bool fold = alpha == 1.0 || alpha == -1.0;
   dim3 grid((m + BM - 1) / BM, (n + BN - 1) / BN);
   if (dt == MPI_DOUBLE) {
     size_t sm = (size_t)STAGES * (BK * LDA_S + BN * LDB_S) * sizeof(double);
@@ -286,9 +303,15 @@ extern "C" int pla_k_gemm(int dt, int transa, int transb, int m, int n, int k, d
     double *c = (double *)C;
 #define L(TA_, TB_)                                                                          \
   do {                                                                                       \
-    set_smem(dgemm_k<TA_, TB_>, sm);                                                         \
-    dgemm_k<TA_, TB_><<<grid, THREADS, sm, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, \
-                                                uplo_c, status);                             \
+    if (fold) {                                                                              \
+      set_smem(dgemm_k<TA_, TB_, true>, sm);                                                 \
+      dgemm_k<TA_, TB_, true><<<grid, THREADS, sm, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, \
+                                                        c, ldc, uplo_c, status);             \
+    } else {                                                                                 \
+      set_smem(dgemm_k<TA_, TB_, false>, sm);                                                \
+      dgemm_k<TA_, TB_, false><<<grid, THREADS, sm, s>>>(m, n, k, alpha, a, lda, b, ldb,      \
+                                                         beta, c, ldc, uplo_c, status);      \
+    }                                                                                        \
   } while (0)
     if (!ta && !tb) L(false, false);
     else if (!ta && tb) L(false, true);
@@ -299,11 +322,19 @@ extern "C" int pla_k_gemm(int dt, int transa, int transb, int m, int n, int k, d
     size_t sm = (size_t)STAGES * (BK * LDA_S + BN * LDB_S) * sizeof(float);
     const float *a = (const float *)A, *b = (const float *)B;
     float *c = (float *)C;
-#define L(TA_, TB_)                                                                            \
-  do {                                                                                         \
-    set_smem(sgemm_k<TA_, TB_>, sm);                                                           \
-    sgemm_k<TA_, TB_><<<grid, THREADS, sm, s>>>(m, n, k, (float)alpha, a, lda, b, ldb,          \
-                                                (float)beta, c, ldc, uplo_c, status);          \
+#define L(TA_, TB_)                                                                          \
+  do {                                                                                       \
+    if (fold) {                                                                              \
+      set_smem(sgemm_k<TA_, TB_, true>, sm);                                                 \
+      sgemm_k<TA_, TB_, true><<<grid, THREADS, sm, s>>>(m, n, k, (float)alpha, a, lda, b,     \
+                                                        ldb, (float)beta, c, ldc, uplo_c,    \
+                                                        status);                             \
+    } else {                                                                                 \
+      set_smem(sgemm_k<TA_, TB_, false>, sm);                                                \
+      sgemm_k<TA_, TB_, false><<<grid, THREADS, sm, s>>>(m, n, k, (float)alpha, a, lda, b,    \
+                                                         ldb, (float)beta, c, ldc, uplo_c,   \
+                                                         status);                            \
+    }                                                                                        \
   } while (0)
     if (!ta && !tb) L(false, false);
     else if (!ta && tb) L(false, true);

@@ -204,7 +204,10 @@ def test_trsv_trsm_golden(pla_session, golden, restated):
 
 
 @pytest.mark.parametrize("m,n,k", [(37, 29, 17), (300, 200, 128), (513, 257, 96), (1, 1, 1)])
-def test_gemm_all_transposes(pla_session, m, n, k):
+@pytest.mark.parametrize("alpha,beta", [(-1.0, 0.5), (1.0, 1.0), (0.75, -0.5), (-1.0, 0.0)])
+def test_gemm_all_transposes(pla_session, m, n, k, alpha, beta):
+    """alpha = +-1 starts the accumulators from beta C, other alphas read C in
+    the epilogue; beta = 0 must not read C at all (C is NaN there)."""
     from plapack_b200 import pla
     s = pla_session
     rng = np.random.default_rng(m * 7 + n)
@@ -212,15 +215,18 @@ def test_gemm_all_transposes(pla_session, m, n, k):
         for tb in (pla.PLA_NO_TRANSPOSE, pla.PLA_TRANSPOSE):
             A = rng.standard_normal((m, k) if ta == pla.PLA_NO_TRANSPOSE else (k, m))
             B = rng.standard_normal((k, n) if tb == pla.PLA_NO_TRANSPOSE else (n, k))
-            C = rng.standard_normal((m, n))
+            C = rng.standard_normal((m, n)) if beta != 0.0 else np.full((m, n), np.nan)
             a, b, c = s.matrix(*A.shape), s.matrix(*B.shape), s.matrix(m, n)
             s.put(a, A), s.put(b, B), s.put(c, C)
-            al, be = s.scalar(-1.0), s.scalar(0.5)
+            al, be = s.scalar(alpha), s.scalar(beta)
             pla.check(s.lib.PLA_Gemm(ta, tb, al, a, b, be, c), "Gemm")
             opA = A if ta == pla.PLA_NO_TRANSPOSE else A.T
             opB = B if tb == pla.PLA_NO_TRANSPOSE else B.T
-            ref = -opA @ opB + 0.5 * C
-            assert np.abs(s.get(c) - ref).max() <= 4 * k * EPS * (np.abs(opA) @ np.abs(opB)).max() + 1e-15
+            ref = alpha * (opA @ opB) + (beta * C if beta != 0.0 else 0.0)
+            got = s.get(c)
+            assert np.isfinite(got).all()
+            scale = (np.abs(opA) @ np.abs(opB)).max() + abs(beta) * np.nan_to_num(np.abs(C)).max()
+            assert np.abs(got - ref).max() <= 4 * k * EPS * scale + 1e-15
             s.free(a, b, c, al, be)
 
 
