@@ -3,13 +3,16 @@
 // SOLVERS/Cholesky/PLA_Chol.c:207-210).
 //
 // FP64: tensor-core DMMA (mma.sync m16n8k8 .f64; tcgen05 has no f64 kind).
-//   CTA tile 128 x 64, k-step 16, 8 warps as 4 (M) x 2 (N) with a 32 x 32
-//   warp tile; three cp.async stages; two CTAs per SM so one CTA's epilogue
-//   (the stores of C) overlaps the other's main loop.  The stages
-//   are stored permuted (rows g and g+8, k and k+4 side by side) so that
-//   each thread's fragment pairs are single 16-byte loads, and padded so
-//   those loads are bank-conflict free: A stage [16][128+4], B stage [64][16+8].
-// FP32: the same tiling with SIMT FFMA (used for float objects).
+//   CTA tile 64 x 64, k-step 16, 4 warps as 2 (M) x 2 (N) with a 32 x 32
+//   warp tile; two cp.async stages; four CTAs per SM, so that the start of
+//   one tile (the reads of C and the first stage) and the stores at its end
+//   overlap the other CTAs' main loops.  (Measured at M = N = 16384, K = 128:
+//   27.4 TF/s against 23.8 for 128 x 64 tiles with 2 CTAs per SM; persistent
+//   CTAs walking several tiles were slower.)  The stages are stored permuted
+//   (rows g and g+8, k and k+4 side by side) so that each thread's fragment
+//   pairs are single 16-byte loads, and padded so those loads are
+//   bank-conflict free: A stage [16][64+4], B stage [64][16+8].
+// FP32: SIMT FFMA with 128 x 64 tiles, 8 warps and three stages.
 #include <cstdint>
 
 #include "PLA.h"
@@ -17,9 +20,16 @@
 
 namespace {
 
-constexpr int BM = 128, BN = 64, BK = 16, STAGES = 3, THREADS = 256;
-constexpr int LDA_S = BM + 4;  // doubles per k-row of the A stage
-constexpr int LDB_S = BK + 8;  // per n-row of the B stage (16-byte loads conflict free)
+// tile shapes: BM x BN per CTA, BK per stage, THREADS threads
+template <int BM_, int BN_, int STAGES_, int THREADS_>
+struct Tile {
+  static constexpr int BM = BM_, BN = BN_, BK = 16, STAGES = STAGES_, THREADS = THREADS_;
+  static constexpr int LDA_S = BM + 4;  // elements per k-row of the A stage
+  static constexpr int LDB_S = BK + 8;  // per n-row of the B stage (16-byte loads conflict free)
+  static constexpr int STAGE = BK * LDA_S + BN * LDB_S;
+};
+using DT = Tile<64, 64, 2, 128>;   // FP64 tensor-core kernel
+using ST = Tile<128, 64, 3, 256>;  // FP32 SIMT kernel
 
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool valid) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -57,10 +67,12 @@ __device__ __forceinline__ int pos_k(int kk) {
 }
 
 // Stage one k-slab of op(A) (BM x BK) and op(B) (BK x BN) into shared memory.
-template <typename T, bool TA, bool TB, bool PERM = false>
+template <typename T, typename TL, bool TA, bool TB, bool PERM = false>
 __device__ __forceinline__ void load_stage(T *As, T *Bs, const T *A, long lda, const T *B,
                                            long ldb, int m, int n, int k, int m0, int n0,
                                            int k0, int tid) {
+  constexpr int BM = TL::BM, BN = TL::BN, BK = TL::BK, THREADS = TL::THREADS;
+  constexpr int LDA_S = TL::LDA_S, LDB_S = TL::LDB_S;
   // A: element (row, kk) of op(A) -> As[kk * LDA_S + row]
 #pragma unroll
   for (int it = 0; it < (BM * BK) / THREADS; it++) {
@@ -105,10 +117,12 @@ __device__ __forceinline__ bool keep(int uplo, int i, int j) {
 // reads of C are issued before the main loop, under the pipeline fill, and the
 // epilogue only stores.  Without FOLD the epilogue reads C.
 template <bool TA, bool TB, bool FOLD>
-__global__ void __launch_bounds__(THREADS, 2)
+__global__ void __launch_bounds__(DT::THREADS, 4)
 dgemm_k(int m, int n, int k, double alpha, const double *__restrict__ A, long lda,
         const double *__restrict__ B, long ldb, double beta, double *C, long ldc, int uplo,
         const int *status) {
+  constexpr int BM = DT::BM, BN = DT::BN, BK = DT::BK, STAGES = DT::STAGES;
+  constexpr int LDA_S = DT::LDA_S, LDB_S = DT::LDB_S;
   extern __shared__ __align__(16) double smem[];
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
   if (uplo == 'L' && m0 + BM - 1 < n0) return;  // tile strictly above the diagonal
@@ -117,7 +131,7 @@ dgemm_k(int m, int n, int k, double alpha, const double *__restrict__ A, long ld
   double *As = smem;                          // [STAGES][BK][LDA_S]
   double *Bs = smem + STAGES * BK * LDA_S;    // [STAGES][BN][LDB_S]
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;  // 2 x 2 warps
   const int g = lane >> 2, t = lane & 3;
 
   const double ab = FOLD && beta != 0.0 ? alpha * beta : 0.0;
@@ -141,7 +155,7 @@ dgemm_k(int m, int n, int k, double alpha, const double *__restrict__ A, long ld
 #pragma unroll
   for (int s = 0; s < STAGES - 1; s++) {
     if (s < nk)
-      load_stage<double, TA, TB, true>(As + s * BK * LDA_S, Bs + s * BN * LDB_S, A, lda, B, ldb,
+      load_stage<double, DT, TA, TB, true>(As + s * BK * LDA_S, Bs + s * BN * LDB_S, A, lda, B, ldb,
                                        m, n, k, m0, n0, s * BK, tid);
     cp_commit();
   }
@@ -152,7 +166,7 @@ dgemm_k(int m, int n, int k, double alpha, const double *__restrict__ A, long ld
       int ks = kt + STAGES - 1;
       if (ks < nk) {
         int slot = ks % STAGES;
-        load_stage<double, TA, TB, true>(As + slot * BK * LDA_S, Bs + slot * BN * LDB_S, A, lda,
+        load_stage<double, DT, TA, TB, true>(As + slot * BK * LDA_S, Bs + slot * BN * LDB_S, A, lda,
                                          B, ldb, m, n, k, m0, n0, ks * BK, tid);
       }
       cp_commit();
@@ -208,10 +222,12 @@ dgemm_k(int m, int n, int k, double alpha, const double *__restrict__ A, long ld
 
 // FP32 SIMT GEMM with the same staging; each thread computes an 8 x 4 block
 template <bool TA, bool TB, bool FOLD>
-__global__ void __launch_bounds__(THREADS, 2)
+__global__ void __launch_bounds__(ST::THREADS, 2)
 sgemm_k(int m, int n, int k, float alpha, const float *__restrict__ A, long lda,
         const float *__restrict__ B, long ldb, float beta, float *C, long ldc, int uplo,
         const int *status) {
+  constexpr int BM = ST::BM, BN = ST::BN, BK = ST::BK, STAGES = ST::STAGES;
+  constexpr int LDA_S = ST::LDA_S, LDB_S = ST::LDB_S;
   extern __shared__ __align__(16) float fsm[];
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
   if (uplo == 'L' && m0 + BM - 1 < n0) return;
@@ -234,7 +250,7 @@ sgemm_k(int m, int n, int k, float alpha, const float *__restrict__ A, long lda,
 #pragma unroll
   for (int s = 0; s < STAGES - 1; s++) {
     if (s < nk)
-      load_stage<float, TA, TB>(As + s * BK * LDA_S, Bs + s * BN * LDB_S, A, lda, B, ldb, m, n,
+      load_stage<float, ST, TA, TB>(As + s * BK * LDA_S, Bs + s * BN * LDB_S, A, lda, B, ldb, m, n,
                                 k, m0, n0, s * BK, tid);
     cp_commit();
   }
@@ -244,7 +260,7 @@ sgemm_k(int m, int n, int k, float alpha, const float *__restrict__ A, long lda,
     int ks = kt + STAGES - 1;
     if (ks < nk) {
       int slot = ks % STAGES;
-      load_stage<float, TA, TB>(As + slot * BK * LDA_S, Bs + slot * BN * LDB_S, A, lda, B, ldb,
+      load_stage<float, ST, TA, TB>(As + slot * BK * LDA_S, Bs + slot * BN * LDB_S, A, lda, B, ldb,
                                 m, n, k, m0, n0, ks * BK, tid);
     }
     cp_commit();
@@ -284,6 +300,8 @@ void set_smem(K kern, size_t bytes) {
 
 }  // namespace
 
+extern "C" int pla_k_gemm_tile_rows(int dt) { return dt == MPI_DOUBLE ? DT::BM : ST::BM; }
+
 extern "C" int pla_k_gemm(int dt, int transa, int transb, int m, int n, int k, double alpha,
                           const void *A, long lda, const void *B, long ldb, double beta, void *C,
                           long ldc, int uplo_c, const int *status, cudaStream_t s) {
@@ -296,9 +314,10 @@ extern "C" int pla_k_gemm(int dt, int transa, int transb, int m, int n, int k, d
   }
   const bool ta = transa != PLA_NO_TRANSPOSE, tb = transb != PLA_NO_TRANSPOSE;
   const bool fold = alpha == 1.0 || alpha == -1.0;
-  dim3 grid((m + BM - 1) / BM, (n + BN - 1) / BN);
   if (dt == MPI_DOUBLE) {
-    size_t sm = (size_t)STAGES * (BK * LDA_S + BN * LDB_S) * sizeof(double);
+    dim3 grid((m + DT::BM - 1) / DT::BM, (n + DT::BN - 1) / DT::BN);
+    const unsigned THREADS = DT::THREADS;
+    size_t sm = (size_t)DT::STAGES * DT::STAGE * sizeof(double);
     const double *a = (const double *)A, *b = (const double *)B;
     double *c = (double *)C;
 #define L(TA_, TB_)                                                                          \
@@ -319,7 +338,9 @@ extern "C" int pla_k_gemm(int dt, int transa, int transb, int m, int n, int k, d
     else L(true, true);
 #undef L
   } else if (dt == MPI_FLOAT) {
-    size_t sm = (size_t)STAGES * (BK * LDA_S + BN * LDB_S) * sizeof(float);
+    dim3 grid((m + ST::BM - 1) / ST::BM, (n + ST::BN - 1) / ST::BN);
+    const unsigned THREADS = ST::THREADS;
+    size_t sm = (size_t)ST::STAGES * ST::STAGE * sizeof(float);
     const float *a = (const float *)A, *b = (const float *)B;
     float *c = (float *)C;
 #define L(TA_, TB_)                                                                          \

@@ -10,13 +10,26 @@
 //
 // Layout: CTA b owns rows [b*R, b*R + R) of the r x w panel.  When they fit,
 // the CTA keeps its rows in shared memory for the whole panel; otherwise it
-// works in place in global memory (the panel is L2-resident).  Each column
-// costs one grid barrier: before it, every CTA publishes its best candidate
-// (|value|, row, the whole row) and the owner of row j publishes row j, so
-// after it every CTA can perform the swap and the update without reading a
-// row another CTA may be writing.  Candidate buffers alternate between two
-// slots by column parity.  The barrier is a monotonically increasing counter
-// with a bounded spin; on timeout the kernel records PLA_K_TIMEOUT and exits.
+// works in place in global memory (the panel is L2-resident).
+//
+// Exchange, one round per column: every CTA publishes a record -- its best
+// candidate (|value|, row) as two 64-bit words that each carry a generation
+// bit, the candidate's whole row, and, from the owner of the diagonal row,
+// that row -- and then gathers every CTA's record.  All CTAs pick the same
+// winner from the same records, so no barrier precedes the reads.  Records
+// alternate between two slots by column parity; the generation bit
+// ((j >> 1) & 1) ^ 1 tells the record of column j from that of column j - 2
+// in the same slot, and the slots are zeroed before each launch (generation
+// 0, which no record of column 0 or 1 has).  A CTA can only overwrite a slot
+// after every CTA has published the next column, that is after every CTA has
+// finished reading the slot.
+//
+// Lookahead inside the panel: after the pivot of column j a CTA updates only
+// column j + 1 of its rows, publishes the record of column j + 1 (its rows
+// carry the rest of the update, computed with the same fma as below, so the
+// published values are bitwise those the CTA stores later), and then updates
+// its remaining columns while the other CTAs publish.  Every wait is bounded;
+// on timeout the kernel records PLA_K_TIMEOUT and exits.
 #include <climits>
 #include <cstdio>
 #include <mutex>
@@ -27,33 +40,32 @@
 namespace {
 
 constexpr int kThreads = 256;
-constexpr long kSpinLimit = 4000000;  // ~0.5-1 s of polling, then give up
+constexpr long kSpinLimit = 4000000;  // polls of one record before giving up (~1 s)
 
-__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ void st_relaxed64(unsigned long long *p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
 
-// returns false when the wait timed out (status already recorded)
-__device__ bool grid_barrier(unsigned *bar, unsigned target, int *status, int *s_abort) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(bar, 1u);
-    long spins = 0;
-    while (ld_acquire(bar) < target) {
-      if (++spins > kSpinLimit || *(volatile int *)status != PLA_K_OK) {
-        atomicCAS(status, PLA_K_OK, PLA_K_TIMEOUT);
-        *s_abort = 1;
-        break;
-      }
-      __nanosleep(20);
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return *s_abort == 0;
+// record words: bit 63 the generation, below it |value| (>= 0, so its own
+// sign bit is free) or the row index
+template <typename T>
+__device__ __forceinline__ unsigned long long enc_val(T v, unsigned long long gen) {
+  if constexpr (sizeof(T) == 8)
+    return (gen << 63) | (unsigned long long)__double_as_longlong(v);
+  else
+    return (gen << 63) | (unsigned long long)__float_as_uint(v);
+}
+template <typename T>
+__device__ __forceinline__ T dec_val(unsigned long long w) {
+  if constexpr (sizeof(T) == 8)
+    return __longlong_as_double((long long)(w & ~(1ull << 63)));
+  else
+    return __uint_as_float((unsigned)(w & 0xffffffffull));
 }
 
 // (abs, idx) ordering: larger |value| first, then smaller index
@@ -88,15 +100,15 @@ __device__ void block_argmax(T &v, int &i, T *sv, int *si) {
   i = si[0];
 }
 
+// rec: [2 slots][P CTAs][2 words]; cand_row: [2][P][w]; top_row: [2][w]
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 1)
 panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *status,
-           int *zero_info, int row_base, unsigned *bar, T *cand_abs, int *cand_idx, T *cand_row,
-           T *top_row) {
+           int *zero_info, int row_base, unsigned long long *rec, T *cand_row, T *top_row) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ T s_v[32];
   __shared__ int s_i[32];
-  __shared__ int s_abort, s_p;
+  __shared__ int s_abort, s_p, s_q;
 
   const int P = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
   const int row0 = b * R;
@@ -120,58 +132,97 @@ panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *sta
   __syncthreads();
 #define E(i, c) S[(long)(i) + (long)(c) * lds]
 
-  unsigned phase = 0;
-  // publish the candidate for a column `col` into slot `par`
-  auto publish = [&](int col, int par) {
+  // Publish the record of column `col`.  With `pend` the rows still owe the
+  // rank-1 update of pivot col - 1 in the columns right of col (multiplier
+  // E(., col - 1), pivot row u): the published rows include it.
+  auto publish = [&](int col, bool pend) {
+    const int par = col & 1;
+    const unsigned long long gen = (unsigned long long)(((col >> 1) & 1) ^ 1);
     T best = T(-1);
     int bidx = INT_MAX;
-    int lo = max(col - row0, 0);
+    const int lo = max(col - row0, 0);
     for (int li = lo + tid; li < nrows; li += kThreads) {
       T v = fabs(E(li, col));
       if (better(v, row0 + li, best, bidx)) { best = v; bidx = row0 + li; }
     }
     block_argmax(best, bidx, s_v, s_i);
-    if (tid == 0) {
-      cand_abs[par * P + b] = best;
-      cand_idx[par * P + b] = bidx;
-    }
+    auto row_val = [&](int li, int c) -> T {
+      const T e = E(li, c);
+      return (pend && c > col) ? fma(E(li, col - 1), -u[c], e) : e;
+    };
     if (bidx != INT_MAX)
-      for (int c = tid; c < w; c += kThreads) cand_row[((long)par * P + b) * w + c] = E(bidx - row0, c);
+      for (int c = tid; c < w; c += kThreads)
+        cand_row[((long)par * P + b) * w + c] = row_val(bidx - row0, c);
     if (col >= row0 && col < row1)
-      for (int c = tid; c < w; c += kThreads) top_row[(long)par * w + c] = E(col - row0, c);
+      for (int c = tid; c < w; c += kThreads) top_row[(long)par * w + c] = row_val(col - row0, c);
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      unsigned long long *rp = rec + ((long)par * P + b) * 2;
+      const bool none = bidx == INT_MAX;  // no candidate: every entry is NaN
+      st_relaxed64(rp, enc_val<T>(none ? T(0) : best, gen));
+      st_relaxed64(rp + 1, (gen << 63) | (unsigned)(none ? INT_MAX : bidx));
+    }
   };
 
-  publish(0, 0);
-  if (!grid_barrier(bar, ++phase * P, status, &s_abort)) return;
-
-  for (int j = 0; j < w; j++) {
-    const int par = j & 1;
-    // winner over all CTAs' candidates
+  // Gather the records of column `col` into (s_p = winning row or INT_MAX,
+  // s_q = its CTA); false when a wait gave up.
+  auto gather = [&](int col) -> bool {
+    const int par = col & 1;
+    const unsigned long long gen = (unsigned long long)(((col >> 1) & 1) ^ 1);
     if (tid < 32) {
       T bv = T(-1);
-      int bi = INT_MAX, bb = 0;
-      for (int q = tid; q < P; q += 32) {
-        // other CTAs wrote these: read through L2, never a stale L1 line
-        T v = __ldcg(&cand_abs[par * P + q]);
-        int ix = __ldcg(&cand_idx[par * P + q]);
-        if (better(v, ix, bv, bi)) { bv = v; bi = ix; bb = q; }
+      int bi = INT_MAX, bq = 0;
+      bool ok = true;
+      for (int q = tid; q < P && ok; q += 32) {
+        const unsigned long long *rp = rec + ((long)par * P + q) * 2;
+        unsigned long long w0 = 0, w1 = 0;
+        for (long spins = 0;; spins++) {
+          w0 = ld_acquire64(rp);
+          w1 = ld_acquire64(rp + 1);
+          if ((w0 >> 63) == gen && (w1 >> 63) == gen) break;
+          if (spins > kSpinLimit || *(volatile int *)status != PLA_K_OK) {
+            ok = false;
+            break;
+          }
+          __nanosleep(20);
+        }
+        if (!ok) break;
+        const T v = dec_val<T>(w0);
+        const int ix = (int)(unsigned)(w1 & 0xffffffffull);
+        if (better(v, ix, bv, bi)) { bv = v; bi = ix; bq = q; }
       }
+      const bool all_ok = __all_sync(0xffffffffu, ok);
       for (int o = 16; o; o >>= 1) {
         T ov = __shfl_down_sync(0xffffffffu, bv, o);
         int oi = __shfl_down_sync(0xffffffffu, bi, o);
-        int ob = __shfl_down_sync(0xffffffffu, bb, o);
-        if (better(ov, oi, bv, bi)) { bv = ov; bi = oi; bb = ob; }
+        int oq = __shfl_down_sync(0xffffffffu, bq, o);
+        if (better(ov, oi, bv, bi)) { bv = ov; bi = oi; bq = oq; }
       }
-      if (tid == 0) { s_p = bi; s_i[0] = bb; }
+      if (tid == 0) {
+        if (!all_ok) {
+          atomicCAS(status, PLA_K_OK, PLA_K_TIMEOUT);
+          s_abort = 1;
+        }
+        s_p = bi;
+        s_q = bq;
+      }
     }
     __syncthreads();
+    return s_abort == 0;
+  };
+
+  publish(0, false);
+  for (int j = 0; j < w; j++) {
+    if (!gather(j)) return;
+    const int par = j & 1;
     // A column of NaNs has no candidate (NaN never compares greater): keep
     // row j as its own pivot, whose contents the owner of row j published.
     const bool none = s_p == INT_MAX;
-    const int p = none ? j : s_p, wb = s_i[0];
+    const int p = none ? j : s_p, wq = s_q;
     for (int c = tid; c < w; c += kThreads)
       u[c] = none ? __ldcg(&top_row[(long)par * w + c])
-                  : __ldcg(&cand_row[((long)par * P + wb) * w + c]);
+                  : __ldcg(&cand_row[((long)par * P + wq) * w + c]);
     __syncthreads();
     // the interchange of rows j and p over the panel width
     if (j >= row0 && j < row1)
@@ -183,18 +234,23 @@ panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *sta
       if (zero_info && u[j] == T(0)) atomicCAS(zero_info, 0, row_base + j + 1);
     }
     __syncthreads();
-    // scale by the reciprocal, then the rank-1 update of the columns to the right
+    // scale by the reciprocal and update the next column first ...
     const T inv = T(1) / u[j];
     const int lo = max(j + 1 - row0, 0);
     for (int li = lo + tid; li < nrows; li += kThreads) {
-      T l = E(li, j) * inv;
+      const T l = E(li, j) * inv;
       E(li, j) = l;
-      for (int c = j + 1; c < w; c++) E(li, c) = fma(l, -u[c], E(li, c));
+      if (j + 1 < w) E(li, j + 1) = fma(l, -u[j + 1], E(li, j + 1));
     }
     if (j + 1 < w) {
       __syncthreads();
-      publish(j + 1, par ^ 1);
-      if (!grid_barrier(bar, ++phase * P, status, &s_abort)) return;
+      publish(j + 1, true);
+      // ... then the rest of the rank-1 update while the others publish
+      for (int li = lo + tid; li < nrows; li += kThreads) {
+        const T l = E(li, j);
+        for (int c = j + 2; c < w; c++) E(li, c) = fma(l, -u[c], E(li, c));
+      }
+      __syncthreads();
     }
   }
   if (use_smem) {
@@ -205,6 +261,21 @@ panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *sta
     }
   }
 #undef E
+}
+
+// workspace layout for P CTAs and width w: the record slots (zeroed before
+// every launch), the candidate rows and the diagonal rows
+struct Layout {
+  size_t rec_bytes, off_row, off_top, total;
+};
+template <typename T>
+Layout layout(int P, int w) {
+  Layout l;
+  l.rec_bytes = ((size_t)2 * P * 2 * sizeof(unsigned long long) + 255) & ~(size_t)255;
+  l.off_row = l.rec_bytes;
+  l.off_top = l.off_row + (size_t)2 * P * w * sizeof(T);
+  l.total = l.off_top + (size_t)2 * w * sizeof(T);
+  return l;
 }
 
 struct Workspace {
@@ -248,23 +319,17 @@ int launch(int r, int w, void *A, long lda, int *piv, int *status, int *zero_inf
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, panel_lu_k<T>, kThreads, dyn);
   if (per_sm * g_sms < P) return (int)cudaErrorCooperativeLaunchTooLarge;
-  // workspace: barrier | cand_abs[2P] | cand_idx[2P] | cand_row[2P*w] | top_row[2w]
-  size_t off_abs = 256, off_idx = off_abs + 2 * P * sizeof(T);
-  size_t off_row = (off_idx + 2 * P * sizeof(int) + 255) & ~(size_t)255;
-  size_t off_top = off_row + (size_t)2 * P * w * sizeof(T);
-  size_t total = off_top + (size_t)2 * w * sizeof(T);
-  char *ws = (char *)workspace(total);
+  const Layout lay = layout<T>(P, w);
+  char *ws = (char *)workspace(lay.total);
   if (!ws) return (int)cudaErrorMemoryAllocation;
-  cudaError_t e = cudaMemsetAsync(ws, 0, 256, s);
+  cudaError_t e = cudaMemsetAsync(ws, 0, lay.rec_bytes, s);
   if (e) return (int)e;
-  unsigned *bar = (unsigned *)ws;
-  T *cand_abs = (T *)(ws + off_abs);
-  int *cand_idx = (int *)(ws + off_idx);
-  T *cand_row = (T *)(ws + off_row);
-  T *top_row = (T *)(ws + off_top);
+  unsigned long long *rec = (unsigned long long *)ws;
+  T *cand_row = (T *)(ws + lay.off_row);
+  T *top_row = (T *)(ws + lay.off_top);
   T *Ap = (T *)A;
-  void *args[] = {&Ap, &lda, &r, &w, &R, &use_smem, &piv, &status, &zero_info, &row_base, &bar,
-                  &cand_abs, &cand_idx, &cand_row, &top_row};
+  void *args[] = {&Ap, &lda, &r, &w, &R, &use_smem, &piv, &status, &zero_info, &row_base, &rec,
+                  &cand_row, &top_row};
   e = cudaLaunchCooperativeKernel((void *)panel_lu_k<T>, dim3(P), dim3(kThreads), args, dyn, s);
   pla_k_count(1);
   return (int)e;
@@ -294,23 +359,21 @@ extern "C" void pla_kernels_release(void) {
 // is owned by another allocator (a framework's caching allocator that has
 // reserved the device, for instance), and memory-budgeted or real-time
 // services that forbid allocation once they are running.  For them the panel
-// kernel's workspace -- the grid-barrier counter and the per-CTA pivot
-// candidates -- lives in the fixed device array below instead of memory the
-// library allocates.  The array holds the workspace of at most kNoAllocCtas
-// CTAs for panels of at most kNoAllocWidth columns in double precision
-// (about 334 KB); every GPU that loads the library keeps it until the process
-// exits.  Every call shares it, so calls whose kernels overlap on the GPU (on
-// different streams, or from different host threads) race.
+// kernel's workspace -- the per-CTA pivot records and candidate rows -- lives
+// in the fixed device array below instead of memory the library allocates.
+// The array holds the workspace of at most kNoAllocCtas CTAs for panels of at
+// most kNoAllocWidth columns in double precision (about 335 KB); every GPU
+// that loads the library keeps it until the process exits.  Every call shares
+// it, so calls whose kernels overlap on the GPU (on different streams, or from
+// different host threads) race.
 namespace {
 constexpr int kNoAllocCtas = 160;
 constexpr int kNoAllocWidth = 128;
-constexpr size_t kNoAllocAbs = 256;  // bytes [0, 256): the barrier counter
-constexpr size_t kNoAllocIdx = kNoAllocAbs + 2 * kNoAllocCtas * sizeof(double);
-constexpr size_t kNoAllocRow =
-    (kNoAllocIdx + 2 * kNoAllocCtas * sizeof(int) + 255) & ~(size_t)255;
-constexpr size_t kNoAllocTop =
-    kNoAllocRow + (size_t)2 * kNoAllocCtas * kNoAllocWidth * sizeof(double);
-constexpr size_t kNoAllocBytes = kNoAllocTop + (size_t)2 * kNoAllocWidth * sizeof(double);
+// the double-precision layout at the limits; a float panel needs less
+constexpr size_t kNoAllocRec = ((size_t)2 * kNoAllocCtas * 2 * 8 + 255) & ~(size_t)255;
+constexpr size_t kNoAllocBytes = kNoAllocRec +
+                                 (size_t)2 * kNoAllocCtas * kNoAllocWidth * sizeof(double) +
+                                 (size_t)2 * kNoAllocWidth * sizeof(double);
 }  // namespace
 
 static __device__ __align__(256) unsigned char g_panel_scratch[kNoAllocBytes];
@@ -362,20 +425,20 @@ int launch_noalloc(int r, int w, T *A, long lda, int *piv, int *status, cudaStre
   char *ws = nullptr;
   int rc = noalloc_scratch(&ws);
   if (rc) return rc;
-  // the barrier counter must start at zero; the candidate slots are written
-  // before they are read, so the last call's contents are harmless
-  e = cudaMemsetAsync(ws, 0, kNoAllocAbs, s);
+  // the record slots must start at zero (their generation bits); the
+  // candidate rows are written before they are read, so the last call's
+  // contents are harmless
+  const Layout lay = layout<T>(P, w);
+  if (lay.total > kNoAllocBytes) return (int)cudaErrorInvalidValue;
+  e = cudaMemsetAsync(ws, 0, lay.rec_bytes, s);
   if (e != cudaSuccess) return (int)e;
-  unsigned *bar = (unsigned *)ws;
-  T *cand_abs = (T *)(ws + kNoAllocAbs);
-  int *cand_idx = (int *)(ws + kNoAllocIdx);
-  T *cand_row = (T *)(ws + kNoAllocRow);
-  T *top_row = (T *)(ws + kNoAllocTop);
+  unsigned long long *rec = (unsigned long long *)ws;
+  T *cand_row = (T *)(ws + lay.off_row);
+  T *top_row = (T *)(ws + lay.off_top);
   int *zero_info = nullptr;
   int row_base = 0;
-  void *args[] = {&A,   &lda,        &r,         &w,        &R,         &use_smem,
-                  &piv, &status,     &zero_info, &row_base, &bar,       &cand_abs,
-                  &cand_idx, &cand_row, &top_row};
+  void *args[] = {&A,        &lda,      &r,   &w,        &R,        &use_smem, &piv,
+                  &status,   &zero_info, &row_base, &rec, &cand_row, &top_row};
   e = cudaLaunchCooperativeKernel((void *)panel_lu_k<T>, dim3(P), dim3(kThreads), args, dyn, s);
   pla_k_count(1);
   return (int)e;

@@ -64,7 +64,7 @@ double scalar_value(PLA_Obj s) {
   char tmp[16];
   const char *p = at(s, 0, 0);
   if (!s->base->on_host) {
-    cudaMemcpy(tmp, p, s->base->esize, cudaMemcpyDeviceToHost);
+    d2h(tmp, p, s->base->esize);
     p = tmp;
   }
   switch (s->base->datatype) {
@@ -81,10 +81,18 @@ struct Scratch {
   void *ptr = nullptr;
   size_t bytes = 0;
 };
-Scratch g_scratch[16];
+constexpr int kScratchSlots = 24;
+Scratch g_scratch[kScratchSlots];
 }  // namespace
 
+cudaError_t d2h(void *dst, const void *src, size_t bytes) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, stream());
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(stream());
+}
+
 void *scratch(int slot, size_t bytes) {
+  if (slot < 0 || slot >= kScratchSlots) return nullptr;
   Scratch &s = g_scratch[slot];
   if (s.bytes >= bytes && s.ptr) return s.ptr;
   if (s.ptr) {

@@ -92,6 +92,10 @@ int fail(const char *message, int line, const char *file);
 int cuda_fail(cudaError_t e, int line, const char *file);
 void warn(const char *message);
 
+// device -> host copy ordered after everything queued on the library stream
+// (which is non-blocking: a plain cudaMemcpy would not wait for it)
+cudaError_t d2h(void *dst, const void *src, size_t bytes);
+
 // device scratch owned by the library (grown on demand, freed at PLA_Finalize)
 void *scratch(int slot, size_t bytes);
 void release_scratch();

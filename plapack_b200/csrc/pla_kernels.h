@@ -52,6 +52,9 @@ int pla_k_laswp_rows(int dt, void *B, long ldb, int ncols, int npiv, const int *
 
 /* ---- GEMM: C := alpha op(A) op(B) + beta C; uplo_c = 0 full, 'L' lower only,
  * 'U' upper only (SYRK-shaped updates). */
+/* rows of C one CTA of pla_k_gemm covers: a GEMM whose C is also its B is
+ * safe only when m is at most this (every column tile then has one CTA) */
+int pla_k_gemm_tile_rows(int dt);
 int pla_k_gemm(int dt, int transa, int transb, int m, int n, int k, double alpha,
                const void *A, long lda, const void *B, long ldb, double beta, void *C,
                long ldc, int uplo_c, const int *status, cudaStream_t s);

@@ -51,9 +51,9 @@ int gemm_t(int t) { return t == PLA_NO_TRANSPOSE ? PLA_NO_TRANSPOSE : PLA_TRANSP
 
 // Left-side solve with one diagonal block of order kb <= 128 against `other`
 // columns.  For many columns the block is inverted once (substitution against
-// the identity) and applied as a GEMM, B := alpha inv(op(T)) B; the GEMM may
-// run in place because its M extent (kb) is a single 128-row tile, so every
-// column tile of B is read and written by one CTA only.
+// the identity) and applied as a GEMM, B := alpha inv(op(T)) B.  The GEMM runs
+// in place when kb rows fit one CTA tile of the GEMM (every column tile of B
+// is then read and written by one CTA only); otherwise B is first copied.
 int trsm_left_block(int dt, char uplo, char trans, char diag, int kb, int other, double alpha,
                     const char *T, long ldt, char *B, long ldb, const int *status) {
   if (other < 1024)
@@ -66,8 +66,17 @@ int trsm_left_block(int dt, char uplo, char trans, char diag, int kb, int other,
   if (!r) r = pla_k_fill(dt, 1, kb, inv, kb + 1, 1.0, stream());  // the diagonal
   if (!r) r = pla_k_trsm_small(dt, 'L', uplo, trans, diag, kb, kb, 1.0, T, ldt, inv, kb, status,
                                stream());
-  if (!r) r = pla_k_gemm(dt, PLA_NO_TRANSPOSE, PLA_NO_TRANSPOSE, kb, other, kb, alpha, inv, kb, B,
-                         ldb, 0.0, B, ldb, 0, status, stream());
+  const char *src = B;
+  long lds = ldb;
+  if (!r && kb > pla_k_gemm_tile_rows(dt)) {
+    char *copy = (char *)scratch(17, (size_t)kb * other * es);
+    if (!copy) return (int)cudaErrorMemoryAllocation;
+    r = pla_k_copy(dt, PLA_NO_TRANSPOSE, kb, other, B, ldb, copy, kb, stream());
+    src = copy;
+    lds = kb;
+  }
+  if (!r) r = pla_k_gemm(dt, PLA_NO_TRANSPOSE, PLA_NO_TRANSPOSE, kb, other, kb, alpha, inv, kb, src,
+                         lds, 0.0, B, ldb, 0, status, stream());
   return r;
 }
 
@@ -335,7 +344,7 @@ int PLA_Apply_pivots_to_rows(PLA_Obj A, PLA_Obj ipiv) {
   {
     // a pivot vector from the caller must name rows of A (the kernel trusts it)
     std::vector<int> h(npiv);
-    PLA_CUDA(cudaMemcpy(h.data(), at(ipiv, 0, 0), npiv * sizeof(int), cudaMemcpyDefault));
+    PLA_CUDA(d2h(h.data(), at(ipiv, 0, 0), npiv * sizeof(int)));
     for (int i = 0; i < npiv; i++)
       if (h[i] < 0 || i + h[i] >= A->length) PLA_FAIL("pivot entry outside the rows of A");
   }
@@ -350,7 +359,7 @@ int PLA_Apply_pivots_to_columns_in_reverse(PLA_Obj A, PLA_Obj ipiv) {
   if (ipiv->objtype != PLA_MVECTOR) PLA_FAIL("not yet implemented");
   int npiv = std::min(vlen(ipiv), A->width);
   std::vector<int> h(npiv);
-  PLA_CUDA(cudaMemcpy(h.data(), at(ipiv, 0, 0), npiv * sizeof(int), cudaMemcpyDeviceToHost));
+  PLA_CUDA(d2h(h.data(), at(ipiv, 0, 0), npiv * sizeof(int)));
   for (int j = npiv - 1; j >= 0; j--) {
     int p = j + h[j];
     if (p == j) continue;
