@@ -67,6 +67,7 @@ long PLA_B200_kernel_launches(void);
 #define PLA_B200_PREC_BF16   1   /* trailing update in bf16, fp32 accumulate */
 #define PLA_B200_PREC_FP16   2   /* trailing update in fp16, fp32 accumulate */
 #define PLA_B200_PREC_FP32   3   /* fp32 throughout                          */
+#define PLA_B200_PREC_FP64   4   /* FP64 factors (the plain PLA_LU / PLA_Chol) */
 #define PLA_B200_IR_LU       1   /* classic iterative refinement             */
 #define PLA_B200_IR_GMRES    2   /* GMRES-IR                                 */
 
@@ -76,6 +77,12 @@ typedef struct {
   int max_iterations;   /* outer refinement steps (default 50)              */
   int gmres_restart;    /* inner GMRES iterations per step (default 30)     */
   int nb;               /* block size of the low-precision factorization; 0 = nb_alg */
+  int escalate;         /* 1 (default): when the refinement stagnates (less than
+                           a halving of the backward error twice in a row, a
+                           non-finite iterate, max_iterations reached) or the
+                           low-precision Cholesky breaks down, refactor one
+                           precision higher (BF16/FP16 -> FP32 -> FP64) and
+                           continue from the current iterate                 */
   double tol;           /* target backward error; <= 0 selects n * 2^-53    */
 } PLA_Mixed_params;
 
@@ -87,6 +94,8 @@ typedef struct {
   double backward_error;  /* max over columns                               */
   double factor_ms;       /* device time of the factorization               */
   double refine_ms;       /* device time of the refinement                  */
+  int precision_used;     /* PLA_B200_PREC_* of the factors that finished   */
+  int factorizations;     /* 1 + the number of escalations                  */
 } PLA_Mixed_report;
 
 void PLA_Mixed_params_default(PLA_Mixed_params *p);
@@ -104,7 +113,7 @@ int PLA_Pos_def_solve_mixed(PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *params
  * a bounded wait in the kernel gave up.
  * For callers that cannot let the library call cudaMalloc -- programs whose
  * GPU memory belongs to another allocator, or services that forbid allocation
- * while running: the kernel's workspace is a fixed array of about 334 KB in
+ * while running: the kernel's workspace is a fixed array of about 335 KB in
  * device memory, present on every GPU that loads the library until the
  * process exits, instead of memory the library allocates.  Limit: w <= 128
  * (larger panels return PLA_ERROR with a message in PLA_Last_error).

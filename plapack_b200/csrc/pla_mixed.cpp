@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <vector>
 
 #include "pla_internal.h"
@@ -23,6 +24,8 @@
 using namespace pla;
 
 namespace pla {
+int lu_on_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, int *zero_info_host);
+int chol_on_device(int dt, int n, char *A, long lda, int nb, int *info_host);
 int trsm_device(int dt, char side, char uplo, char trans, char diag, int nt, int other,
                 double alpha, const char *T, long ldt, char *B, long ldb);
 int panel_lu(int dt, int r, int b, char *P, long lda, int *piv, int *status, int *zero_info,
@@ -38,13 +41,14 @@ namespace {
   } while (0)
 
 enum Slots { kSlotA32 = 4, kSlotL = 5, kSlotU = 6, kSlotPiv = 7, kSlotVec = 8, kSlotWork = 9,
-             kSlotV = 10, kSlotSt = 11 };
+             kSlotV = 10, kSlotSt = 11, kSlotA64 = 16 };
 
 long round_up(long v, long m) { return (v + m - 1) / m * m; }
 
 struct Factor {
   int n = 0, ld = 0, prec = 0, kind = 0;  // kind 0 = LU, 1 = Cholesky
-  float *a = nullptr;
+  float *a = nullptr;     // fp32 factors (BF16, FP16, FP32)
+  double *a64 = nullptr;  // FP64 factors (FP64)
   int *piv = nullptr;
   int *status = nullptr;  // [status, info, zero_info]
   // inverses of the 128 x 128 diagonal blocks of the two triangular factors
@@ -157,10 +161,35 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
   return PLA_SUCCESS;
 }
 
-// out (fp64, n x nrhs, ldo) := M^{-1} v (fp64, ldv) with the fp32 factors
+// FP64 factors: the plain blocked PLA_LU / PLA_Chol loops on a copy of A.
+// Returns PLA_SUCCESS; the LU's first exact zero pivot or the failing
+// Cholesky column goes to *info.
+int factor_fp64(Factor &F, const double *A, long lda, int *info) {
+  const int n = F.n;
+  F.a64 = (double *)scratch(kSlotA64, (size_t)F.ld * n * sizeof(double));
+  if (!F.a64) PLA_FAIL("cannot allocate the FP64 factors");
+  K(pla_k_copy(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, n, A, lda, F.a64, F.ld, stream()));
+  const int nb = 128;
+  if (F.kind == 0) return lu_on_device(MPI_DOUBLE, n, n, (char *)F.a64, F.ld, F.piv, nb, info);
+  return chol_on_device(MPI_DOUBLE, n, (char *)F.a64, F.ld, nb, info);
+}
+
+// out (fp64, n x nrhs, ldo) := M^{-1} v (fp64, ldv) with the factors
 int precond(const Factor &F, const double *v, long ldv, double *out, long ldo, int nrhs,
             float *t32) {
   const int n = F.n;
+  if (F.prec == PLA_B200_PREC_FP64) {
+    K(pla_k_copy(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, nrhs, v, ldv, out, ldo, stream()));
+    if (F.kind == 0) {
+      K(pla_k_laswp_rows(MPI_DOUBLE, out, ldo, nrhs, n, F.piv, stream()));
+      K(pla_k_trsv_blocked(MPI_DOUBLE, 'L', 'N', 'U', n, nrhs, F.a64, F.ld, out, ldo, stream()));
+      K(pla_k_trsv_blocked(MPI_DOUBLE, 'U', 'N', 'N', n, nrhs, F.a64, F.ld, out, ldo, stream()));
+    } else {
+      K(pla_k_trsv_blocked(MPI_DOUBLE, 'L', 'N', 'N', n, nrhs, F.a64, F.ld, out, ldo, stream()));
+      K(pla_k_trsv_blocked(MPI_DOUBLE, 'L', 'T', 'N', n, nrhs, F.a64, F.ld, out, ldo, stream()));
+    }
+    return PLA_SUCCESS;
+  }
   K(pla_k_convert(MPI_DOUBLE, v, ldv, MPI_FLOAT, t32, n, n, nrhs, stream()));
   if (F.kind == 0) K(pla_k_laswp_rows(MPI_FLOAT, t32, n, nrhs, n, F.piv, stream()));
   const char u1 = 'L', t1 = 'N', d1 = F.kind == 0 ? 'U' : 'N';
@@ -290,6 +319,12 @@ int gmres(const Factor &F, const double *A, long lda, const double *r, double *d
   return PLA_SUCCESS;
 }
 
+// the next precision up when the refinement stagnates (0: none left)
+int escalated(int prec) {
+  if (prec == PLA_B200_PREC_FP64) return 0;
+  return prec == PLA_B200_PREC_FP32 ? PLA_B200_PREC_FP64 : PLA_B200_PREC_FP32;
+}
+
 int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
                 PLA_Mixed_report *rep) {
   if (!valid(A) || !valid(B)) PLA_FAIL("invalid object");
@@ -300,37 +335,28 @@ int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
   if (pin) p = *pin;
   if (p.max_iterations <= 0) p.max_iterations = 50;
   if (p.gmres_restart <= 0) p.gmres_restart = 30;
+  if (p.precision < PLA_B200_PREC_BF16 || p.precision > PLA_B200_PREC_FP64)
+    PLA_FAIL("unknown precision");
   const int n = A->length, nrhs = B->width;
   if (n == 0 || nrhs == 0) {
-    if (rep) *rep = PLA_Mixed_report{1, 0, 0, 0, 0.0, 0.0, 0.0};
+    if (rep) *rep = PLA_Mixed_report{1, 0, 0, 0, 0.0, 0.0, 0.0, p.precision, 0};
     return PLA_SUCCESS;
   }
   if (nrhs > 16) PLA_FAIL("at most 16 right-hand sides per mixed-precision solve");
-  int nb = p.nb;
-  if (nb <= 0) PLA_Environ_nb_alg(PLA_OP_PAN_PAN, A->templ, &nb);
-  if (p.precision != PLA_B200_PREC_FP32) {
-    nb = std::max(64, nb / 64 * 64);
-    nb = std::min(nb, kind == 0 ? 256 : 128);
-  } else if (kind == 1) {
-    nb = std::min(nb, 128);
-  }
+  int nb0 = p.nb;
+  if (nb0 <= 0) PLA_Environ_nb_alg(PLA_OP_PAN_PAN, A->templ, &nb0);
   const double tol = p.tol > 0 ? p.tol : n * std::ldexp(1.0, -53);
   const double *Ad = (const double *)at(A, 0, 0);
   const long lda = ld(A);
   double *Bd = (double *)at(B, 0, 0);
   const long ldb = ld(B);
 
-  Factor F;
-  F.n = n;
-  F.ld = (int)round_up(n, 32);
-  F.prec = p.precision;
-  F.kind = kind;
-  F.a = (float *)scratch(kSlotA32, (size_t)F.ld * n * sizeof(float));
-  F.piv = (int *)scratch(kSlotPiv, (size_t)n * sizeof(int) + 64);
-  F.status = (int *)scratch(kSlotSt, 64);
+  const long ldf = round_up(n, 32);
+  int *piv = (int *)scratch(kSlotPiv, (size_t)n * sizeof(int) + 64);
+  int *status = (int *)scratch(kSlotSt, 64);
   const size_t vec = (size_t)n * 16;
   double *X = (double *)scratch(kSlotVec, (5 * vec + 64) * sizeof(double));
-  if (!F.a || !F.piv || !F.status || !X) PLA_FAIL("cannot allocate the mixed-precision workspace");
+  if (!piv || !status || !X) PLA_FAIL("cannot allocate the mixed-precision workspace");
   double *R = X + vec, *Dv = R + vec, *Bsave = Dv + vec, *tmp = Bsave + vec;
   float *t32b = (float *)scratch(kSlotWork + 3, vec * sizeof(float) + 256);
   double *work = (double *)scratch(kSlotWork, std::max(pla_k_residual_work(n, n, nrhs),
@@ -342,70 +368,125 @@ int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
   }
   if (!t32b || !work || (p.refinement == PLA_B200_IR_GMRES && !V))
     PLA_FAIL("cannot allocate the refinement workspace");
-  PLA_CUDA(cudaMemsetAsync(F.status, 0, 64, stream()));
 
-  PLA_Mixed_report r{};
-  // ---- factorization ----
-  {
-    EventTimer t;
-    int rc = factor_mixed(F, Ad, lda, nb);
-    if (rc) return rc;
-    r.factor_ms = t.stop();
-  }
-  int hst[3];
-  PLA_CUDA(cudaMemcpy(hst, F.status, sizeof hst, cudaMemcpyDeviceToHost));
-  if (hst[0] == PLA_K_TIMEOUT) PLA_FAIL("factorization: a bounded wait timed out");
-  r.info = kind == 0 ? hst[2] : (hst[0] == PLA_K_NOT_SPD ? hst[1] : 0);
-  if (kind == 1 && r.info) {
-    if (rep) *rep = r;
-    return r.info;  // not positive definite in low precision
-  }
-
-  // ---- refinement ----
-  EventTimer t;
-
-  {
-    int rc0 = prepare_solves(F);
-    if (rc0) return rc0;
-  }
+  // norms of A and b, and a copy of b (B receives x at the end)
   Norms nm;
   K(pla_k_residual(n, n, 1, Ad, lda, nullptr, n, nullptr, n, tmp, n, 1, work, stream()));
   nm.a_inf = host_max(tmp, n);
   K(pla_k_col_abs_max(MPI_DOUBLE, n, nrhs, Bd, ldb, tmp, stream()));
   nm.b_inf.resize(nrhs);
-  PLA_CUDA(cudaMemcpy(nm.b_inf.data(), tmp, nrhs * sizeof(double), cudaMemcpyDeviceToHost));
-  // keep b, start from x = M^{-1} b
+  PLA_CUDA(d2h(nm.b_inf.data(), tmp, nrhs * sizeof(double)));
   K(pla_k_copy(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, nrhs, Bd, ldb, Bsave, n, stream()));
-  int rc = precond(F, Bsave, n, X, n, nrhs, t32b);
-  if (rc) return rc;
-  std::vector<double> eta;
-  int it = 0;
-  for (;; it++) {
-    K(pla_k_residual(n, n, nrhs, Ad, lda, X, n, Bsave, n, R, n, 0, work, stream()));
-    rc = backward_errors(n, nrhs, R, n, X, n, nm, tmp, eta);
-    if (rc) return rc;
-    double worst = *std::max_element(eta.begin(), eta.end());
-    r.backward_error = worst;
-    if (worst <= tol || !(worst == worst)) break;
-    if (it >= p.max_iterations) break;
-    if (p.refinement == PLA_B200_IR_GMRES) {
-      for (int j = 0; j < nrhs; j++) {
-        rc = gmres(F, Ad, lda, R + (long)j * n, Dv + (long)j * n, p.gmres_restart, 1e-8, V, w,
-                   tmp, t32b, work, &r.inner_iterations);
+
+  PLA_Mixed_report r{};
+  r.backward_error = std::numeric_limits<double>::infinity();
+  bool have_x = false;
+  double refine_ms = 0;
+  for (int prec = p.precision; prec;) {
+    Factor F;
+    F.n = n;
+    F.ld = (int)ldf;
+    F.prec = prec;
+    F.kind = kind;
+    F.piv = piv;
+    F.status = status;
+    PLA_CUDA(cudaMemsetAsync(status, 0, 64, stream()));
+    // ---- factorization ----
+    int info = 0;
+    {
+      EventTimer t;
+      if (prec == PLA_B200_PREC_FP64) {
+        int rc = factor_fp64(F, Ad, lda, &info);
+        if (rc) return rc;
+      } else {
+        F.a = (float *)scratch(kSlotA32, (size_t)ldf * n * sizeof(float));
+        if (!F.a) PLA_FAIL("cannot allocate the fp32 working copy");
+        int nb = nb0;
+        if (prec != PLA_B200_PREC_FP32) {
+          nb = std::max(64, nb / 64 * 64);
+          nb = std::min(nb, kind == 0 ? 256 : 128);
+        } else if (kind == 1) {
+          nb = std::min(nb, 128);
+        }
+        int rc = factor_mixed(F, Ad, lda, nb);
+        if (rc) return rc;
+        int hst[3];
+        PLA_CUDA(d2h(hst, status, sizeof hst));  // after the factorization's kernels
+        if (hst[0] == PLA_K_TIMEOUT) PLA_FAIL("factorization: a bounded wait timed out");
+        info = kind == 0 ? hst[2] : (hst[0] == PLA_K_NOT_SPD ? hst[1] : 0);
+      }
+      r.factor_ms += t.stop();
+    }
+    r.factorizations++;
+    r.precision_used = prec;
+    r.info = info;
+    if (kind == 1 && info) {  // not positive definite at this precision
+      if (!p.escalate || !escalated(prec)) break;
+      prec = escalated(prec);
+      continue;
+    }
+
+    // ---- refinement ----
+    EventTimer t;
+    if (prec != PLA_B200_PREC_FP64) {
+      int rc0 = prepare_solves(F);
+      if (rc0) return rc0;
+    }
+    if (!have_x) {  // start from x = M^{-1} b
+      int rc = precond(F, Bsave, n, X, n, nrhs, t32b);
+      if (rc) return rc;
+      have_x = true;
+    }
+    std::vector<double> eta;
+    double prev = std::numeric_limits<double>::infinity();
+    int slow = 0, it = 0;
+    bool stalled = false;
+    for (;; it++) {
+      K(pla_k_residual(n, n, nrhs, Ad, lda, X, n, Bsave, n, R, n, 0, work, stream()));
+      int rc = backward_errors(n, nrhs, R, n, X, n, nm, tmp, eta);
+      if (rc) return rc;
+      double worst = 0;
+      bool finite = true;
+      for (double e : eta) {
+        if (!(e == e) || std::isinf(e)) finite = false;
+        worst = std::max(worst, e);
+      }
+      r.backward_error = finite ? worst : std::numeric_limits<double>::quiet_NaN();
+      if (finite && worst <= tol) break;
+      if (!finite) {  // a zero or tiny pivot at this precision: restart the iterate
+        have_x = false;
+        stalled = true;
+        break;
+      }
+      slow = worst > 0.5 * prev ? slow + 1 : 0;
+      prev = worst;
+      if (it >= p.max_iterations || (p.escalate && slow >= 2)) {
+        stalled = true;
+        break;
+      }
+      if (p.refinement == PLA_B200_IR_GMRES) {
+        for (int j = 0; j < nrhs; j++) {
+          rc = gmres(F, Ad, lda, R + (long)j * n, Dv + (long)j * n, p.gmres_restart, 1e-8, V, w,
+                     tmp, t32b, work, &r.inner_iterations);
+          if (rc) return rc;
+        }
+      } else {
+        rc = precond(F, R, n, Dv, n, nrhs, t32b);
         if (rc) return rc;
       }
-    } else {
-      rc = precond(F, R, n, Dv, n, nrhs, t32b);
-      if (rc) return rc;
+      K(pla_k_axpby(MPI_DOUBLE, n, nrhs, 1.0, Dv, n, 1.0, X, n, stream()));
     }
-    K(pla_k_axpby(MPI_DOUBLE, n, nrhs, 1.0, Dv, n, 1.0, X, n, stream()));
+    r.iterations += it;
+    refine_ms += t.stop();
+    if (!stalled || !p.escalate || !escalated(prec)) break;
+    prec = escalated(prec);
   }
-  r.iterations = it;
   r.converged = r.backward_error <= tol;
-  K(pla_k_copy(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, nrhs, X, n, Bd, ldb, stream()));
-  r.refine_ms = t.stop();
+  r.refine_ms = refine_ms;
+  if (have_x) K(pla_k_copy(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, nrhs, X, n, Bd, ldb, stream()));
   PLA_CUDA(cudaStreamSynchronize(stream()));
   if (rep) *rep = r;
+  if (kind == 1 && r.info && !r.converged) return r.info;  // not positive definite
   return PLA_SUCCESS;
 }
 
@@ -420,6 +501,7 @@ void PLA_Mixed_params_default(PLA_Mixed_params *p) {
   p->max_iterations = 50;
   p->gmres_restart = 30;
   p->nb = 0;
+  p->escalate = 1;
   p->tol = 0.0;
 }
 

@@ -33,7 +33,7 @@ PLA_UNIT_DIAG, PLA_NONUNIT_DIAG = 101, 102
 PLA_SUCCESS, PLA_ALIGN_FIRST, PLA_DIM_ALL = 0, -200, -201
 PLA_ERROR = -1000
 
-PLA_B200_PREC_BF16, PLA_B200_PREC_FP16, PLA_B200_PREC_FP32 = 1, 2, 3
+PLA_B200_PREC_BF16, PLA_B200_PREC_FP16, PLA_B200_PREC_FP32, PLA_B200_PREC_FP64 = 1, 2, 3, 4
 PLA_B200_IR_LU, PLA_B200_IR_GMRES = 1, 2
 
 _DT = {np.dtype(np.float64): MPI_DOUBLE, np.dtype(np.float32): MPI_FLOAT,
@@ -54,12 +54,13 @@ class PhaseTimes(ctypes.Structure):
 
 class MixedParams(ctypes.Structure):
     _fields_ = [("precision", _i), ("refinement", _i), ("max_iterations", _i),
-                ("gmres_restart", _i), ("nb", _i), ("tol", _d)]
+                ("gmres_restart", _i), ("nb", _i), ("escalate", _i), ("tol", _d)]
 
 
 class MixedReport(ctypes.Structure):
     _fields_ = [("converged", _i), ("iterations", _i), ("inner_iterations", _i), ("info", _i),
-                ("backward_error", _d), ("factor_ms", _d), ("refine_ms", _d)]
+                ("backward_error", _d), ("factor_ms", _d), ("refine_ms", _d),
+                ("precision_used", _i), ("factorizations", _i)]
 
 
 class BatchInstance(ctypes.Structure):

@@ -43,7 +43,8 @@ def tc_update(lib, torch, prec, M, N, K, L, U, C, row0, col0, lower=0):
 
 
 @pytest.mark.parametrize("prec,dt", [(1001, "bfloat16"), (1002, "float16")])
-@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (300, 257, 128), (1000, 777, 256), (64, 200, 192)])
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (300, 257, 128), (1000, 777, 256), (64, 200, 192),
+                                   (4096, 3000, 128), (2100, 2100, 256)])
 def test_tc_update_matches_fp32_product(env, prec, dt, M, N, K):
     s, torch, pla = env
     g = torch.Generator(device="cuda").manual_seed(M + N + K)
@@ -216,3 +217,79 @@ def test_pos_def_mixed_reports_not_spd(env):
     B = np.ones((n, 1), order="F")
     rc, X, rep, _ = solve_mixed(s, pla, A, B, "chol", 2, 1)
     assert rc == 101 and rep.info == 101
+
+
+def solve_mixed_params(s, pla, A, B, kind, **kw):
+    n = A.shape[0]
+    a = s.matrix(n, n)
+    s.set(a, A)
+    b = s.matrix(*B.shape)
+    s.set(b, B)
+    p = pla.MixedParams()
+    s.lib.PLA_Mixed_params_default(ctypes.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    rep = pla.MixedReport()
+    fn = s.lib.PLA_General_solve_mixed if kind == "lu" else s.lib.PLA_Pos_def_solve_mixed
+    rc = fn(a, b, ctypes.byref(p), ctypes.byref(rep))
+    X = s.get(b)
+    s.free(a, b)
+    return rc, X, rep
+
+
+@pytest.mark.parametrize("prec", [1, 2])
+def test_kappa_1e10_escalates_to_fp64_backward_error(env, prec):
+    """kappa = 1e10 is out of reach of bf16/fp16 factors (kappa * u_f >> 1):
+    the refinement stagnates and the solver refactors one precision higher,
+    ending at FP64 backward error; the forward error is checked against the
+    FP64 LAPACK solution."""
+    s, torch, pla = env
+    n = 2048
+    A = c3_matrix(n, 1e10, 11)
+    x_true = np.random.default_rng(12).standard_normal((n, 1))
+    B = A @ x_true
+    rc, X, rep = solve_mixed_params(s, pla, A, B, "lu", precision=prec, refinement=2)
+    assert rc == 0 and rep.converged == 1, (rep.iterations, rep.backward_error)
+    assert rep.precision_used >= prec and rep.factorizations >= 1
+    assert backward_error(A, X, B) <= n * 2.0 ** -53
+    Xr = np.linalg.solve(A, B)
+    fwd = np.abs(X - Xr).max() / np.abs(Xr).max()
+    assert fwd <= 1e10 * n * 2.0 ** -53, fwd
+
+
+def test_no_escalation_reports_stagnation(env):
+    s, torch, pla = env
+    n = 1024
+    A = c3_matrix(n, 1e10, 13)
+    B = A @ np.ones((n, 1))
+    rc, X, rep = solve_mixed_params(s, pla, A, B, "lu", precision=1, refinement=1, escalate=0,
+                                    max_iterations=6)
+    assert rc == 0 and rep.factorizations == 1 and rep.precision_used == 1
+    assert rep.converged == 0 and rep.iterations <= 6
+
+
+@pytest.mark.parametrize("kind", ["lu", "chol"])
+def test_fp64_precision_requested(env, kind):
+    s, torch, pla = env
+    n = 777
+    rng = np.random.default_rng(14)
+    G = rng.standard_normal((n, n))
+    A = np.asfortranarray(G if kind == "lu" else G @ G.T / n + np.eye(n))
+    B = np.asfortranarray(rng.standard_normal((n, 2)))
+    rc, X, rep = solve_mixed_params(s, pla, A, B, kind, precision=pla.PLA_B200_PREC_FP64)
+    assert rc == 0 and rep.converged == 1 and rep.precision_used == pla.PLA_B200_PREC_FP64
+    assert backward_error(A, X, B) <= n * 2.0 ** -53
+
+
+@pytest.mark.parametrize("prec", [1, 2])
+def test_sixteen_right_hand_sides(env, prec):
+    s, torch, pla = env
+    n = 1024
+    A = c3_matrix(n, 1e6, 15)
+    Xt = np.random.default_rng(16).standard_normal((n, 16))
+    B = np.asfortranarray(A @ Xt)
+    rc, X, rep = solve_mixed_params(s, pla, A, B, "lu", precision=prec, refinement=2)
+    assert rc == 0 and rep.converged == 1, (rep.iterations, rep.backward_error)
+    assert backward_error(A, X, B) <= n * 2.0 ** -53
+    Xr = np.linalg.solve(A, B)
+    assert np.abs(X - Xr).max() / np.abs(Xr).max() <= 1e6 * n * 2.0 ** -53
