@@ -38,9 +38,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "n=32768 solve time: mixed-prec LU-IR vs FP64 LU, same B200, both at FP64 bkwd err"
-# DRAM bytes per tensor-core update launch as a fraction of its algorithmic
-# bytes, from the ncu capture summarised in profiles/ (None until captured)
-TC_UPDATE_TRAFFIC_RATIO = None
+# DRAM bytes (read + write) of one tensor-core update launch as a fraction of
+# its algorithmic bytes: 139.3 MB measured against 194.3 MB for the launch
+# with rest = 4864, K = 256 captured by ncu (profiles/tc_update_k_lu_n8192.md).
+# Below 1 because the last C tiles written are still dirty in L2 at exit.
+TC_UPDATE_TRAFFIC_RATIO = 139.3 / 194.25
 
 
 def parse():
@@ -58,6 +60,9 @@ def parse():
     p.add_argument("--skip-fp64", action="store_true")
     p.add_argument("--skip-e2e", action="store_true")
     p.add_argument("--skip-cpu", action="store_true")
+    p.add_argument("--skip-chol", action="store_true", help="skip the FP64 Cholesky solve")
+    p.add_argument("--skip-batched", action="store_true", help="skip the batched workload")
+    p.add_argument("--batch-count", type=int, default=20000)
     p.add_argument("--cpu-seconds", type=float, default=12.0,
                    help="target length of one reference sample on the host")
     return p.parse_args()
@@ -159,6 +164,24 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def fp64_gemm_peak(torch, device):
+    """FP64 roofline denominator: cuBLAS DGEMM (torch.matmul) at 8192^3, best
+    of 5 CUDA-event-timed calls (MEASURED_PEAKS.json carries no FP64 figure)."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=device)
+    b = torch.randn(8192, 8192, dtype=torch.float64, device=device)
+    c = a @ b
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b, c
+    return 2.0 * 8192 ** 3 / best / 1e12
+
+
 def cpu_cores():
     try:
         return len(os.sched_getaffinity(0))
@@ -227,6 +250,127 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------- our arm ---
+def batched_workload(torch, pla, device, dtype, count, seed):
+    """Independent instances, n log-uniform in [8, 512], even-numbered ones LU
+    on i.i.d. uniform[-1, 1] matrices, odd-numbered ones Cholesky on
+    G G'/n + I (G standard normal), 1-4 right-hand sides each.  Matrices of
+    one order share a tensor; `A0`/`B0` keep copies to restore them."""
+    rng = np.random.default_rng(seed)
+    ns = np.round(np.exp(rng.uniform(np.log(8), np.log(512), count))).astype(int)
+    nrhs = rng.integers(1, 5, count)
+    kinds = np.arange(count) % 2
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    es = 8 if dtype == torch.float64 else 4
+    arr = (pla.BatchInstance * count)()
+    groups = []
+    piv = torch.zeros(int(ns.sum()), dtype=torch.int32, device=device)
+    poff = np.concatenate([[0], np.cumsum(ns)[:-1]])
+    flops = 0.0
+    for n in np.unique(ns):
+        n = int(n)
+        idx = np.nonzero(ns == n)[0]
+        lu = idx[kinds[idx] == 0]
+        ch = idx[kinds[idx] == 1]
+        A = torch.empty((len(idx), n, n), dtype=dtype, device=device)
+        if len(lu):
+            A[:len(lu)] = torch.rand((len(lu), n, n), generator=gen, device=device,
+                                     dtype=torch.float64).mul_(2).sub_(1).to(dtype)
+        if len(ch):
+            G = torch.randn((len(ch), n, n), generator=gen, device=device, dtype=torch.float64)
+            S = torch.bmm(G, G.transpose(1, 2)).div_(n)
+            S.diagonal(dim1=1, dim2=2).add_(1.0)
+            A[len(lu):] = S.to(dtype)
+            del G, S
+        B = torch.randn((len(idx), 4, n), generator=gen, device=device,
+                        dtype=torch.float64).to(dtype)
+        order = np.concatenate([lu, ch])
+        for j, k in enumerate(order):
+            k = int(k)
+            arr[k].n, arr[k].nrhs, arr[k].kind = n, int(nrhs[k]), int(kinds[k])
+            arr[k].A = int(A.data_ptr() + j * n * n * es)
+            arr[k].B = int(B.data_ptr() + j * 4 * n * es)
+            arr[k].pivots = ctypes.cast(int(piv.data_ptr() + int(poff[k]) * 4),
+                                        ctypes.POINTER(ctypes.c_int))
+            flops += (2.0 / 3.0 if kinds[k] == 0 else 1.0 / 3.0) * n ** 3 + 2.0 * n * n * nrhs[k]
+        groups.append({"n": n, "order": order, "A": A, "B": B,
+                       "A0": A.clone(), "B0": B.clone()})
+    return arr, groups, piv, flops
+
+
+def batched_backward_error(torch, groups, nrhs_of):
+    """max over instances of ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf),
+    A and b the pristine inputs, x the solution left in B (in float64)."""
+    worst = 0.0
+    for gr in groups:
+        A0 = gr["A0"].double()                 # row-major storage = A' of the column-major A
+        X = gr["B"].double()                   # [cnt, 4, n]: column c of instance j is X[j, c]
+        B0 = gr["B0"].double()
+        R = B0 - torch.bmm(X, A0)              # (A x)' = x' A'
+        mask = torch.tensor([[c < nrhs_of[int(k)] for c in range(4)] for k in gr["order"]],
+                            device=X.device)
+        a_inf = A0.abs().sum(dim=1).max(dim=1).values   # max row sum of A = max col sum of A'
+        num = R.abs().amax(dim=2)
+        den = a_inf[:, None] * X.abs().amax(dim=2) + B0.abs().amax(dim=2)
+        eta = torch.where(mask, num / den, torch.zeros_like(num))
+        worst = max(worst, float(eta.max()))
+    return worst
+
+
+def run_batched(torch, pla, lib, device, stream, dtype, steps, warmup, count=20000, seed=3):
+    arr, groups, piv, flops = batched_workload(torch, pla, device, dtype, count, seed)
+    nrhs_of = [arr[k].nrhs for k in range(count)]
+    dt = pla.MPI_DOUBLE if dtype == torch.float64 else pla.MPI_FLOAT
+    info = torch.full((count,), -1, dtype=torch.int32, device=device)
+
+    def restore():
+        for gr in groups:
+            gr["A"].copy_(gr["A0"])
+            gr["B"].copy_(gr["B0"])
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plan = ctypes.c_void_p()
+    pla.check(lib.PLA_Batch_plan_create(dt, count, arr, ctypes.c_void_p(info.data_ptr()), 1,
+                                        ctypes.byref(plan)), "PLA_Batch_plan_create")
+    plan_s = time.perf_counter() - t0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    times = []
+    for it in range(warmup + steps):
+        restore()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        pla.check(lib.PLA_Batch_plan_execute(plan), "PLA_Batch_plan_execute")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if it >= warmup:
+            times.append(e0.elapsed_time(e1) / 1e3)
+    bad = int((info != 0).sum())
+    eta = batched_backward_error(torch, groups, nrhs_of)
+    lib.PLA_Batch_plan_free(ctypes.byref(plan))
+    # the per-instance launch loop of the plain kernels, same instances
+    restore()
+    torch.cuda.synchronize()
+    pla.check(lib.PLA_Batched_factor_solve_loop(dt, count, arr), "loop warm-up")
+    restore()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    pla.check(lib.PLA_Batched_factor_solve_loop(dt, count, arr), "PLA_Batched_factor_solve_loop")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    loop_s = e0.elapsed_time(e1) / 1e3
+    loop_eta = batched_backward_error(torch, groups, nrhs_of)
+    batched_s = sum(times) / len(times)
+    del groups, piv
+    torch.cuda.empty_cache()
+    return {"workload": f"{count} instances, n log-uniform [8, 512], half LU half Cholesky, "
+                        "1-4 rhs", "dtype": "f64" if dtype == torch.float64 else "f32",
+            "batched_s": batched_s, "loop_s": loop_s, "speedup_vs_loop": loop_s / batched_s,
+            "gflops": flops / batched_s / 1e9, "loop_gflops": flops / loop_s / 1e9,
+            "plan_create_s": plan_s, "instances_failed": bad,
+            "backward_error_max": eta, "loop_backward_error_max": loop_eta}
+
+
 def run_ours(args):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -338,6 +482,7 @@ def run_ours(args):
     fp64_s = None
     fp64_eta = None
     fp64_detail = None
+    fp64_peak = fp64_gemm_peak(torch, device) if not (args.skip_fp64 and args.skip_chol) else None
     if not args.skip_fp64:
         s.set_nb_alg(args.nb_fp64)
         piv = s.mvector(n, 1, np.int32)
@@ -369,12 +514,76 @@ def run_ours(args):
         fp64_detail["dgemm_tflops"] = (gemm_flops * args.steps / (ph64.update_ms / 1e3) / 1e12
                                        if ph64.update_ms > 0 else None)
         fp64_detail["lu_tflops_effective"] = (2.0 / 3.0 * n ** 3) / fp64_s / 1e12
+        fp64_detail["fp64_peak_tflops"] = fp64_peak
+        fp64_detail["fp64_peak_source"] = "cuBLAS DGEMM 8192^3 measured in this run"
+        fp64_detail["lu_frac_of_peak"] = fp64_detail["lu_tflops_effective"] / fp64_peak
+        if fp64_detail["dgemm_tflops"]:
+            fp64_detail["dgemm_frac_of_peak"] = fp64_detail["dgemm_tflops"] / fp64_peak
         check(lib.PLA_Obj_get_local_contents_device(bo, ctypes.c_void_p(x.data_ptr()), n), "x")
         r = b - T.t() @ x
         fp64_eta = (r.abs().max() / (a_inf * x.abs().max() + b.abs().max())).item()
         s.free(piv)
         # leave A as it was for the end-to-end arm
         check(lib.PLA_Obj_set_local_contents_device(ctypes.c_void_p(T.data_ptr()), n, a), "A")
+
+    # ---- FP64 Cholesky arm (PLA_Pos_def_solve) on A = G G'/n + I ----
+    chol = None
+    if not args.skip_chol:
+        g = torch.Generator(device=device).manual_seed(2 + 1000 * rank)
+        G = torch.randn((n, n), dtype=torch.float64, device=device, generator=g)
+        S = G @ G.t()
+        del G
+        S.div_(n)
+        S.diagonal().add_(1.0)
+        xs = torch.randn(n, 1, dtype=torch.float64, device=device, generator=g)
+        bs = S @ xs                               # S is symmetric: row- and column-major agree
+        s.set_nb_alg(args.nb_fp64)
+
+        def chol_step():
+            check(lib.PLA_Obj_set_local_contents_device(ctypes.c_void_p(S.data_ptr()), n, a), "A")
+            check(lib.PLA_Obj_set_local_contents_device(ctypes.c_void_p(bs.data_ptr()), n, bo), "b")
+            check(lib.PLA_Pos_def_solve(a, bo), "PLA_Pos_def_solve")
+
+        for _ in range(args.warmup):
+            chol_step()
+        lib.PLA_B200_set_phase_timing(1)
+        lib.PLA_B200_reset_phase_times()
+        barrier()
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        for _ in range(args.steps):
+            chol_step()
+        c1.record(stream)
+        barrier()
+        chol_s = max_over_ranks(c0.elapsed_time(c1) / 1e3 / args.steps)
+        phc = pla.PhaseTimes()
+        lib.PLA_B200_phase_times(ctypes.byref(phc))
+        lib.PLA_B200_set_phase_timing(0)
+        nbf = args.nb_fp64
+        syrk_flops = sum(float(n - k - nbf) * (n - k - nbf + 1) * nbf
+                         for k in range(0, n, nbf) if n - k - nbf > 0)
+        check(lib.PLA_Obj_get_local_contents_device(bo, ctypes.c_void_p(x.data_ptr()), n), "x")
+        rc = bs - S @ x
+        s_inf = S.abs().sum(dim=0).max().item()
+        chol = {"workload": f"PLA_Pos_def_solve n={n}, A = G G'/n + I, 1 rhs, nb={nbf}",
+                "solve_s": chol_s,
+                "chol_tflops_effective": (n ** 3 / 3.0) / chol_s / 1e12,
+                "chol_frac_of_peak": (n ** 3 / 3.0) / chol_s / 1e12 / fp64_peak,
+                "update_tflops": (syrk_flops * args.steps / (phc.update_ms / 1e3) / 1e12
+                                  if phc.update_ms > 0 else None),
+                "phase_ms_per_step": {k: getattr(phc, k) / args.steps for k in
+                                      ("panel_ms", "trsm_ms", "update_ms", "solve_ms")},
+                "backward_error": (rc.abs().max() / (s_inf * x.abs().max() + bs.abs().max())).item()}
+        del S, bs, xs, rc
+        torch.cuda.empty_cache()
+        check(lib.PLA_Obj_set_local_contents_device(ctypes.c_void_p(T.data_ptr()), n, a), "A")
+
+    # ---- batched factor-and-solve: one persistent graph launch vs a launch loop ----
+    batched = None
+    if not args.skip_batched:
+        batched = [run_batched(torch, pla, lib, device, stream, dt, args.steps, args.warmup,
+                               count=args.batch_count, seed=3 + 1000 * rank)
+                   for dt in (torch.float64, torch.float32)]
 
     # ---- end to end: host buffers in, host solution out ----
     e2e = None
@@ -437,6 +646,7 @@ def run_ours(args):
                "refinement_iterations": report.iterations,
                "gmres_iterations": report.inner_iterations,
                "factor_ms": report.factor_ms, "refine_ms": report.refine_ms,
+               "fp64_cholesky": chol, "batched": batched,
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                "clocks": clock_summary, "gpu_launches": launches}
         print(json.dumps(out))

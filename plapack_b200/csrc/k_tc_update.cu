@@ -3,18 +3,21 @@
 //     C(row0 + i, col0 + j) += alpha * sum_k L(i, k) * U(j, k)
 //
 // with L (M x K) and U (N x K) in bf16 or fp16, both K-contiguous, and C the
-// fp32 working copy of the matrix (column-major).  One CTA per 128 x 128
-// tile of C, 128 threads:
-//   thread 0   : TMA loads of the whole K extent of both operands (128-byte
-//                swizzle, one mbarrier), then K/16 tcgen05.mma (kind::f16,
-//                fp32 accumulate in TMEM), then tcgen05.commit;
-//   all warps  : wait for the MMAs, tcgen05.ld their 32 TMEM lanes, scale by
-//                alpha and stage the tile in shared memory (reusing the
-//                operand buffers), then one TMA reduce-add folds the tile
-//                into C in L2 -- the read-modify-write of C never passes
-//                through the SM.
-// Every wait is bounded: on timeout the kernel records PLA_K_TIMEOUT, waits
-// (bounded) for its own copies, frees its TMEM and returns.
+// fp32 working copy of the matrix (column-major).  The C traffic (an fp32
+// read and write per element) is the bound, so the kernel is built to keep
+// HBM busy: one persistent CTA per SM walks 128 x 128 tiles of C with three
+// roles that overlap one tile's epilogue with the next tile's loads and MMAs:
+//   warp 0 (one thread): TMA loads of 64-wide K chunks of L and U (128-byte
+//            swizzle) into a ring of kStages shared-memory stages;
+//   warp 1 (one thread): tcgen05.mma (kind::f16, fp32 accumulate) into one of
+//            two TMEM accumulators; tcgen05.commit frees each stage and, after
+//            the last chunk, hands the accumulator to the epilogue;
+//   warps 2-5: tcgen05.ld 32 columns at a time, scale by alpha, stage them in
+//            one of kChunks shared-memory buffers and fold them into C with a
+//            TMA reduce-add (the read-modify-write of C happens in L2).
+// Every wait is bounded: on timeout the kernel records PLA_K_TIMEOUT, stops
+// issuing work, waits (bounded) for its own copies and MMAs, frees its TMEM
+// and returns.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -26,9 +29,16 @@
 
 namespace {
 
-constexpr int TM = 128, TN = 128, KBOX = 64, THREADS = 128;
-constexpr int BOX_BYTES = TM * KBOX * 2;  // 16 KB: 128 rows x 128 bytes
-constexpr long kSpin = 20000000;          // bounded polling (~1-2 s)
+constexpr int TM = 128, TN = 128, KBOX = 64;
+constexpr int BOX_BYTES = TM * KBOX * 2;      // 16 KB: 128 rows x 128 bytes
+constexpr int kStages = 4;                    // operand ring: (L box, U box) per stage
+constexpr int STAGE_BYTES = 2 * BOX_BYTES;    // 32 KB
+constexpr int CW = 32;                        // epilogue chunk: 32 columns of a tile
+constexpr int kChunks = 4;                    // staging buffers for the reduce-adds
+constexpr int CHUNK_BYTES = TM * CW * 4;      // 16 KB of fp32
+constexpr int THREADS = 192;                  // TMA warp, MMA warp, 4 epilogue warps
+constexpr int SMEM_BYTES = kStages * STAGE_BYTES + kChunks * CHUNK_BYTES + 1024;
+constexpr long kSpin = 20000000;              // bounded polling (~1-2 s)
 
 __device__ __forceinline__ uint32_t su32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -80,9 +90,18 @@ __device__ __forceinline__ void tma_reduce_add_2d(const CUtensorMap *map, const 
       : "memory");
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+template <int N>
 __device__ __forceinline__ void bulk_wait_read() {
-  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
 }
+__device__ __forceinline__ void bulk_wait_all() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(bar)) : "memory");
+}
+// barrier 1 among the 128 epilogue threads (warps 2-5)
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
@@ -143,89 +162,171 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-template <int KB>
 __global__ void __launch_bounds__(THREADS, 1)
 tc_update_k(const __grid_constant__ CUtensorMap mapL, const __grid_constant__ CUtensorMap mapU,
-            const __grid_constant__ CUtensorMap mapC, int row0, int col0, float alpha,
-            uint32_t idesc, int lower, int *status) {
+            const __grid_constant__ CUtensorMap mapC, int M, int N, int kchunks, int row0,
+            int col0, float alpha, uint32_t idesc, int lower, int *status) {
   extern __shared__ uint8_t smem_raw[];
-  __shared__ __align__(8) uint64_t bar_full, bar_mma;
+  __shared__ __align__(8) uint64_t full[kStages], empty[kStages], acc_full[2], acc_empty[2],
+      bar_drain;
   __shared__ uint32_t tmem_s;
-  __shared__ int s_bad;
+  __shared__ volatile int s_abort;
+  __shared__ int s_skip, s_epi_stop;
   uint8_t *base = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint8_t *sL = base;
-  uint8_t *sU = base + KB * BOX_BYTES;
-  float *sC = reinterpret_cast<float *>(base);  // reused once the MMAs are done
+  uint8_t *ring = base;                                   // kStages x (L box, U box)
+  float *stagec = reinterpret_cast<float *>(base + kStages * STAGE_BYTES);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
-  // SYRK-shaped update: tiles strictly above the diagonal are not needed
-  if (lower && m0 + TM - 1 < n0) return;
-  if (*(volatile int *)status != PLA_K_OK) return;
+  const int tiles_m = (M + TM - 1) / TM, tiles_n = (N + TN - 1) / TN;
+  const int ntiles = tiles_m * tiles_n;
+  // one thread reads the status so that every thread takes the same branch
+  if (threadIdx.x == 0) s_skip = *(volatile int *)status != PLA_K_OK;
+  __syncthreads();
+  if (s_skip) return;
 
-  if (warp == 0) tmem_alloc(&tmem_s, TN);
-  if (threadIdx.x == 32) {
-    mbar_init(&bar_full, 1);
-    mbar_init(&bar_mma, 1);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 128);
+    }
+    mbar_init(&bar_drain, 1);
     mbar_fence_init();
-    s_bad = 0;
+    s_abort = 0;
   }
+  if (warp == 1) tmem_alloc(&tmem_s, 2 * TN);  // two 128-column fp32 accumulators
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_s;
-
-  if (threadIdx.x == 0) {
-    mbar_expect_tx(&bar_full, 2 * KB * BOX_BYTES);
-#pragma unroll
-    for (int kb = 0; kb < KB; kb++) {
-      tma_load_2d(sL + kb * BOX_BYTES, &mapL, &bar_full, kb * KBOX, m0);
-      tma_load_2d(sU + kb * BOX_BYTES, &mapU, &bar_full, kb * KBOX, n0);
-    }
-    if (!mbar_wait(&bar_full, 0)) {
-      s_bad = 1;
-      atomicCAS(status, PLA_K_OK, PLA_K_TIMEOUT);
-      mbar_wait(&bar_full, 0);  // give the copies in flight one more bounded chance
-    } else {
-      tc_fence_after();
-#pragma unroll
-      for (int k = 0; k < KB * (KBOX / 16); k++) {
-        const int kb = k / (KBOX / 16), kk = k % (KBOX / 16);
-        mma_f16(tmem, sdesc(sL + kb * BOX_BYTES + kk * 32), sdesc(sU + kb * BOX_BYTES + kk * 32),
-                idesc, k > 0 ? 1u : 0u);
-      }
-      mma_commit(&bar_mma);
-    }
-  }
-  __syncthreads();
-  bool ok = s_bad == 0;
-  if (ok && !mbar_wait(&bar_mma, 0)) {
+  auto fail = [&]() {
     atomicCAS(status, PLA_K_OK, PLA_K_TIMEOUT);
-    ok = false;
-  }
-  __syncthreads();
-  if (ok && s_bad == 0) {
-    tc_fence_after();
-#pragma unroll
-    for (int c0 = 0; c0 < TN; c0 += 32) {
-      uint32_t r[32];
-      tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + c0, r);
-#pragma unroll
-      for (int j = 0; j < 32; j++)
-        sC[(c0 + j) * TM + warp * 32 + lane] = alpha * __uint_as_float(r[j]);
-    }
-    fence_proxy_async();
-  }
-  tc_fence_before();
-  __syncthreads();
-  if (threadIdx.x == 0 && ok && s_bad == 0) {
-    tma_reduce_add_2d(&mapC, sC, row0 + m0, col0 + n0);
-    bulk_commit();
-    bulk_wait_read();
-  }
-  __syncthreads();
+    s_abort = 1;
+  };
+  // SYRK-shaped update: tiles strictly above the diagonal are not needed
+  auto skip = [&](int tm, int tn) { return lower && tm * TM + TM - 1 < tn * TN; };
+
   if (warp == 0) {
+    if (lane == 0) {  // ---- TMA producer ----
+      int stage = 0;
+      uint32_t ph = 0;
+      int issued_ph[kStages];
+      for (int s = 0; s < kStages; s++) issued_ph[s] = -1;
+      for (int t = blockIdx.x; t < ntiles && !s_abort; t += gridDim.x) {
+        const int tm = t % tiles_m, tn = t / tiles_m;
+        if (skip(tm, tn)) continue;
+        for (int kc = 0; kc < kchunks && !s_abort; kc++) {
+          if (!mbar_wait(&empty[stage], ph ^ 1)) {
+            fail();
+            break;
+          }
+          uint8_t *sl = ring + stage * STAGE_BYTES;
+          mbar_expect_tx(&full[stage], STAGE_BYTES);
+          tma_load_2d(sl, &mapL, &full[stage], kc * KBOX, tm * TM);
+          tma_load_2d(sl + BOX_BYTES, &mapU, &full[stage], kc * KBOX, tn * TN);
+          issued_ph[stage] = (int)ph;
+          if (++stage == kStages) {
+            stage = 0;
+            ph ^= 1;
+          }
+        }
+      }
+      // every load must have landed before the shared memory is released
+      for (int s = 0; s < kStages; s++)
+        if (issued_ph[s] >= 0 && !mbar_wait(&full[s], (uint32_t)issued_ph[s])) fail();
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // ---- MMA issuer ----
+      int stage = 0, count = 0;
+      uint32_t ph = 0;
+      bool issued = false;
+      for (int t = blockIdx.x; t < ntiles && !s_abort; t += gridDim.x) {
+        const int tm = t % tiles_m, tn = t / tiles_m;
+        if (skip(tm, tn)) continue;
+        const int ab = count & 1;
+        if (!mbar_wait(&acc_empty[ab], ((count >> 1) & 1) ^ 1)) {
+          fail();
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(ab * TN);
+        bool ok = true;
+        for (int kc = 0; kc < kchunks; kc++) {
+          if (!mbar_wait(&full[stage], ph)) {
+            fail();
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          uint8_t *sl = ring + stage * STAGE_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < KBOX / 16; kk++)
+            mma_f16(d, sdesc(sl + kk * 32), sdesc(sl + BOX_BYTES + kk * 32), idesc,
+                    (kc | kk) ? 1u : 0u);
+          issued = true;
+          mma_commit(&empty[stage]);  // the stage is free once these MMAs have read it
+          if (++stage == kStages) {
+            stage = 0;
+            ph ^= 1;
+          }
+        }
+        if (!ok) break;
+        mma_commit(&acc_full[ab]);
+        count++;
+      }
+      // all MMAs complete before the TMEM is freed
+      if (issued) {
+        mma_commit(&bar_drain);
+        if (!mbar_wait(&bar_drain, 0)) fail();
+      }
+    }
+  } else {  // ---- epilogue: warps 2-5, TMEM lanes 32 * (warp % 4) ----
+    // The 128 epilogue threads meet at named barrier 1, so they must leave
+    // the tile loop together: the decision to stop is sampled by one thread
+    // and read by all from s_epi_stop.
+    const int lanes = 32 * (warp & 3);
+    const int row = lanes + lane;
+    const bool elected = threadIdx.x == 64;
+    int count = 0, chunk = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      const int tm = t % tiles_m, tn = t / tiles_m;
+      if (skip(tm, tn)) continue;
+      const int ab = count & 1;
+      if (!mbar_wait(&acc_full[ab], (count >> 1) & 1)) fail();
+      epi_sync();
+      if (elected) s_epi_stop = s_abort;
+      epi_sync();
+      if (s_epi_stop) break;
+      tc_fence_after();
+#pragma unroll 1
+      for (int c = 0; c < TN / CW; c++) {
+        float *sc = stagec + (chunk % kChunks) * (TM * CW);
+        if (elected) bulk_wait_read<kChunks - 1>();  // the reduce that used sc has read it
+        epi_sync();
+        uint32_t r[32];
+        tmem_ld32(tmem + ((uint32_t)lanes << 16) + (uint32_t)(ab * TN + c * CW), r);
+#pragma unroll
+        for (int j = 0; j < CW; j++) sc[j * TM + row] = alpha * __uint_as_float(r[j]);
+        fence_proxy_async();
+        epi_sync();
+        if (elected) {
+          tma_reduce_add_2d(&mapC, sc, row0 + tm * TM, col0 + tn * TN + c * CW);
+          bulk_commit();
+        }
+        chunk++;
+      }
+      tc_fence_before();
+      mbar_arrive(&acc_empty[ab]);  // this thread's reads of the accumulator are done
+      count++;
+    }
+    if (elected) bulk_wait_all();
+  }
+  __syncthreads();
+  if (warp == 1) {
     tc_fence_after();
-    tmem_dealloc(tmem, TN);
+    tmem_dealloc(tmem, 2 * TN);
   }
 }
 
@@ -258,16 +359,21 @@ int encode(CUtensorMap *map, CUtensorMapDataType dt, int esize, const void *ptr,
   return r == CUDA_SUCCESS ? 0 : (int)cudaErrorInvalidValue;
 }
 
-template <int KB>
+int g_sms = 0;
+
 int launch(const CUtensorMap &mL, const CUtensorMap &mU, const CUtensorMap &mC, int M, int N,
-           int row0, int col0, float alpha, uint32_t idesc, int lower, int *status,
+           int kchunks, int row0, int col0, float alpha, uint32_t idesc, int lower, int *status,
            cudaStream_t s) {
-  // operand tiles, reused afterwards as the 128 x 128 fp32 staging tile
-  size_t ops = (size_t)2 * KB * BOX_BYTES, stage = (size_t)TM * TN * sizeof(float);
-  size_t sm = (ops > stage ? ops : stage) + 1024;
-  cudaFuncSetAttribute(tc_update_k<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  dim3 grid((M + TM - 1) / TM, (N + TN - 1) / TN);
-  tc_update_k<KB><<<grid, THREADS, sm, s>>>(mL, mU, mC, row0, col0, alpha, idesc, lower, status);
+  if (!g_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  cudaFuncSetAttribute(tc_update_k, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  const long tiles = (long)((M + TM - 1) / TM) * ((N + TN - 1) / TN);
+  const int grid = (int)(tiles < g_sms ? tiles : g_sms);
+  tc_update_k<<<grid, THREADS, SMEM_BYTES, s>>>(mL, mU, mC, M, N, kchunks, row0, col0, alpha,
+                                                idesc, lower, status);
   pla_k_count(1);
   return (int)cudaGetLastError();
 }
@@ -279,7 +385,7 @@ extern "C" int pla_k_tc_update(int prec, int M, int N, int K, float alpha, const
                                float *C, long ldc, long c_rows, long c_cols, int row0, int col0,
                                int lower, int *status, cudaStream_t s) {
   if (M <= 0 || N <= 0 || K <= 0) return 0;
-  if (K % KBOX != 0 || K > 4 * KBOX) return (int)cudaErrorInvalidValue;
+  if (K % KBOX != 0) return (int)cudaErrorInvalidValue;
   if (ldl % 8 || ldu % 8 || ldc % 4 || (row0 % 4) || ((uintptr_t)C % 16) || ((uintptr_t)L % 16) ||
       ((uintptr_t)U % 16))
     return (int)cudaErrorMisalignedAddress;
@@ -294,17 +400,12 @@ extern "C" int pla_k_tc_update(int prec, int M, int N, int K, float alpha, const
                   CU_TENSOR_MAP_SWIZZLE_128B)))
     return r;
   if ((r = encode(&mC, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, C, (uint64_t)c_rows, (uint64_t)c_cols,
-                  (uint64_t)ldc, TM, TN, CU_TENSOR_MAP_SWIZZLE_NONE)))
+                  (uint64_t)ldc, TM, CW, CU_TENSOR_MAP_SWIZZLE_NONE)))
     return r;
   // instruction descriptor: fp32 accumulate, A/B bf16 (1) or fp16 (0), both
   // K-major, N = 128, M = 128
   const uint32_t ab = prec == PLA_K_BF16 ? 1u : 0u;
   const uint32_t idesc = (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)(TN >> 3) << 17) |
                          ((uint32_t)(TM >> 4) << 24);
-  switch (K / KBOX) {
-    case 1: return launch<1>(mL, mU, mC, M, N, row0, col0, alpha, idesc, lower, status, s);
-    case 2: return launch<2>(mL, mU, mC, M, N, row0, col0, alpha, idesc, lower, status, s);
-    case 3: return launch<3>(mL, mU, mC, M, N, row0, col0, alpha, idesc, lower, status, s);
-    default: return launch<4>(mL, mU, mC, M, N, row0, col0, alpha, idesc, lower, status, s);
-  }
+  return launch(mL, mU, mC, M, N, K / KBOX, row0, col0, alpha, idesc, lower, status, s);
 }
