@@ -40,11 +40,12 @@
 namespace {
 
 constexpr int kThreads = 256;
-constexpr long kSpinLimit = 4000000;  // polls of one record before giving up (~1 s)
+constexpr long kSpinLimit = 4000000;  // polls before giving up (~1-2 s)
+constexpr int kPerLane = 5;           // records per lane of the gathering warp: P <= 160
 
-__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long *p) {
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long *p) {
   unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
 __device__ __forceinline__ void st_relaxed64(unsigned long long *p, unsigned long long v) {
@@ -166,30 +167,52 @@ panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *sta
   };
 
   // Gather the records of column `col` into (s_p = winning row or INT_MAX,
-  // s_q = its CTA); false when a wait gave up.
+  // s_q = its CTA); false when a wait gave up.  Lane l of warp 0 watches the
+  // records of CTAs l, l + 32, ...: each poll loads all of them at once
+  // (independent loads, one round trip), and one acquire fence follows once
+  // every record carries the column's generation.
   auto gather = [&](int col) -> bool {
     const int par = col & 1;
     const unsigned long long gen = (unsigned long long)(((col >> 1) & 1) ^ 1);
     if (tid < 32) {
+      unsigned long long w0[kPerLane], w1[kPerLane];
+      bool done[kPerLane];
+#pragma unroll
+      for (int i = 0; i < kPerLane; i++) {
+        done[i] = tid + 32 * i >= P;
+        w0[i] = w1[i] = 0;
+      }
+      bool ok = true;
+      for (long spins = 0;; spins++) {
+#pragma unroll
+        for (int i = 0; i < kPerLane; i++)
+          if (!done[i]) {
+            const unsigned long long *rp = rec + ((long)par * P + tid + 32 * i) * 2;
+            w0[i] = ld_relaxed64(rp);
+            w1[i] = ld_relaxed64(rp + 1);
+          }
+        bool all = true;
+#pragma unroll
+        for (int i = 0; i < kPerLane; i++)
+          if (!done[i]) {
+            if ((w0[i] >> 63) == gen && (w1[i] >> 63) == gen) done[i] = true;
+            else all = false;
+          }
+        if (all) break;
+        if (spins > kSpinLimit || *(volatile int *)status != PLA_K_OK) {
+          ok = false;
+          break;
+        }
+      }
+      __threadfence();  // acquire: the rows published before the records are visible
       T bv = T(-1);
       int bi = INT_MAX, bq = 0;
-      bool ok = true;
-      for (int q = tid; q < P && ok; q += 32) {
-        const unsigned long long *rp = rec + ((long)par * P + q) * 2;
-        unsigned long long w0 = 0, w1 = 0;
-        for (long spins = 0;; spins++) {
-          w0 = ld_acquire64(rp);
-          w1 = ld_acquire64(rp + 1);
-          if ((w0 >> 63) == gen && (w1 >> 63) == gen) break;
-          if (spins > kSpinLimit || *(volatile int *)status != PLA_K_OK) {
-            ok = false;
-            break;
-          }
-          __nanosleep(20);
-        }
-        if (!ok) break;
-        const T v = dec_val<T>(w0);
-        const int ix = (int)(unsigned)(w1 & 0xffffffffull);
+#pragma unroll
+      for (int i = 0; i < kPerLane; i++) {
+        const int q = tid + 32 * i;
+        if (q >= P) continue;
+        const T v = dec_val<T>(w0[i]);
+        const int ix = (int)(unsigned)(w1[i] & 0xffffffffull);
         if (better(v, ix, bv, bi)) { bv = v; bi = ix; bq = q; }
       }
       const bool all_ok = __all_sync(0xffffffffu, ok);
@@ -308,6 +331,7 @@ int launch(int r, int w, void *A, long lda, int *piv, int *status, int *zero_inf
   // rows per CTA: at least 32, at most enough CTAs for one per SM
   int P = (r + 31) / 32;
   if (P > g_sms) P = g_sms;
+  if (P > 32 * kPerLane) P = 32 * kPerLane;  // the records one warp gathers
   if (P < 1) P = 1;
   int R = (r + P - 1) / P;
   P = (r + R - 1) / R;
@@ -411,6 +435,7 @@ int launch_noalloc(int r, int w, T *A, long lda, int *piv, int *status, cudaStre
   int P = (r + 31) / 32;
   if (P > sms) P = sms;
   if (P > kNoAllocCtas) P = kNoAllocCtas;
+  if (P > 32 * kPerLane) P = 32 * kPerLane;
   if (P < 1) P = 1;
   int R = (r + P - 1) / P;
   P = (r + R - 1) / R;
