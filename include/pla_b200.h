@@ -68,6 +68,10 @@ long PLA_B200_kernel_launches(void);
 #define PLA_B200_PREC_FP16   2   /* trailing update in fp16, fp32 accumulate */
 #define PLA_B200_PREC_FP32   3   /* fp32 throughout                          */
 #define PLA_B200_PREC_FP64   4   /* FP64 factors (the plain PLA_LU / PLA_Chol) */
+#define PLA_B200_PREC_FP8    5   /* trailing update in fp8 E4M3 with one power-of-two
+                                    scale per 128-row tile, fp32 accumulate; the
+                                    Cholesky factors D A D, D = diag(A)^-1/2, and
+                                    refines with M^-1 = D (L L')^-1 D */
 #define PLA_B200_IR_LU       1   /* classic iterative refinement             */
 #define PLA_B200_IR_GMRES    2   /* GMRES-IR                                 */
 
@@ -81,7 +85,8 @@ typedef struct {
                            a halving of the backward error twice in a row, a
                            non-finite iterate, max_iterations reached) or the
                            low-precision Cholesky breaks down, refactor one
-                           precision higher (BF16/FP16 -> FP32 -> FP64) and
+                           precision higher (FP8 -> BF16, BF16/FP16 -> FP32
+                           -> FP64) and
                            continue from the current iterate                 */
   double tol;           /* target backward error; <= 0 selects n * 2^-53    */
 } PLA_Mixed_params;

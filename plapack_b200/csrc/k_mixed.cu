@@ -2,12 +2,19 @@
 //   pack_rows   : fp32 column-major panel -> bf16/fp16 row-major (K-contiguous)
 //                 operand of the tensor-core trailing update, through a
 //                 32 x 32 shared tile so reads and writes stay coalesced;
+//   pack_fp8    : the same operand in fp8 E4M3 with a power-of-two scale per
+//                 128 rows;
+//   sym_scale   : d = diag(A)^-1/2 and the fp32 copy of D A D (the unit-diagonal
+//                 matrix the fp8 Cholesky factors);
 //   residual    : R = B - A X (or row sums of |A|) in FP64, split over column
 //                 slices so every SM streams A at full bandwidth; partial sums
 //                 land in a [slices][n] workspace and a second pass adds them
 //                 in a fixed order (deterministic).
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <cuda_fp8.h>
+
+#include <cstdint>
 
 #include "PLA.h"
 #include "pla_kernels.h"
@@ -35,6 +42,73 @@ __global__ void pack_rows_k(int m, int kdim, const float *src, long lds, D *dst,
     int i = i0 + r, k = k0 + threadIdx.x;
     if (i < m && k < kdim) dst[(long)i * ldd + k] = from_f32<D>(tile[threadIdx.x][r]);
   }
+}
+
+// fp8 E4M3 operand with one power-of-two scale per block of 128 rows.  For
+// block b the scale is 2^e, e the largest integer with max|x| * 2^e <= 448
+// (the largest finite E4M3 value), so the block uses the top of the E4M3
+// range without overflow; dst[i * ldd + k] = e4m3(x(i, k) * 2^e) and
+// inv[b] = 2^-e.  Source element (i, k) is src[i * si + k * sk].  Powers of
+// two scale exactly, so the only rounding is the conversion itself.
+__global__ void __launch_bounds__(256)
+pack_fp8_k(int m, int kdim, const float *__restrict__ src, long si, long sk,
+           uint8_t *__restrict__ dst, long ldd, float *__restrict__ inv) {
+  __shared__ float red[8];
+  __shared__ float s_scale;
+  const int b = blockIdx.x, i0 = b * 128;
+  const int rows = min(128, m - i0);
+  const int total = rows * kdim;
+  float amax = 0.f;
+  for (int e = threadIdx.x; e < total; e += 256) {
+    const int i = e % rows, k = e / rows;
+    amax = fmaxf(amax, fabsf(src[(long)(i0 + i) * si + (long)k * sk]));
+  }
+  for (int o = 16; o; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = amax;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float a = red[0];
+    for (int w = 1; w < 8; w++) a = fmaxf(a, red[w]);
+    float sc = 1.f;
+    if (a > 0.f && isfinite(a)) {
+      int E;
+      const float f = frexpf(a, &E);  // a = f * 2^E, f in [0.5, 1); 448 = 0.875 * 2^9
+      sc = ldexpf(1.f, f <= 0.875f ? 9 - E : 8 - E);
+    }
+    s_scale = sc;
+    inv[b] = 1.f / sc;
+  }
+  __syncthreads();
+  const float sc = s_scale;
+  for (int e = threadIdx.x; e < total; e += 256) {
+    const int k = e % kdim, i = e / kdim;
+    const float x = src[(long)(i0 + i) * si + (long)k * sk] * sc;
+    dst[(long)(i0 + i) * ldd + k] = (uint8_t)__nv_cvt_float_to_fp8(x, __NV_SATFINITE, __NV_E4M3);
+  }
+}
+
+// Diagonal scaling of an SPD matrix for the fp8 Cholesky: d(i) = 1 / sqrt(A(i, i))
+// (1 where A(i, i) <= 0: the factorization then reports the failure itself)
+__global__ void diag_rsqrt_k(int n, const double *__restrict__ A, long lda, double *__restrict__ d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double a = A[i + (long)i * lda];
+  d[i] = a > 0.0 ? 1.0 / sqrt(a) : 1.0;
+}
+// dst(i, j) = fp32(d(i) * A(i, j) * d(j)), column j = blockIdx.y
+__global__ void scale_convert_k(int n, const double *__restrict__ A, long lda,
+                                const double *__restrict__ d, float *__restrict__ dst, long ldd) {
+  const int j = blockIdx.y;
+  const double dj = d[j];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    dst[i + (long)j * ldd] = (float)(d[i] * A[i + (long)j * lda] * dj);
+}
+// X(i, r) *= d(i)
+__global__ void diag_mul_k(int n, int nrhs, const double *__restrict__ d, double *X, long ldx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double di = d[i];
+  for (int r = 0; r < nrhs; r++) X[i + (long)r * ldx] *= di;
 }
 
 constexpr int kRows = 256;
@@ -102,6 +176,32 @@ extern "C" int pla_k_pack_rows(int prec, int m, int kdim, const float *src, long
     pack_rows_k<__nv_bfloat16><<<grid, block, 0, s>>>(m, kdim, src, lds, (__nv_bfloat16 *)dst, ldd);
   else
     pack_rows_k<__half><<<grid, block, 0, s>>>(m, kdim, src, lds, (__half *)dst, ldd);
+  pla_k_count(1);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int pla_k_pack_fp8(int m, int kdim, const float *src, long si, long sk, void *dst,
+                              long ldd, float *inv, cudaStream_t s) {
+  if (m <= 0 || kdim <= 0) return 0;
+  pack_fp8_k<<<(m + 127) / 128, 256, 0, s>>>(m, kdim, src, si, sk, (uint8_t *)dst, ldd, inv);
+  pla_k_count(1);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int pla_k_sym_scale(int n, const double *A, long lda, double *d, float *dst, long ldd,
+                               cudaStream_t s) {
+  if (n <= 0) return 0;
+  diag_rsqrt_k<<<(n + 255) / 256, 256, 0, s>>>(n, A, lda, d);
+  dim3 grid((n + 1023) / 1024 < 8 ? (n + 1023) / 1024 : 8, n);
+  scale_convert_k<<<grid, 256, 0, s>>>(n, A, lda, d, dst, ldd);
+  pla_k_count(2);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int pla_k_diag_mul(int n, int nrhs, const double *d, double *X, long ldx,
+                              cudaStream_t s) {
+  if (n <= 0 || nrhs <= 0) return 0;
+  diag_mul_k<<<(n + 255) / 256, 256, 0, s>>>(n, nrhs, d, X, ldx);
   pla_k_count(1);
   return (int)cudaGetLastError();
 }

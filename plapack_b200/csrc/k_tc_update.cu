@@ -2,8 +2,10 @@
 //
 //     C(row0 + i, col0 + j) += alpha * sum_k L(i, k) * U(j, k)
 //
-// with L (M x K) and U (N x K) in bf16 or fp16, both K-contiguous, and C the
-// fp32 working copy of the matrix (column-major).  The C traffic (an fp32
+// with L (M x K) and U (N x K) in bf16 or fp16 (kind::f16), or in fp8 E4M3
+// with one power-of-two scale per 128-row tile of each operand (kind::f8f6f4,
+// the scales applied in the epilogue), both K-contiguous, and C the fp32
+// working copy of the matrix (column-major).  The C traffic (an fp32
 // read and write per element) is the bound, so the kernel is built to keep
 // HBM busy: one persistent CTA per SM walks 128 x 128 tiles of C with three
 // roles that overlap one tile's epilogue with the next tile's loads and MMAs:
@@ -143,6 +145,16 @@ __device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t ad, uint64_t b
       "l"(ad), "l"(bd), "r"(idesc), "r"(accumulate)
       : "memory");
 }
+// fp8 operands (E4M3 x E4M3, fp32 accumulate): K = 32 per instruction, so a
+// 128-byte row of the swizzled box is again four instructions 32 bytes apart
+__device__ __forceinline__ void mma_f8(uint32_t tmem_d, uint64_t ad, uint64_t bd, uint32_t idesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(ad), "l"(bd), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
   asm volatile(
       "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
@@ -162,10 +174,15 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// F8: E4M3 operands with one power-of-two scale per 128-row tile of L and of
+// U (inv_l, inv_u); a K chunk is then 128 elements (still 128 bytes per row)
+template <bool F8>
 __global__ void __launch_bounds__(THREADS, 1)
 tc_update_k(const __grid_constant__ CUtensorMap mapL, const __grid_constant__ CUtensorMap mapU,
             const __grid_constant__ CUtensorMap mapC, int M, int N, int kchunks, int row0,
-            int col0, float alpha, uint32_t idesc, int lower, int *status) {
+            int col0, float alpha, uint32_t idesc, int lower, const float *inv_l,
+            const float *inv_u, int *status) {
+  constexpr int KE = F8 ? 128 : KBOX;  // elements per K chunk
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t full[kStages], empty[kStages], acc_full[2], acc_empty[2],
       bar_drain;
@@ -224,8 +241,8 @@ tc_update_k(const __grid_constant__ CUtensorMap mapL, const __grid_constant__ CU
           }
           uint8_t *sl = ring + stage * STAGE_BYTES;
           mbar_expect_tx(&full[stage], STAGE_BYTES);
-          tma_load_2d(sl, &mapL, &full[stage], kc * KBOX, tm * TM);
-          tma_load_2d(sl + BOX_BYTES, &mapU, &full[stage], kc * KBOX, tn * TN);
+          tma_load_2d(sl, &mapL, &full[stage], kc * KE, tm * TM);
+          tma_load_2d(sl + BOX_BYTES, &mapU, &full[stage], kc * KE, tn * TN);
           issued_ph[stage] = (int)ph;
           if (++stage == kStages) {
             stage = 0;
@@ -262,9 +279,14 @@ tc_update_k(const __grid_constant__ CUtensorMap mapL, const __grid_constant__ CU
           tc_fence_after();
           uint8_t *sl = ring + stage * STAGE_BYTES;
 #pragma unroll
-          for (int kk = 0; kk < KBOX / 16; kk++)
-            mma_f16(d, sdesc(sl + kk * 32), sdesc(sl + BOX_BYTES + kk * 32), idesc,
-                    (kc | kk) ? 1u : 0u);
+          for (int kk = 0; kk < 4; kk++) {  // 32-byte K steps through the 128-byte rows
+            if constexpr (F8)
+              mma_f8(d, sdesc(sl + kk * 32), sdesc(sl + BOX_BYTES + kk * 32), idesc,
+                     (kc | kk) ? 1u : 0u);
+            else
+              mma_f16(d, sdesc(sl + kk * 32), sdesc(sl + BOX_BYTES + kk * 32), idesc,
+                      (kc | kk) ? 1u : 0u);
+          }
           issued = true;
           mma_commit(&empty[stage]);  // the stage is free once these MMAs have read it
           if (++stage == kStages) {
@@ -299,6 +321,7 @@ tc_update_k(const __grid_constant__ CUtensorMap mapL, const __grid_constant__ CU
       if (elected) s_epi_stop = s_abort;
       epi_sync();
       if (s_epi_stop) break;
+      const float scale = F8 ? alpha * inv_l[tm] * inv_u[tn] : alpha;
       tc_fence_after();
 #pragma unroll 1
       for (int c = 0; c < TN / CW; c++) {
@@ -308,7 +331,7 @@ tc_update_k(const __grid_constant__ CUtensorMap mapL, const __grid_constant__ CU
         uint32_t r[32];
         tmem_ld32(tmem + ((uint32_t)lanes << 16) + (uint32_t)(ab * TN + c * CW), r);
 #pragma unroll
-        for (int j = 0; j < CW; j++) sc[j * TM + row] = alpha * __uint_as_float(r[j]);
+        for (int j = 0; j < CW; j++) sc[j * TM + row] = scale * __uint_as_float(r[j]);
         fence_proxy_async();
         epi_sync();
         if (elected) {
@@ -361,19 +384,20 @@ int encode(CUtensorMap *map, CUtensorMapDataType dt, int esize, const void *ptr,
 
 int g_sms = 0;
 
+template <bool F8>
 int launch(const CUtensorMap &mL, const CUtensorMap &mU, const CUtensorMap &mC, int M, int N,
-           int kchunks, int row0, int col0, float alpha, uint32_t idesc, int lower, int *status,
-           cudaStream_t s) {
+           int kchunks, int row0, int col0, float alpha, uint32_t idesc, int lower,
+           const float *inv_l, const float *inv_u, int *status, cudaStream_t s) {
   if (!g_sms) {
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
   }
-  cudaFuncSetAttribute(tc_update_k, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  cudaFuncSetAttribute(tc_update_k<F8>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
   const long tiles = (long)((M + TM - 1) / TM) * ((N + TN - 1) / TN);
   const int grid = (int)(tiles < g_sms ? tiles : g_sms);
-  tc_update_k<<<grid, THREADS, SMEM_BYTES, s>>>(mL, mU, mC, M, N, kchunks, row0, col0, alpha,
-                                                idesc, lower, status);
+  tc_update_k<F8><<<grid, THREADS, SMEM_BYTES, s>>>(mL, mU, mC, M, N, kchunks, row0, col0, alpha,
+                                                    idesc, lower, inv_l, inv_u, status);
   pla_k_count(1);
   return (int)cudaGetLastError();
 }
@@ -407,5 +431,37 @@ extern "C" int pla_k_tc_update(int prec, int M, int N, int K, float alpha, const
   const uint32_t ab = prec == PLA_K_BF16 ? 1u : 0u;
   const uint32_t idesc = (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)(TN >> 3) << 17) |
                          ((uint32_t)(TM >> 4) << 24);
-  return launch(mL, mU, mC, M, N, K / KBOX, row0, col0, alpha, idesc, lower, status, s);
+  return launch<false>(mL, mU, mC, M, N, K / KBOX, row0, col0, alpha, idesc, lower, nullptr,
+                       nullptr, status, s);
+}
+
+// The same update with fp8 E4M3 operands (row-major, K-contiguous, ldl / ldu
+// bytes) and per-128-row-tile inverse scales: C += alpha * inv_l[i / 128] *
+// inv_u[j / 128] * sum_k L(i, k) U(j, k).
+extern "C" int pla_k_tc_update_fp8(int M, int N, int K, float alpha, const void *L, long ldl,
+                                   long l_rows, const float *inv_l, const void *U, long ldu,
+                                   long u_rows, const float *inv_u, float *C, long ldc,
+                                   long c_rows, long c_cols, int row0, int col0, int lower,
+                                   int *status, cudaStream_t s) {
+  if (M <= 0 || N <= 0 || K <= 0) return 0;
+  if (K % 128 != 0 || !inv_l || !inv_u) return (int)cudaErrorInvalidValue;
+  if (ldl % 16 || ldu % 16 || ldc % 4 || (row0 % 4) || ((uintptr_t)C % 16) ||
+      ((uintptr_t)L % 16) || ((uintptr_t)U % 16))
+    return (int)cudaErrorMisalignedAddress;
+  CUtensorMap mL, mU, mC;
+  int r;
+  if ((r = encode(&mL, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, L, (uint64_t)K, (uint64_t)l_rows,
+                  (uint64_t)ldl, 128, TM, CU_TENSOR_MAP_SWIZZLE_128B)))
+    return r;
+  if ((r = encode(&mU, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, U, (uint64_t)K, (uint64_t)u_rows,
+                  (uint64_t)ldu, 128, TN, CU_TENSOR_MAP_SWIZZLE_128B)))
+    return r;
+  if ((r = encode(&mC, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, C, (uint64_t)c_rows, (uint64_t)c_cols,
+                  (uint64_t)ldc, TM, CW, CU_TENSOR_MAP_SWIZZLE_NONE)))
+    return r;
+  // instruction descriptor, kind::f8f6f4: fp32 accumulate, A and B both E4M3
+  // (format 0), both K-major, N = 128, M = 128
+  const uint32_t idesc = (1u << 4) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+  return launch<true>(mL, mU, mC, M, N, K / 128, row0, col0, alpha, idesc, lower, inv_l, inv_u,
+                      status, s);
 }

@@ -109,9 +109,25 @@ int pla_k_tc_update(int prec, int M, int N, int K, float alpha, const void *L, l
                     long l_rows, const void *U, long ldu, long u_rows, float *C, long ldc,
                     long c_rows, long c_cols, int row0, int col0, int lower, int *status,
                     cudaStream_t s);
+/* pla_k_tc_update with fp8 E4M3 operands (ldl / ldu in bytes, K % 128 == 0)
+ * and per-128-row-tile inverse scales of L (inv_l) and of U (inv_u) */
+int pla_k_tc_update_fp8(int M, int N, int K, float alpha, const void *L, long ldl, long l_rows,
+                        const float *inv_l, const void *U, long ldu, long u_rows,
+                        const float *inv_u, float *C, long ldc, long c_rows, long c_cols,
+                        int row0, int col0, int lower, int *status, cudaStream_t s);
 /* dst (bf16/fp16, row-major, ldd) := src (fp32, m x kdim column-major, lds) */
 int pla_k_pack_rows(int prec, int m, int kdim, const float *src, long lds, void *dst, long ldd,
                     cudaStream_t s);
+/* dst (fp8 E4M3, row-major, ldd bytes) := x(i, k) * 2^e(i / 128) for i < m,
+ * k < kdim, x(i, k) = src[i * si + k * sk] (fp32); e(b) the largest power with
+ * max |x| of rows [128 b, 128 b + 128) * 2^e <= 448; inv[b] := 2^-e(b). */
+int pla_k_pack_fp8(int m, int kdim, const float *src, long si, long sk, void *dst, long ldd,
+                   float *inv, cudaStream_t s);
+/* d := diag(A)^-1/2 (1 where A(i, i) <= 0); dst (fp32, ldd) := D A D */
+int pla_k_sym_scale(int n, const double *A, long lda, double *d, float *dst, long ldd,
+                    cudaStream_t s);
+/* X(i, r) *= d(i) for r < nrhs (FP64) */
+int pla_k_diag_mul(int n, int nrhs, const double *d, double *X, long ldx, cudaStream_t s);
 /* R := B - A X in FP64 (A n x ncols, X ncols x nrhs, nrhs <= 16); with
  * abs_rows, R(:,0) := row sums of |A|.  work: pla_k_residual_work() bytes. */
 /* single-launch fp32 triangular solve with one right-hand side: the inverses

@@ -41,7 +41,7 @@ namespace {
   } while (0)
 
 enum Slots { kSlotA32 = 4, kSlotL = 5, kSlotU = 6, kSlotPiv = 7, kSlotVec = 8, kSlotWork = 9,
-             kSlotV = 10, kSlotSt = 11, kSlotA64 = 16 };
+             kSlotV = 10, kSlotSt = 11, kSlotA64 = 16, kSlotScales = 18, kSlotDiag = 19 };
 
 long round_up(long v, long m) { return (v + m - 1) / m * m; }
 
@@ -49,6 +49,7 @@ struct Factor {
   int n = 0, ld = 0, prec = 0, kind = 0;  // kind 0 = LU, 1 = Cholesky
   float *a = nullptr;     // fp32 factors (BF16, FP16, FP32)
   double *a64 = nullptr;  // FP64 factors (FP64)
+  double *dsc = nullptr;  // d = diag(A)^-1/2 when the factors are those of D A D
   int *piv = nullptr;
   int *status = nullptr;  // [status, info, zero_info]
   // inverses of the 128 x 128 diagonal blocks of the two triangular factors
@@ -100,14 +101,26 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
   const int n = F.n;
   const long ld = F.ld;
   auto at = [&](long i, long j) { return F.a + i + j * ld; };
-  K(pla_k_convert(MPI_DOUBLE, A, lda, MPI_FLOAT, F.a, ld, n, n, stream()));
+  if (F.dsc)  // the unit-diagonal D A D of the fp8 Cholesky
+    K(pla_k_sym_scale(n, A, lda, F.dsc, F.a, ld, stream()));
+  else
+    K(pla_k_convert(MPI_DOUBLE, A, lda, MPI_FLOAT, F.a, ld, n, n, stream()));
   const bool lowp = F.prec != PLA_B200_PREC_FP32;
+  const bool f8 = F.prec == PLA_B200_PREC_FP8;
   const int kprec = F.prec == PLA_B200_PREC_BF16 ? PLA_K_BF16 : PLA_K_FP16;
+  const int kmult = f8 ? 128 : 64;  // K granularity of the tensor-core update
   void *Lp = nullptr, *Up = nullptr;
+  float *inv_l = nullptr, *inv_u = nullptr;
   if (lowp) {
     Lp = scratch(kSlotL, (size_t)n * nb * 2 + 256);
     Up = scratch(kSlotU, (size_t)n * nb * 2 + 256);
     if (!Lp || !Up) PLA_FAIL("cannot allocate the low-precision panels");
+    if (f8) {  // one scale per 128 rows of L and of U'
+      const size_t tiles = (size_t)(n + 127) / 128 + 1;
+      inv_l = (float *)scratch(kSlotScales, 2 * tiles * sizeof(float) + 256);
+      if (!inv_l) PLA_FAIL("cannot allocate the fp8 tile scales");
+      inv_u = inv_l + tiles;
+    }
   }
   int *st = F.status;
   PLA_Phase_times &ph = state().phases;
@@ -136,7 +149,25 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
       K(pla_k_trsm_small(MPI_FLOAT, 'R', 'L', 'T', 'N', b, rest, 1.0, at(k, k), ld, at(k + b, k),
                          ld, &st[0], stream()));
     }
-    if (lowp && b % 64 == 0) {
+    if (lowp && f8 && b % kmult == 0) {
+      // L (rest x b, column-major) and U' (U is b x rest: element (j, kk) at
+      // kk + j ld) packed row-major in fp8 with their tile scales
+      const void *Uop = Lp;
+      const float *su = inv_l;
+      {
+        PhaseTimer t(&ph.convert_ms);
+        K(pla_k_pack_fp8(rest, b, at(k + b, k), 1, ld, Lp, nb, inv_l, stream()));
+        if (F.kind == 0) {
+          K(pla_k_pack_fp8(rest, b, at(k, k + b), ld, 1, Up, nb, inv_u, stream()));
+          Uop = Up;
+          su = inv_u;
+        }
+      }
+      PhaseTimer t(&ph.update_ms);
+      K(pla_k_tc_update_fp8(rest, rest, b, -1.0f, Lp, nb, n, inv_l, Uop, nb, n, su, F.a, ld, ld,
+                            n, k + b, k + b, F.kind == 1, &st[0], stream()));
+      if (t.on) ph.update_launches++;
+    } else if (lowp && !f8 && b % kmult == 0) {
       const void *Uop = Lp;
       {
         PhaseTimer t(&ph.convert_ms);
@@ -190,7 +221,13 @@ int precond(const Factor &F, const double *v, long ldv, double *out, long ldo, i
     }
     return PLA_SUCCESS;
   }
-  K(pla_k_convert(MPI_DOUBLE, v, ldv, MPI_FLOAT, t32, n, n, nrhs, stream()));
+  if (F.dsc) {  // M^{-1} = D (L L')^{-1} D: scale in FP64 through `out`
+    K(pla_k_copy(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, nrhs, v, ldv, out, ldo, stream()));
+    K(pla_k_diag_mul(n, nrhs, F.dsc, out, ldo, stream()));
+    K(pla_k_convert(MPI_DOUBLE, out, ldo, MPI_FLOAT, t32, n, n, nrhs, stream()));
+  } else {
+    K(pla_k_convert(MPI_DOUBLE, v, ldv, MPI_FLOAT, t32, n, n, nrhs, stream()));
+  }
   if (F.kind == 0) K(pla_k_laswp_rows(MPI_FLOAT, t32, n, nrhs, n, F.piv, stream()));
   const char u1 = 'L', t1 = 'N', d1 = F.kind == 0 ? 'U' : 'N';
   const char u2 = F.kind == 0 ? 'U' : 'L', t2 = F.kind == 0 ? 'N' : 'T', d2 = 'N';
@@ -207,6 +244,7 @@ int precond(const Factor &F, const double *v, long ldv, double *out, long ldo, i
     K(pla_k_trsv_blocked(MPI_FLOAT, u2, t2, d2, n, nrhs, F.a, F.ld, t32, n, stream()));
   }
   K(pla_k_convert(MPI_FLOAT, t32, n, MPI_DOUBLE, out, ldo, n, nrhs, stream()));
+  if (F.dsc) K(pla_k_diag_mul(n, nrhs, F.dsc, out, ldo, stream()));
   return PLA_SUCCESS;
 }
 
@@ -321,8 +359,13 @@ int gmres(const Factor &F, const double *A, long lda, const double *r, double *d
 
 // the next precision up when the refinement stagnates (0: none left)
 int escalated(int prec) {
-  if (prec == PLA_B200_PREC_FP64) return 0;
-  return prec == PLA_B200_PREC_FP32 ? PLA_B200_PREC_FP64 : PLA_B200_PREC_FP32;
+  switch (prec) {
+    case PLA_B200_PREC_FP8: return PLA_B200_PREC_BF16;
+    case PLA_B200_PREC_BF16:
+    case PLA_B200_PREC_FP16: return PLA_B200_PREC_FP32;
+    case PLA_B200_PREC_FP32: return PLA_B200_PREC_FP64;
+    default: return 0;
+  }
 }
 
 int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
@@ -335,7 +378,7 @@ int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
   if (pin) p = *pin;
   if (p.max_iterations <= 0) p.max_iterations = 50;
   if (p.gmres_restart <= 0) p.gmres_restart = 30;
-  if (p.precision < PLA_B200_PREC_BF16 || p.precision > PLA_B200_PREC_FP64)
+  if (p.precision < PLA_B200_PREC_BF16 || p.precision > PLA_B200_PREC_FP8)
     PLA_FAIL("unknown precision");
   const int n = A->length, nrhs = B->width;
   if (n == 0 || nrhs == 0) {
@@ -402,11 +445,17 @@ int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
         F.a = (float *)scratch(kSlotA32, (size_t)ldf * n * sizeof(float));
         if (!F.a) PLA_FAIL("cannot allocate the fp32 working copy");
         int nb = nb0;
-        if (prec != PLA_B200_PREC_FP32) {
+        if (prec == PLA_B200_PREC_FP8) {
+          nb = std::min(std::max(128, nb / 128 * 128), kind == 0 ? 256 : 128);
+        } else if (prec != PLA_B200_PREC_FP32) {
           nb = std::max(64, nb / 64 * 64);
           nb = std::min(nb, kind == 0 ? 256 : 128);
         } else if (kind == 1) {
           nb = std::min(nb, 128);
+        }
+        if (prec == PLA_B200_PREC_FP8 && kind == 1) {
+          F.dsc = (double *)scratch(kSlotDiag, (size_t)n * sizeof(double) + 256);
+          if (!F.dsc) PLA_FAIL("cannot allocate the diagonal scaling");
         }
         int rc = factor_mixed(F, Ad, lda, nb);
         if (rc) return rc;

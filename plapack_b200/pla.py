@@ -34,6 +34,7 @@ PLA_SUCCESS, PLA_ALIGN_FIRST, PLA_DIM_ALL = 0, -200, -201
 PLA_ERROR = -1000
 
 PLA_B200_PREC_BF16, PLA_B200_PREC_FP16, PLA_B200_PREC_FP32, PLA_B200_PREC_FP64 = 1, 2, 3, 4
+PLA_B200_PREC_FP8 = 5
 PLA_B200_IR_LU, PLA_B200_IR_GMRES = 1, 2
 
 _DT = {np.dtype(np.float64): MPI_DOUBLE, np.dtype(np.float32): MPI_FLOAT,

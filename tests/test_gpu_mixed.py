@@ -293,3 +293,112 @@ def test_sixteen_right_hand_sides(env, prec):
     assert backward_error(A, X, B) <= n * 2.0 ** -53
     Xr = np.linalg.solve(A, B)
     assert np.abs(X - Xr).max() / np.abs(Xr).max() <= 1e6 * n * 2.0 ** -53
+
+
+def fp8_pack(lib, torch, X, si_rows=True):
+    """Pack the rows of X (fp32, m x k) with pla_k_pack_fp8; returns (bytes
+    m x k uint8, inverse scales per 128 rows)."""
+    m, k = X.shape
+    Xc = X.t().contiguous() if si_rows else X.contiguous()  # column-major or row-major source
+    si, sk = (1, m) if si_rows else (k, 1)
+    dst = torch.zeros(m, k, dtype=torch.uint8, device="cuda")
+    inv = torch.zeros((m + 127) // 128, dtype=torch.float32, device="cuda")
+    fn = lib.pla_k_pack_fp8
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_long, ctypes.c_long,
+                   ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p, ctypes.c_void_p]
+    assert fn(m, k, Xc.data_ptr(), si, sk, dst.data_ptr(), k, inv.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    return dst, inv
+
+
+@pytest.mark.parametrize("si_rows", [True, False])
+def test_fp8_pack_scales_and_bytes(env, si_rows):
+    s, torch, pla = env
+    g = torch.Generator(device="cuda").manual_seed(21)
+    m, k = 300, 128
+    X = torch.randn(m, k, device="cuda", generator=g) * torch.logspace(-3, 3, m, device="cuda")[:, None]
+    q, inv = fp8_pack(s.lib, torch, X, si_rows)
+    for b in range(inv.numel()):
+        blk = X[128 * b:128 * b + 128]
+        scale = 1.0 / inv[b].item()
+        assert scale == 2.0 ** round(np.log2(scale))           # a power of two
+        amax = blk.abs().max().item()
+        assert amax * scale <= 448.0 < 2 * amax * scale        # the largest that fits
+        want = (blk * scale).to(torch.float8_e4m3fn).view(torch.uint8)
+        assert torch.equal(q[128 * b:128 * b + 128], want)     # round to nearest even
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 128, 128), (1000, 777, 256), (4096, 3000, 128)])
+def test_tc_update_fp8_matches_dequantized_product(env, M, N, K):
+    s, torch, pla = env
+    g = torch.Generator(device="cuda").manual_seed(M + N)
+    L = torch.randn(M, K, device="cuda", generator=g) * 3.0
+    U = torch.randn(N, K, device="cuda", generator=g) * 0.01
+    Lq, il = fp8_pack(s.lib, torch, L)
+    Uq, iu = fp8_pack(s.lib, torch, U)
+    deq = lambda q, inv: q.view(torch.float8_e4m3fn).float() * inv.repeat_interleave(128)[:q.shape[0], None]
+    ld = (M + 8 + 31) // 32 * 32
+    Cc = torch.randn(N + 12, ld, device="cuda", generator=g)
+    ref = Cc.clone()
+    r0, c0 = 4, 12
+    status = torch.zeros(4, dtype=torch.int32, device="cuda")
+    fn = s.lib.pla_k_tc_update_fp8
+    fn.restype = ctypes.c_int
+    vp, lg, i = ctypes.c_void_p, ctypes.c_long, ctypes.c_int
+    fn.argtypes = [i, i, i, ctypes.c_float, vp, lg, lg, vp, vp, lg, lg, vp, vp, lg, lg, lg, i, i,
+                   i, vp, vp]
+    rc = fn(M, N, K, -1.0, Lq.data_ptr(), K, M, il.data_ptr(), Uq.data_ptr(), K, N, iu.data_ptr(),
+            Cc.data_ptr(), ld, ld, N + 12, r0, c0, 0, status.data_ptr(), None)
+    torch.cuda.synchronize()
+    assert rc == 0 and status[0].item() == 0
+    prod = deq(Lq, il) @ deq(Uq, iu).T
+    ref[c0:c0 + N, r0:r0 + M] -= prod.T
+    assert (Cc - ref).abs().max().item() <= 1e-5 * K * max(1.0, prod.abs().max().item())
+    mask = torch.ones_like(Cc, dtype=torch.bool)
+    mask[c0:c0 + N, r0:r0 + M] = False
+    assert torch.equal(Cc[mask], ref[mask])
+
+
+def spd_family(n, kappa, seed):
+    """A = Q diag(lambda) Q' with lambda log-uniform in [1/kappa, 1] and Q a
+    product of 8 Householder reflectors with seeded Gaussian vectors."""
+    rng = np.random.default_rng(seed)
+    lam = np.exp(rng.uniform(np.log(1.0 / kappa), 0.0, n))
+    lam[0], lam[-1] = 1.0, 1.0 / kappa
+    A = np.diag(lam)
+    for _ in range(8):
+        v = rng.standard_normal(n)
+        A -= (2.0 / (v @ v)) * np.outer(v, v @ A)
+        A -= (2.0 / (v @ v)) * np.outer(A @ v, v)
+    return np.asfortranarray((A + A.T) / 2)
+
+
+@pytest.mark.parametrize("kappa", [1e3, 1e7])
+def test_fp8_cholesky_ir(env, kappa):
+    """FP8 E4M3 trailing updates with per-tile scaling and diagonal scaling,
+    8 right-hand sides: FP64 backward error, forward error against LAPACK;
+    the solver may escalate past FP8 (reported in precision_used)."""
+    s, torch, pla = env
+    n = 2048
+    A = spd_family(n, kappa, 31)
+    Xt = np.random.default_rng(32).standard_normal((n, 8))
+    B = np.asfortranarray(A @ Xt)
+    rc, X, rep = solve_mixed_params(s, pla, A, B, "chol", precision=pla.PLA_B200_PREC_FP8,
+                                    refinement=2)
+    assert rc == 0 and rep.converged == 1, (rep.iterations, rep.backward_error)
+    assert rep.precision_used in (pla.PLA_B200_PREC_FP8, 1, 3, 4)
+    assert backward_error(A, X, B) <= n * 2.0 ** -53
+    Xr = np.linalg.solve(A, B)
+    assert np.abs(X - Xr).max() / np.abs(Xr).max() <= kappa * n * 2.0 ** -53
+
+
+def test_fp8_lu_ir(env):
+    s, torch, pla = env
+    n = 1536
+    A = c3_matrix(n, 1e2, 33)
+    B = np.asfortranarray(A @ np.random.default_rng(34).standard_normal((n, 2)))
+    rc, X, rep = solve_mixed_params(s, pla, A, B, "lu", precision=pla.PLA_B200_PREC_FP8,
+                                    refinement=2)
+    assert rc == 0 and rep.converged == 1, (rep.iterations, rep.backward_error)
+    assert backward_error(A, X, B) <= n * 2.0 ** -53
