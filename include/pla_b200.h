@@ -118,7 +118,7 @@ int PLA_Pos_def_solve_mixed(PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *params
  * a bounded wait in the kernel gave up.
  * For callers that cannot let the library call cudaMalloc -- programs whose
  * GPU memory belongs to another allocator, or services that forbid allocation
- * while running: the kernel's workspace is a fixed array of about 335 KB in
+ * while running: the kernel's workspace is a fixed array of about 667 KB in
  * device memory, present on every GPU that loads the library until the
  * process exits, instead of memory the library allocates.  Limit: w <= 128
  * (larger panels return PLA_ERROR with a message in PLA_Last_error).

@@ -12,16 +12,17 @@
 // the CTA keeps its rows in shared memory for the whole panel; otherwise it
 // works in place in global memory (the panel is L2-resident).
 //
-// Exchange, one round per column: every CTA publishes a record -- its best
-// candidate (|value|, row) as two 64-bit words that each carry a generation
-// bit, the candidate's whole row, and, from the owner of the diagonal row,
-// that row -- and then gathers every CTA's record.  All CTAs pick the same
-// winner from the same records, so no barrier precedes the reads.  Records
-// alternate between two slots by column parity; the generation bit
-// ((j >> 1) & 1) ^ 1 tells the record of column j from that of column j - 2
-// in the same slot, and the slots are zeroed before each launch (generation
-// 0, which no record of column 0 or 1 has).  A CTA can only overwrite a slot
-// after every CTA has published the next column, that is after every CTA has
+// Exchange, one round per column, with no grid barrier and no memory fence:
+// every CTA publishes a record -- its best candidate (|value|, row) -- the
+// candidate's whole row, and, from the owner of the diagonal row, that row.
+// Every 32-bit datum travels in a 64-bit word together with the tag of its
+// launch and column, so a reader that polls a word until the tag matches has
+// the datum, whatever order the writer's stores became visible in.  Warp 0
+// of every CTA polls all records in one batch of loads per round and picks
+// the winner; then the CTA polls the winner's row and the diagonal row.  All
+// CTAs pick the same winner from the same records.  Records alternate
+// between two slots by column parity: a CTA can only overwrite a slot after
+// every CTA has published the next column, that is after every CTA has
 // finished reading the slot.
 //
 // Lookahead inside the panel: after the pivot of column j a CTA updates only
@@ -30,6 +31,7 @@
 // published values are bitwise those the CTA stores later), and then updates
 // its remaining columns while the other CTAs publish.  Every wait is bounded;
 // on timeout the kernel records PLA_K_TIMEOUT and exits.
+#include <atomic>
 #include <climits>
 #include <cstdio>
 #include <mutex>
@@ -42,6 +44,7 @@ namespace {
 constexpr int kThreads = 256;
 constexpr long kSpinLimit = 4000000;  // polls before giving up (~1-2 s)
 constexpr int kPerLane = 5;           // records per lane of the gathering warp: P <= 160
+constexpr int kMaxWidth = 256;        // columns per launch: the column is 8 bits of the tag
 
 __device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long *p) {
   unsigned long long v;
@@ -52,21 +55,35 @@ __device__ __forceinline__ void st_relaxed64(unsigned long long *p, unsigned lon
   asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// record words: bit 63 the generation, below it |value| (>= 0, so its own
-// sign bit is free) or the row index
-template <typename T>
-__device__ __forceinline__ unsigned long long enc_val(T v, unsigned long long gen) {
-  if constexpr (sizeof(T) == 8)
-    return (gen << 63) | (unsigned long long)__double_as_longlong(v);
-  else
-    return (gen << 63) | (unsigned long long)__float_as_uint(v);
+// Published words: the high 32 bits carry the tag of the column they belong
+// to, (launch sequence << 8) | column, the low 32 bits one 32-bit datum (a
+// float, half of a double, or a row index).  A 64-bit relaxed load sees a
+// whole word, so a reader that finds the expected tag has the datum of this
+// launch and column, whatever order the writer's stores became visible in.
+__device__ __forceinline__ unsigned long long word(unsigned tag, unsigned bits) {
+  return ((unsigned long long)tag << 32) | bits;
 }
 template <typename T>
-__device__ __forceinline__ T dec_val(unsigned long long w) {
+__device__ __forceinline__ unsigned half_bits(T v, int h) {
+  if constexpr (sizeof(T) == 8) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return h ? (unsigned)(b >> 32) : (unsigned)b;
+  } else {
+    return __float_as_uint(v);
+  }
+}
+// store element v as sizeof(T) / 4 tagged words at p
+template <typename T>
+__device__ __forceinline__ void put(unsigned long long *p, T v, unsigned tag) {
+#pragma unroll
+  for (int h = 0; h < (int)(sizeof(T) / 4); h++) st_relaxed64(p + h, word(tag, half_bits(v, h)));
+}
+template <typename T>
+__device__ __forceinline__ T join(const unsigned *bits) {
   if constexpr (sizeof(T) == 8)
-    return __longlong_as_double((long long)(w & ~(1ull << 63)));
+    return __longlong_as_double((long long)(((unsigned long long)bits[1] << 32) | bits[0]));
   else
-    return __uint_as_float((unsigned)(w & 0xffffffffull));
+    return __uint_as_float(bits[0]);
 }
 
 // (abs, idx) ordering: larger |value| first, then smaller index
@@ -101,25 +118,33 @@ __device__ void block_argmax(T &v, int &i, T *sv, int *si) {
   i = si[0];
 }
 
-// rec: [2 slots][P CTAs][2 words]; cand_row: [2][P][w]; top_row: [2][w]
+// Workspace, in tagged words (NW = sizeof(T) / 4 words per element), two
+// slots by column parity:
+//   rec  [2][P][NW + 1]  |value| of each CTA's candidate, then its row index
+//   crow [2][P][w][NW]   each candidate's row
+//   trow [2][w][NW]      the diagonal row, published by its owner
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 1)
 panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *status,
-           int *zero_info, int row_base, unsigned long long *rec, T *cand_row, T *top_row) {
+           int *zero_info, int row_base, unsigned seq, unsigned long long *rec,
+           unsigned long long *crow, unsigned long long *trow) {
+  constexpr int NW = (int)(sizeof(T) / 4), NR = NW + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ T s_v[32];
   __shared__ int s_i[32];
-  __shared__ int s_abort, s_p, s_q;
+  __shared__ int s_p, s_q;
 
   const int P = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
   const int row0 = b * R;
   const int row1 = min(row0 + R, r);
   const int nrows = max(row1 - row0, 0);
-  T *u = reinterpret_cast<T *>(smem_raw);  // pivot row, w entries
+  const int wp = (w + 1) & ~1;
+  T *u = reinterpret_cast<T *>(smem_raw);  // the pivot row, w entries
+  T *tr = u + wp;                          // the diagonal row as it was before the swap
   T *S;
   long lds;
   if (use_smem) {
-    S = u + ((w + 1) & ~1);
+    S = tr + wp;
     lds = R;
     for (long t = tid; t < (long)nrows * w; t += kThreads) {
       int i = (int)(t % nrows), c = (int)(t / nrows);
@@ -129,8 +154,8 @@ panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *sta
     S = A + row0;
     lds = lda;
   }
-  if (tid == 0) s_abort = 0;
   __syncthreads();
+  const unsigned tag0 = (seq & 0xffffffu) << 8;
 #define E(i, c) S[(long)(i) + (long)(c) * lds]
 
   // Publish the record of column `col`.  With `pend` the rows still owe the
@@ -138,7 +163,7 @@ panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *sta
   // E(., col - 1), pivot row u): the published rows include it.
   auto publish = [&](int col, bool pend) {
     const int par = col & 1;
-    const unsigned long long gen = (unsigned long long)(((col >> 1) & 1) ^ 1);
+    const unsigned tag = tag0 | (unsigned)col;
     T best = T(-1);
     int bidx = INT_MAX;
     const int lo = max(col - row0, 0);
@@ -153,49 +178,51 @@ panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *sta
     };
     if (bidx != INT_MAX)
       for (int c = tid; c < w; c += kThreads)
-        cand_row[((long)par * P + b) * w + c] = row_val(bidx - row0, c);
+        put<T>(crow + (((long)par * P + b) * w + c) * NW, row_val(bidx - row0, c), tag);
     if (col >= row0 && col < row1)
-      for (int c = tid; c < w; c += kThreads) top_row[(long)par * w + c] = row_val(col - row0, c);
-    __syncthreads();
+      for (int c = tid; c < w; c += kThreads)
+        put<T>(trow + ((long)par * w + c) * NW, row_val(col - row0, c), tag);
     if (tid == 0) {
-      __threadfence();
-      unsigned long long *rp = rec + ((long)par * P + b) * 2;
+      unsigned long long *rp = rec + ((long)par * P + b) * NR;
       const bool none = bidx == INT_MAX;  // no candidate: every entry is NaN
-      st_relaxed64(rp, enc_val<T>(none ? T(0) : best, gen));
-      st_relaxed64(rp + 1, (gen << 63) | (unsigned)(none ? INT_MAX : bidx));
+      put<T>(rp, none ? T(0) : best, tag);
+      st_relaxed64(rp + NW, word(tag, (unsigned)(none ? INT_MAX : bidx)));
     }
+    __syncthreads();  // the rows above are read before the update below writes them
   };
 
-  // Gather the records of column `col` into (s_p = winning row or INT_MAX,
-  // s_q = its CTA); false when a wait gave up.  Lane l of warp 0 watches the
-  // records of CTAs l, l + 32, ...: each poll loads all of them at once
-  // (independent loads, one round trip), and one acquire fence follows once
-  // every record carries the column's generation.
+  // Gather column `col`: warp 0 polls every CTA's record (one batch of loads
+  // per poll) and picks the winner; then all threads poll the winner's row
+  // into u and the diagonal row into tr.  False when a wait gave up.
   auto gather = [&](int col) -> bool {
     const int par = col & 1;
-    const unsigned long long gen = (unsigned long long)(((col >> 1) & 1) ^ 1);
+    const unsigned tag = tag0 | (unsigned)col;
+    bool ok = true;
     if (tid < 32) {
-      unsigned long long w0[kPerLane], w1[kPerLane];
+      unsigned long long wv[kPerLane][NR];
       bool done[kPerLane];
 #pragma unroll
       for (int i = 0; i < kPerLane; i++) {
         done[i] = tid + 32 * i >= P;
-        w0[i] = w1[i] = 0;
+#pragma unroll
+        for (int h = 0; h < NR; h++) wv[i][h] = 0;
       }
-      bool ok = true;
       for (long spins = 0;; spins++) {
 #pragma unroll
         for (int i = 0; i < kPerLane; i++)
           if (!done[i]) {
-            const unsigned long long *rp = rec + ((long)par * P + tid + 32 * i) * 2;
-            w0[i] = ld_relaxed64(rp);
-            w1[i] = ld_relaxed64(rp + 1);
+            const unsigned long long *rp = rec + ((long)par * P + tid + 32 * i) * NR;
+#pragma unroll
+            for (int h = 0; h < NR; h++) wv[i][h] = ld_relaxed64(rp + h);
           }
         bool all = true;
 #pragma unroll
         for (int i = 0; i < kPerLane; i++)
           if (!done[i]) {
-            if ((w0[i] >> 63) == gen && (w1[i] >> 63) == gen) done[i] = true;
+            bool v = true;
+#pragma unroll
+            for (int h = 0; h < NR; h++) v = v && (unsigned)(wv[i][h] >> 32) == tag;
+            if (v) done[i] = true;
             else all = false;
           }
         if (all) break;
@@ -204,18 +231,19 @@ panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *sta
           break;
         }
       }
-      __threadfence();  // acquire: the rows published before the records are visible
       T bv = T(-1);
       int bi = INT_MAX, bq = 0;
 #pragma unroll
       for (int i = 0; i < kPerLane; i++) {
         const int q = tid + 32 * i;
         if (q >= P) continue;
-        const T v = dec_val<T>(w0[i]);
-        const int ix = (int)(unsigned)(w1[i] & 0xffffffffull);
+        unsigned bits[NW];
+#pragma unroll
+        for (int h = 0; h < NW; h++) bits[h] = (unsigned)wv[i][h];
+        const T v = join<T>(bits);
+        const int ix = (int)(unsigned)wv[i][NW];
         if (better(v, ix, bv, bi)) { bv = v; bi = ix; bq = q; }
       }
-      const bool all_ok = __all_sync(0xffffffffu, ok);
       for (int o = 16; o; o >>= 1) {
         T ov = __shfl_down_sync(0xffffffffu, bv, o);
         int oi = __shfl_down_sync(0xffffffffu, bi, o);
@@ -223,35 +251,51 @@ panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *sta
         if (better(ov, oi, bv, bi)) { bv = ov; bi = oi; bq = oq; }
       }
       if (tid == 0) {
-        if (!all_ok) {
-          atomicCAS(status, PLA_K_OK, PLA_K_TIMEOUT);
-          s_abort = 1;
-        }
         s_p = bi;
         s_q = bq;
       }
     }
-    __syncthreads();
-    return s_abort == 0;
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) atomicCAS(status, PLA_K_OK, PLA_K_TIMEOUT);
+      return false;
+    }
+    // A column of NaNs has no candidate (NaN never compares greater): row col
+    // stays its own pivot, and u is the diagonal row.
+    const bool none = s_p == INT_MAX;
+    const int q = s_q, half = w * NW;
+    unsigned *ub = reinterpret_cast<unsigned *>(u), *tb = reinterpret_cast<unsigned *>(tr);
+    for (int e = tid; e < 2 * half; e += kThreads) {
+      const bool top = e >= half || none;
+      const int k = e < half ? e : e - half;
+      const unsigned long long *src =
+          top ? trow + (long)par * half + k : crow + ((long)par * P + q) * half + k;
+      unsigned long long v = 0;
+      for (long spins = 0;; spins++) {
+        v = ld_relaxed64(src);
+        if ((unsigned)(v >> 32) == tag) break;
+        if (spins > kSpinLimit || *(volatile int *)status != PLA_K_OK) {
+          ok = false;
+          break;
+        }
+      }
+      (e < half ? ub : tb)[k] = (unsigned)v;
+    }
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) atomicCAS(status, PLA_K_OK, PLA_K_TIMEOUT);
+      return false;
+    }
+    return true;
   };
 
   publish(0, false);
   for (int j = 0; j < w; j++) {
     if (!gather(j)) return;
-    const int par = j & 1;
-    // A column of NaNs has no candidate (NaN never compares greater): keep
-    // row j as its own pivot, whose contents the owner of row j published.
-    const bool none = s_p == INT_MAX;
-    const int p = none ? j : s_p, wq = s_q;
-    for (int c = tid; c < w; c += kThreads)
-      u[c] = none ? __ldcg(&top_row[(long)par * w + c])
-                  : __ldcg(&cand_row[((long)par * P + wq) * w + c]);
-    __syncthreads();
+    const int p = s_p == INT_MAX ? j : s_p;
     // the interchange of rows j and p over the panel width
     if (j >= row0 && j < row1)
       for (int c = tid; c < w; c += kThreads) E(j - row0, c) = u[c];
     if (p != j && p >= row0 && p < row1)
-      for (int c = tid; c < w; c += kThreads) E(p - row0, c) = __ldcg(&top_row[(long)par * w + c]);
+      for (int c = tid; c < w; c += kThreads) E(p - row0, c) = tr[c];
     if (b == 0 && tid == 0) {
       piv[j] = p - j;
       if (zero_info && u[j] == T(0)) atomicCAS(zero_info, 0, row_base + j + 1);
@@ -286,19 +330,28 @@ panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *sta
 #undef E
 }
 
-// workspace layout for P CTAs and width w: the record slots (zeroed before
-// every launch), the candidate rows and the diagonal rows
+// workspace layout for P CTAs and width w, in tagged words
 struct Layout {
-  size_t rec_bytes, off_row, off_top, total;
+  size_t off_crow, off_trow, words;
 };
 template <typename T>
 Layout layout(int P, int w) {
+  const size_t nw = sizeof(T) / 4;
   Layout l;
-  l.rec_bytes = ((size_t)2 * P * 2 * sizeof(unsigned long long) + 255) & ~(size_t)255;
-  l.off_row = l.rec_bytes;
-  l.off_top = l.off_row + (size_t)2 * P * w * sizeof(T);
-  l.total = l.off_top + (size_t)2 * w * sizeof(T);
+  l.off_crow = (size_t)2 * P * (nw + 1);
+  l.off_trow = l.off_crow + (size_t)2 * P * w * nw;
+  l.words = l.off_trow + (size_t)2 * w * nw;
   return l;
+}
+
+// launch sequence number for the tags: never 0 in its low 24 bits, so no tag
+// matches a zeroed word
+std::atomic<unsigned> g_seq{0};
+unsigned next_seq() {
+  unsigned v;
+  do v = ++g_seq;
+  while ((v & 0xffffffu) == 0);
+  return v;
 }
 
 struct Workspace {
@@ -335,7 +388,7 @@ int launch(int r, int w, void *A, long lda, int *piv, int *status, int *zero_inf
   if (P < 1) P = 1;
   int R = (r + P - 1) / P;
   P = (r + R - 1) / R;
-  size_t ubytes = (size_t)((w + 1) & ~1) * sizeof(T);
+  size_t ubytes = (size_t)2 * ((w + 1) & ~1) * sizeof(T);  // u and tr
   size_t sbytes = ubytes + (size_t)R * w * sizeof(T);
   int use_smem = sbytes + 1024 <= (size_t)g_smem_optin - 2048;
   size_t dyn = use_smem ? sbytes : ubytes;
@@ -344,17 +397,16 @@ int launch(int r, int w, void *A, long lda, int *piv, int *status, int *zero_inf
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, panel_lu_k<T>, kThreads, dyn);
   if (per_sm * g_sms < P) return (int)cudaErrorCooperativeLaunchTooLarge;
   const Layout lay = layout<T>(P, w);
-  char *ws = (char *)workspace(lay.total);
+  unsigned long long *ws =
+      (unsigned long long *)workspace(lay.words * sizeof(unsigned long long));
   if (!ws) return (int)cudaErrorMemoryAllocation;
-  cudaError_t e = cudaMemsetAsync(ws, 0, lay.rec_bytes, s);
-  if (e) return (int)e;
-  unsigned long long *rec = (unsigned long long *)ws;
-  T *cand_row = (T *)(ws + lay.off_row);
-  T *top_row = (T *)(ws + lay.off_top);
+  unsigned long long *rec = ws, *crow = ws + lay.off_crow, *trow = ws + lay.off_trow;
+  unsigned seq = next_seq();
   T *Ap = (T *)A;
-  void *args[] = {&Ap, &lda, &r, &w, &R, &use_smem, &piv, &status, &zero_info, &row_base, &rec,
-                  &cand_row, &top_row};
-  e = cudaLaunchCooperativeKernel((void *)panel_lu_k<T>, dim3(P), dim3(kThreads), args, dyn, s);
+  void *args[] = {&Ap, &lda, &r, &w, &R, &use_smem, &piv, &status, &zero_info, &row_base, &seq,
+                  &rec, &crow, &trow};
+  cudaError_t e =
+      cudaLaunchCooperativeKernel((void *)panel_lu_k<T>, dim3(P), dim3(kThreads), args, dyn, s);
   pla_k_count(1);
   return (int)e;
 }
@@ -364,7 +416,7 @@ int launch(int r, int w, void *A, long lda, int *piv, int *status, int *zero_inf
 extern "C" int pla_k_lu_panel(int dt, int r, int w, void *A, long lda, int *piv, int *status,
                               int *zero_info, int row_base, cudaStream_t s) {
   if (r <= 0 || w <= 0) return 0;
-  if (w > r) return (int)cudaErrorInvalidValue;
+  if (w > r || w > kMaxWidth) return (int)cudaErrorInvalidValue;
   if (dt == MPI_DOUBLE) return launch<double>(r, w, A, lda, piv, status, zero_info, row_base, s);
   if (dt == MPI_FLOAT) return launch<float>(r, w, A, lda, piv, status, zero_info, row_base, s);
   return (int)cudaErrorInvalidValue;
@@ -386,18 +438,18 @@ extern "C" void pla_kernels_release(void) {
 // kernel's workspace -- the per-CTA pivot records and candidate rows -- lives
 // in the fixed device array below instead of memory the library allocates.
 // The array holds the workspace of at most kNoAllocCtas CTAs for panels of at
-// most kNoAllocWidth columns in double precision (about 335 KB); every GPU
+// most kNoAllocWidth columns in double precision (about 667 KB); every GPU
 // that loads the library keeps it until the process exits.  Every call shares
 // it, so calls whose kernels overlap on the GPU (on different streams, or from
 // different host threads) race.
 namespace {
 constexpr int kNoAllocCtas = 160;
 constexpr int kNoAllocWidth = 128;
-// the double-precision layout at the limits; a float panel needs less
-constexpr size_t kNoAllocRec = ((size_t)2 * kNoAllocCtas * 2 * 8 + 255) & ~(size_t)255;
-constexpr size_t kNoAllocBytes = kNoAllocRec +
-                                 (size_t)2 * kNoAllocCtas * kNoAllocWidth * sizeof(double) +
-                                 (size_t)2 * kNoAllocWidth * sizeof(double);
+// the double-precision layout at the limits, in 8-byte words; a float panel
+// needs less
+constexpr size_t kNoAllocBytes =
+    8 * ((size_t)2 * kNoAllocCtas * 3 + (size_t)2 * kNoAllocCtas * kNoAllocWidth * 2 +
+         (size_t)2 * kNoAllocWidth * 2);
 }  // namespace
 
 static __device__ __align__(256) unsigned char g_panel_scratch[kNoAllocBytes];
@@ -439,7 +491,7 @@ int launch_noalloc(int r, int w, T *A, long lda, int *piv, int *status, cudaStre
   if (P < 1) P = 1;
   int R = (r + P - 1) / P;
   P = (r + R - 1) / R;
-  size_t ubytes = (size_t)((w + 1) & ~1) * sizeof(T);
+  size_t ubytes = (size_t)2 * ((w + 1) & ~1) * sizeof(T);  // u and tr
   size_t sbytes = ubytes + (size_t)R * w * sizeof(T);
   int use_smem = sbytes + 1024 <= (size_t)optin - 2048;
   size_t dyn = use_smem ? sbytes : ubytes;
@@ -450,20 +502,17 @@ int launch_noalloc(int r, int w, T *A, long lda, int *piv, int *status, cudaStre
   char *ws = nullptr;
   int rc = noalloc_scratch(&ws);
   if (rc) return rc;
-  // the record slots must start at zero (their generation bits); the
-  // candidate rows are written before they are read, so the last call's
-  // contents are harmless
+  // Nothing in the array needs clearing: every word a call reads carries the
+  // call's own tag, so what earlier calls left there is never taken for data.
   const Layout lay = layout<T>(P, w);
-  if (lay.total > kNoAllocBytes) return (int)cudaErrorInvalidValue;
-  e = cudaMemsetAsync(ws, 0, lay.rec_bytes, s);
-  if (e != cudaSuccess) return (int)e;
-  unsigned long long *rec = (unsigned long long *)ws;
-  T *cand_row = (T *)(ws + lay.off_row);
-  T *top_row = (T *)(ws + lay.off_top);
+  if (lay.words * sizeof(unsigned long long) > kNoAllocBytes) return (int)cudaErrorInvalidValue;
+  unsigned long long *wsw = (unsigned long long *)ws;
+  unsigned long long *rec = wsw, *crow = wsw + lay.off_crow, *trow = wsw + lay.off_trow;
+  unsigned seq = next_seq();
   int *zero_info = nullptr;
   int row_base = 0;
-  void *args[] = {&A,        &lda,      &r,   &w,        &R,        &use_smem, &piv,
-                  &status,   &zero_info, &row_base, &rec, &cand_row, &top_row};
+  void *args[] = {&A,   &lda,      &r,        &w,   &R,   &use_smem, &piv,
+                  &status, &zero_info, &row_base, &seq, &rec, &crow,  &trow};
   e = cudaLaunchCooperativeKernel((void *)panel_lu_k<T>, dim3(P), dim3(kThreads), args, dyn, s);
   pla_k_count(1);
   return (int)e;
