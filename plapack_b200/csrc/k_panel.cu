@@ -374,7 +374,7 @@ int g_sms = 0, g_smem_optin = 0;
 
 template <typename T>
 int launch(int r, int w, void *A, long lda, int *piv, int *status, int *zero_info, int row_base,
-           cudaStream_t s) {
+           int max_ctas, cudaStream_t s) {
   if (!g_sms) {
     int dev;
     cudaGetDevice(&dev);
@@ -385,6 +385,7 @@ int launch(int r, int w, void *A, long lda, int *piv, int *status, int *zero_inf
   int P = (r + 31) / 32;
   if (P > g_sms) P = g_sms;
   if (P > 32 * kPerLane) P = 32 * kPerLane;  // the records one warp gathers
+  if (max_ctas > 0 && P > max_ctas) P = max_ctas;
   if (P < 1) P = 1;
   int R = (r + P - 1) / P;
   P = (r + R - 1) / R;
@@ -413,13 +414,20 @@ int launch(int r, int w, void *A, long lda, int *piv, int *status, int *zero_inf
 
 }  // namespace
 
-extern "C" int pla_k_lu_panel(int dt, int r, int w, void *A, long lda, int *piv, int *status,
-                              int *zero_info, int row_base, cudaStream_t s) {
+extern "C" int pla_k_lu_panel_ex(int dt, int r, int w, void *A, long lda, int *piv, int *status,
+                                 int *zero_info, int row_base, int max_ctas, cudaStream_t s) {
   if (r <= 0 || w <= 0) return 0;
   if (w > r || w > kMaxWidth) return (int)cudaErrorInvalidValue;
-  if (dt == MPI_DOUBLE) return launch<double>(r, w, A, lda, piv, status, zero_info, row_base, s);
-  if (dt == MPI_FLOAT) return launch<float>(r, w, A, lda, piv, status, zero_info, row_base, s);
+  if (dt == MPI_DOUBLE)
+    return launch<double>(r, w, A, lda, piv, status, zero_info, row_base, max_ctas, s);
+  if (dt == MPI_FLOAT)
+    return launch<float>(r, w, A, lda, piv, status, zero_info, row_base, max_ctas, s);
   return (int)cudaErrorInvalidValue;
+}
+
+extern "C" int pla_k_lu_panel(int dt, int r, int w, void *A, long lda, int *piv, int *status,
+                              int *zero_info, int row_base, cudaStream_t s) {
+  return pla_k_lu_panel_ex(dt, r, w, A, lda, piv, status, zero_info, row_base, 0, s);
 }
 
 extern "C" void pla_kernels_release(void) {

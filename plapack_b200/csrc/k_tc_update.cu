@@ -387,7 +387,7 @@ int g_sms = 0;
 template <bool F8>
 int launch(const CUtensorMap &mL, const CUtensorMap &mU, const CUtensorMap &mC, int M, int N,
            int kchunks, int row0, int col0, float alpha, uint32_t idesc, int lower,
-           const float *inv_l, const float *inv_u, int *status, cudaStream_t s) {
+           const float *inv_l, const float *inv_u, int max_ctas, int *status, cudaStream_t s) {
   if (!g_sms) {
     int dev = 0;
     cudaGetDevice(&dev);
@@ -395,7 +395,8 @@ int launch(const CUtensorMap &mL, const CUtensorMap &mU, const CUtensorMap &mC, 
   }
   cudaFuncSetAttribute(tc_update_k<F8>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
   const long tiles = (long)((M + TM - 1) / TM) * ((N + TN - 1) / TN);
-  const int grid = (int)(tiles < g_sms ? tiles : g_sms);
+  const int cap = max_ctas > 0 && max_ctas < g_sms ? max_ctas : g_sms;
+  const int grid = (int)(tiles < cap ? tiles : cap);
   tc_update_k<F8><<<grid, THREADS, SMEM_BYTES, s>>>(mL, mU, mC, M, N, kchunks, row0, col0, alpha,
                                                     idesc, lower, inv_l, inv_u, status);
   pla_k_count(1);
@@ -404,10 +405,10 @@ int launch(const CUtensorMap &mL, const CUtensorMap &mU, const CUtensorMap &mC, 
 
 }  // namespace
 
-extern "C" int pla_k_tc_update(int prec, int M, int N, int K, float alpha, const void *L,
-                               long ldl, long l_rows, const void *U, long ldu, long u_rows,
-                               float *C, long ldc, long c_rows, long c_cols, int row0, int col0,
-                               int lower, int *status, cudaStream_t s) {
+extern "C" int pla_k_tc_update_ex(int prec, int M, int N, int K, float alpha, const void *L,
+                                  long ldl, long l_rows, const void *U, long ldu, long u_rows,
+                                  float *C, long ldc, long c_rows, long c_cols, int row0,
+                                  int col0, int lower, int max_ctas, int *status, cudaStream_t s) {
   if (M <= 0 || N <= 0 || K <= 0) return 0;
   if (K % KBOX != 0) return (int)cudaErrorInvalidValue;
   if (ldl % 8 || ldu % 8 || ldc % 4 || (row0 % 4) || ((uintptr_t)C % 16) || ((uintptr_t)L % 16) ||
@@ -432,17 +433,25 @@ extern "C" int pla_k_tc_update(int prec, int M, int N, int K, float alpha, const
   const uint32_t idesc = (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)(TN >> 3) << 17) |
                          ((uint32_t)(TM >> 4) << 24);
   return launch<false>(mL, mU, mC, M, N, K / KBOX, row0, col0, alpha, idesc, lower, nullptr,
-                       nullptr, status, s);
+                       nullptr, max_ctas, status, s);
+}
+
+extern "C" int pla_k_tc_update(int prec, int M, int N, int K, float alpha, const void *L,
+                               long ldl, long l_rows, const void *U, long ldu, long u_rows,
+                               float *C, long ldc, long c_rows, long c_cols, int row0, int col0,
+                               int lower, int *status, cudaStream_t s) {
+  return pla_k_tc_update_ex(prec, M, N, K, alpha, L, ldl, l_rows, U, ldu, u_rows, C, ldc, c_rows,
+                            c_cols, row0, col0, lower, 0, status, s);
 }
 
 // The same update with fp8 E4M3 operands (row-major, K-contiguous, ldl / ldu
 // bytes) and per-128-row-tile inverse scales: C += alpha * inv_l[i / 128] *
 // inv_u[j / 128] * sum_k L(i, k) U(j, k).
-extern "C" int pla_k_tc_update_fp8(int M, int N, int K, float alpha, const void *L, long ldl,
-                                   long l_rows, const float *inv_l, const void *U, long ldu,
-                                   long u_rows, const float *inv_u, float *C, long ldc,
-                                   long c_rows, long c_cols, int row0, int col0, int lower,
-                                   int *status, cudaStream_t s) {
+extern "C" int pla_k_tc_update_fp8_ex(int M, int N, int K, float alpha, const void *L,
+                                      long ldl, long l_rows, const float *inv_l, const void *U,
+                                      long ldu, long u_rows, const float *inv_u, float *C,
+                                      long ldc, long c_rows, long c_cols, int row0, int col0,
+                                      int lower, int max_ctas, int *status, cudaStream_t s) {
   if (M <= 0 || N <= 0 || K <= 0) return 0;
   if (K % 128 != 0 || !inv_l || !inv_u) return (int)cudaErrorInvalidValue;
   if (ldl % 16 || ldu % 16 || ldc % 4 || (row0 % 4) || ((uintptr_t)C % 16) ||
@@ -463,5 +472,14 @@ extern "C" int pla_k_tc_update_fp8(int M, int N, int K, float alpha, const void 
   // (format 0), both K-major, N = 128, M = 128
   const uint32_t idesc = (1u << 4) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
   return launch<true>(mL, mU, mC, M, N, K / 128, row0, col0, alpha, idesc, lower, inv_l, inv_u,
-                      status, s);
+                      max_ctas, status, s);
+}
+
+extern "C" int pla_k_tc_update_fp8(int M, int N, int K, float alpha, const void *L, long ldl,
+                                   long l_rows, const float *inv_l, const void *U, long ldu,
+                                   long u_rows, const float *inv_u, float *C, long ldc,
+                                   long c_rows, long c_cols, int row0, int col0, int lower,
+                                   int *status, cudaStream_t s) {
+  return pla_k_tc_update_fp8_ex(M, N, K, alpha, L, ldl, l_rows, inv_l, U, ldu, u_rows, inv_u, C,
+                                ldc, c_rows, c_cols, row0, col0, lower, 0, status, s);
 }

@@ -34,10 +34,32 @@ bool valid(PLA_Template t) { return t != nullptr && t->magic == kTempMagic; }
 
 cudaStream_t stream() {
   State &s = state();
+  if (s.override_stream) return s.override_stream;
   if (s.stream) return s.stream;
   if (!s.own_stream) cudaStreamCreateWithFlags(&s.own_stream, cudaStreamNonBlocking);
   return s.own_stream;
 }
+
+cudaStream_t lookahead_stream() {
+  State &s = state();
+  if (!s.la_stream) {
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    cudaStreamCreateWithPriority(&s.la_stream, cudaStreamNonBlocking, hi);
+  }
+  return s.la_stream;
+}
+
+cudaEvent_t lookahead_event(int i) {
+  State &s = state();
+  if (!s.la_events[i]) cudaEventCreateWithFlags(&s.la_events[i], cudaEventDisableTiming);
+  return s.la_events[i];
+}
+
+OnStream::OnStream(cudaStream_t st) : saved(state().override_stream) {
+  state().override_stream = st;
+}
+OnStream::~OnStream() { state().override_stream = saved; }
 
 int fail(const char *message, int line, const char *file) {
   State &s = state();
@@ -283,6 +305,16 @@ int PLA_Finalize(void) {
   cudaStreamSynchronize(stream());
   release_scratch();
   pla_kernels_release();
+  if (s.la_stream) {
+    cudaStreamSynchronize(s.la_stream);
+    cudaStreamDestroy(s.la_stream);
+    s.la_stream = nullptr;
+  }
+  for (auto &e : s.la_events)
+    if (e) {
+      cudaEventDestroy(e);
+      e = nullptr;
+    }
   if (s.own_stream) {
     cudaStreamDestroy(s.own_stream);
     s.own_stream = nullptr;

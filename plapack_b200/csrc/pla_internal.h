@@ -65,6 +65,9 @@ struct State {
   std::string last_message;
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;
+  cudaStream_t override_stream = nullptr;  // set by OnStream while a scope queues elsewhere
+  cudaStream_t la_stream = nullptr;        // high-priority stream of the lookahead panels
+  cudaEvent_t la_events[2] = {nullptr, nullptr};
   int phase_timing = 0;
   PLA_Phase_times phases{};
 };
@@ -74,6 +77,22 @@ int esize_of(MPI_Datatype dt);
 bool valid(PLA_Obj obj);
 bool valid(PLA_Template t);
 cudaStream_t stream();
+
+// Lookahead: panels run on a second, high-priority stream while the trailing
+// update of the previous step runs on stream(); two events order them.
+// CTAs of a panel that runs beside a trailing update: few enough to leave the
+// update most SMs, enough that a 32-column FP64 sub-panel of 32768 rows still
+// fits in their shared memory (683 rows x 32 x 8 bytes each)
+constexpr int kLookaheadCtas = 48;
+cudaStream_t lookahead_stream();
+cudaEvent_t lookahead_event(int i);
+// while alive, stream() returns `s` (host code is sequential, so the switch
+// only affects the calls made inside the scope)
+struct OnStream {
+  cudaStream_t saved;
+  explicit OnStream(cudaStream_t s);
+  ~OnStream();
+};
 
 // typed pointer to element (i, j) of a view (device pointer unless on_host)
 inline char *at(PLA_Obj v, long i, long j) {

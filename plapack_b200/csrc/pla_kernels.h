@@ -38,6 +38,10 @@ int pla_k_convert(int dt_src, const void *src, long lds, int dt_dst, void *dst, 
 /* ---- panel LU: factor the r x w panel at A in place with partial pivoting.
  * piv[j] = offset from row j to the pivot row (reference encoding).
  * zero_info (optional): set to the 1-based first exact zero pivot + row_base. */
+/* the same with at most max_ctas CTAs (0: one per SM), leaving the other SMs
+ * to kernels that run beside it */
+int pla_k_lu_panel_ex(int dt, int r, int w, void *A, long lda, int *piv, int *status,
+                      int *zero_info, int row_base, int max_ctas, cudaStream_t s);
 int pla_k_lu_panel(int dt, int r, int w, void *A, long lda, int *piv, int *status,
                    int *zero_info, int row_base, cudaStream_t s);
 
@@ -109,6 +113,16 @@ int pla_k_tc_update(int prec, int M, int N, int K, float alpha, const void *L, l
                     long l_rows, const void *U, long ldu, long u_rows, float *C, long ldc,
                     long c_rows, long c_cols, int row0, int col0, int lower, int *status,
                     cudaStream_t s);
+/* the tensor-core updates on at most max_ctas persistent CTAs (0: one per SM) */
+int pla_k_tc_update_ex(int prec, int M, int N, int K, float alpha, const void *L, long ldl,
+                       long l_rows, const void *U, long ldu, long u_rows, float *C, long ldc,
+                       long c_rows, long c_cols, int row0, int col0, int lower, int max_ctas,
+                       int *status, cudaStream_t s);
+int pla_k_tc_update_fp8_ex(int M, int N, int K, float alpha, const void *L, long ldl,
+                           long l_rows, const float *inv_l, const void *U, long ldu, long u_rows,
+                           const float *inv_u, float *C, long ldc, long c_rows, long c_cols,
+                           int row0, int col0, int lower, int max_ctas, int *status,
+                           cudaStream_t s);
 /* pla_k_tc_update with fp8 E4M3 operands (ldl / ldu in bytes, K % 128 == 0)
  * and per-128-row-tile inverse scales of L (inv_l) and of U (inv_u) */
 int pla_k_tc_update_fp8(int M, int N, int K, float alpha, const void *L, long ldl, long l_rows,

@@ -29,7 +29,7 @@ int chol_on_device(int dt, int n, char *A, long lda, int nb, int *info_host);
 int trsm_device(int dt, char side, char uplo, char trans, char diag, int nt, int other,
                 double alpha, const char *T, long ldt, char *B, long ldb);
 int panel_lu(int dt, int r, int b, char *P, long lda, int *piv, int *status, int *zero_info,
-             int row_base);
+             int row_base, int max_ctas);
 }
 
 namespace {
@@ -124,12 +124,28 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
   }
   int *st = F.status;
   PLA_Phase_times &ph = state().phases;
+  // LU lookahead, as in the FP64 loop: panel k+1 on the lookahead stream
+  // beside the rest of update k, which then keeps kLookaheadCtas SMs free
+  const bool la = F.kind == 0 && n >= 4 * nb;
+  cudaStream_t s0 = stream(), s1 = la ? lookahead_stream() : s0;
+  cudaEvent_t ev_next = la ? lookahead_event(0) : nullptr, ev_panel = la ? lookahead_event(1) : nullptr;
+  int sms = 0;
+  {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  const int side_ctas = std::max(1, sms - kLookaheadCtas);
+  const int esz = f8 ? 1 : 2;  // bytes per packed element
+  int ready = -1;
   for (int k = 0; k < n; k += nb) {
-    const int b = std::min(nb, n - k), rest = n - k - b;
+    const int b = std::min(nb, n - k), rest = n - k - b, k2 = k + b;
     if (F.kind == 0) {
-      {
+      if (ready == k) {
+        PLA_CUDA(cudaStreamWaitEvent(s0, ev_panel, 0));
+      } else {
         PhaseTimer t(&ph.panel_ms);
-        K(panel_lu(MPI_FLOAT, n - k, b, (char *)at(k, k), ld, F.piv + k, &st[0], &st[2], k));
+        K(panel_lu(MPI_FLOAT, n - k, b, (char *)at(k, k), ld, F.piv + k, &st[0], &st[2], k, 0));
       }
       {
         PhaseTimer t(&ph.swap_ms);
@@ -149,38 +165,60 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
       K(pla_k_trsm_small(MPI_FLOAT, 'R', 'L', 'T', 'N', b, rest, 1.0, at(k, k), ld, at(k + b, k),
                          ld, &st[0], stream()));
     }
-    if (lowp && f8 && b % kmult == 0) {
+    if (lowp && b % kmult == 0) {
       // L (rest x b, column-major) and U' (U is b x rest: element (j, kk) at
-      // kk + j ld) packed row-major in fp8 with their tile scales
-      const void *Uop = Lp;
+      // kk + j ld) packed row-major, in fp8 with their tile scales or in
+      // bf16 / fp16
+      const char *Uop = (const char *)Lp;
       const float *su = inv_l;
       {
         PhaseTimer t(&ph.convert_ms);
-        K(pla_k_pack_fp8(rest, b, at(k + b, k), 1, ld, Lp, nb, inv_l, stream()));
-        if (F.kind == 0) {
-          K(pla_k_pack_fp8(rest, b, at(k, k + b), ld, 1, Up, nb, inv_u, stream()));
-          Uop = Up;
-          su = inv_u;
+        if (f8) {
+          K(pla_k_pack_fp8(rest, b, at(k + b, k), 1, ld, Lp, nb, inv_l, stream()));
+          if (F.kind == 0) {
+            K(pla_k_pack_fp8(rest, b, at(k, k + b), ld, 1, Up, nb, inv_u, stream()));
+            Uop = (const char *)Up;
+            su = inv_u;
+          }
+        } else {
+          K(pla_k_pack_rows(kprec, rest, b, at(k + b, k), ld, Lp, nb, stream()));
+          if (F.kind == 0) {
+            K(pla_k_convert(MPI_FLOAT, at(k, k + b), ld, kprec, Up, nb, b, rest, stream()));
+            Uop = (const char *)Up;
+          }
         }
       }
-      PhaseTimer t(&ph.update_ms);
-      K(pla_k_tc_update_fp8(rest, rest, b, -1.0f, Lp, nb, n, inv_l, Uop, nb, n, su, F.a, ld, ld,
-                            n, k + b, k + b, F.kind == 1, &st[0], stream()));
-      if (t.on) ph.update_launches++;
-    } else if (lowp && !f8 && b % kmult == 0) {
-      const void *Uop = Lp;
-      {
-        PhaseTimer t(&ph.convert_ms);
-        K(pla_k_pack_rows(kprec, rest, b, at(k + b, k), ld, Lp, nb, stream()));
-        if (F.kind == 0) {
-          K(pla_k_convert(MPI_FLOAT, at(k, k + b), ld, kprec, Up, nb, b, rest, stream()));
-          Uop = Up;
+      // C(:, c0 : c0 + nc) of the trailing matrix, on at most `cap` CTAs
+      auto upd = [&](int c0, int nc, int cap) -> int {
+        const long off = (long)(c0 - k2);  // rows of U' skipped (multiple of 128)
+        PhaseTimer t(&ph.update_ms);
+        int r = f8 ? pla_k_tc_update_fp8_ex(rest, nc, b, -1.0f, Lp, nb, n, inv_l,
+                                            Uop + off * nb * esz, nb, n - off, su + off / 128,
+                                            F.a, ld, ld, n, k2, c0, F.kind == 1, cap, &st[0],
+                                            stream())
+                   : pla_k_tc_update_ex(kprec, rest, nc, b, -1.0f, Lp, nb, n,
+                                        Uop + off * nb * esz, nb, n - off, F.a, ld, ld, n, k2, c0,
+                                        F.kind == 1, cap, &st[0], stream());
+        if (t.on) ph.update_launches++;
+        return r;
+      };
+      const int b2 = std::min(nb, rest);
+      if (la && b2 % 128 == 0 && rest > b2) {
+        K(upd(k2, b2, 0));  // the next panel's columns first
+        PLA_CUDA(cudaEventRecord(ev_next, s0));
+        PLA_CUDA(cudaStreamWaitEvent(s1, ev_next, 0));
+        {
+          OnStream on(s1);
+          PhaseTimer t(&ph.panel_ms);
+          K(panel_lu(MPI_FLOAT, n - k2, b2, (char *)at(k2, k2), ld, F.piv + k2, &st[0], &st[2],
+                     k2, kLookaheadCtas));
         }
+        PLA_CUDA(cudaEventRecord(ev_panel, s1));
+        ready = k2;
+        K(upd(k2 + b2, rest - b2, side_ctas));
+      } else {
+        K(upd(k2, rest, 0));
       }
-      PhaseTimer t(&ph.update_ms);
-      K(pla_k_tc_update(kprec, rest, rest, b, -1.0f, Lp, nb, n, Uop, nb, n, F.a, ld, ld, n, k + b,
-                        k + b, F.kind == 1, &st[0], stream()));
-      if (t.on) ph.update_launches++;
     } else if (F.kind == 0) {
       K(pla_k_gemm(MPI_FLOAT, PLA_NO_TRANSPOSE, PLA_NO_TRANSPOSE, rest, rest, b, -1.0, at(k + b, k),
                    ld, at(k, k + b), ld, 1.0, at(k + b, k + b), ld, 0, &st[0], stream()));

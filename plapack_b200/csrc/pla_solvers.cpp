@@ -152,16 +152,17 @@ namespace pla {
 // rank-kSub update.  Pivot choices are those of the column-by-column loop;
 // only the rounding order of the panel's trailing columns differs.
 int panel_lu(int dt, int r, int b, char *P, long lda, int *piv, int *status, int *zero_info,
-             int row_base) {
+             int row_base, int max_ctas) {
   constexpr int kSub = 32;
   const int es = dt == MPI_DOUBLE ? 8 : 4;
   auto at = [&](long i, long j) { return P + (i + j * lda) * es; };
   if (b <= kSub)
-    return pla_k_lu_panel(dt, r, b, P, lda, piv, status, zero_info, row_base, stream());
+    return pla_k_lu_panel_ex(dt, r, b, P, lda, piv, status, zero_info, row_base, max_ctas,
+                             stream());
   for (int s = 0; s < b; s += kSub) {
     const int sb = std::min(kSub, b - s), rest = b - s - sb;
-    int e = pla_k_lu_panel(dt, r - s, sb, at(s, s), lda, piv + s, status, zero_info,
-                           row_base + s, stream());
+    int e = pla_k_lu_panel_ex(dt, r - s, sb, at(s, s), lda, piv + s, status, zero_info,
+                              row_base + s, max_ctas, stream());
     if (e) return e;
     e = pla_k_laswp(dt, at(s, 0), lda, sb, piv + s, 0, s, s + sb, b, stream());
     if (e) return e;
@@ -182,38 +183,69 @@ int panel_lu(int dt, int r, int b, char *P, long lda, int *piv, int *status, int
 
 namespace {
 
-// Blocked right-looking LU (SOLVERS/LU/PLA_LU.c:103-192) on device memory.
+// Blocked right-looking LU (SOLVERS/LU/PLA_LU.c:103-192) on device memory,
+// with a lookahead of one panel.  After the TRSM of step k the columns of
+// panel k+1 are updated first; panel k+1 is then factored on the
+// high-priority lookahead stream, on at most kLookaheadCtas CTAs, while the
+// rest of the trailing update of step k runs on the library stream.  The two
+// touch disjoint columns, and step k+1 starts (row interchanges across the
+// full width) only after both.  Every operation and its operands are those
+// of the loop without lookahead, so the pivots and factors are the same.
 int lu_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, Status *st) {
   const int es = dt == MPI_DOUBLE ? 8 : 4;
   auto at = [&](long i, long j) { return A + (i + j * lda) * es; };
   const int kmax = std::min(m, n);
   PLA_Phase_times &ph = state().phases;
+  const bool la = kmax >= 4 * nb;  // worth a second stream
+  cudaStream_t s0 = stream(), s1 = la ? lookahead_stream() : s0;
+  cudaEvent_t ev_next = la ? lookahead_event(0) : nullptr, ev_panel = la ? lookahead_event(1) : nullptr;
+  auto update = [&](int k, int b, int c0, int nc) -> int {
+    PhaseTimer t(&ph.update_ms);
+    int r = pla_k_gemm(dt, PLA_NO_TRANSPOSE, PLA_NO_TRANSPOSE, m - k - b, nc, b, -1.0,
+                       at(k + b, k), lda, at(k, c0), lda, 1.0, at(k + b, c0), lda, 0, &st->status,
+                       stream());
+    if (t.on) ph.update_launches++;
+    return r;
+  };
+  int ready = -1;  // step whose panel the lookahead stream has factored
   for (int k = 0; k < kmax; k += nb) {
     const int b = std::min(nb, kmax - k), r = m - k;
-    {
+    if (ready == k) {
+      PLA_CUDA(cudaStreamWaitEvent(s0, ev_panel, 0));
+    } else {
       PhaseTimer t(&ph.panel_ms);
-      K(panel_lu(dt, r, b, at(k, k), lda, piv + k, &st->status, &st->zero_info, k));
+      K(panel_lu(dt, r, b, at(k, k), lda, piv + k, &st->status, &st->zero_info, k, 0));
     }
     {
       PhaseTimer t(&ph.swap_ms);
       K(pla_k_laswp(dt, at(k, 0), lda, b, piv + k, 0, k, k + b, n, stream()));
     }
-    if (k + b < n) {
+    if (k + b >= n) continue;
+    {
+      PhaseTimer t(&ph.trsm_ms);
+      K(trsm_blocked(dt, 'L', 'L', 'N', 'U', b, n - k - b, 1.0, at(k, k), lda, at(k, k + b), lda,
+                     &st->status));
+    }
+    if (m - k - b <= 0) continue;
+    const int k2 = k + b, b2 = std::min(nb, kmax - k2);
+    if (la && b2 > 0) {
+      K(update(k, b, k2, b2));  // the next panel's columns first
+      PLA_CUDA(cudaEventRecord(ev_next, s0));
+      PLA_CUDA(cudaStreamWaitEvent(s1, ev_next, 0));
       {
-        PhaseTimer t(&ph.trsm_ms);
-        K(trsm_blocked(dt, 'L', 'L', 'N', 'U', b, n - k - b, 1.0, at(k, k), lda, at(k, k + b),
-                       lda, &st->status));
+        OnStream on(s1);
+        PhaseTimer t(&ph.panel_ms);
+        K(panel_lu(dt, m - k2, b2, at(k2, k2), lda, piv + k2, &st->status, &st->zero_info, k2,
+                   kLookaheadCtas));
       }
-      if (m - k - b > 0) {
-        PhaseTimer t(&ph.update_ms);
-        K(pla_k_gemm(dt, PLA_NO_TRANSPOSE, PLA_NO_TRANSPOSE, m - k - b, n - k - b, b, -1.0,
-                     at(k + b, k), lda, at(k, k + b), lda, 1.0, at(k + b, k + b), lda, 0,
-                     &st->status, stream()));
-        if (t.on) ph.update_launches++;
-      }
+      PLA_CUDA(cudaEventRecord(ev_panel, s1));
+      ready = k2;
+      if (n - k2 - b2 > 0) K(update(k, b, k2 + b2, n - k2 - b2));
+    } else {
+      K(update(k, b, k2, n - k2));
     }
   }
-  return 0;
+  return 0;  // every lookahead panel was awaited at its own step
 }
 
 // Blocked right-looking lower Cholesky (SOLVERS/Cholesky/PLA_Chol.c:159-224).
