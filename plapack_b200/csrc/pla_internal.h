@@ -81,9 +81,14 @@ cudaStream_t stream();
 // Lookahead: panels run on a second, high-priority stream while the trailing
 // update of the previous step runs on stream(); two events order them.
 // CTAs of a panel that runs beside a trailing update: few enough to leave the
-// update most SMs, enough that a 32-column FP64 sub-panel of 32768 rows still
-// fits in their shared memory (683 rows x 32 x 8 bytes each)
-constexpr int kLookaheadCtas = 48;
+// update most SMs, enough that a 32-column sub-panel of 32768 rows still fits
+// in their shared memory.  Measured at n = 32768 (CTAs: mixed / FP64 solve):
+// 32: 0.358 / 1.148 s, 48: 0.331 / 1.143 s, 72: 0.310 / 1.159 s,
+// 100: 0.316 / 1.177 s.  The fp32 panel of the mixed LU runs beside a short
+// HBM-bound update and wants more CTAs; the FP64 panel beside the long DGEMM
+// fewer.
+constexpr int kLookaheadCtasF32 = 72;
+constexpr int kLookaheadCtasF64 = 48;
 cudaStream_t lookahead_stream();
 cudaEvent_t lookahead_event(int i);
 // while alive, stream() returns `s` (host code is sequential, so the switch
