@@ -39,10 +39,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "n=32768 solve time: mixed-prec LU-IR vs FP64 LU, same B200, both at FP64 bkwd err"
 # DRAM bytes (read + write) of one tensor-core update launch as a fraction of
-# its algorithmic bytes: 139.3 MB measured against 194.3 MB for the launch
-# with rest = 4864, K = 256 captured by ncu (profiles/tc_update_k_lu_n8192.md).
-# Below 1 because the last C tiles written are still dirty in L2 at exit.
-TC_UPDATE_TRAFFIC_RATIO = 139.3 / 194.25
+# its algorithmic bytes: 486.5 MB measured against 545.3 MB for the
+# M = N = 8192, K = 256 launch captured by ncu
+# (profiles/tc_update_k_fp16_fp8_8192_k256.md).  Below 1 because the last C
+# tiles written are still dirty in L2 when the launch ends.
+TC_UPDATE_TRAFFIC_RATIO = 486.5 / 545.3
 
 
 def parse():
@@ -63,6 +64,9 @@ def parse():
     p.add_argument("--skip-chol", action="store_true", help="skip the FP64 Cholesky solve")
     p.add_argument("--skip-batched", action="store_true", help="skip the batched workload")
     p.add_argument("--batch-count", type=int, default=20000)
+    p.add_argument("--skip-chol-mixed", action="store_true",
+                   help="skip the fp8 / bf16 Cholesky-IR at --chol-n")
+    p.add_argument("--chol-n", type=int, default=49152)
     p.add_argument("--cpu-seconds", type=float, default=12.0,
                    help="target length of one reference sample on the host")
     return p.parse_args()
@@ -371,6 +375,73 @@ def run_batched(torch, pla, lib, device, stream, dtype, steps, warmup, count=200
             "backward_error_max": eta, "loop_backward_error_max": loop_eta}
 
 
+def spd_device(n, kappa, seed, torch, device):
+    """A = Q diag(lambda) Q' with lambda log-uniform in [1/kappa, 1] and Q a
+    product of 8 Householder reflectors with seeded Gaussian vectors."""
+    g = torch.Generator(device=device).manual_seed(seed)
+    u = torch.rand(n, dtype=torch.float64, device=device, generator=g)
+    lam = torch.exp(u * -np.log(kappa))
+    lam[0], lam[-1] = 1.0, 1.0 / kappa
+    A = torch.diag(lam)
+    for _ in range(8):                      # A <- H A H
+        v = torch.randn(n, dtype=torch.float64, device=device, generator=g)
+        c = -2.0 / float(v @ v)
+        A.addr_(v, v @ A, alpha=c)
+        A.addr_(A @ v, v, alpha=c)
+    A.add_(A.t().clone()).mul_(0.5)
+    return A
+
+
+def run_chol_mixed(torch, pla, lib, s, device, stream, n, kappas, precs, nrhs, steps, warmup):
+    """Mixed-precision Cholesky-IR (PLA_Pos_def_solve_mixed, GMRES-IR) on the
+    SPD family above: time, the precision that finished, iterations and the
+    backward and forward errors of each (kappa, precision)."""
+    out = []
+    a = s.matrix(n, n)
+    bo = s.matrix(n, nrhs)
+    for kappa in kappas:
+        A = spd_device(n, kappa, 41, torch, device)
+        g = torch.Generator(device=device).manual_seed(42)
+        Xt = torch.randn(nrhs, n, dtype=torch.float64, device=device, generator=g)  # X' row-major
+        Bt = Xt @ A                                   # (A X)' = X' A (A symmetric)
+        a_inf = A.abs().sum(dim=0).max().item()
+        for name, prec in precs:
+            params = pla.MixedParams()
+            lib.PLA_Mixed_params_default(ctypes.byref(params))
+            params.precision = prec
+            params.refinement = pla.PLA_B200_IR_GMRES
+            rep = pla.MixedReport()
+            times = []
+            for it in range(warmup + steps):
+                pla.check(lib.PLA_Obj_set_local_contents_device(ctypes.c_void_p(A.data_ptr()), n, a), "A")
+                pla.check(lib.PLA_Obj_set_local_contents_device(ctypes.c_void_p(Bt.data_ptr()), n, bo), "B")
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                rc = lib.PLA_Pos_def_solve_mixed(a, bo, ctypes.byref(params), ctypes.byref(rep))
+                e1.record(stream)
+                torch.cuda.synchronize()
+                if it >= warmup:
+                    times.append(e0.elapsed_time(e1) / 1e3)
+            X = torch.empty(nrhs, n, dtype=torch.float64, device=device)
+            pla.check(lib.PLA_Obj_get_local_contents_device(bo, ctypes.c_void_p(X.data_ptr()), n), "X")
+            R = Bt - X @ A
+            eta = (R.abs().amax(dim=1) / (a_inf * X.abs().amax(dim=1) + Bt.abs().amax(dim=1))).max().item()
+            fwd = ((X - Xt).abs().max() / Xt.abs().max()).item()
+            out.append({"kappa": kappa, "precision": name, "rc": rc, "solve_s": min(times),
+                        "precision_used": {1: "bf16", 2: "fp16", 3: "fp32", 4: "fp64",
+                                           5: "fp8"}.get(rep.precision_used),
+                        "factorizations": rep.factorizations, "iterations": rep.iterations,
+                        "gmres_iterations": rep.inner_iterations, "factor_ms": rep.factor_ms,
+                        "refine_ms": rep.refine_ms, "backward_error": eta,
+                        "backward_error_target": n * 2.0 ** -53, "forward_error": fwd})
+        del A, Xt, Bt
+        torch.cuda.empty_cache()
+    s.free(a, bo)
+    return {"workload": f"PLA_Pos_def_solve_mixed n={n}, A = Q diag(lambda) Q', {nrhs} rhs, "
+                        "GMRES-IR", "results": out}
+
+
 def run_ours(args):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -585,6 +656,13 @@ def run_ours(args):
                                count=args.batch_count, seed=3 + 1000 * rank)
                    for dt in (torch.float64, torch.float32)]
 
+    # ---- mixed-precision Cholesky-IR: fp8 E4M3 vs bf16 trailing updates ----
+    chol_mixed = None
+    if not args.skip_chol_mixed:
+        chol_mixed = run_chol_mixed(torch, pla, lib, s, device, stream, args.chol_n, (1e3, 1e7),
+                                    (("fp8", pla.PLA_B200_PREC_FP8),
+                                     ("bf16", pla.PLA_B200_PREC_BF16)), 8, 1, 1)
+
     # ---- end to end: host buffers in, host solution out ----
     e2e = None
     if not args.skip_e2e:
@@ -646,7 +724,7 @@ def run_ours(args):
                "refinement_iterations": report.iterations,
                "gmres_iterations": report.inner_iterations,
                "factor_ms": report.factor_ms, "refine_ms": report.refine_ms,
-               "fp64_cholesky": chol, "batched": batched,
+               "fp64_cholesky": chol, "batched": batched, "cholesky_mixed": chol_mixed,
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                "clocks": clock_summary, "gpu_launches": launches}
         print(json.dumps(out))

@@ -1,0 +1,230 @@
+"""Run one kernel of the library at a stated size, through its C ABI, for
+profiling and timing.  Every case allocates its operands with torch on
+cuda:0, launches the kernel `--reps` times after `--warmup` launches, and
+prints the mean CUDA-event time per launch with the kernel's algorithmic
+bytes or flops and the rate they imply.
+
+    python -m plapack_b200.kernel_cases dgemm --m 16384 --n 16384 --k 128
+    python -m plapack_b200.kernel_cases tc_update --m 8192 --n 8192 --k 256
+    python -m plapack_b200.kernel_cases tc_update_fp8 --m 8192 --n 8192 --k 256
+    python -m plapack_b200.kernel_cases panel --m 32768 --k 32 [--dtype f64]
+    python -m plapack_b200.kernel_cases laswp --m 32768 --n 32768 --k 256
+    python -m plapack_b200.kernel_cases trsv --n 32768
+    python -m plapack_b200.kernel_cases residual --n 32768
+    python -m plapack_b200.kernel_cases batched --count 2000
+
+The cases mirror the calls the solvers make (the trailing update of one LU
+step, one 32-column sub-panel, the row interchanges of one panel, the
+single-launch triangular solve and the FP64 residual of the refinement, one
+batched factor-and-solve).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import sys
+
+import numpy as np
+
+from . import pla
+
+vp, lg, i32, f32, f64 = ctypes.c_void_p, ctypes.c_long, ctypes.c_int, ctypes.c_float, ctypes.c_double
+ch = ctypes.c_char
+
+
+def _fn(lib, name, argtypes):
+    f = getattr(lib, name)
+    f.argtypes = argtypes
+    f.restype = ctypes.c_int
+    return f
+
+
+def _time(torch, launch, warmup, reps):
+    for _ in range(warmup):
+        rc = launch()
+        assert rc == 0, rc
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        launch()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / reps
+
+
+def case_dgemm(torch, lib, a):
+    m, n, k = a.m, a.n, a.k
+    A = torch.randn(k, m, dtype=torch.float64, device="cuda")   # column-major m x k
+    B = torch.randn(n, k, dtype=torch.float64, device="cuda")   # column-major k x n
+    C = torch.randn(n, m, dtype=torch.float64, device="cuda")   # column-major m x n
+    g = _fn(lib, "pla_k_gemm", [i32] * 6 + [f64, vp, lg, vp, lg, f64, vp, lg, i32, vp, vp])
+    t = _time(torch, lambda: g(pla.MPI_DOUBLE, pla.PLA_NO_TRANSPOSE, pla.PLA_NO_TRANSPOSE, m, n, k,
+                               -1.0, A.data_ptr(), m, B.data_ptr(), k, 1.0, C.data_ptr(), m, 0,
+                               None, None), a.warmup, a.reps)
+    fl = 2.0 * m * n * k
+    return {"case": f"FP64 trailing update C -= A B, m={m} n={n} k={k}", "s": t,
+            "tflops": fl / t / 1e12}
+
+
+def _tc(torch, lib, a, fp8):
+    m, n, k = a.m, a.n, a.k
+    ld = (m + 31) // 32 * 32
+    C = torch.randn(n, ld, dtype=torch.float32, device="cuda")
+    st = torch.zeros(4, dtype=torch.int32, device="cuda")
+    if fp8:
+        L = torch.randint(0, 120, (m, k), dtype=torch.uint8, device="cuda")
+        U = torch.randint(0, 120, (n, k), dtype=torch.uint8, device="cuda")
+        il = torch.full(((m + 127) // 128,), 2.0 ** -8, device="cuda")
+        iu = torch.full(((n + 127) // 128,), 2.0 ** -8, device="cuda")
+        g = _fn(lib, "pla_k_tc_update_fp8", [i32, i32, i32, f32, vp, lg, lg, vp, vp, lg, lg, vp, vp,
+                                             lg, lg, lg, i32, i32, i32, vp, vp])
+        launch = lambda: g(m, n, k, -1.0, L.data_ptr(), k, m, il.data_ptr(), U.data_ptr(), k, n,
+                           iu.data_ptr(), C.data_ptr(), ld, ld, n, 0, 0, 0, st.data_ptr(), None)
+        esz = 1
+    else:
+        L = torch.randn(m, k, device="cuda").half()
+        U = torch.randn(n, k, device="cuda").half()
+        g = _fn(lib, "pla_k_tc_update", [i32] * 4 + [f32, vp, lg, lg, vp, lg, lg, vp, lg, lg, lg,
+                                                     i32, i32, i32, vp, vp])
+        launch = lambda: g(1002, m, n, k, -1.0, L.data_ptr(), k, m, U.data_ptr(), k, n,
+                           C.data_ptr(), ld, ld, n, 0, 0, 0, st.data_ptr(), None)
+        esz = 2
+    t = _time(torch, launch, a.warmup, a.reps)
+    assert st[0].item() == 0
+    byt = m * n * 8.0 + (m + n) * k * esz
+    return {"case": f"tensor-core trailing update ({'fp8 e4m3' if fp8 else 'fp16'}), m={m} n={n} "
+                    f"k={k}", "s": t, "algorithmic_bytes": byt, "gbs": byt / t / 1e9,
+            "tflops": 2.0 * m * n * k / t / 1e12}
+
+
+def case_tc_update(torch, lib, a):
+    return _tc(torch, lib, a, False)
+
+
+def case_tc_update_fp8(torch, lib, a):
+    return _tc(torch, lib, a, True)
+
+
+def case_panel(torch, lib, a):
+    r, w = a.m, a.k
+    dt = pla.MPI_DOUBLE if a.dtype == "f64" else pla.MPI_FLOAT
+    tdt = torch.float64 if a.dtype == "f64" else torch.float32
+    A0 = torch.randn(w, r, dtype=tdt, device="cuda")
+    A = A0.clone()
+    piv = torch.zeros(w, dtype=torch.int32, device="cuda")
+    st = torch.zeros(4, dtype=torch.int32, device="cuda")
+    g = _fn(lib, "pla_k_lu_panel", [i32, i32, i32, vp, lg, vp, vp, vp, i32, vp])
+
+    def launch():
+        A.copy_(A0)
+        return g(dt, r, w, A.data_ptr(), r, piv.data_ptr(), st.data_ptr(), None, 0, None)
+
+    t = _time(torch, launch, a.warmup, a.reps)
+    assert st[0].item() == 0
+    es = 8 if dt == pla.MPI_DOUBLE else 4
+    return {"case": f"panel LU {r} x {w} ({a.dtype}), copy of the panel included", "s": t,
+            "us_per_column": t / w * 1e6, "bytes_read_written": 2.0 * r * w * es,
+            "gbs": 2.0 * r * w * es / t / 1e9}
+
+
+def case_laswp(torch, lib, a):
+    m, n, npiv = a.m, a.n, a.k
+    A = torch.randn(n, m, dtype=torch.float64, device="cuda")
+    rng = np.random.default_rng(1)
+    piv = torch.from_numpy(np.array([rng.integers(0, m - i) for i in range(npiv)], dtype=np.int32)).cuda()
+    g = _fn(lib, "pla_k_laswp", [i32, vp, lg, i32, vp, i32, i32, i32, i32, vp])
+    t = _time(torch, lambda: g(pla.MPI_DOUBLE, A.data_ptr(), m, npiv, piv.data_ptr(), 0, 0, npiv,
+                               n, None), a.warmup, a.reps)
+    byt = 2.0 * 2 * npiv * (n - npiv) * 8
+    return {"case": f"row interchanges of one panel: {npiv} pivots over {n - npiv} columns (FP64)",
+            "s": t, "algorithmic_bytes": byt, "gbs": byt / t / 1e9}
+
+
+def case_trsv(torch, lib, a):
+    n = a.n
+    ld = (n + 31) // 32 * 32
+    M = torch.randn(n, ld, device="cuda") * 0.01
+    M.diagonal()[:n] += 1.0
+    ldd = (n + 127) // 128 * 128
+    Dinv = torch.zeros(128, ldd, device="cuda")
+    b = torch.randn(n, device="cuda")
+    x = torch.empty_like(b)
+    st = torch.zeros(4, dtype=torch.int32, device="cuda")
+    inv = _fn(lib, "pla_k_trsv_inv_blocks", [i32, ch, ch, ch, i32, vp, lg, vp, lg, vp])
+    assert inv(pla.MPI_FLOAT, b"L", b"N", b"U", n, M.data_ptr(), ld, Dinv.data_ptr(), ldd, None) == 0
+    g = _fn(lib, "pla_k_trsv_ticket", [i32, ch, ch, i32, vp, lg, vp, lg, vp, vp, vp, vp])
+    t = _time(torch, lambda: g(pla.MPI_FLOAT, b"L", b"N", n, M.data_ptr(), ld, Dinv.data_ptr(),
+                               ldd, b.data_ptr(), x.data_ptr(), st.data_ptr(), None),
+              a.warmup, a.reps)
+    byt = 4.0 * n * n / 2
+    return {"case": f"single-launch unit-lower triangular solve, n={n} (fp32 factor)", "s": t,
+            "algorithmic_bytes": byt, "gbs": byt / t / 1e9}
+
+
+def case_residual(torch, lib, a):
+    n = a.n
+    A = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    X = torch.randn(n, dtype=torch.float64, device="cuda")
+    B = torch.randn(n, dtype=torch.float64, device="cuda")
+    R = torch.empty_like(B)
+    wk = _fn(lib, "pla_k_residual_work", [i32, i32, i32])
+    wk.restype = ctypes.c_size_t
+    work = torch.empty(wk(n, n, 1) // 8 + 64, dtype=torch.float64, device="cuda")
+    g = _fn(lib, "pla_k_residual", [i32, i32, i32, vp, lg, vp, lg, vp, lg, vp, lg, i32, vp, vp])
+    t = _time(torch, lambda: g(n, n, 1, A.data_ptr(), n, X.data_ptr(), n, B.data_ptr(), n,
+                               R.data_ptr(), n, 0, work.data_ptr(), None), a.warmup, a.reps)
+    byt = 8.0 * n * n
+    return {"case": f"FP64 residual b - A x, n={n}", "s": t, "algorithmic_bytes": byt,
+            "gbs": byt / t / 1e9}
+
+
+def case_batched(torch, lib, a):
+    sys.path.insert(0, __import__("os").path.dirname(__import__("os").path.dirname(
+        __import__("os").path.abspath(__file__))))
+    import bench  # the bench's workload generator: n log-uniform in [8, 512], LU and Cholesky
+    dtype = torch.float64 if a.dtype == "f64" else torch.float32
+    arr, groups, piv, flops = bench.batched_workload(torch, pla, torch.device("cuda", 0), dtype,
+                                                     a.count, 3)
+    info = torch.zeros(a.count, dtype=torch.int32, device="cuda")
+    dt = pla.MPI_DOUBLE if a.dtype == "f64" else pla.MPI_FLOAT
+    plan = ctypes.c_void_p()
+    pla.check(lib.PLA_Batch_plan_create(dt, a.count, arr, ctypes.c_void_p(info.data_ptr()), 1,
+                                        ctypes.byref(plan)), "plan")
+
+    def launch():
+        for gr in groups:
+            gr["A"].copy_(gr["A0"])
+            gr["B"].copy_(gr["B0"])
+        return lib.PLA_Batch_plan_execute(plan)
+
+    t = _time(torch, launch, a.warmup, a.reps)
+    lib.PLA_Batch_plan_free(ctypes.byref(plan))
+    return {"case": f"batched factor-and-solve, {a.count} instances ({a.dtype}), input restore "
+                    "included", "s": t, "gflops": flops / t / 1e9}
+
+
+CASES = {k[5:]: v for k, v in globals().items() if k.startswith("case_")}
+
+
+def main(argv=None):
+    p = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    p.add_argument("case", choices=sorted(CASES))
+    p.add_argument("--m", type=int, default=16384)
+    p.add_argument("--n", type=int, default=16384)
+    p.add_argument("--k", type=int, default=128)
+    p.add_argument("--count", type=int, default=2000)
+    p.add_argument("--dtype", choices=["f32", "f64"], default="f32")
+    p.add_argument("--warmup", type=int, default=2)
+    p.add_argument("--reps", type=int, default=3)
+    a = p.parse_args(argv)
+    import torch
+    torch.cuda.set_device(0)
+    lib = pla.lib()
+    print(json.dumps(CASES[a.case](torch, lib, a)))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
