@@ -1,4 +1,5 @@
-// Triangular solve with one right-hand side in a single launch.
+// Triangular solve with one right-hand side in a single launch (fp32 with
+// 128 x 128 blocks, FP64 with 64 x 64 blocks).
 //
 //   tri_inv_blocks_k : inverse of every TB x TB diagonal block of op(A)
 //                      (computed once per factor, reused by every solve);
@@ -19,7 +20,7 @@
 
 namespace {
 
-constexpr int TB = 128, THREADS = 256;
+constexpr int TB = 128, TB64 = 64, THREADS = 256;  // fp32 and FP64 block orders
 constexpr long kSpin = 20000000;
 
 template <typename T>
@@ -28,15 +29,16 @@ __device__ __forceinline__ T opA(const T *A, long lda, bool trans, long i, long 
 }
 
 // inverse of the TB x TB diagonal block `blockIdx.x` of op(A) into Dinv
-// (element (r, c) of block i at Dinv[i*TB + r + c*ldd])
-template <typename T>
+// (element (r, c) of block i at Dinv[i*TB + r + c*ldd]); TB = 128 for fp32,
+// 64 for FP64 (two TB x (TB + 1) blocks must fit in shared memory)
+template <typename T, int TB>
 __global__ void __launch_bounds__(THREADS)
 tri_inv_blocks_k(int n, const T *A, long lda, bool lower_op, bool trans, bool unit, T *Dinv,
                  long ldd) {
   extern __shared__ __align__(16) unsigned char sm[];
   T *D = (T *)sm;                 // TB x TB, ld TB + 1
   T *X = D + TB * (TB + 1);       // TB x TB, ld TB + 1
-  constexpr int L = TB + 1;
+  constexpr int L = TB + 1, NT = THREADS / TB;  // NT threads per column
   const int blk = blockIdx.x, r0 = blk * TB, nb = min(TB, n - r0);
   for (int t = threadIdx.x; t < TB * TB; t += THREADS) {
     int i = t % TB, j = t / TB;
@@ -47,17 +49,17 @@ tri_inv_blocks_k(int n, const T *A, long lda, bool lower_op, bool trans, bool un
     X[i + j * L] = i == j ? T(1) : T(0);
   }
   __syncthreads();
-  // solve D X = I; column c is handled by the two threads with c = tid % TB
-  const int c = threadIdx.x % TB, half = threadIdx.x / TB;
+  // solve D X = I; column c is handled by the NT threads with c = tid % TB
+  const int c = threadIdx.x % TB, part = threadIdx.x / TB;
   for (int step = 0; step < TB; step++) {
     const int l = lower_op ? step : TB - 1 - step;
-    if (half == 0) X[l + c * L] = X[l + c * L] / D[l + l * L];
+    if (part == 0) X[l + c * L] = X[l + c * L] / D[l + l * L];
     __syncthreads();
     const T xl = X[l + c * L];
     if (lower_op)
-      for (int i = l + 1 + half; i < TB; i += 2) X[i + c * L] -= D[i + l * L] * xl;
+      for (int i = l + 1 + part; i < TB; i += NT) X[i + c * L] -= D[i + l * L] * xl;
     else
-      for (int i = half; i < l; i += 2) X[i + c * L] -= D[i + l * L] * xl;
+      for (int i = part; i < l; i += NT) X[i + c * L] -= D[i + l * L] * xl;
     __syncthreads();
   }
   for (int t = threadIdx.x; t < TB * TB; t += THREADS) {
@@ -222,6 +224,132 @@ trsv_ticket_k(int n, int nblk, const T *A, long lda, bool lower_op, bool trans, 
   }
 }
 
+// The FP64 form: 64 x 64 blocks (a 64 x 64 FP64 inverse is 32 KB), each tile
+// read as 8 independent 16-byte loads per thread.  No transpose: thread
+// (rg, cg) owns rows 2rg, 2rg+1 and columns 8cg .. 8cg+7; transpose: thread
+// (r, quarter) reads 16 contiguous values of column r of A.
+__global__ void __launch_bounds__(THREADS)
+trsv_ticket64_k(int n, int nblk, const double *A, long lda, bool lower_op, bool trans,
+                const double *Dinv, long ldd, const double *b, double *x, int *ticket, int *flags,
+                int *status, bool vec_ok) {
+  constexpr int T64 = TB64;
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  double *Ds = reinterpret_cast<double *>(dyn_smem);  // T64 x T64 inverse diagonal block
+  __shared__ double xs[T64];
+  __shared__ double part[4][T64];
+  __shared__ double red[8][T64];
+  __shared__ int s_blk, s_bad;
+  const int r = threadIdx.x % T64, quarter = threadIdx.x / T64;
+  const int rg = threadIdx.x & 31, cg = threadIdx.x >> 5;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_blk = atomicAdd(ticket, 1);
+      s_bad = 0;
+    }
+    __syncthreads();
+    const int q = s_blk;
+    if (q >= nblk) return;
+    const int i = lower_op ? q : nblk - 1 - q;
+    const long r0 = (long)i * T64;
+    const int nbi = min(T64, n - (int)r0);
+    double acc2[2] = {0.0, 0.0};
+    double acc = 0.0;
+    for (int u = threadIdx.x; u < T64 * T64 / 2; u += THREADS) {
+      const int c = u / (T64 / 2), r2 = (u % (T64 / 2)) * 2;
+      cp_async16(&Ds[c * T64 + r2], Dinv + (r0 + r2) + (long)c * ldd);
+    }
+    cp_async_commit();
+    for (int s2 = 0; s2 < q; s2++) {
+      const int j = lower_op ? s2 : nblk - 1 - s2;
+      const long c0 = (long)j * T64;
+      const int nbj = min(T64, n - (int)c0);
+      const bool full = nbi == T64 && nbj == T64 && vec_ok;
+      // the tile does not depend on x_j: its loads are issued before waiting
+      double2 v[8];
+      if (full) {
+        const double *base = trans ? A + (r0 + r) * lda + c0 + 16 * quarter
+                                   : A + (r0 + 2 * rg) + (c0 + 8 * cg) * lda;
+        const long step = trans ? 2 : lda;
+#pragma unroll
+        for (int u = 0; u < 8; u++) v[u] = *reinterpret_cast<const double2 *>(base + u * step);
+      }
+      if (threadIdx.x == 0) {
+        long spins = 0;
+        while (ld_acquire(&flags[j]) == 0) {
+          if (++spins > kSpin || *(volatile int *)status != PLA_K_OK) {
+            atomicCAS(status, PLA_K_OK, PLA_K_TIMEOUT);
+            s_bad = 1;
+            break;
+          }
+          __nanosleep(32);
+        }
+      }
+      __syncthreads();
+      if (s_bad) return;
+      if (threadIdx.x < nbj) xs[threadIdx.x] = __ldcg(&x[c0 + threadIdx.x]);
+      __syncthreads();
+      if (full && !trans) {
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const double xv = xs[8 * cg + u];
+          acc2[0] += v[u].x * xv;
+          acc2[1] += v[u].y * xv;
+        }
+      } else if (full) {
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const int c = 16 * quarter + 2 * u;
+          acc += v[u].x * xs[c] + v[u].y * xs[c + 1];
+        }
+      } else if (r < nbi) {
+        if (!trans) {
+          for (int c = quarter; c < nbj; c += 4) acc += A[(r0 + r) + (c0 + c) * lda] * xs[c];
+        } else {
+          const int cb = quarter * (T64 / 4), ce = min(cb + T64 / 4, nbj);
+          const double *col = A + (r0 + r) * lda + c0;
+          for (int c = cb; c < ce; c++) acc += col[c] * xs[c];
+        }
+      }
+      __syncthreads();
+    }
+    red[cg][2 * rg] = acc2[0];
+    red[cg][2 * rg + 1] = acc2[1];
+    part[quarter][r] = acc;
+    __syncthreads();
+    if (threadIdx.x < T64) {
+      double sacc = part[0][r] + part[1][r] + part[2][r] + part[3][r];
+#pragma unroll
+      for (int g = 0; g < 8; g++) sacc += red[g][r];
+      xs[threadIdx.x] = r < nbi ? b[r0 + r] - sacc : 0.0;
+    }
+    __syncthreads();
+    cp_async_wait_all();
+    __syncthreads();
+    {
+      double y2[2] = {0.0, 0.0};
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const double2 d = *reinterpret_cast<const double2 *>(&Ds[(8 * cg + u) * T64 + 2 * rg]);
+        const double xv = xs[8 * cg + u];
+        y2[0] += d.x * xv;
+        y2[1] += d.y * xv;
+      }
+      red[cg][2 * rg] = y2[0];
+      red[cg][2 * rg + 1] = y2[1];
+    }
+    __syncthreads();
+    if (threadIdx.x < nbi) {
+      double y = 0.0;
+#pragma unroll
+      for (int g = 0; g < 8; g++) y += red[g][threadIdx.x];
+      x[r0 + threadIdx.x] = y;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) st_release(&flags[i], 1);
+  }
+}
+
 void *g_flags = nullptr;
 size_t g_flags_bytes = 0;
 
@@ -239,15 +367,16 @@ int *flags_for(int nblk) {
 
 int g_sms = 0;
 
-template <typename T>
+template <typename T, int TBK>
 int inv_blocks(char uplo, char trans, char diag, int n, const void *A, long lda, void *Dinv,
                long ldd, cudaStream_t s) {
   const bool tr = trans != 'N', lower_op = (uplo == 'L') != tr, unit = diag == 'U';
-  const int nblk = (n + TB - 1) / TB;
-  size_t sm = (size_t)2 * TB * (TB + 1) * sizeof(T);
-  cudaFuncSetAttribute(tri_inv_blocks_k<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  tri_inv_blocks_k<T><<<nblk, THREADS, sm, s>>>(n, (const T *)A, lda, lower_op, tr, unit,
-                                                (T *)Dinv, ldd);
+  const int nblk = (n + TBK - 1) / TBK;
+  size_t sm = (size_t)2 * TBK * (TBK + 1) * sizeof(T);
+  cudaFuncSetAttribute(tri_inv_blocks_k<T, TBK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sm);
+  tri_inv_blocks_k<T, TBK><<<nblk, THREADS, sm, s>>>(n, (const T *)A, lda, lower_op, tr, unit,
+                                                     (T *)Dinv, ldd);
   pla_k_count(1);
   return (int)cudaGetLastError();
 }
@@ -278,15 +407,41 @@ int ticket_solve(char uplo, char trans, int n, const void *A, long lda, const vo
   return (int)cudaGetLastError();
 }
 
+int ticket_solve64(char uplo, char trans, int n, const void *A, long lda, const void *Dinv,
+                   long ldd, const void *b, void *x, int *status, cudaStream_t s) {
+  const bool tr = trans != 'N', lower_op = (uplo == 'L') != tr;
+  const int nblk = (n + TB64 - 1) / TB64;
+  int *fl = flags_for(nblk);
+  if (!fl) return (int)cudaErrorMemoryAllocation;
+  cudaError_t e = cudaMemsetAsync(fl, 0, (size_t)(nblk + 8) * sizeof(int), s);
+  if (e) return (int)e;
+  if (!g_sms) {
+    int d;
+    cudaGetDevice(&d);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, d);
+  }
+  if (ldd % TB64 || (uintptr_t)Dinv % 16) return (int)cudaErrorMisalignedAddress;
+  const bool vec_ok = lda % 2 == 0 && (uintptr_t)A % 16 == 0;
+  int grid = nblk < 3 * g_sms ? nblk : 3 * g_sms;
+  const size_t dyn = (size_t)TB64 * TB64 * sizeof(double);
+  trsv_ticket64_k<<<grid, THREADS, dyn, s>>>(n, nblk, (const double *)A, lda, lower_op, tr,
+                                             (const double *)Dinv, ldd, (const double *)b,
+                                             (double *)x, fl + nblk, fl, status, vec_ok);
+  pla_k_count(1);
+  return (int)cudaGetLastError();
+}
+
 }  // namespace
 
-// Dinv must hold ldd x 128 elements with ldd >= n rounded up to 128.
+// Dinv must hold ldd x TB elements with ldd >= n rounded up to TB (TB = 128
+// for fp32, 64 for FP64).
 extern "C" int pla_k_trsv_inv_blocks(int dt, char uplo, char trans, char diag, int n,
                                      const void *A, long lda, void *Dinv, long ldd,
                                      cudaStream_t s) {
   if (n <= 0) return 0;
-  // fp32 only: two 128 x 129 fp64 blocks would not fit in shared memory
-  if (dt == MPI_FLOAT) return inv_blocks<float>(uplo, trans, diag, n, A, lda, Dinv, ldd, s);
+  if (dt == MPI_FLOAT) return inv_blocks<float, TB>(uplo, trans, diag, n, A, lda, Dinv, ldd, s);
+  if (dt == MPI_DOUBLE)
+    return inv_blocks<double, TB64>(uplo, trans, diag, n, A, lda, Dinv, ldd, s);
   return (int)cudaErrorInvalidValue;
 }
 
@@ -296,6 +451,7 @@ extern "C" int pla_k_trsv_ticket(int dt, char uplo, char trans, int n, const voi
   if (n <= 0) return 0;
   if (dt == MPI_FLOAT)
     return ticket_solve<float>(uplo, trans, n, A, lda, Dinv, ldd, b, x, status, s);
+  if (dt == MPI_DOUBLE) return ticket_solve64(uplo, trans, n, A, lda, Dinv, ldd, b, x, status, s);
   return (int)cudaErrorInvalidValue;
 }
 

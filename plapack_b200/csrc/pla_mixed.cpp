@@ -25,6 +25,8 @@ using namespace pla;
 
 namespace pla {
 int lu_on_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, int *zero_info_host);
+int tri_solve(int dt, char uplo, char trans, char diag, int n, int nrhs, const char *T, long ldt,
+              char *X, long ldx);
 int chol_on_device(int dt, int n, char *A, long lda, int nb, int *info_host);
 int trsm_device(int dt, char side, char uplo, char trans, char diag, int nt, int other,
                 double alpha, const char *T, long ldt, char *B, long ldb);
@@ -251,11 +253,13 @@ int precond(const Factor &F, const double *v, long ldv, double *out, long ldo, i
     K(pla_k_copy(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, nrhs, v, ldv, out, ldo, stream()));
     if (F.kind == 0) {
       K(pla_k_laswp_rows(MPI_DOUBLE, out, ldo, nrhs, n, F.piv, stream()));
-      K(pla_k_trsv_blocked(MPI_DOUBLE, 'L', 'N', 'U', n, nrhs, F.a64, F.ld, out, ldo, stream()));
-      K(pla_k_trsv_blocked(MPI_DOUBLE, 'U', 'N', 'N', n, nrhs, F.a64, F.ld, out, ldo, stream()));
+      const char *f = (const char *)F.a64;
+      K(tri_solve(MPI_DOUBLE, 'L', 'N', 'U', n, nrhs, f, F.ld, (char *)out, ldo));
+      K(tri_solve(MPI_DOUBLE, 'U', 'N', 'N', n, nrhs, f, F.ld, (char *)out, ldo));
     } else {
-      K(pla_k_trsv_blocked(MPI_DOUBLE, 'L', 'N', 'N', n, nrhs, F.a64, F.ld, out, ldo, stream()));
-      K(pla_k_trsv_blocked(MPI_DOUBLE, 'L', 'T', 'N', n, nrhs, F.a64, F.ld, out, ldo, stream()));
+      const char *f = (const char *)F.a64;
+      K(tri_solve(MPI_DOUBLE, 'L', 'N', 'N', n, nrhs, f, F.ld, (char *)out, ldo));
+      K(tri_solve(MPI_DOUBLE, 'L', 'T', 'N', n, nrhs, f, F.ld, (char *)out, ldo));
     }
     return PLA_SUCCESS;
   }

@@ -248,29 +248,93 @@ int lu_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, Status 
   return 0;  // every lookahead panel was awaited at its own step
 }
 
-// Blocked right-looking lower Cholesky (SOLVERS/Cholesky/PLA_Chol.c:159-224).
+// A21 := A21 inv(L11)' for the rest x b block column below a b x b diagonal
+// block (b <= 128).  For tall blocks L11 is inverted once (substitution
+// against the identity) and applied as a GEMM from a copy of A21.
+int trsm_right_lower_t(int dt, int b, int rest, const char *L11, long lda, char *A21,
+                       const int *status) {
+  if (rest < 1024)
+    return pla_k_trsm_small(dt, 'R', 'L', 'T', 'N', b, rest, 1.0, L11, lda, A21, lda, status,
+                            stream());
+  const int es = dt == MPI_DOUBLE ? 8 : 4;
+  char *inv = (char *)scratch(20, (size_t)kTri * kTri * es);
+  char *copy = (char *)scratch(21, (size_t)rest * b * es);
+  if (!inv || !copy) return (int)cudaErrorMemoryAllocation;
+  int r = pla_k_fill(dt, b, b, inv, b, 0.0, stream());
+  if (!r) r = pla_k_fill(dt, 1, b, inv, b + 1, 1.0, stream());  // the diagonal
+  if (!r) r = pla_k_trsm_small(dt, 'L', 'L', 'N', 'N', b, b, 1.0, L11, lda, inv, b, status,
+                               stream());
+  if (!r) r = pla_k_copy(dt, PLA_NO_TRANSPOSE, rest, b, A21, lda, copy, rest, stream());
+  if (!r) r = pla_k_gemm(dt, PLA_NO_TRANSPOSE, PLA_TRANSPOSE, rest, b, b, 1.0, copy, rest, inv, b,
+                         0.0, A21, lda, 0, status, stream());
+  return r;
+}
+
+// Blocked right-looking lower Cholesky (SOLVERS/Cholesky/PLA_Chol.c:159-224),
+// with the lookahead of the LU loop: after step k the block column k+1 is
+// updated first, its diagonal factorization and solve run on the lookahead
+// stream, and the rest of the SYRK update of step k runs beside them.
 int chol_device(int dt, int n, char *A, long lda, int nb, Status *st) {
   const int es = dt == MPI_DOUBLE ? 8 : 4;
   auto at = [&](long i, long j) { return A + (i + j * lda) * es; };
-  nb = std::min(nb, kTri);
+  nb = std::min(nb, 2 * kTri);  // a block column of up to 256, factored in steps of <= 128
   PLA_Phase_times &ph = state().phases;
+  const bool la = n >= 4 * nb;
+  cudaStream_t s0 = stream(), s1 = la ? lookahead_stream() : s0;
+  cudaEvent_t ev_next = la ? lookahead_event(0) : nullptr, ev_panel = la ? lookahead_event(1) : nullptr;
+  // block column [k, k + b): inner steps of at most 128 columns (diagonal
+  // block, the solve below it, the update of the block column's remaining
+  // columns), so the trailing SYRK of the outer loop has K = b
+  auto panel = [&](int k, int b) -> int {
+    for (int kk = k; kk < k + b; kk += kTri) {
+      const int bb = std::min(kTri, k + b - kk), rest = n - kk - bb;
+      {
+        PhaseTimer t(&ph.panel_ms);
+        K(pla_k_potrf_lower(dt, bb, at(kk, kk), lda, &st->status, &st->info, kk, stream()));
+      }
+      if (rest <= 0) break;
+      {
+        PhaseTimer t(&ph.trsm_ms);
+        K(trsm_right_lower_t(dt, bb, rest, at(kk, kk), lda, at(kk + bb, kk), &st->status));
+      }
+      const int inner = k + b - kk - bb;  // columns of the block column still to update
+      if (inner > 0) {
+        PhaseTimer t(&ph.panel_ms);
+        K(pla_k_gemm(dt, PLA_NO_TRANSPOSE, PLA_TRANSPOSE, rest, inner, bb, -1.0, at(kk + bb, kk),
+                     lda, at(kk + bb, kk), lda, 1.0, at(kk + bb, kk + bb), lda, 'L', &st->status,
+                     stream()));
+      }
+    }
+    return 0;
+  };
+  // columns [c0, c0 + nc) of the trailing matrix (rows c0 .. n-1, lower part)
+  auto syrk = [&](int k, int b, int c0, int nc) -> int {
+    PhaseTimer t(&ph.update_ms);
+    int r = pla_k_gemm(dt, PLA_NO_TRANSPOSE, PLA_TRANSPOSE, n - c0, nc, b, -1.0, at(c0, k), lda,
+                       at(c0, k), lda, 1.0, at(c0, c0), lda, 'L', &st->status, stream());
+    if (t.on) ph.update_launches++;
+    return r;
+  };
+  int ready = -1;
   for (int k = 0; k < n; k += nb) {
-    const int b = std::min(nb, n - k), rest = n - k - b;
-    {
-      PhaseTimer t(&ph.panel_ms);
-      K(pla_k_potrf_lower(dt, b, at(k, k), lda, &st->status, &st->info, k, stream()));
-    }
+    const int b = std::min(nb, n - k), rest = n - k - b, k2 = k + b;
+    if (ready == k) PLA_CUDA(cudaStreamWaitEvent(s0, ev_panel, 0));
+    else K(panel(k, b));
     if (rest <= 0) continue;
-    {
-      PhaseTimer t(&ph.trsm_ms);
-      K(pla_k_trsm_small(dt, 'R', 'L', 'T', 'N', b, rest, 1.0, at(k, k), lda, at(k + b, k), lda,
-                         &st->status, stream()));
-    }
-    {
-      PhaseTimer t(&ph.update_ms);
-      K(pla_k_gemm(dt, PLA_NO_TRANSPOSE, PLA_TRANSPOSE, rest, rest, b, -1.0, at(k + b, k), lda,
-                   at(k + b, k), lda, 1.0, at(k + b, k + b), lda, 'L', &st->status, stream()));
-      if (t.on) ph.update_launches++;
+    const int b2 = std::min(nb, rest);
+    if (la) {
+      K(syrk(k, b, k2, b2));  // block column k+1 first
+      PLA_CUDA(cudaEventRecord(ev_next, s0));
+      PLA_CUDA(cudaStreamWaitEvent(s1, ev_next, 0));
+      {
+        OnStream on(s1);
+        K(panel(k2, b2));
+      }
+      PLA_CUDA(cudaEventRecord(ev_panel, s1));
+      ready = k2;
+      if (rest - b2 > 0) K(syrk(k, b, k2 + b2, rest - b2));
+    } else {
+      K(syrk(k, b, k2, rest));
     }
   }
   return 0;
@@ -431,15 +495,55 @@ int PLA_Local_chol(int uplo, PLA_Obj A) {
 }
 
 // --------------------------------------------------------------- solves ----
+}  // extern "C"
+
+namespace pla {
+// x := inv(op(T)) x for nrhs columns of x: one or two columns of order >= 1024
+// go through the single-launch solve (inverse diagonal blocks first, then one
+// launch per column); other shapes through the blocked solve.  Queued on the
+// library stream; a bounded wait that gives up is reported by finish_solve.
+int tri_solve(int dt, char uplo, char trans, char diag, int n, int nrhs, const char *T, long ldt,
+              char *X, long ldx) {
+  if (n <= 0 || nrhs <= 0) return 0;
+  if (n < 1024 || nrhs > 2)
+    return pla_k_trsv_blocked(dt, uplo, trans, diag, n, nrhs, T, ldt, X, ldx, stream());
+  const int es = dt == MPI_DOUBLE ? 8 : 4, tb = dt == MPI_DOUBLE ? 64 : 128;
+  const long ldd = ((long)n + tb - 1) / tb * tb;
+  char *dinv = (char *)scratch(22, (size_t)ldd * tb * es);
+  int *status = (int *)scratch(23, 64);
+  if (!dinv || !status) return (int)cudaErrorMemoryAllocation;
+  cudaError_t e = cudaMemsetAsync(status, 0, sizeof(int), stream());
+  if (e) return (int)e;
+  int r = pla_k_trsv_inv_blocks(dt, uplo, trans, diag, n, T, ldt, dinv, ldd, stream());
+  for (int c = 0; c < nrhs && !r; c++) {
+    char *col = X + (long)c * ldx * es;
+    r = pla_k_trsv_ticket(dt, uplo, trans, n, T, ldt, dinv, ldd, col, col, status, stream());
+  }
+  return r;
+}
+// after tri_solve: wait, and report a solve whose bounded wait gave up
+int finish_solve(const char *what) {
+  int r = finish(what);
+  if (r) return r;
+  int *status = (int *)scratch(23, 64);
+  int h = 0;
+  if (status) PLA_CUDA(d2h(&h, status, sizeof h));
+  if (h == PLA_K_TIMEOUT) PLA_FAIL("triangular solve: a bounded wait timed out");
+  return PLA_SUCCESS;
+}
+}  // namespace pla
+
+extern "C" {
+
 int PLA_Trsv(int uplo, int trans, int diag, PLA_Obj A, PLA_Obj x) {
   if (!valid(A) || !valid(x)) PLA_FAIL("invalid object");
   if (!numeric(A) || A->base->datatype != x->base->datatype) PLA_FAIL("datatype mismatch");
   if (A->length != A->width || vlen(x) != A->length) PLA_FAIL("nonconformal objects");
   if (vinc(x) != 1) PLA_FAIL("x must be a column vector");
   PhaseTimer t(&state().phases.solve_ms);
-  K(pla_k_trsv_blocked(A->base->datatype, uplo_c(uplo), trans_c(trans), diag_c(diag), A->length,
-                       1, at(A, 0, 0), ld(A), at(x, 0, 0), ld(x), stream()));
-  return finish("trsv");
+  K(tri_solve(A->base->datatype, uplo_c(uplo), trans_c(trans), diag_c(diag), A->length, 1,
+              at(A, 0, 0), ld(A), at(x, 0, 0), ld(x)));
+  return finish_solve("trsv");
 }
 
 int PLA_Local_trsv(int uplo, int trans, int diag, PLA_Obj A, PLA_Obj x) {
@@ -517,12 +621,10 @@ int PLA_General_solve(PLA_Obj A, PLA_Obj ipiv, PLA_Obj B) {
     if (r) return r;
     const int dt = A->base->datatype, n = A->length;
     PhaseTimer t(&state().phases.solve_ms);
-    // Trsm for several right-hand sides, Trsv for one: the same blocked kernel
-    K(pla_k_trsv_blocked(dt, 'L', 'N', 'U', n, B->width, at(A, 0, 0), ld(A), at(B, 0, 0), ld(B),
-                         stream()));
-    K(pla_k_trsv_blocked(dt, 'U', 'N', 'N', n, B->width, at(A, 0, 0), ld(A), at(B, 0, 0), ld(B),
-                         stream()));
-    r = finish("general solve");
+    // Trsv for one or two right-hand sides (single launch), Trsm for more
+    K(tri_solve(dt, 'L', 'N', 'U', n, B->width, at(A, 0, 0), ld(A), at(B, 0, 0), ld(B)));
+    K(tri_solve(dt, 'U', 'N', 'N', n, B->width, at(A, 0, 0), ld(A), at(B, 0, 0), ld(B)));
+    r = finish_solve("general solve");
     if (r) return r;
   }
   return PLA_SUCCESS;
@@ -536,11 +638,9 @@ int PLA_Pos_def_solve(PLA_Obj A, PLA_Obj B) {
   if (!valid(B)) PLA_FAIL("invalid object B");
   const int dt = A->base->datatype, n = A->length;
   PhaseTimer t(&state().phases.solve_ms);
-  K(pla_k_trsv_blocked(dt, 'L', 'N', 'N', n, B->width, at(A, 0, 0), ld(A), at(B, 0, 0), ld(B),
-                       stream()));
-  K(pla_k_trsv_blocked(dt, 'L', 'T', 'N', n, B->width, at(A, 0, 0), ld(A), at(B, 0, 0), ld(B),
-                       stream()));
-  int r = finish("pos def solve");
+  K(tri_solve(dt, 'L', 'N', 'N', n, B->width, at(A, 0, 0), ld(A), at(B, 0, 0), ld(B)));
+  K(tri_solve(dt, 'L', 'T', 'N', n, B->width, at(A, 0, 0), ld(A), at(B, 0, 0), ld(B)));
+  int r = finish_solve("pos def solve");
   return r ? r : value;
 }
 

@@ -288,3 +288,37 @@ def test_api_axpy_accumulates(pla_session):
     exp[1:5, 2:5] = 2 * A
     assert np.array_equal(out, exp)
     s.free(a)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("n", [1024, 3001])
+def test_trsv_single_launch(pla_session, dtype, n):
+    """PLA_Trsv of order >= 1024 runs the single-launch solve (inverse diagonal
+    blocks of 64 in FP64, 128 in fp32): all four triangle / transpose cases,
+    unit and non-unit diagonals, against LAPACK's triangular solve."""
+    from scipy.linalg import solve_triangular
+    from plapack_b200 import pla
+    s = pla_session
+    rng = np.random.default_rng(n)
+    M = rng.standard_normal((n, n)) / np.sqrt(n)
+    M[np.diag_indices(n)] = 1.0 + rng.random(n)
+    cases = [(pla.PLA_LOWER_TRIANGULAR, pla.PLA_NO_TRANSPOSE, pla.PLA_UNIT_DIAG),
+             (pla.PLA_UPPER_TRIANGULAR, pla.PLA_NO_TRANSPOSE, pla.PLA_NONUNIT_DIAG),
+             (pla.PLA_LOWER_TRIANGULAR, pla.PLA_TRANSPOSE, pla.PLA_NONUNIT_DIAG),
+             (pla.PLA_UPPER_TRIANGULAR, pla.PLA_TRANSPOSE, pla.PLA_UNIT_DIAG)]
+    eps = np.finfo(dtype).eps
+    for uplo, trans, diag in cases:
+        A = np.asfortranarray(M.astype(dtype))
+        b = rng.standard_normal((n, 1)).astype(dtype)
+        a = s.matrix(n, n, dtype)
+        x = s.mvector(n, 1, dtype)
+        s.put(a, A)
+        s.put(x, b)
+        pla.check(s.lib.PLA_Trsv(uplo, trans, diag, a, x), "PLA_Trsv")
+        got = s.get(x)[:, 0].astype(np.float64)
+        ref = solve_triangular(A.astype(np.float64), b[:, 0].astype(np.float64),
+                               lower=uplo == pla.PLA_LOWER_TRIANGULAR,
+                               trans=0 if trans == pla.PLA_NO_TRANSPOSE else 1,
+                               unit_diagonal=diag == pla.PLA_UNIT_DIAG)
+        assert np.abs(got - ref).max() <= 64 * n * eps * np.abs(ref).max(), (uplo, trans, diag)
+        s.free(a, x)
