@@ -6,8 +6,11 @@
 //                       matrix in shared memory, warp-synchronous;
 //   mode 1 ("smem")   : one instance per CTA, matrix and right-hand sides in
 //                       shared memory;
-//   mode 2 ("global") : one instance per CTA working in place in global memory
-//                       (an instance of order <= 512 stays resident in L2).
+//   mode 2 ("global") : one instance per CTA working in place in global memory:
+//                       blocked (panels of 16 / 32 columns in shared memory,
+//                       the trailing matrix updated once per panel) when the
+//                       panel fits the launch's shared memory, else the
+//                       column algorithm in place.
 // CTAs pull tasks from an atomic queue, largest first, so the long instances
 // start early and the short ones fill the tail.  Each instance runs the same
 // column algorithms as the reference's sequential kernels: LU as PLA_dlu
@@ -290,10 +293,250 @@ __device__ void cta_instance(const Inst<T> &in, T *M, long lm, T *X, long lx, in
   if (tid == 0) *info = s_bad;
 }
 
+// Blocked form of cta_instance for an instance in global memory (mode 2) whose
+// panel fits the CTA's shared memory: panels of PW columns are factored in
+// shared memory with the column algorithm; then the interchanges go to the
+// other columns, U12 is solved, and the trailing matrix is updated once per
+// panel in chunks of 64 columns (its elements pass through the SM once per
+// panel instead of once per column).  Every element receives the same fma
+// operations in the same order as in the column algorithm, so the factors,
+// pivots and info are bitwise those of cta_instance.
+template <typename T>
+__device__ void cta_blocked(const Inst<T> &in, T *S, int *info) {
+  constexpr int PW = sizeof(T) == 8 ? 16 : 32, CW = 64;
+  __shared__ T sv[32];
+  __shared__ int si[32];
+  __shared__ int s_bad, s_piv[32];
+  const int n = in.n, tid = threadIdx.x;
+  T *A = in.A;
+  T *P = S;              // panel: rows j0 .. n-1 of PW columns, ld n
+  T *Uc = S + (long)n * PW;  // a PW x CW chunk of U12 (LU), ld PW
+  if (tid == 0) s_bad = 0;
+  __syncthreads();
+  for (int j0 = 0; j0 < n; j0 += PW) {
+    const int jb = min(PW, n - j0), m = n - j0;
+    for (int e = tid; e < m * jb; e += THREADS) {
+      const int i = e % m, c = e / m;
+      P[i + (long)c * n] = A[(j0 + i) + (long)(j0 + c) * n];
+    }
+    __syncthreads();
+    if (in.kind == 0) {
+      for (int j = 0; j < jb; j++) {
+        T v = T(-1);
+        int idx = INT_MAX;
+        for (int i = j + tid; i < m; i += THREADS) {
+          const T a = fabs(P[i + (long)j * n]);
+          if (a > v) { v = a; idx = i; }
+        }
+        block_argmax(v, idx, sv, si);
+        const int p = idx == INT_MAX ? j : idx;  // all-NaN column: no interchange
+        if (tid == 0) {
+          in.piv[j0 + j] = p - j;
+          s_piv[j] = p;
+        }
+        if (p != j)
+          for (int c = tid; c < jb; c += THREADS) {
+            const T a = P[j + (long)c * n];
+            P[j + (long)c * n] = P[p + (long)c * n];
+            P[p + (long)c * n] = a;
+          }
+        __syncthreads();
+        const T piv = P[j + (long)j * n];
+        if (tid == 0 && piv == T(0) && !s_bad) s_bad = j0 + j + 1;
+        const T inv = T(1) / piv;
+        for (int i = j + 1 + tid; i < m; i += THREADS) P[i + (long)j * n] *= inv;
+        __syncthreads();
+        const int rows = m - j - 1, cols = jb - j - 1;
+        for (int e = tid; e < rows * cols; e += THREADS) {
+          const int i = j + 1 + e % rows, c = j + 1 + e / rows;
+          P[i + (long)c * n] = fma(P[i + (long)j * n], -P[j + (long)c * n], P[i + (long)c * n]);
+        }
+        __syncthreads();
+      }
+      for (int e = tid; e < m * jb; e += THREADS) {
+        const int i = e % m, c = e / m;
+        A[(j0 + i) + (long)(j0 + c) * n] = P[i + (long)c * n];
+      }
+      // the panel's interchanges on every other column, in order, a column
+      // per thread
+      for (int c = tid; c < n; c += THREADS) {
+        if (c >= j0 && c < j0 + jb) continue;
+        T *col = A + (long)c * n + j0;
+        for (int j = 0; j < jb; j++) {
+          const int p = s_piv[j];
+          if (p != j) {
+            const T a = col[j];
+            col[j] = col[p];
+            col[p] = a;
+          }
+        }
+      }
+      __syncthreads();
+      if (j0 + jb < n) {
+        // U12 := inv(L11) A12, a column per thread (the updates of column i
+        // reach row k in the order i = 0, 1, ... as in the column algorithm)
+        for (int c = j0 + jb + tid; c < n; c += THREADS) {
+          T u[PW];
+          T *col = A + (long)c * n + j0;
+#pragma unroll
+          for (int k = 0; k < PW; k++) u[k] = k < jb ? col[k] : T(0);
+#pragma unroll
+          for (int i = 0; i < PW; i++)
+#pragma unroll
+            for (int k = i + 1; k < PW; k++)
+              if (k < jb) u[k] = fma(P[k + (long)i * n], -u[i], u[k]);
+#pragma unroll
+          for (int k = 0; k < PW; k++)
+            if (k < jb) col[k] = u[k];
+        }
+        __syncthreads();
+        // A22 -= L21 U12 in chunks of CW columns, four columns a thread
+        const int m2 = m - jb;
+        for (int cc = j0 + jb; cc < n; cc += CW) {
+          const int cw = min(CW, n - cc);
+          for (int e = tid; e < jb * cw; e += THREADS) {
+            const int k = e % jb, c = e / jb;
+            Uc[k + c * PW] = A[(j0 + k) + (long)(cc + c) * n];
+          }
+          __syncthreads();
+          const int groups = (cw + 3) / 4;
+          for (int e = tid; e < m2 * groups; e += THREADS) {
+            const int i = e % m2, c4 = 4 * (e / m2);
+            T *row = A + (j0 + jb + i);
+            T acc[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[q] = c4 + q < cw ? row[(long)(cc + c4 + q) * n] : T(0);
+            for (int k = 0; k < jb; k++) {
+              const T l = P[(jb + i) + (long)k * n];
+#pragma unroll
+              for (int q = 0; q < 4; q++) acc[q] = fma(l, -Uc[k + (c4 + q) * PW], acc[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+              if (c4 + q < cw) row[(long)(cc + c4 + q) * n] = acc[q];
+          }
+          __syncthreads();
+        }
+      }
+    } else {
+      bool stop = false;
+      for (int j = 0; j < jb; j++) {
+        const T d = P[j + (long)j * n];
+        if (d <= T(0)) {
+          if (tid == 0) s_bad = j0 + j + 1;
+          stop = true;
+          break;
+        }
+        const T sq = sqrt(d), inv = T(1) / sq;
+        __syncthreads();
+        if (tid == 0) P[j + (long)j * n] = sq;
+        for (int i = j + 1 + tid; i < m; i += THREADS) P[i + (long)j * n] *= inv;
+        __syncthreads();
+        const int rows = m - j - 1, cols = jb - j - 1;
+        for (int e = tid; e < rows * cols; e += THREADS) {
+          const int i = j + 1 + e % rows, c = j + 1 + e / rows;
+          if (i >= c)
+            P[i + (long)c * n] = fma(-P[i + (long)j * n], P[c + (long)j * n], P[i + (long)c * n]);
+        }
+        __syncthreads();
+      }
+      if (stop) break;
+      for (int e = tid; e < m * jb; e += THREADS) {
+        const int i = e % m, c = e / m;
+        if (i >= c) A[(j0 + i) + (long)(j0 + c) * n] = P[i + (long)c * n];
+      }
+      // A22 -= L21 L21' (lower part), L21 read from the panel, 4 columns a thread
+      const int m2 = m - jb;
+      for (int cc = 0; cc < m2; cc += CW) {
+        const int cw = min(CW, m2 - cc);
+        const int groups = (cw + 3) / 4, rows = m2 - cc;  // rows i >= cc of the chunk
+        for (int e = tid; e < rows * groups; e += THREADS) {
+          const int i = cc + e % rows, c4 = cc + 4 * (e / rows);
+          T *row = A + (j0 + jb + i);
+          T acc[4];
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            acc[q] = (c4 + q < cc + cw && i >= c4 + q) ? row[(long)(j0 + jb + c4 + q) * n] : T(0);
+          for (int k = 0; k < jb; k++) {
+            const T l = P[(jb + i) + (long)k * n];
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[q] = fma(-l, P[(jb + c4 + q) + (long)k * n], acc[q]);
+          }
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            if (c4 + q < cc + cw && i >= c4 + q) row[(long)(j0 + jb + c4 + q) * n] = acc[q];
+        }
+      }
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  const int bad = s_bad;
+  // the solves, in global memory, as in cta_instance
+  T *X = in.B;
+  const long lx = n;
+  if (in.kind == 0) {
+    for (int r = tid; r < in.nrhs; r += THREADS)
+      for (int j = 0; j < n; j++) {
+        int p = j + in.piv[j];
+        if (p != j) {
+          T a = X[j + r * lx];
+          X[j + r * lx] = X[p + r * lx];
+          X[p + r * lx] = a;
+        }
+      }
+    __syncthreads();
+    for (int j = 0; j < n; j++) {
+      for (long e = tid; e < (long)(n - j - 1) * in.nrhs; e += THREADS) {
+        const int i = j + 1 + (int)(e % (n - j - 1)), r = (int)(e / (n - j - 1));
+        X[i + r * lx] -= A[i + (long)j * n] * X[j + r * lx];
+      }
+      __syncthreads();
+    }
+    for (int j = n - 1; j >= 0; j--) {
+      if (tid < in.nrhs) X[j + tid * lx] = X[j + tid * lx] / A[j + (long)j * n];
+      __syncthreads();
+      for (long e = tid; e < (long)j * in.nrhs; e += THREADS) {
+        const int i = (int)(e % j), r = (int)(e / j);
+        X[i + r * lx] -= A[i + (long)j * n] * X[j + r * lx];
+      }
+      __syncthreads();
+    }
+  } else if (!bad) {
+    for (int j = 0; j < n; j++) {
+      if (tid < in.nrhs) X[j + tid * lx] = X[j + tid * lx] / A[j + (long)j * n];
+      __syncthreads();
+      for (long e = tid; e < (long)(n - j - 1) * in.nrhs; e += THREADS) {
+        const int i = j + 1 + (int)(e % (n - j - 1)), r = (int)(e / (n - j - 1));
+        X[i + r * lx] -= A[i + (long)j * n] * X[j + r * lx];
+      }
+      __syncthreads();
+    }
+    for (int j = n - 1; j >= 0; j--) {
+      if (tid < in.nrhs) X[j + tid * lx] = X[j + tid * lx] / A[j + (long)j * n];
+      __syncthreads();
+      for (long e = tid; e < (long)j * in.nrhs; e += THREADS) {
+        const int i = (int)(e % j), r = (int)(e / j);
+        X[i + r * lx] -= A[j + (long)i * n] * X[j + r * lx];
+      }
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  if (tid == 0) *info = bad;
+}
+
+// shared memory the blocked form needs for an instance of order n
+template <typename T>
+__host__ __device__ constexpr size_t blocked_smem(int n) {
+  return ((size_t)n * (sizeof(T) == 8 ? 16 : 32) + (size_t)(sizeof(T) == 8 ? 16 : 32) * 64) *
+         sizeof(T);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(THREADS)
 batched_k(const Inst<T> *inst, const int *order, const Task *tasks, int ntasks, int *queue,
-          int *info) {
+          int *info, size_t smem_bytes) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *S = (T *)smem_raw;
   __shared__ int s_task;
@@ -332,6 +575,8 @@ batched_k(const Inst<T> *inst, const int *order, const Task *tasks, int ntasks, 
         if (keep_b)
           for (long e = threadIdx.x; e < (long)n * in.nrhs; e += THREADS)
             in.B[e] = X[(e % n) + (e / n) * lx];
+      } else if (blocked_smem<T>(in.n) <= smem_bytes) {
+        cta_blocked(in, S, &info[id]);
       } else {
         cta_instance(in, in.A, in.n, in.B, in.n, &info[id]);
       }
@@ -357,11 +602,11 @@ extern "C" int pla_k_batched(int dt, const void *inst, const int *order, const v
   if (dt == MPI_DOUBLE) {
     cudaFuncSetAttribute(batched_k<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     batched_k<double><<<grid, THREADS, smem, s>>>((const Inst<double> *)inst, order,
-                                                  (const Task *)tasks, ntasks, queue, info);
+                                                  (const Task *)tasks, ntasks, queue, info, smem);
   } else if (dt == MPI_FLOAT) {
     cudaFuncSetAttribute(batched_k<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     batched_k<float><<<grid, THREADS, smem, s>>>((const Inst<float> *)inst, order,
-                                                 (const Task *)tasks, ntasks, queue, info);
+                                                 (const Task *)tasks, ntasks, queue, info, smem);
   } else {
     return (int)cudaErrorInvalidValue;
   }

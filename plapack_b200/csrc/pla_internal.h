@@ -87,8 +87,11 @@ cudaStream_t stream();
 // 100: 0.316 / 1.177 s.  The fp32 panel of the mixed LU runs beside a short
 // HBM-bound update and wants more CTAs; the FP64 panel beside the long DGEMM
 // fewer.
+#ifndef PLA_LOOKAHEAD_CTAS_F64
+#define PLA_LOOKAHEAD_CTAS_F64 48
+#endif
 constexpr int kLookaheadCtasF32 = 72;
-constexpr int kLookaheadCtasF64 = 48;
+constexpr int kLookaheadCtasF64 = PLA_LOOKAHEAD_CTAS_F64;
 cudaStream_t lookahead_stream();
 cudaEvent_t lookahead_event(int i);
 // while alive, stream() returns `s` (host code is sequential, so the switch

@@ -91,6 +91,20 @@ def test_batched_matches_oracle(env, restated, dtype, autotune):
     s.lib.PLA_Batch_plan_free(ctypes.byref(plan))
 
 
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_batched_large_orders_blocked(env, restated, dtype):
+    """Orders up to 512 go through the blocked global-memory form; its pivots
+    and factors are those of the column algorithm (the oracle's PLA_dlu)."""
+    s, torch, pla = env
+    count = 40
+    arr, host, dev = make_batch(torch, pla, count, dtype, 17, nmax=512)
+    info = torch.full((count,), -1, dtype=torch.int32, device="cuda")
+    dt = pla.MPI_DOUBLE if dtype == np.float64 else pla.MPI_FLOAT
+    pla.check(s.lib.PLA_Batched_factor_solve(dt, count, arr, info.data_ptr()), "batched")
+    torch.cuda.synchronize()
+    check_results(host, dev, info.cpu().numpy(), restated, dtype)
+
+
 def test_batched_reports_failures(env):
     s, torch, pla = env
     arr = (pla.BatchInstance * 3)()
