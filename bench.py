@@ -57,8 +57,9 @@ def parse():
     p.add_argument("--precision", choices=["fp16", "bf16", "fp32"], default="fp16")
     p.add_argument("--refinement", choices=["gmres", "lu"], default="gmres")
     p.add_argument("--nb", type=int, default=256, help="block size of the mixed factorization")
-    p.add_argument("--nb-fp64", type=int, default=256,
-                   help="nb_alg of the FP64 LU and Cholesky (256: K = 256 trailing updates)")
+    p.add_argument("--nb-fp64", type=int, default=512,
+                   help="nb_alg of the FP64 LU (512: K = 512 trailing updates); the Cholesky "
+                        "caps it at 256")
     p.add_argument("--skip-fp64", action="store_true")
     p.add_argument("--skip-e2e", action="store_true")
     p.add_argument("--skip-cpu", action="store_true")
