@@ -10,8 +10,9 @@ reflectors with seeded Gaussian vectors; kappa = 1e6; x_true ~ N(0,1)),
 called through the library's C ABI (PLA_General_solve_mixed; the FP64 arm is
 PLA_General_solve).  Inputs are resident in HBM and larger than L2 (8.6 GB).
 `e2e` repeats the mixed solve with the matrix and right-hand side in pinned
-host memory, copied in through PLA_Obj_set_local_contents and the solution
-read back through PLA_Obj_get_local_contents, every step.
+host memory: b through PLA_Obj_set_local_contents, A through
+PLA_General_solve_mixed_host (which copies it during the factorization), the
+solution read back through PLA_Obj_get_local_contents, every step.
 
 --impl reference times the upstream PLAPACK (compiled from its sources into
 oracle/_ref, linked to a threaded OpenBLAS) on the host cores: PLA_General_solve
@@ -685,11 +686,11 @@ def run_ours(args):
         NT = pla.PLA_NO_TRANSPOSE
 
         def e2e_step():
-            check(lib.PLA_Obj_set_local_contents(NT, n, n, ctypes.c_void_p(Th.data_ptr()), n, 1, a),
-                  "set A")
             check(lib.PLA_Obj_set_local_contents(NT, n, 1, ctypes.c_void_p(bh.data_ptr()), n, 1, bo),
                   "set b")
-            check(lib.PLA_General_solve_mixed(a, bo, ctypes.byref(params), ctypes.byref(report)),
+            # A travels from pinned host memory during the factorization
+            check(lib.PLA_General_solve_mixed_host(a, ctypes.c_void_p(Th.data_ptr()), n, bo,
+                                                   ctypes.byref(params), ctypes.byref(report)),
                   "solve")
             check(lib.PLA_Obj_get_local_contents(bo, NT, None, None, ctypes.c_void_p(xh.data_ptr()),
                                                  n, 1), "get x")
@@ -704,8 +705,9 @@ def run_ours(args):
         barrier()
         e2e = {"value": max_over_ranks(g0.elapsed_time(g1) / 1e3 / args.steps), "unit": "s",
                "h2d_bytes_per_step": n * n * 8 + n * 8, "d2h_bytes_per_step": n * 8,
-               "path": "PLA_Obj_set_local_contents (pinned host) -> PLA_General_solve_mixed -> "
-                       "PLA_Obj_get_local_contents"}
+               "path": "PLA_Obj_set_local_contents (b, pinned host) -> "
+                       "PLA_General_solve_mixed_host (A from pinned host, copied during the "
+                       "factorization) -> PLA_Obj_get_local_contents"}
         del Th
 
     cpu = None

@@ -108,6 +108,16 @@ int PLA_General_solve_mixed(PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *params
                             PLA_Mixed_report *report);
 int PLA_Pos_def_solve_mixed(PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *params,
                             PLA_Mixed_report *report);
+/* PLA_General_solve_mixed for a matrix that is still in host memory: A_host
+ * (n x n FP64, column-major, leading dimension ldh >= n) is copied into the
+ * device object A during the call.  For n >= 4096 and bf16 / fp16 / fp8
+ * factors the copy overlaps the factorization: A travels in groups of
+ * columns and each group joins the right-looking loop when it has arrived,
+ * replaying the steps it missed, so the result does not depend on the
+ * copy's timing.  A_host in page-locked memory (cudaHostAlloc) lets the copy
+ * run asynchronously; pageable memory works, without the overlap. */
+int PLA_General_solve_mixed_host(PLA_Obj A, const void *A_host, int ldh, PLA_Obj B,
+                                 const PLA_Mixed_params *params, PLA_Mixed_report *report);
 
 /* ---- panel factorization that allocates nothing ---------------------------
  * No counterpart in the reference.  Factors the m x w panel A (device memory,

@@ -50,6 +50,16 @@ cudaStream_t lookahead_stream() {
   return s.la_stream;
 }
 
+cudaStream_t copy_stream() {
+  State &s = state();
+  if (!s.copy_stream) {
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    cudaStreamCreateWithPriority(&s.copy_stream, cudaStreamNonBlocking, lo);
+  }
+  return s.copy_stream;
+}
+
 cudaEvent_t lookahead_event(int i) {
   State &s = state();
   if (!s.la_events[i]) cudaEventCreateWithFlags(&s.la_events[i], cudaEventDisableTiming);
@@ -103,7 +113,7 @@ struct Scratch {
   void *ptr = nullptr;
   size_t bytes = 0;
 };
-constexpr int kScratchSlots = 24;
+constexpr int kScratchSlots = 32;
 Scratch g_scratch[kScratchSlots];
 }  // namespace
 
@@ -305,11 +315,12 @@ int PLA_Finalize(void) {
   cudaStreamSynchronize(stream());
   release_scratch();
   pla_kernels_release();
-  if (s.la_stream) {
-    cudaStreamSynchronize(s.la_stream);
-    cudaStreamDestroy(s.la_stream);
-    s.la_stream = nullptr;
-  }
+  for (cudaStream_t *st : {&s.la_stream, &s.copy_stream})
+    if (*st) {
+      cudaStreamSynchronize(*st);
+      cudaStreamDestroy(*st);
+      *st = nullptr;
+    }
   for (auto &e : s.la_events)
     if (e) {
       cudaEventDestroy(e);

@@ -67,6 +67,7 @@ struct State {
   cudaStream_t own_stream = nullptr;
   cudaStream_t override_stream = nullptr;  // set by OnStream while a scope queues elsewhere
   cudaStream_t la_stream = nullptr;        // high-priority stream of the lookahead panels
+  cudaStream_t copy_stream = nullptr;      // host-to-device copies of a streamed solve
   cudaEvent_t la_events[2] = {nullptr, nullptr};
   int phase_timing = 0;
   PLA_Phase_times phases{};
@@ -94,6 +95,7 @@ constexpr int kLookaheadCtasF32 = 72;
 constexpr int kLookaheadCtasF64 = PLA_LOOKAHEAD_CTAS_F64;
 cudaStream_t lookahead_stream();
 cudaEvent_t lookahead_event(int i);
+cudaStream_t copy_stream();
 // while alive, stream() returns `s` (host code is sequential, so the switch
 // only affects the calls made inside the scope)
 struct OnStream {

@@ -36,6 +36,14 @@ int panel_lu(int dt, int r, int b, char *P, long lda, int *piv, int *status, int
 
 namespace {
 
+// a call that already returns a library code (PLA_SUCCESS or PLA_ERROR with
+// its message recorded)
+#define PK(call)        \
+  do {                  \
+    int r_ = (call);    \
+    if (r_) return r_;  \
+  } while (0)
+
 #define K(call)                                                    \
   do {                                                             \
     int r_ = (call);                                               \
@@ -43,7 +51,8 @@ namespace {
   } while (0)
 
 enum Slots { kSlotA32 = 4, kSlotL = 5, kSlotU = 6, kSlotPiv = 7, kSlotVec = 8, kSlotWork = 9,
-             kSlotV = 10, kSlotSt = 11, kSlotA64 = 16, kSlotScales = 18, kSlotDiag = 19 };
+             kSlotV = 10, kSlotSt = 11, kSlotA64 = 16, kSlotScales = 18, kSlotDiag = 19,
+             kSlotLbig = 24, kSlotDinvSteps = 25, kSlotSclSteps = 26, kSlotTmp = 27 };
 
 long round_up(long v, long m) { return (v + m - 1) / m * m; }
 
@@ -399,6 +408,205 @@ int gmres(const Factor &F, const double *A, long lda, const double *r, double *d
   return PLA_SUCCESS;
 }
 
+// LU of a matrix that is still arriving from host memory (bf16 / fp16 / fp8
+// trailing updates).  The copy stream brings A in groups of columns into the
+// FP64 device object and converts each group into the fp32 working copy; an
+// event marks each group.  Every step keeps its packed L panel, the inverse
+// of its unit lower diagonal block and its pivots, so a group that becomes
+// available after some steps replays exactly what those steps would have done
+// to it: the row interchanges, U rows as inverse(L_kk) times the block, and
+// the tensor-core update.  Every element therefore receives the same
+// operations in the same order whatever the arrival times, and the factors
+// do not depend on them.  The host polls the arrival events as it queues the
+// steps, and stays at most two steps ahead of the device.
+int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, long lda, int nb) {
+  const int n = F.n;
+  const long ld = F.ld;
+  auto at = [&](long i, long j) { return F.a + i + j * ld; };
+  const bool f8 = F.prec == PLA_B200_PREC_FP8;
+  const int kprec = F.prec == PLA_B200_PREC_BF16 ? PLA_K_BF16 : PLA_K_FP16;
+  const int esz = f8 ? 1 : 2;
+  const int nsteps = (n + nb - 1) / nb;
+  const int gcols = std::max(nb, (n / 8 + nb - 1) / nb * nb);  // about 8 groups
+  const int ngroups = (n + gcols - 1) / gcols;
+  const int tiles = (n + 127) / 128 + 1;
+  // per-step storage
+  std::vector<size_t> loff(nsteps);
+  size_t lbytes = 0;
+  for (int k = 0; k < nsteps; k++) {
+    const long rest = std::max(0, n - (k + 1) * nb);
+    loff[k] = lbytes;
+    lbytes += (size_t)round_up(rest * nb * esz, 256);
+  }
+  char *Lbig = (char *)scratch(kSlotLbig, lbytes + 256);
+  float *dinv = (float *)scratch(kSlotDinvSteps, (size_t)nsteps * nb * nb * sizeof(float));
+  float *scl = (float *)scratch(kSlotSclSteps, ((size_t)nsteps + 1) * tiles * sizeof(float));
+  float *tmp = (float *)scratch(kSlotTmp, (size_t)nb * n * sizeof(float) + 256);
+  void *Ub = scratch(kSlotU, (size_t)n * nb * 2 + 256);
+  if (!Lbig || !dinv || !scl || !tmp || !Ub) PLA_FAIL("cannot allocate the streamed-solve buffers");
+  float *inv_u = scl + (size_t)nsteps * tiles;  // the U' scales of the launch in flight
+  int *st = F.status;
+  PLA_Phase_times &ph = state().phases;
+  cudaStream_t s0 = stream(), s1 = lookahead_stream(), sc = copy_stream();
+  int sms = 0;
+  {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  const int side_ctas = std::max(1, sms - kLookaheadCtasF32);
+  std::vector<cudaEvent_t> arr(ngroups), thr(4);
+  for (auto &e : arr) PLA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  for (auto &e : thr) PLA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  struct Events {  // destroyed on every return path
+    std::vector<cudaEvent_t> *a, *b;
+    ~Events() {
+      for (auto e : *a) cudaEventDestroy(e);
+      for (auto e : *b) cudaEventDestroy(e);
+    }
+  } guard{&arr, &thr};
+  cudaEvent_t ev_next = lookahead_event(0), ev_panel = lookahead_event(1);
+
+  // 1. the copies and conversions, group by group, on the copy stream
+  for (int g = 0; g < ngroups; g++) {
+    const long c0 = (long)g * gcols, nc = std::min<long>(gcols, n - c0);
+    PLA_CUDA(cudaMemcpy2DAsync(Ad + c0 * lda, lda * sizeof(double), Ah + c0 * ldh,
+                               ldh * sizeof(double), (size_t)n * sizeof(double), nc,
+                               cudaMemcpyHostToDevice, sc));
+    K(pla_k_convert(MPI_DOUBLE, Ad + c0 * lda, lda, MPI_FLOAT, at(0, c0), ld, n, (int)nc, sc));
+    PLA_CUDA(cudaEventRecord(arr[g], sc));
+  }
+  int known = 0;  // groups [0, known) take part (the library stream waited for them)
+  auto poll = [&](int need) -> int {
+    while (known < ngroups) {
+      bool take = known < need;
+      if (!take) {
+        cudaError_t q = cudaEventQuery(arr[known]);
+        cudaGetLastError();  // a "not ready" answer is not an error
+        take = q == cudaSuccess;
+      }
+      if (!take) break;
+      PLA_CUDA(cudaStreamWaitEvent(s0, arr[known], 0));
+      known++;
+    }
+    return 0;
+  };
+  // after panel s (on the current stream): the inverse of its unit lower
+  // diagonal block and its packed L
+  auto post_panel = [&](int s) -> int {
+    const int k0 = s * nb, b = std::min(nb, n - k0), rest = n - k0 - b;
+    float *D = dinv + (size_t)s * nb * nb;
+    K(pla_k_fill(MPI_FLOAT, b, b, D, b, 0.0, stream()));
+    K(pla_k_fill(MPI_FLOAT, 1, b, D, b + 1, 1.0, stream()));
+    K(trsm_device(MPI_FLOAT, 'L', 'L', 'N', 'U', b, b, 1.0, (const char *)at(k0, k0), ld,
+                  (char *)D, b));
+    if (rest <= 0) return 0;
+    PhaseTimer t(&ph.convert_ms);
+    if (f8)
+      K(pla_k_pack_fp8(rest, b, at(k0 + b, k0), 1, ld, Lbig + loff[s], nb,
+                       scl + (size_t)s * tiles, stream()));
+    else
+      K(pla_k_pack_rows(kprec, rest, b, at(k0 + b, k0), ld, Lbig + loff[s], nb, stream()));
+    return 0;
+  };
+  // step s on columns [c0, c1): interchanges, U rows, packed U'
+  auto prep = [&](int s, int c0, int c1) -> int {
+    const int k0 = s * nb, b = std::min(nb, n - k0), nc = c1 - c0;
+    if (nc <= 0) return 0;
+    {
+      PhaseTimer t(&ph.swap_ms);
+      K(pla_k_laswp(MPI_FLOAT, at(k0, 0), ld, b, F.piv + k0, 0, 0, c0, c1, stream()));
+    }
+    {
+      PhaseTimer t(&ph.trsm_ms);
+      K(pla_k_copy(MPI_FLOAT, PLA_NO_TRANSPOSE, b, nc, at(k0, c0), ld, tmp, b, stream()));
+      K(pla_k_gemm(MPI_FLOAT, PLA_NO_TRANSPOSE, PLA_NO_TRANSPOSE, b, nc, b, 1.0,
+                   dinv + (size_t)s * nb * nb, b, tmp, b, 0.0, at(k0, c0), ld, 0, &st[0],
+                   stream()));
+    }
+    if (n - k0 - b <= 0) return 0;
+    PhaseTimer t(&ph.convert_ms);
+    if (f8) K(pla_k_pack_fp8(nc, b, at(k0, c0), ld, 1, Ub, nb, inv_u, stream()));
+    else K(pla_k_convert(MPI_FLOAT, at(k0, c0), ld, kprec, Ub, nb, b, nc, stream()));
+    return 0;
+  };
+  // step s's update of columns [c0, c1), whose U' was packed from column p0
+  auto upd = [&](int s, int c0, int c1, int p0, int cap) -> int {
+    const int k0 = s * nb, b = std::min(nb, n - k0), rest = n - k0 - b, nc = c1 - c0;
+    if (nc <= 0 || rest <= 0) return 0;
+    const long off = c0 - p0;  // columns of U' skipped (a multiple of 128)
+    PhaseTimer t(&ph.update_ms);
+    K(f8 ? pla_k_tc_update_fp8_ex(rest, nc, b, -1.0f, Lbig + loff[s], nb, rest,
+                                  scl + (size_t)s * tiles, (char *)Ub + off * nb * esz, nb, nc,
+                                  inv_u + off / 128, F.a, ld, ld, n, k0 + b, c0, 0, cap, &st[0],
+                                  stream())
+         : pla_k_tc_update_ex(kprec, rest, nc, b, -1.0f, Lbig + loff[s], nb, rest,
+                              (char *)Ub + off * nb * esz, nb, nc, F.a, ld, ld, n, k0 + b, c0, 0,
+                              cap, &st[0], stream()));
+    if (t.on) ph.update_launches++;
+    return 0;
+  };
+
+  // 2. the steps
+  PK(poll(1));
+  {
+    PhaseTimer t(&ph.panel_ms);
+    K(panel_lu(MPI_FLOAT, n, std::min(nb, n), (char *)at(0, 0), ld, F.piv, &st[0], &st[2], 0, 0));
+  }
+  PK(post_panel(0));
+  std::vector<int> applied(ngroups, 0);  // steps already applied to each group
+  for (int k = 0; k < nsteps; k++) {
+    const int k0 = k * nb, b = std::min(nb, n - k0), rest = n - k0 - b;
+    if (k > 0) PLA_CUDA(cudaStreamWaitEvent(s0, ev_panel, 0));
+    if (k >= 2) PLA_CUDA(cudaEventSynchronize(thr[(k - 2) % 4]));
+    // groups through the one holding block k+1 must take part now
+    const int need = (int)((std::min<long>(n, (long)(k + 2) * nb) + gcols - 1) / gcols);
+    const int was = known;
+    PK(poll(need));
+    for (int g = was; g < known; g++) {  // replay the steps a new group missed
+      const int g0 = g * gcols, g1 = std::min(n, g0 + gcols);
+      for (int s2 = applied[g]; s2 < k; s2++) {
+        const int c0 = std::max(g0, (s2 + 1) * nb);
+        PK(prep(s2, c0, g1));
+        PK(upd(s2, c0, g1, c0, 0));
+      }
+      applied[g] = k;
+    }
+    const int kc = std::min(n, known * gcols);  // columns that take part
+    if (rest > 0) {
+      PK(prep(k, k0 + b, kc));
+      const int b2 = std::min(nb, rest);
+      if (k + 1 < nsteps) {
+        PK(upd(k, k0 + b, k0 + b + b2, k0 + b, 0));  // the next panel's columns first
+        PLA_CUDA(cudaEventRecord(ev_next, s0));
+        PLA_CUDA(cudaStreamWaitEvent(s1, ev_next, 0));
+        {
+          OnStream on(s1);
+          {
+            PhaseTimer t(&ph.panel_ms);
+            K(panel_lu(MPI_FLOAT, n - k0 - b, b2, (char *)at(k0 + b, k0 + b), ld, F.piv + k0 + b,
+                       &st[0], &st[2], k0 + b, kLookaheadCtasF32));
+          }
+          PK(post_panel(k + 1));
+        }
+        PLA_CUDA(cudaEventRecord(ev_panel, s1));
+        PK(upd(k, k0 + b + b2, kc, k0 + b, side_ctas));
+      }
+    }
+    for (int g = 0; g < known; g++) applied[g] = k + 1;
+    PLA_CUDA(cudaEventRecord(thr[k % 4], s0));
+  }
+  PK(poll(ngroups));  // the refinement reads all of A
+  // 3. the interchanges of every step on the columns to its left
+  for (int k = 1; k < nsteps; k++) {
+    const int k0 = k * nb, b = std::min(nb, n - k0);
+    PhaseTimer t(&ph.swap_ms);
+    K(pla_k_laswp(MPI_FLOAT, at(k0, 0), ld, b, F.piv + k0, 0, k0, 0, 0, stream()));
+  }
+  PLA_CUDA(cudaStreamSynchronize(s0));
+  return PLA_SUCCESS;
+}
+
 // the next precision up when the refinement stagnates (0: none left)
 int escalated(int prec) {
   switch (prec) {
@@ -410,8 +618,10 @@ int escalated(int prec) {
   }
 }
 
+// Ah: when not null, A's values are in host memory (column-major, ldh) and are
+// copied into the device object A during the call
 int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
-                PLA_Mixed_report *rep) {
+                PLA_Mixed_report *rep, const double *Ah = nullptr, long ldh = 0) {
   if (!valid(A) || !valid(B)) PLA_FAIL("invalid object");
   if (!is_double(A) || !is_double(B)) PLA_FAIL("the mixed-precision solvers take FP64 objects");
   if (A->length != A->width || B->length != A->length) PLA_FAIL("nonconformal objects");
@@ -454,14 +664,29 @@ int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
   if (!t32b || !work || (p.refinement == PLA_B200_IR_GMRES && !V))
     PLA_FAIL("cannot allocate the refinement workspace");
 
-  // norms of A and b, and a copy of b (B receives x at the end)
-  Norms nm;
-  K(pla_k_residual(n, n, 1, Ad, lda, nullptr, n, nullptr, n, tmp, n, 1, work, stream()));
-  nm.a_inf = host_max(tmp, n);
-  K(pla_k_col_abs_max(MPI_DOUBLE, n, nrhs, Bd, ldb, tmp, stream()));
-  nm.b_inf.resize(nrhs);
-  PLA_CUDA(d2h(nm.b_inf.data(), tmp, nrhs * sizeof(double)));
+  if (Ah && ldh < n) PLA_FAIL("leading dimension of the host matrix below n");
+  const bool lowp0 = p.precision == PLA_B200_PREC_BF16 || p.precision == PLA_B200_PREC_FP16 ||
+                     p.precision == PLA_B200_PREC_FP8;
+  // the first factorization overlaps the copy of A when it is an LU with
+  // tensor-core updates; otherwise A is copied first
+  bool stream_first = Ah && kind == 0 && lowp0 && n >= 4096;
+  if (Ah && !stream_first)
+    PLA_CUDA(cudaMemcpy2DAsync((void *)Ad, lda * sizeof(double), Ah, ldh * sizeof(double),
+                               (size_t)n * sizeof(double), n, cudaMemcpyHostToDevice, stream()));
+  // a copy of b (B receives x at the end); the norms of A and b once A is there
   K(pla_k_copy(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, nrhs, Bd, ldb, Bsave, n, stream()));
+  Norms nm;
+  bool have_norms = false;
+  auto norms = [&]() -> int {
+    if (have_norms) return 0;
+    K(pla_k_residual(n, n, 1, Ad, lda, nullptr, n, nullptr, n, tmp, n, 1, work, stream()));
+    nm.a_inf = host_max(tmp, n);
+    K(pla_k_col_abs_max(MPI_DOUBLE, n, nrhs, Bsave, n, tmp, stream()));
+    nm.b_inf.resize(nrhs);
+    PLA_CUDA(d2h(nm.b_inf.data(), tmp, nrhs * sizeof(double)));
+    have_norms = true;
+    return 0;
+  };
 
   PLA_Mixed_report r{};
   r.backward_error = std::numeric_limits<double>::infinity();
@@ -499,7 +724,9 @@ int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
           F.dsc = (double *)scratch(kSlotDiag, (size_t)n * sizeof(double) + 256);
           if (!F.dsc) PLA_FAIL("cannot allocate the diagonal scaling");
         }
-        int rc = factor_mixed(F, Ad, lda, nb);
+        int rc = stream_first ? factor_mixed_streamed(F, Ah, ldh, (double *)Ad, lda, nb)
+                              : factor_mixed(F, Ad, lda, nb);
+        stream_first = false;
         if (rc) return rc;
         int hst[3];
         PLA_CUDA(d2h(hst, status, sizeof hst));  // after the factorization's kernels
@@ -518,6 +745,7 @@ int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
     }
 
     // ---- refinement ----
+    K(norms());
     EventTimer t;
     if (prec != PLA_B200_PREC_FP64) {
       int rc0 = prepare_solves(F);
@@ -604,6 +832,12 @@ int PLA_General_solve_mixed(PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *params
 int PLA_Pos_def_solve_mixed(PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *params,
                             PLA_Mixed_report *report) {
   return solve_mixed(1, A, B, params, report);
+}
+
+int PLA_General_solve_mixed_host(PLA_Obj A, const void *A_host, int ldh, PLA_Obj B,
+                                 const PLA_Mixed_params *params, PLA_Mixed_report *report) {
+  if (!A_host) PLA_FAIL("null host matrix");
+  return solve_mixed(0, A, B, params, report, (const double *)A_host, ldh);
 }
 
 }  // extern "C"

@@ -125,6 +125,8 @@ _SIGS = {
     "PLA_Mixed_params_default": [ctypes.POINTER(MixedParams)],
     "PLA_General_solve_mixed": [Obj, Obj, ctypes.POINTER(MixedParams), ctypes.POINTER(MixedReport)],
     "PLA_Pos_def_solve_mixed": [Obj, Obj, ctypes.POINTER(MixedParams), ctypes.POINTER(MixedReport)],
+    "PLA_General_solve_mixed_host": [Obj, _vp, _i, Obj, ctypes.POINTER(MixedParams),
+                                     ctypes.POINTER(MixedReport)],
     "PLA_Batch_plan_create": [_i, _i, ctypes.POINTER(BatchInstance), _vp, _i, _pobj],
     "PLA_Batch_plan_execute": [_vp], "PLA_Batch_plan_free": [_pobj],
     "PLA_Batched_factor_solve": [_i, _i, ctypes.POINTER(BatchInstance), _vp],

@@ -402,3 +402,56 @@ def test_fp8_lu_ir(env):
                                     refinement=2)
     assert rc == 0 and rep.converged == 1, (rep.iterations, rep.backward_error)
     assert backward_error(A, X, B) <= n * 2.0 ** -53
+
+
+@pytest.mark.parametrize("prec,nb", [(2, 256), (5, 128)])
+def test_streamed_solve_from_host(env, prec, nb):
+    """PLA_General_solve_mixed_host copies A from host memory while the
+    factorization runs: FP64 backward error, A copied into the device object,
+    and a bitwise-identical solution whether the copy overlaps (page-locked
+    memory) or not (pageable memory), because each column group replays the
+    steps it missed in order."""
+    s, torch, pla = env
+    n = 8192
+    A = c3_matrix(n, 1e3, 41)
+    Xt = np.random.default_rng(42).standard_normal((n, 1))
+    B = np.asfortranarray(A @ Xt)
+    pinned = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+    pinned.numpy()[:] = A.T          # row-major view of the column-major matrix
+    pageable = np.ascontiguousarray(A.T)
+    sols = []
+    for host in (pinned.data_ptr(), pageable.ctypes.data):
+        a = s.matrix(n, n)
+        b = s.matrix(n, 1)
+        s.set(b, B)
+        p = pla.MixedParams()
+        s.lib.PLA_Mixed_params_default(ctypes.byref(p))
+        p.precision, p.refinement, p.nb = prec, 2, nb
+        rep = pla.MixedReport()
+        rc = s.lib.PLA_General_solve_mixed_host(a, ctypes.c_void_p(host), n, b, ctypes.byref(p),
+                                                ctypes.byref(rep))
+        assert rc == 0 and rep.converged == 1, (rep.iterations, rep.backward_error)
+        assert np.array_equal(s.get(a), A)
+        X = s.get(b)
+        assert backward_error(A, X, B) <= n * 2.0 ** -53
+        sols.append(X)
+        s.free(a, b)
+    assert np.array_equal(sols[0], sols[1])
+
+
+def test_streamed_solve_small_order_copies_first(env):
+    s, torch, pla = env
+    n = 1000
+    A = c3_matrix(n, 1e2, 43)
+    B = np.asfortranarray(A @ np.ones((n, 2)))
+    host = np.ascontiguousarray(A.T)
+    a, b = s.matrix(n, n), s.matrix(n, 2)
+    s.set(b, B)
+    p = pla.MixedParams()
+    s.lib.PLA_Mixed_params_default(ctypes.byref(p))
+    rep = pla.MixedReport()
+    rc = s.lib.PLA_General_solve_mixed_host(a, ctypes.c_void_p(host.ctypes.data), n, b,
+                                            ctypes.byref(p), ctypes.byref(rep))
+    assert rc == 0 and rep.converged == 1
+    assert backward_error(A, s.get(b), B) <= n * 2.0 ** -53
+    s.free(a, b)
