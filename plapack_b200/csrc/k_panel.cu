@@ -78,49 +78,68 @@ __device__ __forceinline__ void put(unsigned long long *p, T v, unsigned tag) {
 #pragma unroll
   for (int h = 0; h < (int)(sizeof(T) / 4); h++) st_relaxed64(p + h, word(tag, half_bits(v, h)));
 }
+
+// Pivot candidates compare as unsigned integer keys: key(x) = bits(|x|) + 1,
+// and 0 for NaN (and for "no candidate").  For |x| >= 0 the bit pattern
+// orders like the value, so (larger key, then smaller row) picks the pivot of
+// (larger |x|, then smaller row) -- the first index of the maximum, as
+// idamax and BLAS1/PLA_Iamax.c:108-111 -- and a NaN never wins.  Integer
+// comparisons keep the reductions below exact total orders: with
+// floating-point comparisons a NaN that slipped into a reduction compares
+// false both ways and lanes could end with different winners.
 template <typename T>
-__device__ __forceinline__ T join(const unsigned *bits) {
-  if constexpr (sizeof(T) == 8)
-    return __longlong_as_double((long long)(((unsigned long long)bits[1] << 32) | bits[0]));
-  else
-    return __uint_as_float(bits[0]);
+struct KeyOf {
+  using K = unsigned;
+};
+template <>
+struct KeyOf<double> {
+  using K = unsigned long long;
+};
+template <typename T>
+__device__ __forceinline__ typename KeyOf<T>::K pivot_key(T x) {
+  if constexpr (sizeof(T) == 8) {
+    const unsigned long long b =
+        (unsigned long long)__double_as_longlong(x) & 0x7fffffffffffffffull;
+    return b > 0x7ff0000000000000ull ? 0ull : b + 1ull;
+  } else {
+    const unsigned b = __float_as_uint(x) & 0x7fffffffu;
+    return b > 0x7f800000u ? 0u : b + 1u;
+  }
+}
+template <typename K>
+__device__ __forceinline__ bool key_better(K a, int ai, K b, int bi) {
+  return a > b || (a == b && ai < bi);
 }
 
-// (abs, idx) ordering: larger |value| first, then smaller index
-template <typename T>
-__device__ __forceinline__ bool better(T av, int ai, T bv, int bi) {
-  return av > bv || (av == bv && ai < bi);
-}
-
-template <typename T>
-__device__ void block_argmax(T &v, int &i, T *sv, int *si) {
+// CTA argmax with one barrier: every lane of every warp ends with the same
+// (key, index); the lanes past the warp count hold the empty candidate.
+template <typename K>
+__device__ __forceinline__ void block_argmax(K &v, int &i, K *sv, int *si) {
+  const int l = threadIdx.x & 31;
+#pragma unroll
   for (int o = 16; o; o >>= 1) {
-    T ov = __shfl_down_sync(0xffffffffu, v, o);
-    int oi = __shfl_down_sync(0xffffffffu, i, o);
-    if (better(ov, oi, v, i)) { v = ov; i = oi; }
+    const K ov = __shfl_xor_sync(0xffffffffu, v, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+    if (key_better(ov, oi, v, i)) { v = ov; i = oi; }
   }
-  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  __syncthreads();
-  if (l == 0) { sv[w] = v; si[w] = i; }
-  __syncthreads();
-  if (w == 0) {
-    v = l < (kThreads / 32) ? sv[l] : T(-1);
-    i = l < (kThreads / 32) ? si[l] : INT_MAX;
-    for (int o = 16; o; o >>= 1) {
-      T ov = __shfl_down_sync(0xffffffffu, v, o);
-      int oi = __shfl_down_sync(0xffffffffu, i, o);
-      if (better(ov, oi, v, i)) { v = ov; i = oi; }
-    }
-    if (l == 0) { sv[0] = v; si[0] = i; }
+  if (l == 0) {
+    sv[threadIdx.x >> 5] = v;
+    si[threadIdx.x >> 5] = i;
   }
   __syncthreads();
-  v = sv[0];
-  i = si[0];
+  v = l < kThreads / 32 ? sv[l] : K(0);
+  i = l < kThreads / 32 ? si[l] : INT_MAX;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    const K ov = __shfl_xor_sync(0xffffffffu, v, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+    if (key_better(ov, oi, v, i)) { v = ov; i = oi; }
+  }
 }
 
 // Workspace, in tagged words (NW = sizeof(T) / 4 words per element), two
 // slots by column parity:
-//   rec  [2][P][NW + 1]  |value| of each CTA's candidate, then its row index
+//   rec  [2][P][NW + 1]  pivot key of each CTA's candidate, then its row index
 //   crow [2][P][w][NW]   each candidate's row
 //   trow [2][w][NW]      the diagonal row, published by its owner
 template <typename T>
@@ -130,7 +149,8 @@ panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *sta
            unsigned long long *crow, unsigned long long *trow) {
   constexpr int NW = (int)(sizeof(T) / 4), NR = NW + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ T s_v[32];
+  using K = typename KeyOf<T>::K;
+  __shared__ K s_v[32];
   __shared__ int s_i[32];
   __shared__ int s_p, s_q;
 
@@ -164,12 +184,12 @@ panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *sta
   auto publish = [&](int col, bool pend) {
     const int par = col & 1;
     const unsigned tag = tag0 | (unsigned)col;
-    T best = T(-1);
+    K best = 0;
     int bidx = INT_MAX;
     const int lo = max(col - row0, 0);
     for (int li = lo + tid; li < nrows; li += kThreads) {
-      T v = fabs(E(li, col));
-      if (better(v, row0 + li, best, bidx)) { best = v; bidx = row0 + li; }
+      const K v = pivot_key(E(li, col));
+      if (v != 0 && key_better(v, row0 + li, best, bidx)) { best = v; bidx = row0 + li; }
     }
     block_argmax(best, bidx, s_v, s_i);
     auto row_val = [&](int li, int c) -> T {
@@ -185,7 +205,9 @@ panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *sta
     if (tid == 0) {
       unsigned long long *rp = rec + ((long)par * P + b) * NR;
       const bool none = bidx == INT_MAX;  // no candidate: every entry is NaN
-      put<T>(rp, none ? T(0) : best, tag);
+      const K kv = none ? K(0) : best;
+#pragma unroll
+      for (int h = 0; h < NW; h++) st_relaxed64(rp + h, word(tag, (unsigned)(kv >> (32 * h))));
       st_relaxed64(rp + NW, word(tag, (unsigned)(none ? INT_MAX : bidx)));
     }
     __syncthreads();  // the rows above are read before the update below writes them
@@ -231,24 +253,22 @@ panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *sta
           break;
         }
       }
-      T bv = T(-1);
+      K bv = 0;
       int bi = INT_MAX, bq = 0;
 #pragma unroll
       for (int i = 0; i < kPerLane; i++) {
         const int q = tid + 32 * i;
         if (q >= P) continue;
-        unsigned bits[NW];
-#pragma unroll
-        for (int h = 0; h < NW; h++) bits[h] = (unsigned)wv[i][h];
-        const T v = join<T>(bits);
+        K v = (K)(unsigned)wv[i][0];
+        if constexpr (NW == 2) v |= (K)(unsigned)wv[i][1] << 32;
         const int ix = (int)(unsigned)wv[i][NW];
-        if (better(v, ix, bv, bi)) { bv = v; bi = ix; bq = q; }
+        if (v != 0 && key_better(v, ix, bv, bi)) { bv = v; bi = ix; bq = q; }
       }
       for (int o = 16; o; o >>= 1) {
-        T ov = __shfl_down_sync(0xffffffffu, bv, o);
+        K ov = __shfl_down_sync(0xffffffffu, bv, o);
         int oi = __shfl_down_sync(0xffffffffu, bi, o);
         int oq = __shfl_down_sync(0xffffffffu, bq, o);
-        if (better(ov, oi, bv, bi)) { bv = ov; bi = oi; bq = oq; }
+        if (key_better(ov, oi, bv, bi)) { bv = ov; bi = oi; bq = oq; }
       }
       if (tid == 0) {
         s_p = bi;

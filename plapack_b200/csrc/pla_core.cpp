@@ -40,6 +40,20 @@ cudaStream_t stream() {
   return s.own_stream;
 }
 
+int lookahead_ctas(int dt) {
+  static const int f32 = [] {
+    const char *e = std::getenv("PLA_B200_LOOKAHEAD_CTAS_F32");
+    const int v = e ? std::atoi(e) : 0;
+    return v > 0 ? v : kLookaheadCtasF32Default;
+  }();
+  static const int f64 = [] {
+    const char *e = std::getenv("PLA_B200_LOOKAHEAD_CTAS_F64");
+    const int v = e ? std::atoi(e) : 0;
+    return v > 0 ? v : kLookaheadCtasF64Default;
+  }();
+  return dt == MPI_DOUBLE ? f64 : f32;
+}
+
 cudaStream_t lookahead_stream() {
   State &s = state();
   if (!s.la_stream) {

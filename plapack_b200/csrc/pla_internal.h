@@ -87,12 +87,13 @@ cudaStream_t stream();
 // 32: 0.358 / 1.148 s, 48: 0.331 / 1.143 s, 72: 0.310 / 1.159 s,
 // 100: 0.316 / 1.177 s.  The fp32 panel of the mixed LU runs beside a short
 // HBM-bound update and wants more CTAs; the FP64 panel beside the long DGEMM
-// fewer.
-#ifndef PLA_LOOKAHEAD_CTAS_F64
-#define PLA_LOOKAHEAD_CTAS_F64 48
-#endif
-constexpr int kLookaheadCtasF32 = 72;
-constexpr int kLookaheadCtasF64 = PLA_LOOKAHEAD_CTAS_F64;
+// fewer.  With the faster DGEMM the FP64 solve measured 32: 0.843, 48: 0.824,
+// 64: 0.829, 96: 0.830 s.
+// The environment variables PLA_B200_LOOKAHEAD_CTAS_F32 / _F64 (read once)
+// override the defaults, for tuning on other parts.
+constexpr int kLookaheadCtasF32Default = 72;
+constexpr int kLookaheadCtasF64Default = 48;
+int lookahead_ctas(int dt);
 cudaStream_t lookahead_stream();
 cudaEvent_t lookahead_event(int i);
 cudaStream_t copy_stream();

@@ -136,7 +136,7 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
   int *st = F.status;
   PLA_Phase_times &ph = state().phases;
   // LU lookahead, as in the FP64 loop: panel k+1 on the lookahead stream
-  // beside the rest of update k, which then keeps kLookaheadCtasF32 SMs free
+  // beside the rest of update k, which then keeps lookahead_ctas(MPI_FLOAT) SMs free
   const bool la = F.kind == 0 && n >= 4 * nb;
   cudaStream_t s0 = stream(), s1 = la ? lookahead_stream() : s0;
   cudaEvent_t ev_next = la ? lookahead_event(0) : nullptr, ev_panel = la ? lookahead_event(1) : nullptr;
@@ -146,7 +146,7 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   }
-  const int side_ctas = std::max(1, sms - kLookaheadCtasF32);
+  const int side_ctas = std::max(1, sms - lookahead_ctas(MPI_FLOAT));
   const int esz = f8 ? 1 : 2;  // bytes per packed element
   int ready = -1;
   for (int k = 0; k < n; k += nb) {
@@ -222,7 +222,7 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
           OnStream on(s1);
           PhaseTimer t(&ph.panel_ms);
           K(panel_lu(MPI_FLOAT, n - k2, b2, (char *)at(k2, k2), ld, F.piv + k2, &st[0], &st[2],
-                     k2, kLookaheadCtasF32));
+                     k2, lookahead_ctas(MPI_FLOAT)));
         }
         PLA_CUDA(cudaEventRecord(ev_panel, s1));
         ready = k2;
@@ -454,7 +454,7 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   }
-  const int side_ctas = std::max(1, sms - kLookaheadCtasF32);
+  const int side_ctas = std::max(1, sms - lookahead_ctas(MPI_FLOAT));
   std::vector<cudaEvent_t> arr(ngroups), thr(4);
   for (auto &e : arr) PLA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   for (auto &e : thr) PLA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -585,7 +585,7 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
           {
             PhaseTimer t(&ph.panel_ms);
             K(panel_lu(MPI_FLOAT, n - k0 - b, b2, (char *)at(k0 + b, k0 + b), ld, F.piv + k0 + b,
-                       &st[0], &st[2], k0 + b, kLookaheadCtasF32));
+                       &st[0], &st[2], k0 + b, lookahead_ctas(MPI_FLOAT)));
           }
           PK(post_panel(k + 1));
         }

@@ -186,7 +186,7 @@ namespace {
 // Blocked right-looking LU (SOLVERS/LU/PLA_LU.c:103-192) on device memory,
 // with a lookahead of one panel.  After the TRSM of step k the columns of
 // panel k+1 are updated first; panel k+1 is then factored on the
-// high-priority lookahead stream, on at most kLookaheadCtasF64 (F32) CTAs, while the
+// high-priority lookahead stream, on at most lookahead_ctas(dt) CTAs, while the
 // rest of the trailing update of step k runs on the library stream.  The two
 // touch disjoint columns, and step k+1 starts (row interchanges across the
 // full width) only after both.  Every operation and its operands are those
@@ -236,7 +236,7 @@ int lu_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, Status 
         OnStream on(s1);
         PhaseTimer t(&ph.panel_ms);
         K(panel_lu(dt, m - k2, b2, at(k2, k2), lda, piv + k2, &st->status, &st->zero_info, k2,
-                   dt == MPI_DOUBLE ? kLookaheadCtasF64 : kLookaheadCtasF32));
+                   lookahead_ctas(dt)));
       }
       PLA_CUDA(cudaEventRecord(ev_panel, s1));
       ready = k2;

@@ -115,16 +115,17 @@ def case_panel(torch, lib, a):
     A = A0.clone()
     piv = torch.zeros(w, dtype=torch.int32, device="cuda")
     st = torch.zeros(4, dtype=torch.int32, device="cuda")
-    g = _fn(lib, "pla_k_lu_panel", [i32, i32, i32, vp, lg, vp, vp, vp, i32, vp])
+    g = _fn(lib, "pla_k_lu_panel_ex", [i32, i32, i32, vp, lg, vp, vp, vp, i32, i32, vp])
 
     def launch():
         A.copy_(A0)
-        return g(dt, r, w, A.data_ptr(), r, piv.data_ptr(), st.data_ptr(), None, 0, None)
+        return g(dt, r, w, A.data_ptr(), r, piv.data_ptr(), st.data_ptr(), None, 0, a.ctas, None)
 
     t = _time(torch, launch, a.warmup, a.reps)
     assert st[0].item() == 0
     es = 8 if dt == pla.MPI_DOUBLE else 4
-    return {"case": f"panel LU {r} x {w} ({a.dtype}), copy of the panel included", "s": t,
+    return {"case": f"panel LU {r} x {w} ({a.dtype}), at most {a.ctas or 'one per SM'} CTAs, "
+                    f"copy of the panel included", "s": t,
             "us_per_column": t / w * 1e6, "bytes_read_written": 2.0 * r * w * es,
             "gbs": 2.0 * r * w * es / t / 1e9}
 
@@ -218,6 +219,7 @@ def main(argv=None):
     p.add_argument("--dtype", choices=["f32", "f64"], default="f32")
     p.add_argument("--warmup", type=int, default=2)
     p.add_argument("--reps", type=int, default=3)
+    p.add_argument("--ctas", type=int, default=0, help="panel: CTA cap (0: one per SM)")
     a = p.parse_args(argv)
     import torch
     torch.cuda.set_device(0)
