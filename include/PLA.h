@@ -20,6 +20,8 @@
 #ifndef PLA_B200_PLA_H
 #define PLA_B200_PLA_H
 
+#include <stddef.h> /* size_t */
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -240,8 +242,21 @@ int PLA_API_axpy_global_to_matrix(int m, int n, void *alpha, PLA_Obj obj,
                                   int disp_row, int disp_col, void *local_matrix,
                                   int local_ldim);            /* :593 */
 
+/* ---- host memory (OBJ/PLA_Memory.c; INCLUDE/PLA_Memory_prototypes.h) ------ */
+/* as the reference: malloc / calloc with running totals of the bytes held.
+ * Where the reference prints and exits on failure these return NULL and set
+ * PLA_Last_error.  PLA_free returns NULL. */
+void *PLA_malloc(size_t size);                       /* OBJ/PLA_Memory.c:18 */
+void *PLA_calloc(size_t size, size_t typesize);      /* OBJ/PLA_Memory.c:51 */
+void *PLA_free(void *buffer);                        /* OBJ/PLA_Memory.c:68 */
+int PLA_Total_size_malloced(void);                   /* OBJ/PLA_Memory.c:87 */
+int PLA_Max_size_malloced(void);                     /* OBJ/PLA_Memory.c:100 */
+
 /* ---- solvers and parallel BLAS on the dense-solve path ------------------------ */
 int PLA_LU(PLA_Obj A, PLA_Obj pivots);               /* SOLVERS/LU/PLA_LU.c:13 */
+/* the blocked LU whose interchanges skip the columns left of each panel */
+int PLA_LU_linpack(PLA_Obj A, PLA_Obj pivots);       /* SOLVERS/LINPACK/PLA_LU_linpack.c:13 */
+int PLA_LU_linpack_right(int nb_alg, PLA_Obj A, PLA_Obj pivots); /* :30 */
 int PLA_Apply_pivots_to_rows(PLA_Obj A, PLA_Obj pivots); /* PLA_Apply_pivots_new.c:13 */
 int PLA_Apply_pivots_to_columns_in_reverse(PLA_Obj A, PLA_Obj pivots); /* :309 */
 int PLA_General_solve(PLA_Obj A, PLA_Obj pivots, PLA_Obj B); /* PLA_General.c:67 */
@@ -255,6 +270,9 @@ int PLA_Gemm(int transa, int transb, PLA_Obj alpha, PLA_Obj A, PLA_Obj B,
 int PLA_Gemv(int trans, PLA_Obj alpha, PLA_Obj A, PLA_Obj x, PLA_Obj beta,
              PLA_Obj y);                             /* BLAS2/PLA_Gemv.c */
 int PLA_Iamax(PLA_Obj x, PLA_Obj k, PLA_Obj xmax);   /* BLAS1/PLA_Iamax.c:37 */
+int PLA_Axpy(PLA_Obj alpha, PLA_Obj x, PLA_Obj y);   /* BLAS1/PLA_Axpy.c:13 */
+int PLA_Nrm2(PLA_Obj x, PLA_Obj alpha);              /* BLAS1/PLA_Nrm2.c:13 */
+int PLA_Shift(PLA_Obj obj, MPI_Datatype datatype, void *value); /* UTIL/PLA_Shift.c:15 */
 int PLA_Syrk_perform_local_part(int uplo, PLA_Obj alpha, PLA_Obj X,
                                 PLA_Obj X_trans, PLA_Obj beta,
                                 PLA_Obj A);  /* BLAS3/PLA_Syrk_perform_local_part.c:13 */
@@ -268,6 +286,8 @@ int PLA_Local_syrk(int uplo, int trans, PLA_Obj alpha, PLA_Obj A, PLA_Obj beta,
                    PLA_Obj C);                       /* PLA_Local_syrk.c:13 */
 int PLA_Local_iamax(PLA_Obj x, int *index, void *value); /* PLA_Local_iamax.c:17 */
 int PLA_Local_scal(PLA_Obj alpha, PLA_Obj x);        /* PLA_Local_BLAS1.c:68 */
+int PLA_Local_axpy(PLA_Obj alpha, PLA_Obj x, PLA_Obj y); /* PLA_Local_BLAS1.c:327 */
+int PLA_Local_nrm2(PLA_Obj x, PLA_Obj alpha);        /* PLA_Local_BLAS1.c:394 */
 int PLA_Local_inv_scal(PLA_Obj alpha, PLA_Obj x);    /* PLA_Local_BLAS1.c:173 */
 int PLA_Local_swap(PLA_Obj x, PLA_Obj y);            /* PLA_Local_BLAS1.c:562 */
 int PLA_Local_copy(PLA_Obj from, PLA_Obj to);        /* PLA_Local_BLAS1.c:17 */

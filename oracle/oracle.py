@@ -85,6 +85,14 @@ class Restated:
         getattr(self.lib, f"oracle_{self._dt(A)}lu_blocked")(m, n, nb, _ptr(A), m, _ptr(piv))
         return A, piv
 
+    def lu_linpack(self, A: np.ndarray, nb: int):
+        """Blocked LU whose pivots skip the factored L columns (PLA_LU_linpack.c:145)."""
+        A = np.asfortranarray(A.copy())
+        m, n = A.shape
+        piv = np.zeros(min(m, n), dtype=np.int32)
+        getattr(self.lib, f"oracle_{self._dt(A)}lu_linpack")(m, n, nb, _ptr(A), m, _ptr(piv))
+        return A, piv
+
     def chol_blocked(self, A: np.ndarray, nb: int):
         A = np.asfortranarray(A.copy())
         n = A.shape[0]
@@ -162,6 +170,15 @@ class Reference:
         piv = np.zeros(min(m, n), dtype=np.int32)
         t = ctypes.c_double()
         r = self.lib.ref_lu(m, n, self._code(A), _ptr(A), m, _ptr(piv), ctypes.byref(t))
+        return A, piv, r, t.value
+
+    def lu_linpack(self, A: np.ndarray):
+        A = np.asfortranarray(A.copy())
+        m, n = A.shape
+        piv = np.zeros(min(m, n), dtype=np.int32)
+        t = ctypes.c_double()
+        r = self.lib.ref_lu_linpack(m, n, self._code(A), _ptr(A), m, _ptr(piv),
+                                    ctypes.byref(t))
         return A, piv, r, t.value
 
     def chol(self, A: np.ndarray):

@@ -91,8 +91,12 @@ void oracle_fill_drand48(long seed, long count, double *out) {
    *  - the panel's pivots applied to the remaining columns of A_B (the        \
    *    already-factored L columns and the trailing columns, :152)             \
    *  - A12 <- inv(L11) A12 (unit lower, :174-178)                             \
-   *  - A22 <- A22 - A21 A12 (:185-186). */                                    \
-  void oracle_##P##lu_blocked(int m, int n, int nb, T *A, int lda, int *piv) { \
+   *  - A22 <- A22 - A21 A12 (:185-186).                                      \
+   * With left == 0 the pivots skip the already-factored L columns: the       \
+   * LINPACK-style variant, SOLVERS/LINPACK/PLA_LU_linpack.c:145 (pivots      \
+   * applied to A_BR only). */                                                 \
+  static void P##lu_blocked_ex(int m, int n, int nb, T *A, int lda, int *piv,   \
+                               int left) {                                      \
     int k, kmax = m < n ? m : n;                                               \
     for (k = 0; k < kmax; k += nb) {                                           \
       int b = kmax - k < nb ? kmax - k : nb;                                   \
@@ -122,7 +126,8 @@ void oracle_fill_drand48(long seed, long count, double *out) {
         }                                                                      \
       }                                                                        \
       /* pivots to the columns left and right of the panel */                  \
-      oracle_##P##apply_pivots(b, &piv[k], &A[IDX(k, 0, lda)], lda, 0, k);     \
+      if (left)                                                                \
+        oracle_##P##apply_pivots(b, &piv[k], &A[IDX(k, 0, lda)], lda, 0, k);   \
       oracle_##P##apply_pivots(b, &piv[k], &A[IDX(k, 0, lda)], lda, k + b, n); \
       /* A12 <- inv(L11) A12, column by column */                              \
       for (c = k + b; c < n; c++)                                              \
@@ -140,6 +145,12 @@ void oracle_fill_drand48(long seed, long count, double *out) {
             A[IDX(i, c, lda)] += t * A[IDX(i, k + l, lda)];                    \
         }                                                                      \
     }                                                                          \
+  }                                                                            \
+  void oracle_##P##lu_blocked(int m, int n, int nb, T *A, int lda, int *piv) { \
+    P##lu_blocked_ex(m, n, nb, A, lda, piv, 1);                                \
+  }                                                                            \
+  void oracle_##P##lu_linpack(int m, int n, int nb, T *A, int lda, int *piv) { \
+    P##lu_blocked_ex(m, n, nb, A, lda, piv, 0);                                \
   }                                                                            \
                                                                                \
   /* Unblocked lower Cholesky, left-looking column form of PLA_dchol           \

@@ -8,6 +8,8 @@
  *   ref_lu            TEST/test_lu.c:118-139 (PLA_Matrix_create, PLA_Mvector of
  *                     MPI_INT pivots, fill through the local buffer as
  *                     TEST/create_problem.c:38-51 does, PLA_LU)
+ *   ref_lu_linpack    the same with PLA_LU_linpack (SOLVERS/LINPACK/driver.c's
+ *                     augmented-matrix solve factors with the blocked LU)
  *   ref_chol          TEST/test_chol.c:113-135 (PLA_Chol(PLA_LOWER_TRIANGULAR))
  *   ref_general_solve SOLVERS/LU/PLA_General.c:67-119
  *   ref_pos_def_solve SOLVERS/Cholesky/PLA_Pos_def.c:44-99
@@ -20,6 +22,7 @@
 #include <string.h>
 
 int PLA_LU(PLA_Obj, PLA_Obj);
+int PLA_LU_linpack(PLA_Obj, PLA_Obj);
 int PLA_Chol(int, PLA_Obj);
 int PLA_General_solve(PLA_Obj, PLA_Obj, PLA_Obj);
 int PLA_Pos_def_solve(PLA_Obj, PLA_Obj);
@@ -28,6 +31,12 @@ int PLA_Trsm(int, int, int, int, PLA_Obj, PLA_Obj, PLA_Obj);
 int PLA_Gemm(int, int, PLA_Obj, PLA_Obj, PLA_Obj, PLA_Obj, PLA_Obj);
 int PLA_Apply_pivots_to_rows(PLA_Obj, PLA_Obj);
 int pla_Environ_set_nb_alg(int, int);
+int PLA_Set_error_checking(int, int, int, int);
+int PLA_Comm_1D_to_2D(MPI_Comm, int, int, MPI_Comm *);
+int PLA_Init(MPI_Comm);
+int PLA_Finalize(void);
+int PLA_Temp_create(int, int, PLA_Template *);
+int PLA_Temp_free(PLA_Template *);
 
 static PLA_Template templ = NULL;
 static int ready = 0;
@@ -81,8 +90,10 @@ static void get(PLA_Obj A, int m, int n, void *dst, int ld, int code) {
            (size_t)m * e);
 }
 
-/* PLA_LU on an m x n matrix; pivots (length min(m,n)) are PLAPACK's offsets */
-int ref_lu(int m, int n, int code, void *A, int lda, int *piv, double *seconds) {
+/* PLA_LU (linpack == 0) or PLA_LU_linpack (SOLVERS/LINPACK/PLA_LU_linpack.c:13)
+ * on an m x n matrix; pivots (length min(m,n)) are PLAPACK's offsets */
+static int lu_either(int linpack, int m, int n, int code, void *A, int lda, int *piv,
+                     double *seconds) {
   PLA_Obj a = NULL, p = NULL;
   int r, k = m < n ? m : n, *pb;
   double t;
@@ -90,7 +101,7 @@ int ref_lu(int m, int n, int code, void *A, int lda, int *piv, double *seconds) 
   PLA_Mvector_create(MPI_INT, k, 1, templ, PLA_ALIGN_FIRST, &p);
   put(a, m, n, A, lda, code);
   t = MPI_Wtime();
-  r = PLA_LU(a, p);
+  r = linpack ? PLA_LU_linpack(a, p) : PLA_LU(a, p);
   t = MPI_Wtime() - t;
   if (seconds) *seconds = t;
   get(a, m, n, A, lda, code);
@@ -99,6 +110,12 @@ int ref_lu(int m, int n, int code, void *A, int lda, int *piv, double *seconds) 
   PLA_Obj_free(&a);
   PLA_Obj_free(&p);
   return r;
+}
+int ref_lu(int m, int n, int code, void *A, int lda, int *piv, double *seconds) {
+  return lu_either(0, m, n, code, A, lda, piv, seconds);
+}
+int ref_lu_linpack(int m, int n, int code, void *A, int lda, int *piv, double *seconds) {
+  return lu_either(1, m, n, code, A, lda, piv, seconds);
 }
 
 int ref_chol(int n, int code, void *A, int lda, double *seconds) {

@@ -216,6 +216,58 @@ __global__ void col_abs_max_k(int m, int n, const T *X, long ldx, double *out) {
   }
 }
 
+// Euclidean norm of the n elements x[0], x[inc], ... as dnrm2 / snrm2 (called
+// from Local_BLAS/PLA_Local_BLAS1.c:394-441): the largest |x_i| scales the
+// sum of squares, so that neither overflows nor underflows.  One CTA, FP64
+// arithmetic and a fixed reduction order make the result deterministic; a NaN
+// anywhere gives NaN, an infinity (and no NaN) gives infinity.
+template <typename T>
+__global__ void __launch_bounds__(1024) nrm2_k(long n, const T *x, long inc, double *out) {
+  __shared__ double sm[32];
+  __shared__ int s_nan;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  if (tid == 0) s_nan = 0;
+  double mx = 0;
+  bool nan = false;
+  for (long i = tid; i < n; i += blockDim.x) {
+    const double a = fabs((double)x[i * inc]);
+    nan |= a != a;
+    mx = fmax(mx, a);
+  }
+  for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  __syncthreads();
+  if (nan) s_nan = 1;
+  if (lane == 0) sm[warp] = mx;
+  __syncthreads();
+  mx = lane < nw ? sm[lane] : 0.0;
+  for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if (s_nan || mx == 0.0 || isinf(mx)) {
+    if (tid == 0) out[0] = s_nan ? __longlong_as_double(0x7ff8000000000000ll) : mx;
+    return;
+  }
+  double ssq = 0;
+  for (long i = tid; i < n; i += blockDim.x) {
+    const double t = (double)x[i * inc] / mx;
+    ssq = fma(t, t, ssq);
+  }
+  for (int o = 16; o; o >>= 1) ssq += __shfl_down_sync(0xffffffffu, ssq, o);
+  __syncthreads();
+  if (lane == 0) sm[warp] = ssq;
+  __syncthreads();
+  if (warp == 0) {
+    ssq = lane < nw ? sm[lane] : 0.0;
+    for (int o = 16; o; o >>= 1) ssq += __shfl_down_sync(0xffffffffu, ssq, o);
+    if (lane == 0) out[0] = mx * sqrt(ssq);
+  }
+}
+
+// A(i, i) += v for i < n (UTIL/PLA_Shift.c:33-86)
+template <typename T>
+__global__ void shift_diag_k(int n, T *A, long lda, T v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    A[(long)i + (long)i * lda] += v;
+}
+
 std::atomic<long> g_launches{0};
 
 // every launcher below issues exactly one kernel before calling this
@@ -287,6 +339,22 @@ int pla_k_convert(int ds, const void *src, long lds, int dd, void *dst, long ldd
   else if (ds == MPI_FLOAT && dd == MPI_FLOAT) CV(float, float);
   else return (int)cudaErrorInvalidValue;
 #undef CV
+  return status();
+}
+
+int pla_k_nrm2(int dt, long n, const void *x, long inc, double *out, cudaStream_t s) {
+  if (dt == MPI_DOUBLE) nrm2_k<double><<<1, 1024, 0, s>>>(n, (const double *)x, inc, out);
+  else if (dt == MPI_FLOAT) nrm2_k<float><<<1, 1024, 0, s>>>(n, (const float *)x, inc, out);
+  else return (int)cudaErrorInvalidValue;
+  return status();
+}
+
+int pla_k_shift_diag(int dt, int n, void *A, long lda, double v, cudaStream_t s) {
+  if (n <= 0) return 0;
+  const int g = (n + kThreads - 1) / kThreads;
+  if (dt == MPI_DOUBLE) shift_diag_k<double><<<g, kThreads, 0, s>>>(n, (double *)A, lda, v);
+  else if (dt == MPI_FLOAT) shift_diag_k<float><<<g, kThreads, 0, s>>>(n, (float *)A, lda, (float)v);
+  else return (int)cudaErrorInvalidValue;
   return status();
 }
 

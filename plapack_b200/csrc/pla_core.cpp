@@ -1,6 +1,7 @@
 // Library state, templates, block sizes, diagnostics, objects, views and
 // their inquiry functions: the object layer of the reference (OBJ/, TEMPLATE/,
 // INCLUDE/PLA_Obj.h) on a 1x1 template with device-resident buffers.
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -38,6 +39,27 @@ cudaStream_t stream() {
   if (s.stream) return s.stream;
   if (!s.own_stream) cudaStreamCreateWithFlags(&s.own_stream, cudaStreamNonBlocking);
   return s.own_stream;
+}
+
+// ------------------------------------------------------- host memory ---
+// OBJ/PLA_Memory.c: malloc with running totals of the bytes held.  Each block
+// carries its size in a 16-byte header in front of the pointer returned, so
+// that PLA_free can subtract it.  A failed allocation returns NULL and sets
+// the last error; the reference prints and exits.
+std::atomic<long long> g_host_bytes{0}, g_host_bytes_max{0};
+
+void *host_alloc(size_t size, bool zero) {
+  void *p = zero ? std::calloc(1, size + 16) : std::malloc(size + 16);
+  if (!p) {
+    fail("malloc failed in PLA_malloc", __LINE__, __FILE__);
+    return nullptr;
+  }
+  *(size_t *)p = size;
+  const long long now = g_host_bytes += (long long)size;
+  long long m = g_host_bytes_max.load();
+  while (now > m && !g_host_bytes_max.compare_exchange_weak(m, now)) {
+  }
+  return (char *)p + 16;
 }
 
 int lookahead_ctas(int dt) {
@@ -890,4 +912,25 @@ int PLA_Obj_set_local_contents(int trans, int rows_in_buf, int cols_in_buf, void
   return local_contents(true, o, trans, buf, ldim_buf, stride_buf);
 }
 
+}  // extern "C"
+
+extern "C" {
+void *PLA_malloc(size_t size) { return pla::host_alloc(size, false); }
+void *PLA_calloc(size_t size, size_t typesize) {
+  if (typesize && size > (~(size_t)0 - 16) / typesize) {
+    pla::fail("PLA_calloc: size overflows", __LINE__, __FILE__);
+    return nullptr;
+  }
+  return pla::host_alloc(size * typesize, true);
+}
+void *PLA_free(void *buffer) {
+  if (buffer) {
+    char *p = (char *)buffer - 16;
+    pla::g_host_bytes -= (long long)*(size_t *)p;
+    std::free(p);
+  }
+  return nullptr;
+}
+int PLA_Total_size_malloced(void) { return (int)pla::g_host_bytes.load(); }
+int PLA_Max_size_malloced(void) { return (int)pla::g_host_bytes_max.load(); }
 }  // extern "C"

@@ -78,6 +78,11 @@ int pla_k_potrf_lower(int dt, int b, void *A, long lda, int *status, int *info, 
 
 /* ---- level-1/2 helpers ---- */
 int pla_k_scal(int dt, int m, int n, double alpha, void *X, long ldx, cudaStream_t s);
+/* out[0] (device, FP64) := the two-norm of x[0], x[inc], ..., x[(n-1) inc],
+ * scaled by max |x_i| as dnrm2; deterministic */
+int pla_k_nrm2(int dt, long n, const void *x, long inc, double *out, cudaStream_t s);
+/* A(i, i) += v for i < n */
+int pla_k_shift_diag(int dt, int n, void *A, long lda, double v, cudaStream_t s);
 int pla_k_inv_scal(int dt, int m, int n, double alpha, void *X, long ldx, cudaStream_t s);
 int pla_k_swap(int dt, int m, int n, void *X, long ldx, void *Y, long ldy, cudaStream_t s);
 int pla_k_ger(int dt, int m, int n, double alpha, const void *x, long incx, const void *y,

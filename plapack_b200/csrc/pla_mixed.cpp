@@ -24,7 +24,8 @@
 using namespace pla;
 
 namespace pla {
-int lu_on_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, int *zero_info_host);
+int lu_on_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, int *zero_info_host,
+                 bool left_swaps = true);
 int tri_solve(int dt, char uplo, char trans, char diag, int n, int nrhs, const char *T, long ldt,
               char *X, long ldx);
 int chol_on_device(int dt, int n, char *A, long lda, int nb, int *info_host);

@@ -191,7 +191,12 @@ namespace {
 // touch disjoint columns, and step k+1 starts (row interchanges across the
 // full width) only after both.  Every operation and its operands are those
 // of the loop without lookahead, so the pivots and factors are the same.
-int lu_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, Status *st) {
+// With left_swaps false (PLA_LU_linpack_right, SOLVERS/LINPACK/
+// PLA_LU_linpack.c:108-112) each step's interchanges skip the columns left of
+// its panel: the L of earlier steps keeps its rows where they were, as in
+// LINPACK's dgefa.
+int lu_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, Status *st,
+              bool left_swaps = true) {
   const int es = dt == MPI_DOUBLE ? 8 : 4;
   auto at = [&](long i, long j) { return A + (i + j * lda) * es; };
   const int kmax = std::min(m, n);
@@ -218,7 +223,7 @@ int lu_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, Status 
     }
     {
       PhaseTimer t(&ph.swap_ms);
-      K(pla_k_laswp(dt, at(k, 0), lda, b, piv + k, 0, k, k + b, n, stream()));
+      K(pla_k_laswp(dt, at(k, 0), lda, b, piv + k, 0, left_swaps ? k : 0, k + b, n, stream()));
     }
     if (k + b >= n) continue;
     {
@@ -362,11 +367,12 @@ int chol_async(int dt, int n, char *A, long lda, int nb) {
   PLA_CUDA(cudaMemsetAsync(st, 0, sizeof(Status), stream()));
   return chol_device(dt, n, A, lda, nb, st);
 }
-int lu_on_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, int *zero_info_host) {
+int lu_on_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, int *zero_info_host,
+                 bool left_swaps) {
   Status *st = device_status();
   if (!st) PLA_FAIL("cannot allocate the status word");
   PLA_CUDA(cudaMemsetAsync(st, 0, sizeof(Status), stream()));
-  int r = lu_device(dt, m, n, A, lda, piv, nb, st);
+  int r = lu_device(dt, m, n, A, lda, piv, nb, st, left_swaps);
   if (r) return r;
   Status h{};
   PLA_CUDA(cudaMemcpyAsync(&h, st, sizeof h, cudaMemcpyDeviceToHost, stream()));
@@ -398,7 +404,7 @@ int chol_on_device(int dt, int n, char *A, long lda, int nb, int *info_host) {
 extern "C" {
 
 // ------------------------------------------------------------------- LU ----
-int PLA_LU_info(PLA_Obj A, PLA_Obj pivots, int *info) {
+static int lu_entry(PLA_Obj A, PLA_Obj pivots, int nb, bool left_swaps, int *info) {
   State &s = state();
   if (s.check_parameters) {
     int value = PLA_SUCCESS;
@@ -417,17 +423,29 @@ int PLA_LU_info(PLA_Obj A, PLA_Obj pivots, int *info) {
     if (value != PLA_SUCCESS) return value;
   }
   if (!valid(A) || !numeric(A)) PLA_FAIL("PLA_LU needs a float or double matrix");
-  int nb;
-  PLA_Environ_nb_alg(PLA_OP_PAN_PAN, A->templ, &nb);
+  if (nb <= 0) PLA_Environ_nb_alg(PLA_OP_PAN_PAN, A->templ, &nb);
   int zi = 0;
   int r = lu_on_device(A->base->datatype, A->length, A->width, at(A, 0, 0), ld(A),
-                       (int *)at(pivots, 0, 0), nb, &zi);
+                       (int *)at(pivots, 0, 0), nb, &zi, left_swaps);
   if (r) return r;
   if (info) *info = zi;
   return PLA_SUCCESS;  // the reference never reports singularity (PLA_LU.c:29)
 }
 
-int PLA_LU(PLA_Obj A, PLA_Obj pivots) { return PLA_LU_info(A, pivots, nullptr); }
+int PLA_LU_info(PLA_Obj A, PLA_Obj pivots, int *info) {
+  return lu_entry(A, pivots, 0, true, info);
+}
+
+int PLA_LU(PLA_Obj A, PLA_Obj pivots) { return lu_entry(A, pivots, 0, true, nullptr); }
+
+// SOLVERS/LINPACK/PLA_LU_linpack.c:13-28 and :30-208: the blocked LU whose
+// interchanges leave the columns left of each panel alone
+int PLA_LU_linpack(PLA_Obj A, PLA_Obj pivots) { return lu_entry(A, pivots, 0, false, nullptr); }
+
+int PLA_LU_linpack_right(int nb_alg, PLA_Obj A, PLA_Obj pivots) {
+  if (nb_alg <= 0) PLA_FAIL("PLA_LU_linpack_right: nb_alg must be positive");
+  return lu_entry(A, pivots, nb_alg, false, nullptr);
+}
 
 // SOLVERS/LU/PLA_Apply_pivots_new.c:13-179: the interchanges in sequence
 int PLA_Apply_pivots_to_rows(PLA_Obj A, PLA_Obj ipiv) {
@@ -715,6 +733,73 @@ int PLA_Local_ger(PLA_Obj alpha, PLA_Obj x, PLA_Obj y, PLA_Obj A) {
   K(pla_k_ger(A->base->datatype, A->length, A->width, scalar_value(alpha), at(x, 0, 0), vinc(x),
               at(y, 0, 0), vinc(y), at(A, 0, 0), ld(A), stream()));
   return finish("ger");
+}
+
+// y := alpha x + y (Local_BLAS/PLA_Local_BLAS1.c daxpy on the local parts;
+// BLAS1/PLA_Axpy.c:13 redistributes x first, which a 1x1 template never
+// needs).  x may also be the transpose-shaped view of y's data (a row vector
+// against a column vector).
+static int axpy_objs(PLA_Obj alpha, PLA_Obj x, PLA_Obj y, const char *what) {
+  if (!valid(alpha) || !valid(x) || !valid(y)) PLA_FAIL("invalid object");
+  if (x->base->datatype != y->base->datatype) PLA_FAIL("datatype mismatch");
+  if (!numeric(y)) PLA_FAIL("datatype not yet supported");
+  const int dt = y->base->datatype;
+  const double a = scalar_value(alpha);
+  if (x->length == y->length && x->width == y->width) {
+    K(pla_k_axpby(dt, y->length, y->width, a, at(x, 0, 0), ld(x), 1.0, at(y, 0, 0), ld(y),
+                  stream()));
+  } else if (x->length == y->width && x->width == y->length) {
+    char *t = (char *)scratch(28, (size_t)y->length * y->width * y->base->esize);
+    if (!t) PLA_FAIL("cannot allocate scratch");
+    K(pla_k_copy(dt, PLA_TRANSPOSE, y->length, y->width, at(x, 0, 0), ld(x), t, y->length,
+                 stream()));
+    K(pla_k_axpby(dt, y->length, y->width, a, t, y->length, 1.0, at(y, 0, 0), ld(y), stream()));
+  } else {
+    PLA_FAIL("nonconformal objects");
+  }
+  return finish(what);
+}
+int PLA_Axpy(PLA_Obj alpha, PLA_Obj x, PLA_Obj y) { return axpy_objs(alpha, x, y, "axpy"); }
+int PLA_Local_axpy(PLA_Obj alpha, PLA_Obj x, PLA_Obj y) {
+  return axpy_objs(alpha, x, y, "local axpy");
+}
+
+// alpha := || x ||_2 (BLAS1/PLA_Nrm2.c:13-66, Local_BLAS/PLA_Local_BLAS1.c:
+// 394-441): a one-row x is read along its row, anything else down its first
+// column, as the reference's local call does
+int PLA_Local_nrm2(PLA_Obj x, PLA_Obj alpha) {
+  if (!valid(x) || !valid(alpha)) PLA_FAIL("invalid object");
+  if (!numeric(x)) PLA_FAIL("datatype not yet supported");
+  double v = 0.0;
+  if (x->length * x->width != 0) {
+    const bool row = x->length == 1;
+    const long n = row ? x->width : x->length, inc = row ? ld(x) : 1;
+    double *d = (double *)scratch(1, 64);
+    K(pla_k_nrm2(x->base->datatype, n, at(x, 0, 0), inc, d, stream()));
+    PLA_CUDA(cudaMemcpyAsync(&v, d, sizeof v, cudaMemcpyDeviceToHost, stream()));
+    const int r = finish("nrm2");
+    if (r) return r;
+  }
+  if (x->base->datatype == MPI_FLOAT) {
+    float f = (float)v;
+    return PLA_Obj_set(alpha, MPI_FLOAT, &f);
+  }
+  return PLA_Obj_set(alpha, MPI_DOUBLE, &v);
+}
+int PLA_Nrm2(PLA_Obj x, PLA_Obj alpha) { return PLA_Local_nrm2(x, alpha); }
+
+// add *value (of type datatype) to every diagonal element of obj
+// (UTIL/PLA_Shift.c:15-91)
+int PLA_Shift(PLA_Obj obj, MPI_Datatype datatype, void *value) {
+  if (!valid(obj) || !value) PLA_FAIL("invalid object");
+  if (!numeric(obj)) PLA_FAIL("PLA_Shift: Datatype not yet implemented");
+  double v;
+  if (datatype == MPI_DOUBLE) v = *(const double *)value;
+  else if (datatype == MPI_FLOAT) v = *(const float *)value;
+  else PLA_FAIL("Datatype not yet implemented");
+  K(pla_k_shift_diag(obj->base->datatype, std::min(obj->length, obj->width), at(obj, 0, 0),
+                     ld(obj), v, stream()));
+  return finish("shift");
 }
 
 // ----------------------------------------------------------------- copies ---

@@ -105,6 +105,11 @@ _SIGS = {
     "PLA_API_axpy_vector_to_global": [_i, _vp, _vp, _i, Obj, _i],
     "PLA_API_axpy_global_to_vector": [_i, _vp, Obj, _i, _vp, _i],
     "PLA_LU": [Obj, Obj], "PLA_LU_info": [Obj, Obj, _pi],
+    "PLA_LU_linpack": [Obj, Obj], "PLA_LU_linpack_right": [_i, Obj, Obj],
+    "PLA_Axpy": [Obj, Obj, Obj], "PLA_Nrm2": [Obj, Obj], "PLA_Shift": [Obj, _i, _vp],
+    "PLA_Local_axpy": [Obj, Obj, Obj], "PLA_Local_nrm2": [Obj, Obj],
+    "PLA_malloc": [ctypes.c_size_t], "PLA_calloc": [ctypes.c_size_t, ctypes.c_size_t],
+    "PLA_free": [_vp], "PLA_Total_size_malloced": [], "PLA_Max_size_malloced": [],
     "PLA_Apply_pivots_to_rows": [Obj, Obj], "PLA_General_solve": [Obj, Obj, Obj],
     "PLA_Chol": [_i, Obj], "PLA_Pos_def_solve": [Obj, Obj],
     "PLA_Trsv": [_i, _i, _i, Obj, Obj], "PLA_Trsm": [_i, _i, _i, _i, Obj, Obj, Obj],
@@ -135,7 +140,8 @@ _SIGS = {
     "PLA_Obj_get_local_contents_device": [Obj, _vp, _i],
 }
 _RESTYPE = {"PLA_B200_get_stream": _vp, "PLA_Mixed_params_default": None,
-            "PLA_B200_kernel_launches": ctypes.c_long}
+            "PLA_B200_kernel_launches": ctypes.c_long, "PLA_malloc": _vp, "PLA_calloc": _vp,
+            "PLA_free": _vp}
 
 
 class PLAError(RuntimeError):

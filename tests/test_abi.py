@@ -17,7 +17,8 @@ def declared_functions():
     for h in ("PLA.h", "pla_b200.h"):
         text = open(os.path.join(ROOT, "include", h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-        for m in re.finditer(r"^\s*(?:int|void\s*\*|void)\s+(\w+)\s*\(", text, flags=re.M):
+        for m in re.finditer(r"^\s*(?:int\s+|void\s*\*\s*|void\s+)(\w+)\s*\(", text,
+                             flags=re.M):
             names.add(m.group(1))
     return sorted(names)
 
@@ -49,3 +50,31 @@ def test_binding_loads(built_lib):
     from plapack_b200 import pla
     lib = pla.load()
     assert lib.PLA_LU.restype is ctypes.c_int
+
+
+def test_header_declares_what_the_reference_drivers_call():
+    # the PLA_* calls of TEST/test_lu.c, TEST/test_chol.c, the EXAMPLES drivers
+    # and SOLVERS/LINPACK/driver.c outside the out-of-core family
+    names = set(declared_functions())
+    for need in ["PLA_Axpy", "PLA_Nrm2", "PLA_Shift", "PLA_malloc", "PLA_calloc", "PLA_free",
+                 "PLA_LU_linpack", "PLA_LU_linpack_right", "PLA_Copy", "PLA_Iamax",
+                 "PLA_Obj_get_local_contents", "PLA_Create_constants_conf_to"]:
+        assert need in names, need
+
+
+def test_host_memory_helpers(built_lib):
+    # OBJ/PLA_Memory.c: malloc / calloc with running totals; host memory only
+    from plapack_b200 import pla
+    lib = pla.load()
+    base = lib.PLA_Total_size_malloced()
+    p = lib.PLA_malloc(1000)
+    q = lib.PLA_calloc(250, 8)
+    assert p and q
+    assert lib.PLA_Total_size_malloced() == base + 3000
+    assert lib.PLA_Max_size_malloced() >= base + 3000
+    assert bytes((ctypes.c_char * 2000).from_address(q)) == b"\0" * 2000
+    ctypes.memset(p, 7, 1000)                      # the whole block is usable
+    assert lib.PLA_free(p) is None
+    assert lib.PLA_free(q) is None
+    assert lib.PLA_free(None) is None              # freeing NULL is a no-op
+    assert lib.PLA_Total_size_malloced() == base

@@ -154,3 +154,23 @@ def test_restatement_matches_compiled_reference_fresh_inputs(restated):
         LUo, po = restated.lu_blocked(A, nb)
         assert np.array_equal(pr, po)
         assert np.array_equal(LUr, LUo)
+
+
+@pytest.mark.skipif(not os.path.exists(_REF), reason="compiled reference not built here")
+def test_linpack_restatement_matches_compiled_reference(restated):
+    # SOLVERS/LINPACK/PLA_LU_linpack.c compiled from the reference sources
+    ref = orc.Reference("netlib", nb_distr=64, nb_alg=64)
+    rng = np.random.default_rng(12)
+    for (m, n, nb) in [(77, 78, 8), (200, 120, 24), (90, 140, 16)]:
+        A = np.asfortranarray(rng.standard_normal((m, n)))
+        ref.set_nb_alg(nb)
+        LUr, pr, rc, _ = ref.lu_linpack(A)
+        LUo, po = restated.lu_linpack(A, nb)
+        assert rc == 0
+        assert np.array_equal(pr, po)
+        assert np.array_equal(LUr, LUo)
+        # and it differs from PLA_LU only below the diagonal (L's row order)
+        LUs, ps, _, _ = ref.lu(A)
+        assert np.array_equal(ps, pr)
+        assert np.array_equal(np.triu(LUs), np.triu(LUr))
+    ref.set_nb_alg(64)
