@@ -252,6 +252,26 @@ void *PLA_free(void *buffer);                        /* OBJ/PLA_Memory.c:68 */
 int PLA_Total_size_malloced(void);                   /* OBJ/PLA_Memory.c:87 */
 int PLA_Max_size_malloced(void);                     /* OBJ/PLA_Memory.c:100 */
 
+/* ---- out-of-core matrices (IO/PLA_File.c, OBJ/PLA_Obj_ooc.c) --------------- */
+/* an out-of-core matrix keeps its data in a file (column-major, leading
+ * dimension local_ldim elements); PLA_Copy moves blocks between its views and
+ * in-core objects.  Errors return PLA_ERROR where the reference aborts. */
+int PLA_OOC_Matrix_create_without_fd(MPI_Datatype datatype, int global_length,
+                                     int global_width, PLA_Template templ,
+                                     int global_align_row, int global_align_col,
+                                     PLA_Obj *new_obj);   /* OBJ/PLA_Obj_ooc.c:50 */
+int PLA_Obj_attach_fd(PLA_Obj obj, int fd, int local_ldim,
+                      int user_buffer);       /* OBJ/PLA_Obj_management.c:146 */
+int PLA_File_create(char *filename, MPI_Datatype datatype, int size, int *fd); /* IO/PLA_File.c:25 */
+int PLA_File_open(char *filename, MPI_Datatype datatype, int size, int *fd);   /* :47 */
+int PLA_File_close(int fd);                          /* IO/PLA_File.c:61 */
+int PLA_File_unlink(char *filename);                 /* IO/PLA_File.c:72 */
+int PLA_File_stats_start(void);                      /* IO/PLA_File_stats.c:21 */
+int PLA_File_stats_stop(void);                       /* IO/PLA_File_stats.c:53 */
+/* left-looking tile Cholesky of the lower triangle of an out-of-core matrix;
+ * returns 0 or the global 1-based failing column (the reference discards it) */
+int PLA_OOC_Chol(int nb_ooc, int nb_tile, PLA_Obj A); /* POOCLAPACK/OOC_Cholesky/PLA_OOC_Chol.c:13 */
+
 /* ---- solvers and parallel BLAS on the dense-solve path ------------------------ */
 int PLA_LU(PLA_Obj A, PLA_Obj pivots);               /* SOLVERS/LU/PLA_LU.c:13 */
 /* the blocked LU whose interchanges skip the columns left of each panel */

@@ -171,6 +171,11 @@ int PLA_Batched_factor_solve(MPI_Datatype datatype, int count,
 int PLA_Batched_factor_solve_loop(MPI_Datatype datatype, int count,
                                   const PLA_Batch_instance *instances);
 
+/* The counters of PLA_File_stats_start/stop: bytes and seconds of the file
+ * reads and writes since the last PLA_File_stats_start. */
+int PLA_B200_file_stats(double *read_bytes, double *read_seconds, double *write_bytes,
+                        double *write_seconds);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,6 +1,7 @@
 // Library state, templates, block sizes, diagnostics, objects, views and
 // their inquiry functions: the object layer of the reference (OBJ/, TEMPLATE/,
 // INCLUDE/PLA_Obj.h) on a 1x1 template with device-resident buffers.
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <cstdlib>
@@ -30,7 +31,12 @@ int esize_of(MPI_Datatype dt) {
   }
 }
 
-bool valid(PLA_Obj o) { return o != nullptr && o->magic == kObjMagic && o->base != nullptr; }
+bool valid_any(PLA_Obj o) {
+  return o != nullptr && o->magic == kObjMagic && o->base != nullptr;
+}
+// an object whose data is in device (or pinned host) memory: everything that
+// reads or writes the data refuses out-of-core objects, which have none
+bool valid(PLA_Obj o) { return valid_any(o) && !o->base->ooc; }
 bool valid(PLA_Template t) { return t != nullptr && t->magic == kTempMagic; }
 
 cudaStream_t stream() {
@@ -276,6 +282,30 @@ static pla_base *new_base(MPI_Datatype dt, int length, int width, bool on_host, 
   return b;
 }
 
+// a matrix whose data will live in a file (OBJ/PLA_Obj_ooc.c:50-72): no
+// buffer, no file until PLA_Obj_attach_fd
+static pla_base *new_ooc_base(MPI_Datatype dt, int length, int width, int *err) {
+  *err = PLA_SUCCESS;
+  const int es = esize_of(dt);
+  if (es == 0 || dt == MPI_INT) {
+    *err = fail("unsupported datatype", __LINE__, __FILE__);
+    return nullptr;
+  }
+  if (length < 0 || width < 0) {
+    *err = fail("negative object dimension", __LINE__, __FILE__);
+    return nullptr;
+  }
+  pla_base *b = new pla_base();
+  b->datatype = dt;
+  b->esize = es;
+  b->length = length;
+  b->width = width;
+  b->ldim = length > 0 ? length : 1;
+  b->ooc = 1;
+  b->fd = -1;
+  return b;
+}
+
 static PLA_Obj new_view(pla_base *b, int objtype, PLA_Template templ) {
   PLA_Obj v = new PLA_Obj_view_struct();
   v->magic = kObjMagic;
@@ -350,6 +380,7 @@ int PLA_Finalize(void) {
   if (!s.initialized) PLA_FAIL("PLAPACK not yet initialized");
   cudaStreamSynchronize(stream());
   release_scratch();
+  release_ooc();
   pla_kernels_release();
   for (cudaStream_t *st : {&s.la_stream, &s.copy_stream})
     if (*st) {
@@ -524,6 +555,37 @@ int PLA_B200_reset_phase_times(void) {
 long PLA_B200_kernel_launches(void) { return pla_k_launches(); }
 
 // ---------------------------------------------------------------- creation --
+int PLA_OOC_Matrix_create_without_fd(MPI_Datatype datatype, int global_length,
+                                     int global_width, PLA_Template templ,
+                                     int global_align_row, int global_align_col,
+                                     PLA_Obj *new_obj) {
+  if (!new_obj) PLA_FAIL("null output handle");
+  if (state().check_parameters && !valid(templ)) PLA_FAIL("invalid template");
+  int err;
+  pla_base *b = new_ooc_base(datatype, global_length, global_width, &err);
+  if (!b) return err;
+  PLA_Obj v = new_view(b, PLA_MATRIX, templ);
+  v->align_row = global_align_row;
+  v->align_col = global_align_col;
+  if (*new_obj && valid_any(*new_obj)) drop_view(*new_obj);
+  *new_obj = v;
+  return PLA_SUCCESS;
+}
+
+// OBJ/PLA_Obj_management.c:146-166: the file and its leading dimension (in
+// elements); the reference exits when a file is already attached
+int PLA_Obj_attach_fd(PLA_Obj obj, int fd, int local_ldim, int user_buffer) {
+  if (!valid_any(obj) || !obj->base->ooc) PLA_FAIL("PLA_Obj_attach_fd: not an out-of-core object");
+  if (obj->base->fd != -1) PLA_FAIL("PLA_Obj_attach_fd: object already has file descriptor");
+  if (fd < 0) PLA_FAIL("PLA_Obj_attach_fd: invalid file descriptor");
+  if (local_ldim < std::max(obj->base->length, 1))
+    PLA_FAIL("PLA_Obj_attach_fd: leading dimension smaller than the object's length");
+  obj->base->fd = fd;
+  obj->base->ldim = local_ldim;
+  obj->base->user_buffer = user_buffer;
+  return PLA_SUCCESS;
+}
+
 int PLA_Matrix_create(MPI_Datatype dt, int length, int width, PLA_Template templ,
                       int align_row, int align_col, PLA_Obj *obj) {
   int r = create(dt, PLA_MATRIX, length, width, templ, false, obj);
@@ -567,27 +629,27 @@ int PLA_Pmvector_create(MPI_Datatype dt, int project_onto, int owner, int length
 }
 
 int PLA_Matrix_create_conf_to(PLA_Obj o, PLA_Obj *obj) {
-  if (!valid(o)) PLA_FAIL("invalid object");
+  if (!valid_any(o)) PLA_FAIL("invalid object");
   return PLA_Matrix_create(o->base->datatype, o->length, o->width, o->templ, o->align_row,
                            o->align_col, obj);
 }
 
 int PLA_Mvector_create_conf_to(PLA_Obj o, int width, PLA_Obj *obj) {
-  if (!valid(o)) PLA_FAIL("invalid object");
+  if (!valid_any(o)) PLA_FAIL("invalid object");
   // conformal to the object's length (a row projection already stores the
   // matrix's row dimension as its length)
   return PLA_Mvector_create(o->base->datatype, o->length, width, o->templ, o->align_row, obj);
 }
 
 int PLA_Mscalar_create_conf_to(PLA_Obj o, int owner_row, int owner_col, PLA_Obj *obj) {
-  if (!valid(o)) PLA_FAIL("invalid object");
+  if (!valid_any(o)) PLA_FAIL("invalid object");
   return PLA_Mscalar_create(o->base->datatype, owner_row, owner_col, o->length, o->width,
                             o->templ, obj);
 }
 
 int PLA_Pmvector_create_conf_to(PLA_Obj o, int project_onto, int owner, int width,
                                 PLA_Obj *obj) {
-  if (!valid(o)) PLA_FAIL("invalid object");
+  if (!valid_any(o)) PLA_FAIL("invalid object");
   int length = project_onto == PLA_PROJ_ONTO_COL ? o->length : o->width;
   int r = PLA_Pmvector_create(o->base->datatype, project_onto, owner, length, width, o->templ,
                               o->align_row, obj);
@@ -596,7 +658,7 @@ int PLA_Pmvector_create_conf_to(PLA_Obj o, int project_onto, int owner, int widt
 
 int PLA_Create_constants_conf_to(PLA_Obj o, PLA_Obj *minus_one, PLA_Obj *zero,
                                  PLA_Obj *one) {
-  if (!valid(o)) PLA_FAIL("invalid object");
+  if (!valid_any(o)) PLA_FAIL("invalid object");
   MPI_Datatype dt = o->base->datatype;
   if (dt == MPI_INT) dt = MPI_DOUBLE;
   const double vals[3] = {-1.0, 0.0, 1.0};
@@ -614,7 +676,7 @@ int PLA_Create_constants_conf_to(PLA_Obj o, PLA_Obj *minus_one, PLA_Obj *zero,
 
 int PLA_Obj_free(PLA_Obj *obj) {
   if (!obj || !*obj) return PLA_SUCCESS;
-  if (!valid(*obj)) PLA_FAIL("invalid object");
+  if (!valid_any(*obj)) PLA_FAIL("invalid object");
   drop_view(*obj);
   *obj = nullptr;
   return PLA_SUCCESS;
@@ -628,11 +690,11 @@ static void assign(PLA_Obj *out, PLA_Obj v) {
   }
   PLA_Obj old = *out;
   *out = v;
-  if (old && valid(old)) drop_view(old);
+  if (old && valid_any(old)) drop_view(old);
 }
 
 int PLA_Obj_view(PLA_Obj o, int length, int width, int disp_row, int disp_col, PLA_Obj *view) {
-  if (!valid(o)) PLA_FAIL("invalid object");
+  if (!valid_any(o)) PLA_FAIL("invalid object");
   if (length == PLA_DIM_ALL) length = o->length - disp_row;
   if (width == PLA_DIM_ALL) width = o->width - disp_col;
   if (disp_row < 0 || disp_col < 0 || length < 0 || width < 0 ||
@@ -651,7 +713,7 @@ int PLA_Obj_view(PLA_Obj o, int length, int width, int disp_row, int disp_col, P
 }
 
 int PLA_Obj_view_all(PLA_Obj o, PLA_Obj *view) {
-  if (!valid(o)) PLA_FAIL("invalid object");
+  if (!valid_any(o)) PLA_FAIL("invalid object");
   PLA_Obj v = copy_view(o);
   v->fixed = 0;
   assign(view, v);
@@ -660,7 +722,7 @@ int PLA_Obj_view_all(PLA_Obj o, PLA_Obj *view) {
 
 int PLA_Obj_split_4(PLA_Obj o, int length, int width, PLA_Obj *tl, PLA_Obj *tr, PLA_Obj *bl,
                     PLA_Obj *br) {
-  if (!valid(o)) PLA_FAIL("invalid object");
+  if (!valid_any(o)) PLA_FAIL("invalid object");
   // sign selects which block the size describes (OBJ/PLA_Obj.c:2078-2088)
   int top = length >= 0 ? length : o->length + length;
   int left = width >= 0 ? width : o->width + width;
@@ -691,19 +753,19 @@ int PLA_Obj_split_4(PLA_Obj o, int length, int width, PLA_Obj *tl, PLA_Obj *tr, 
 }
 
 int PLA_Obj_horz_split_2(PLA_Obj o, int length, PLA_Obj *top, PLA_Obj *bottom) {
-  if (!valid(o)) PLA_FAIL("invalid object");
+  if (!valid_any(o)) PLA_FAIL("invalid object");
   return PLA_Obj_split_4(o, length, o->width, top, nullptr, bottom, nullptr);
 }
 
 int PLA_Obj_vert_split_2(PLA_Obj o, int width, PLA_Obj *left, PLA_Obj *right) {
-  if (!valid(o)) PLA_FAIL("invalid object");
+  if (!valid_any(o)) PLA_FAIL("invalid object");
   return PLA_Obj_split_4(o, o->length, width, left, right, nullptr, nullptr);
 }
 
 // positive moves a boundary down / right (OBJ/PLA_Obj.c:3189-3201)
 int PLA_Obj_view_shift(PLA_Obj o, int shift_top, int shift_left, int shift_right,
                        int shift_bottom) {
-  if (!valid(o)) PLA_FAIL("invalid object");
+  if (!valid_any(o)) PLA_FAIL("invalid object");
   int row0 = o->row0 + shift_top, col0 = o->col0 + shift_left;
   int length = o->length - shift_top + shift_bottom;
   int width = o->width - shift_left + shift_right;
@@ -729,7 +791,7 @@ int PLA_Obj_view_swap(PLA_Obj *a, PLA_Obj *b) {
 // ----------------------------------------------------------------- inquiry --
 #define INQ(name, expr)                          \
   int name(PLA_Obj o, int *out) {                \
-    if (!valid(o)) PLA_FAIL("invalid object");   \
+    if (!valid_any(o)) PLA_FAIL("invalid object");   \
     *out = (expr);                               \
     return PLA_SUCCESS;                          \
   }
@@ -749,25 +811,26 @@ INQ(PLA_Obj_project_onto, o->proj_onto)
 #undef INQ
 
 int PLA_Obj_datatype(PLA_Obj o, MPI_Datatype *dt) {
-  if (!valid(o)) PLA_FAIL("invalid object");
+  if (!valid_any(o)) PLA_FAIL("invalid object");
   *dt = o->base->datatype;
   return PLA_SUCCESS;
 }
 
 int PLA_Obj_template(PLA_Obj o, PLA_Template *t) {
-  if (!valid(o)) PLA_FAIL("invalid object");
+  if (!valid_any(o)) PLA_FAIL("invalid object");
   *t = o->templ;
   return PLA_SUCCESS;
 }
 
 int PLA_Obj_local_buffer(PLA_Obj o, void **buffer) {
-  if (!valid(o)) PLA_FAIL("invalid object");
-  *buffer = at(o, 0, 0);
+  if (!valid_any(o)) PLA_FAIL("invalid object");
+  // an out-of-core object has no buffer (OBJ/PLA_Obj_management.c:161-163)
+  *buffer = o->base->ooc ? nullptr : at(o, 0, 0);
   return PLA_SUCCESS;
 }
 
 int PLA_Obj_set_orientation(PLA_Obj o, int project_onto) {
-  if (!valid(o)) PLA_FAIL("invalid object");
+  if (!valid_any(o)) PLA_FAIL("invalid object");
   o->proj_onto = project_onto;
   return PLA_SUCCESS;
 }

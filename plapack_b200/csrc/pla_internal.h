@@ -22,6 +22,8 @@ struct pla_base {
   int views;           // number of live views
   int user_buffer;     // buffer not owned by the library
   int on_host;         // buf is pinned host memory (duplicated multiscalars)
+  int ooc;             // out-of-core: the data lives in file fd (buf is null)
+  int fd;              // file of an out-of-core object, -1 until attached
 };
 
 // A view: a rectangular window into a base object (INCLUDE/PLA_Obj.h:49-82).
@@ -75,7 +77,8 @@ struct State {
 State &state();
 
 int esize_of(MPI_Datatype dt);
-bool valid(PLA_Obj obj);
+bool valid(PLA_Obj obj);      // a live object with its data in memory
+bool valid_any(PLA_Obj obj);  // a live object, out-of-core ones included
 bool valid(PLA_Template t);
 cudaStream_t stream();
 
@@ -129,6 +132,11 @@ cudaError_t d2h(void *dst, const void *src, size_t bytes);
 // device scratch owned by the library (grown on demand, freed at PLA_Finalize)
 void *scratch(int slot, size_t bytes);
 void release_scratch();
+
+// out-of-core objects (pla_ooc.cpp): PLA_Copy between a file-backed view and
+// a device object, and the pinned staging buffers released at PLA_Finalize
+int ooc_copy(PLA_Obj from, PLA_Obj to);
+void release_ooc();
 
 // phase timing: events recorded on the library stream, resolved later
 struct PhaseTimer {

@@ -804,7 +804,8 @@ int PLA_Shift(PLA_Obj obj, MPI_Datatype datatype, void *value) {
 
 // ----------------------------------------------------------------- copies ---
 static int copy_objs(PLA_Obj from, PLA_Obj to) {
-  if (!valid(from) || !valid(to)) PLA_FAIL("invalid object");
+  if (!valid_any(from) || !valid_any(to)) PLA_FAIL("invalid object");
+  if (from->base->ooc || to->base->ooc) return ooc_copy(from, to);
   if (from->base->datatype != to->base->datatype) PLA_FAIL("datatype mismatch");
   const int dt = from->base->datatype;
   const int es = from->base->esize;

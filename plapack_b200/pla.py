@@ -110,6 +110,12 @@ _SIGS = {
     "PLA_Local_axpy": [Obj, Obj, Obj], "PLA_Local_nrm2": [Obj, Obj],
     "PLA_malloc": [ctypes.c_size_t], "PLA_calloc": [ctypes.c_size_t, ctypes.c_size_t],
     "PLA_free": [_vp], "PLA_Total_size_malloced": [], "PLA_Max_size_malloced": [],
+    "PLA_OOC_Matrix_create_without_fd": [_i, _i, _i, Templ, _i, _i, _pobj],
+    "PLA_Obj_attach_fd": [Obj, _i, _i, _i], "PLA_File_create": [ctypes.c_char_p, _i, _i, _pi],
+    "PLA_File_open": [ctypes.c_char_p, _i, _i, _pi], "PLA_File_close": [_i],
+    "PLA_File_unlink": [ctypes.c_char_p], "PLA_File_stats_start": [], "PLA_File_stats_stop": [],
+    "PLA_OOC_Chol": [_i, _i, Obj],
+    "PLA_B200_file_stats": [ctypes.POINTER(ctypes.c_double)] * 4,
     "PLA_Apply_pivots_to_rows": [Obj, Obj], "PLA_General_solve": [Obj, Obj, Obj],
     "PLA_Chol": [_i, Obj], "PLA_Pos_def_solve": [Obj, Obj],
     "PLA_Trsv": [_i, _i, _i, Obj, Obj], "PLA_Trsm": [_i, _i, _i, _i, Obj, Obj, Obj],

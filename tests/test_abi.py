@@ -78,3 +78,24 @@ def test_host_memory_helpers(built_lib):
     assert lib.PLA_free(q) is None
     assert lib.PLA_free(None) is None              # freeing NULL is a no-op
     assert lib.PLA_Total_size_malloced() == base
+
+
+def test_file_layer_without_gpu(built_lib, tmp_path):
+    # IO/PLA_File.c: create (sized), close, open again, unlink; IO/PLA_File_stats.c counters
+    from plapack_b200 import pla
+    lib = pla.load()
+    name = str(tmp_path / "ooc.bin").encode()
+    fd = ctypes.c_int(-1)
+    assert lib.PLA_File_create(name, pla.MPI_DOUBLE, 1000, ctypes.byref(fd)) == 0
+    assert fd.value >= 0
+    assert os.path.getsize(name) == 8000
+    assert lib.PLA_File_close(fd.value) == 0
+    assert lib.PLA_File_open(name, pla.MPI_DOUBLE, 1000, ctypes.byref(fd)) == 0
+    assert lib.PLA_File_close(fd.value) == 0
+    assert lib.PLA_File_unlink(name) == 0
+    assert not os.path.exists(name)
+    assert lib.PLA_File_open(name, pla.MPI_DOUBLE, 1000, ctypes.byref(fd)) == pla.PLA_ERROR
+    assert lib.PLA_File_stats_start() == 0
+    v = [ctypes.c_double(-1) for _ in range(4)]
+    assert lib.PLA_B200_file_stats(*[ctypes.byref(x) for x in v]) == 0
+    assert [x.value for x in v] == [0.0, 0.0, 0.0, 0.0]
