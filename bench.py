@@ -65,6 +65,9 @@ def parse():
     p.add_argument("--skip-e2e", action="store_true")
     p.add_argument("--skip-cpu", action="store_true")
     p.add_argument("--skip-chol", action="store_true", help="skip the FP64 Cholesky solve")
+    p.add_argument("--skip-ooc", action="store_true", help="skip the out-of-core Cholesky")
+    p.add_argument("--ooc-tile", type=int, default=8192, help="nb_tile of PLA_OOC_Chol")
+    p.add_argument("--ooc-nb", type=int, default=256, help="nb_ooc of PLA_OOC_Chol")
     p.add_argument("--skip-batched", action="store_true", help="skip the batched workload")
     p.add_argument("--batch-count", type=int, default=20000)
     p.add_argument("--skip-chol-mixed", action="store_true",
@@ -395,6 +398,75 @@ def spd_device(n, kappa, seed, torch, device):
     return A
 
 
+def ooc_dir(nbytes):
+    """A directory with room for the out-of-core file: host memory first."""
+    for d in ("/dev/shm", tempfile.gettempdir()):
+        try:
+            st = os.statvfs(d)
+        except OSError:
+            continue
+        if st.f_bavail * st.f_frsize > 1.2 * nbytes:
+            return d
+    return None
+
+
+def run_ooc_chol(torch, pla, lib, s, device, S, a_in, n, args, in_core_factor_s):
+    """PLA_OOC_Chol of the n x n SPD matrix S kept in a file (host memory when
+    /dev/shm has room): factor time (file restored before each step, outside
+    the timed region), the file traffic, and the largest difference from the
+    in-core factor the FP64 Cholesky arm left in a_in."""
+    d = ooc_dir(8.0 * n * n)
+    if d is None:
+        return {"unavailable": f"no directory with {8.0 * n * n / 1e9:.1f} GB free for the file"}
+    path = os.path.join(d, f"pla_ooc_{os.getpid()}.bin").encode()
+    T, nb_ooc = args.ooc_tile, args.ooc_nb
+    A = ctypes.c_void_p()
+    fd = ctypes.c_int(-1)
+    src = s.matrix(n, n)
+    try:
+        pla.check(lib.PLA_OOC_Matrix_create_without_fd(pla.MPI_DOUBLE, n, n, s.templ,
+                                                   pla.PLA_ALIGN_FIRST, pla.PLA_ALIGN_FIRST,
+                                                   ctypes.byref(A)), "OOC create")
+        pla.check(lib.PLA_File_create(path, pla.MPI_DOUBLE, n * n if n * n < 2 ** 31 else 0,
+                                  ctypes.byref(fd)), "File_create")
+        pla.check(lib.PLA_Obj_attach_fd(A, fd.value, n, 1), "attach_fd")
+        pla.check(lib.PLA_Obj_set_local_contents_device(ctypes.c_void_p(S.data_ptr()), n, src), "S")
+        times = []
+        rd = [ctypes.c_double() for _ in range(4)]
+        for step in range(1 + args.steps):          # one warm-up run
+            pla.check(lib.PLA_Copy(src, A), "S to the file")
+            lib.PLA_File_stats_start()
+            t0 = time.perf_counter()
+            rc = lib.PLA_OOC_Chol(nb_ooc, T, A)
+            t1 = time.perf_counter()
+            lib.PLA_B200_file_stats(*[ctypes.byref(x) for x in rd])
+            if rc != 0:
+                raise RuntimeError(f"PLA_OOC_Chol returned {rc}: {pla.last_error()}")
+            if step:
+                times.append(t1 - t0)
+        pla.check(lib.PLA_Copy(A, src), "factor from the file")
+        L = torch.empty((n, n), dtype=torch.float64, device=device)
+        pla.check(lib.PLA_Obj_get_local_contents_device(src, ctypes.c_void_p(L.data_ptr()), n), "L")
+        Li = torch.empty_like(L)
+        pla.check(lib.PLA_Obj_get_local_contents_device(a_in, ctypes.c_void_p(Li.data_ptr()), n), "Li")
+        # row-major views of column-major data: the lower triangle is the upper here
+        diff = (torch.triu(L) - torch.triu(Li)).abs().max().item() / torch.triu(Li).abs().max().item()
+        del L, Li
+        t = min(times)
+        return {"workload": f"PLA_OOC_Chol n={n} FP64, file in {d}, nb_tile={T}, nb_ooc={nb_ooc}",
+                "factor_s": t, "tflops": (n ** 3 / 3.0) / t / 1e12,
+                "in_core_factor_s": in_core_factor_s,
+                "read_gb": rd[0].value / 1e9, "write_gb": rd[2].value / 1e9,
+                "read_gbs": rd[0].value / rd[1].value / 1e9 if rd[1].value else None,
+                "write_gbs": rd[2].value / rd[3].value / 1e9 if rd[3].value else None,
+                "max_rel_diff_vs_in_core": diff}
+    finally:
+        if fd.value >= 0:
+            lib.PLA_File_close(fd.value)
+            lib.PLA_File_unlink(path)
+        s.free(src, A)
+
+
 def run_chol_mixed(torch, pla, lib, s, device, stream, n, kappas, precs, nrhs, steps, warmup):
     """Mixed-precision Cholesky-IR (PLA_Pos_def_solve_mixed, GMRES-IR) on the
     SPD family above: time, the precision that finished, iterations and the
@@ -608,6 +680,7 @@ def run_ours(args):
 
     # ---- FP64 Cholesky arm (PLA_Pos_def_solve) on A = G G'/n + I ----
     chol = None
+    ooc = None
     if not args.skip_chol:
         g = torch.Generator(device=device).manual_seed(2 + 1000 * rank)
         G = torch.randn((n, n), dtype=torch.float64, device=device, generator=g)
@@ -657,6 +730,9 @@ def run_ours(args):
                 "phase_ms_per_step": {k: getattr(phc, k) / args.steps for k in
                                       ("panel_ms", "trsm_ms", "update_ms", "solve_ms")},
                 "backward_error": (rc.abs().max() / (s_inf * x.abs().max() + bs.abs().max())).item()}
+        # ---- out-of-core Cholesky (PLA_OOC_Chol) of the same S from a file in host memory ----
+        if not args.skip_ooc:
+            ooc = run_ooc_chol(torch, pla, lib, s, device, S, a, n, args, chol["chol_factor_s"])
         del S, bs, xs, rc
         torch.cuda.empty_cache()
         check(lib.PLA_Obj_set_local_contents_device(ctypes.c_void_p(T.data_ptr()), n, a), "A")
@@ -737,7 +813,8 @@ def run_ours(args):
                "refinement_iterations": report.iterations,
                "gmres_iterations": report.inner_iterations,
                "factor_ms": report.factor_ms, "refine_ms": report.refine_ms,
-               "fp64_cholesky": chol, "batched": batched, "cholesky_mixed": chol_mixed,
+               "fp64_cholesky": chol, "ooc_cholesky": ooc, "batched": batched,
+               "cholesky_mixed": chol_mixed,
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                "clocks": clock_summary, "gpu_launches": launches}
         print(json.dumps(out))

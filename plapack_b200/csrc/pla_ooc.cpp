@@ -25,14 +25,18 @@
 // copy on the copy stream: two pinned staging buffers and two device chunk
 // buffers alternate, each reused only after the event of its last use.
 #include <fcntl.h>
+#include <sys/mman.h>
 #include <sys/stat.h>
 #include <unistd.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
+#include <vector>
 
 #include "pla_internal.h"
 #include "pla_kernels.h"
@@ -60,39 +64,152 @@ double now_s() {
       .count();
 }
 
-int io_read(int fd, char *dst, size_t bytes, off_t off) {
-  const double t = now_s();
+// one contiguous range; false on an error
+bool pread_all(int fd, char *dst, size_t bytes, off_t off) {
   size_t done = 0;
   while (done < bytes) {
     const ssize_t r = pread(fd, dst + done, bytes - done, off + (off_t)done);
-    if (r < 0) PLA_FAIL("error reading file");
+    if (r < 0) return false;
     if (r == 0) {  // past the end of the file: never written, reads as zero
       std::memset(dst + done, 0, bytes - done);
       break;
     }
     done += (size_t)r;
   }
+  return true;
+}
+bool pwrite_all(int fd, const char *src, size_t bytes, off_t off) {
+  size_t done = 0;
+  while (done < bytes) {
+    const ssize_t r = pwrite(fd, src + done, bytes - done, off + (off_t)done);
+    if (r <= 0) return false;
+    done += (size_t)r;
+  }
+  return true;
+}
+
+// A file region of `count` pieces of `piece` bytes, piece k at file offset
+// off + k * stride and at buffer offset k * piece, moved by up to kIoThreads
+// host threads: one thread copies from the page cache (or tmpfs) at a few
+// GB/s, several at the host's memory bandwidth.
+constexpr int kIoThreads = 8;
+constexpr size_t kIoSplit = size_t(4) << 20;  // bytes below which one thread moves it all
+
+template <typename Op>
+bool io_pieces(long count, size_t piece, off_t off, off_t stride, Op op) {
+  const size_t total = (size_t)count * piece;
+  int nt = (int)std::min<size_t>(kIoThreads, total / kIoSplit);
+  if (nt <= 1) {
+    for (long k = 0; k < count; k++)
+      if (!op(k * piece, piece, off + (off_t)k * stride)) return false;
+    return true;
+  }
+  // split the pieces, or, for one large piece, its bytes
+  std::atomic<bool> ok{true};
+  std::vector<std::thread> th;
+  if (count >= nt) {
+    for (int w = 0; w < nt; w++)
+      th.emplace_back([&, w] {
+        for (long k = count * w / nt; k < count * (w + 1) / nt && ok; k++)
+          if (!op(k * piece, piece, off + (off_t)k * stride)) ok = false;
+      });
+  } else {
+    for (long k = 0; k < count; k++) {
+      const size_t part = (piece + nt - 1) / nt;
+      for (int w = 0; w < nt; w++) {
+        const size_t b0 = (size_t)w * part, b1 = std::min(piece, b0 + part);
+        if (b0 >= b1) break;
+        th.emplace_back([&, k, b0, b1] {
+          if (!op(k * piece + b0, b1 - b0, off + (off_t)k * stride + (off_t)b0)) ok = false;
+        });
+      }
+      for (std::thread &t : th) t.join();
+      th.clear();
+    }
+  }
+  for (std::thread &t : th) t.join();
+  return ok;
+}
+
+// The file of the current out-of-core call mapped into memory (MapScope):
+// parallel writes through pwrite queue on the file's inode lock, copies into
+// a shared mapping only take page locks.  Ranges outside it use pread/pwrite.
+struct FileMap {
+  int fd = -1;
+  char *base = nullptr;
+  size_t len = 0;
+};
+FileMap g_map;
+
+struct MapScope {
+  bool mine = false;
+  explicit MapScope(int fd) {
+    if (g_map.fd != -1) return;
+    struct stat st;
+    if (fstat(fd, &st) != 0 || st.st_size <= 0) return;
+    void *p = mmap(nullptr, (size_t)st.st_size, PROT_READ | PROT_WRITE, MAP_SHARED, fd, 0);
+    if (p == MAP_FAILED) return;
+    g_map.fd = fd;
+    g_map.base = (char *)p;
+    g_map.len = (size_t)st.st_size;
+    mine = true;
+  }
+  ~MapScope() {
+    if (!mine) return;
+    munmap(g_map.base, g_map.len);
+    g_map = FileMap();
+  }
+};
+
+bool mapped(int fd, off_t off, size_t bytes) {
+  return fd == g_map.fd && off >= 0 && (size_t)off + bytes <= g_map.len;
+}
+
+int io_read(int fd, char *dst, long count, size_t piece, off_t off, off_t stride) {
+  const double t = now_s();
+  const size_t span = count > 0 ? (size_t)(count - 1) * stride + piece : 0;
+  if (mapped(fd, off, span)) {
+    io_pieces(count, piece, off, stride, [&](size_t at, size_t n, off_t fo) {
+      std::memcpy(dst + at, g_map.base + fo, n);
+      return true;
+    });
+  } else if (!io_pieces(count, piece, off, stride, [&](size_t at, size_t n, off_t fo) {
+               return pread_all(fd, dst + at, n, fo);
+             })) {
+    PLA_FAIL("error reading file");
+  }
   if (g_io.on) {
-    g_io.read_bytes += (double)bytes;
+    g_io.read_bytes += (double)count * piece;
     g_io.read_s += now_s() - t;
   }
   return PLA_SUCCESS;
 }
 
-int io_write(int fd, const char *src, size_t bytes, off_t off) {
+int io_write(int fd, const char *src, long count, size_t piece, off_t off, off_t stride) {
   const double t = now_s();
-  size_t done = 0;
-  while (done < bytes) {
-    const ssize_t r = pwrite(fd, src + done, bytes - done, off + (off_t)done);
-    if (r <= 0) PLA_FAIL("error writing file");
-    done += (size_t)r;
+  const size_t span = count > 0 ? (size_t)(count - 1) * stride + piece : 0;
+  if (mapped(fd, off, span)) {
+    io_pieces(count, piece, off, stride, [&](size_t at, size_t n, off_t fo) {
+      std::memcpy(g_map.base + fo, src + at, n);
+      return true;
+    });
+  } else if (!io_pieces(count, piece, off, stride, [&](size_t at, size_t n, off_t fo) {
+               return pwrite_all(fd, src + at, n, fo);
+             })) {
+    PLA_FAIL("error writing file");
   }
   if (g_io.on) {
-    g_io.write_bytes += (double)bytes;
+    g_io.write_bytes += (double)count * piece;
     g_io.write_s += now_s() - t;
   }
   return PLA_SUCCESS;
 }
+
+#define R(call)         \
+  do {                  \
+    int r_ = (call);    \
+    if (r_) return r_;  \
+  } while (0)
 
 // pinned staging buffers and the events of their last copy
 constexpr size_t kStageBytes = size_t(64) << 20;
@@ -133,16 +250,12 @@ int read_block(PLA_Obj v, long i0, long j0, long m, long n, char *dst, long ldd,
     next ^= 1;
     PLA_CUDA(cudaEventSynchronize(g_stage.done[b]));
     char *h = g_stage.buf[b];
-    if (i0 + m == v->base->ldim - v->row0 && v->row0 == 0 && i0 == 0) {
-      // whole columns of the file: one read
-      int r = io_read(v->base->fd, h, (size_t)m * nc * es, file_off(v, 0, j0 + c0));
-      if (r) return r;
+    if (m == v->base->ldim && v->row0 == 0 && i0 == 0) {
+      // whole columns of the file: one range
+      R(io_read(v->base->fd, h, 1, (size_t)m * nc * es, file_off(v, 0, j0 + c0), 0));
     } else {
-      for (long j = 0; j < nc; j++) {
-        int r = io_read(v->base->fd, h + (size_t)j * m * es, (size_t)m * es,
-                        file_off(v, i0, j0 + c0 + j));
-        if (r) return r;
-      }
+      R(io_read(v->base->fd, h, nc, (size_t)m * es, file_off(v, i0, j0 + c0),
+                (off_t)v->base->ldim * es));
     }
     PLA_CUDA(cudaMemcpy2DAsync(dst + (size_t)c0 * ldd * es, (size_t)ldd * es, h, (size_t)m * es,
                                (size_t)m * es, nc, cudaMemcpyHostToDevice, s));
@@ -165,12 +278,8 @@ int write_block(PLA_Obj v, long i0, long j0, long m, long n, const char *src, lo
   auto flush = [&]() -> int {
     if (pending < 0) return PLA_SUCCESS;
     PLA_CUDA(cudaEventSynchronize(g_stage.done[pb]));
-    const char *h = g_stage.buf[pb];
-    for (long j = 0; j < pending_n; j++) {
-      int r = io_write(v->base->fd, h + (size_t)j * m * es, (size_t)m * es,
-                       file_off(v, i0, j0 + pending + j));
-      if (r) return r;
-    }
+    R(io_write(v->base->fd, g_stage.buf[pb], pending_n, (size_t)m * es,
+               file_off(v, i0, j0 + pending), (off_t)v->base->ldim * es));
     pending = -1;
     return PLA_SUCCESS;
   };
@@ -219,12 +328,6 @@ struct Events {
     int r_ = (call);                                               \
     if (r_) return cuda_fail((cudaError_t)r_, __LINE__, __FILE__); \
   } while (0)
-#define R(call)         \
-  do {                  \
-    int r_ = (call);    \
-    if (r_) return r_;  \
-  } while (0)
-
 // HBM held for the resident L10 block of one tile column: 16 GB, or the
 // bytes in PLA_B200_OOC_RESIDENT_BYTES (0 streams L10 with L20 always)
 size_t resident_budget() {
@@ -245,6 +348,7 @@ int ooc_copy(PLA_Obj from, PLA_Obj to) {
   if (from->base->datatype != to->base->datatype) PLA_FAIL("datatype mismatch");
   if (from->length != to->length || from->width != to->width) PLA_FAIL("objects do not conform");
   R(staging());
+  MapScope map(f->base->fd);
   cudaStream_t s = stream();
   if (from->base->ooc)
     R(read_block(f, 0, 0, f->length, f->width, at(d, 0, 0), ld(d), s));
@@ -420,6 +524,7 @@ int PLA_OOC_Chol(int nb_ooc, int nb_tile, PLA_Obj A) {
   char *dx[2] = {cx0.p, cx1.p}, *dy[2] = {cy0.p, cy1.p};
   Events ev;
   R(ev.create());
+  MapScope map(A->base->fd);
   cudaStream_t s0 = stream();
   for (int j0 = 0; j0 < n; j0 += T) {
     const int t = std::min(T, n - j0);
