@@ -94,6 +94,10 @@ typedef int MPI_Comm;
 #define PLA_OP_MAT_PAN       (PLA_OP_OFFSET + 1)
 #define PLA_OP_PAN_MAT       (PLA_OP_OFFSET + 2)
 #define PLA_OP_PAN_PAN       (PLA_OP_OFFSET + 3)
+/* INCLUDE/PLA_Versions.h:11-13: the stationary operand of PLA_Gemm_x */
+#define PLA_VERSION_A        100
+#define PLA_VERSION_B        200
+#define PLA_VERSION_C        300
 #define PLA_OP_PAN_TRIAN_MAT (PLA_OP_OFFSET + 4)
 #define PLA_OP_SYM_PAN_PAN   (PLA_OP_OFFSET + 5)
 #define PLA_OP_TRIAN_MAT_PAN (PLA_OP_OFFSET + 6)
@@ -242,6 +246,11 @@ int PLA_API_axpy_global_to_matrix(int m, int n, void *alpha, PLA_Obj obj,
                                   int disp_row, int disp_col, void *local_matrix,
                                   int local_ldim);            /* :593 */
 
+/* ---- timings (OBJ/PLA_Timings.c): the library's phase timers -------------- */
+int PLA_Timings_initialize(void);                    /* OBJ/PLA_Timings.c:17 */
+int PLA_Timings_print(void);                         /* OBJ/PLA_Timings.c:41 */
+int PLA_Timings_average(void);                       /* OBJ/PLA_Timings.c:127 */
+
 /* ---- host memory (OBJ/PLA_Memory.c; INCLUDE/PLA_Memory_prototypes.h) ------ */
 /* as the reference: malloc / calloc with running totals of the bytes held.
  * Where the reference prints and exits on failure these return NULL and set
@@ -274,6 +283,9 @@ int PLA_OOC_Chol(int nb_ooc, int nb_tile, PLA_Obj A); /* POOCLAPACK/OOC_Cholesky
 
 /* ---- solvers and parallel BLAS on the dense-solve path ------------------------ */
 int PLA_LU(PLA_Obj A, PLA_Obj pivots);               /* SOLVERS/LU/PLA_LU.c:13 */
+int PLA_LU_right(int nb_alg, PLA_Obj A, PLA_Obj pivots); /* SOLVERS/LU/PLA_LU.c:37 */
+/* the unblocked panel factorization; A_11_msc receives the factored top block */
+int PLA_LU_right_mv(PLA_Obj A_mv, PLA_Obj A_11_msc, PLA_Obj pivots_msc); /* PLA_LU_mv.c:13 */
 /* the blocked LU whose interchanges skip the columns left of each panel */
 int PLA_LU_linpack(PLA_Obj A, PLA_Obj pivots);       /* SOLVERS/LINPACK/PLA_LU_linpack.c:13 */
 int PLA_LU_linpack_right(int nb_alg, PLA_Obj A, PLA_Obj pivots); /* :30 */
@@ -287,6 +299,8 @@ int PLA_Trsm(int side, int uplo, int trans, int diag, PLA_Obj alpha, PLA_Obj A,
              PLA_Obj B);                             /* BLAS3/PLA_Trsm.c:13 */
 int PLA_Gemm(int transa, int transb, PLA_Obj alpha, PLA_Obj A, PLA_Obj B,
              PLA_Obj beta, PLA_Obj C);               /* BLAS3/PLA_Gemm.c:13 */
+int PLA_Gemm_x(int version, int transa, int transb, PLA_Obj alpha, PLA_Obj A,
+               PLA_Obj B, PLA_Obj beta, PLA_Obj C);  /* BLAS3/PLA_Gemm_x.c:13 */
 int PLA_Gemv(int trans, PLA_Obj alpha, PLA_Obj A, PLA_Obj x, PLA_Obj beta,
              PLA_Obj y);                             /* BLAS2/PLA_Gemv.c */
 int PLA_Iamax(PLA_Obj x, PLA_Obj k, PLA_Obj xmax);   /* BLAS1/PLA_Iamax.c:37 */

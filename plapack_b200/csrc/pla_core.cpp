@@ -997,3 +997,29 @@ void *PLA_free(void *buffer) {
 int PLA_Total_size_malloced(void) { return (int)pla::g_host_bytes.load(); }
 int PLA_Max_size_malloced(void) { return (int)pla::g_host_bytes_max.load(); }
 }  // extern "C"
+
+// OBJ/PLA_Timings.c:17-140: the reference's per-operation timers.  Here they
+// are the library's phase timers: initialize resets and starts them, print
+// writes each nonzero phase as the reference writes each timer, average (a
+// reduction over ranks) has nothing to combine on one GPU.
+extern "C" {
+int PLA_Timings_initialize(void) {
+  PLA_B200_reset_phase_times();
+  return PLA_B200_set_phase_timing(1);
+}
+int PLA_Timings_print(void) {
+  PLA_Phase_times t;
+  int r = PLA_B200_phase_times(&t);
+  if (r) return r;
+  const struct {
+    const char *name;
+    double ms;
+  } rows[] = {{"panel  ", t.panel_ms},  {"swap   ", t.swap_ms},  {"trsm   ", t.trsm_ms},
+              {"update ", t.update_ms}, {"solve  ", t.solve_ms}, {"refine ", t.refine_ms},
+              {"convert", t.convert_ms}};
+  for (const auto &row : rows)
+    if (row.ms != 0) std::printf("%s time = %f\n", row.name, row.ms / 1e3);
+  return PLA_SUCCESS;
+}
+int PLA_Timings_average(void) { return PLA_SUCCESS; }
+}  // extern "C"

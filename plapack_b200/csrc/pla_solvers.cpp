@@ -438,6 +438,39 @@ int PLA_LU_info(PLA_Obj A, PLA_Obj pivots, int *info) {
 
 int PLA_LU(PLA_Obj A, PLA_Obj pivots) { return lu_entry(A, pivots, 0, true, nullptr); }
 
+// SOLVERS/LU/PLA_LU.c:37: the blocked LU with the caller's block size
+int PLA_LU_right(int nb_alg, PLA_Obj A, PLA_Obj pivots) {
+  if (nb_alg <= 0) PLA_FAIL("PLA_LU_right: nb_alg must be positive");
+  return lu_entry(A, pivots, nb_alg, true, nullptr);
+}
+
+// SOLVERS/LU/PLA_LU_mv.c:13-102: factor the panel A_mv in place with partial
+// pivoting; pivots_msc receives the pivots and A_11_msc a copy of the factored
+// top block (row j is copied when it becomes the pivot row, :274, and rows
+// above the current column never change afterwards, so the copy is the final
+// top min(m, n) x n block).  The pivots are those of the column loop.
+int PLA_LU_right_mv(PLA_Obj A_mv, PLA_Obj A_11_msc, PLA_Obj pivots_msc) {
+  if (!valid(A_mv) || !valid(A_11_msc) || !valid(pivots_msc)) PLA_FAIL("invalid object");
+  if (!numeric(A_mv)) PLA_FAIL("datatype not yet supported");
+  if (A_11_msc->base->datatype != A_mv->base->datatype) PLA_FAIL("datatype mismatch");
+  if (pivots_msc->base->datatype != MPI_INT) PLA_FAIL("pivots must be of type MPI_INT");
+  const int m = A_mv->length, n = A_mv->width, k = std::min(m, n);
+  if (A_11_msc->length < k || A_11_msc->width < n) PLA_FAIL("A_11_msc smaller than the panel's top block");
+  if (vlen(pivots_msc) < k || vinc(pivots_msc) != 1) PLA_FAIL("pivots_msc must be a column of min(m, n) entries");
+  if (k == 0) return PLA_SUCCESS;
+  int *dpiv = (int *)scratch(29, (size_t)k * sizeof(int));
+  if (!dpiv) PLA_FAIL("cannot allocate scratch");
+  int r = lu_on_device(A_mv->base->datatype, m, n, at(A_mv, 0, 0), ld(A_mv), dpiv, kTri, nullptr,
+                       true);
+  if (r) return r;
+  const int es = A_mv->base->esize;
+  PLA_CUDA(cudaMemcpy2DAsync(at(A_11_msc, 0, 0), (size_t)ld(A_11_msc) * es, at(A_mv, 0, 0),
+                             (size_t)ld(A_mv) * es, (size_t)k * es, n, cudaMemcpyDefault, stream()));
+  PLA_CUDA(cudaMemcpyAsync(at(pivots_msc, 0, 0), dpiv, (size_t)k * sizeof(int), cudaMemcpyDefault,
+                           stream()));
+  return finish("lu_right_mv");
+}
+
 // SOLVERS/LINPACK/PLA_LU_linpack.c:13-28 and :30-208: the blocked LU whose
 // interchanges leave the columns left of each panel alone
 int PLA_LU_linpack(PLA_Obj A, PLA_Obj pivots) { return lu_entry(A, pivots, 0, false, nullptr); }
@@ -604,6 +637,18 @@ static int gemm_objs(int transa, int transb, PLA_Obj alpha, PLA_Obj A, PLA_Obj B
                at(A, 0, 0), ld(A), at(B, 0, 0), ld(B), scalar_value(beta), at(C, 0, 0), ld(C),
                uplo_c, nullptr, stream()));
   return finish("gemm");
+}
+
+// BLAS3/PLA_Gemm_x.c:13: the GEMM with the caller's choice of stationary
+// operand (PLA_VERSION_A / _B / _C); on a 1x1 template nothing moves, so
+// every version is the same device product
+int PLA_Gemm(int transa, int transb, PLA_Obj alpha, PLA_Obj A, PLA_Obj B, PLA_Obj beta,
+             PLA_Obj C);
+int PLA_Gemm_x(int version, int transa, int transb, PLA_Obj alpha, PLA_Obj A, PLA_Obj B,
+               PLA_Obj beta, PLA_Obj C) {
+  if (version != PLA_VERSION_A && version != PLA_VERSION_B && version != PLA_VERSION_C)
+    PLA_FAIL("PLA_Gemm_x: unknown version");
+  return PLA_Gemm(transa, transb, alpha, A, B, beta, C);
 }
 
 int PLA_Gemm(int transa, int transb, PLA_Obj alpha, PLA_Obj A, PLA_Obj B, PLA_Obj beta,

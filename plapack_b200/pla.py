@@ -28,6 +28,7 @@ PLA_ALL_ROWS, PLA_ALL_COLS = -31, -32
 PLA_SIDE_TOP, PLA_SIDE_BOTTOM, PLA_SIDE_LEFT, PLA_SIDE_RIGHT = 41, 42, 43, 44
 PLA_UPPER_TRIANGULAR, PLA_LOWER_TRIANGULAR = 51, 52
 PLA_OP_PAN_PAN, PLA_OP_ALL_ALG = 83, 87
+PLA_VERSION_A, PLA_VERSION_B, PLA_VERSION_C = 100, 200, 300
 PLA_PROJ_ONTO_COL, PLA_PROJ_ONTO_ROW = 91, 92
 PLA_UNIT_DIAG, PLA_NONUNIT_DIAG = 101, 102
 PLA_SUCCESS, PLA_ALIGN_FIRST, PLA_DIM_ALL = 0, -200, -201
@@ -106,6 +107,9 @@ _SIGS = {
     "PLA_API_axpy_global_to_vector": [_i, _vp, Obj, _i, _vp, _i],
     "PLA_LU": [Obj, Obj], "PLA_LU_info": [Obj, Obj, _pi],
     "PLA_LU_linpack": [Obj, Obj], "PLA_LU_linpack_right": [_i, Obj, Obj],
+    "PLA_LU_right": [_i, Obj, Obj], "PLA_LU_right_mv": [Obj, Obj, Obj],
+    "PLA_Gemm_x": [_i, _i, _i, Obj, Obj, Obj, Obj, Obj],
+    "PLA_Timings_initialize": [], "PLA_Timings_print": [], "PLA_Timings_average": [],
     "PLA_Axpy": [Obj, Obj, Obj], "PLA_Nrm2": [Obj, Obj], "PLA_Shift": [Obj, _i, _vp],
     "PLA_Local_axpy": [Obj, Obj, Obj], "PLA_Local_nrm2": [Obj, Obj],
     "PLA_malloc": [ctypes.c_size_t], "PLA_calloc": [ctypes.c_size_t, ctypes.c_size_t],
