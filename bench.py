@@ -66,6 +66,8 @@ def parse():
     p.add_argument("--skip-cpu", action="store_true")
     p.add_argument("--skip-chol", action="store_true", help="skip the FP64 Cholesky solve")
     p.add_argument("--skip-ooc", action="store_true", help="skip the out-of-core Cholesky")
+    p.add_argument("--skip-sweep", action="store_true",
+                   help="skip the kappa 1e2 / 1e10 and 16-rhs solves")
     p.add_argument("--ooc-tile", type=int, default=8192, help="nb_tile of PLA_OOC_Chol")
     p.add_argument("--ooc-nb", type=int, default=256, help="nb_ooc of PLA_OOC_Chol")
     p.add_argument("--skip-batched", action="store_true", help="skip the batched workload")
@@ -396,6 +398,68 @@ def spd_device(n, kappa, seed, torch, device):
         A.addr_(A @ v, v, alpha=c)
     A.add_(A.t().clone()).mul_(0.5)
     return A
+
+
+def run_mixed_sweep(torch, pla, lib, s, device, stream, a, n, args, params):
+    """The C3 configurations beside the headline one, each solved once after a
+    warm-up solve: kappa 1e2 and 1e10 with one right-hand side (1e10 makes the
+    refinement escalate the factor precision), kappa 1e6 with 16 right-hand
+    sides, and the FP64 PLA_General_solve of the 16-rhs system.  Reports the
+    time, the precision that finished, iterations and the largest normwise
+    backward error over the right-hand sides."""
+    out = []
+    for kappa, nrhs, fp64 in ((1e2, 1, False), (1e10, 1, False), (1e6, 16, False),
+                              (1e6, 16, True)):
+        T, x_true, _ = c3_device(n, kappa, 2000 + int(np.log10(kappa)), torch, device)
+        g = torch.Generator(device=device).manual_seed(77)
+        X = torch.randn(n, nrhs, dtype=torch.float64, device=device, generator=g)
+        X[:, :1] = x_true
+        Bm = (T.t() @ X).contiguous(memory_format=torch.contiguous_format)
+        Bc = Bm.t().contiguous()                     # column-major n x nrhs as a row-major tensor
+        bo = s.matrix(n, nrhs)
+        piv = s.mvector(n, 1, np.int32)
+        rep = pla.MixedReport()
+
+        def solve():
+            pla.check(lib.PLA_Obj_set_local_contents_device(ctypes.c_void_p(T.data_ptr()), n, a),
+                      "A")
+            pla.check(lib.PLA_Obj_set_local_contents_device(ctypes.c_void_p(Bc.data_ptr()), n, bo),
+                      "B")
+            if fp64:
+                pla.check(lib.PLA_General_solve(a, piv, bo), "PLA_General_solve")
+            else:
+                pla.check(lib.PLA_General_solve_mixed(a, bo, ctypes.byref(params),
+                                                      ctypes.byref(rep)), "solve_mixed")
+
+        solve()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        solve()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        Xh = torch.empty_like(Bc)
+        pla.check(lib.PLA_Obj_get_local_contents_device(bo, ctypes.c_void_p(Xh.data_ptr()), n), "X")
+        Xs = Xh.t()                                  # n x nrhs
+        R = Bm - T.t() @ Xs
+        a_inf = T.abs().sum(dim=0).max().item()
+        eta = (R.abs().amax(dim=0) / (a_inf * Xs.abs().amax(dim=0) + Bm.abs().amax(dim=0))).max().item()
+        fwd = ((Xs[:, 0] - x_true[:, 0]).abs().max() / x_true.abs().max()).item()
+        entry = {"kappa": kappa, "nrhs": nrhs, "solver": "PLA_General_solve (FP64)" if fp64 else
+                 f"PLA_General_solve_mixed ({args.precision}, {args.refinement.upper()}-IR)",
+                 "solve_s": t, "backward_error_max": eta, "forward_error_rhs0": fwd}
+        if not fp64:
+            entry.update({"precision_used": {1: "bf16", 2: "fp16", 3: "fp32", 4: "fp64",
+                                             5: "fp8"}.get(rep.precision_used),
+                          "factorizations": rep.factorizations,
+                          "converged": rep.converged, "iterations": rep.iterations,
+                          "gmres_iterations": rep.inner_iterations})
+        out.append(entry)
+        s.free(bo, piv)
+        del T, X, Bm, Bc, Xh, R
+        torch.cuda.empty_cache()
+    return out
 
 
 def ooc_dir(nbytes):
@@ -786,6 +850,13 @@ def run_ours(args):
                        "factorization) -> PLA_Obj_get_local_contents"}
         del Th
 
+    # ---- the other C3 configurations at full size: kappa 1e2 and 1e10, and 16 rhs ----
+    sweep = None
+    if not args.skip_sweep:
+        del T
+        torch.cuda.empty_cache()
+        sweep = run_mixed_sweep(torch, pla, lib, s, device, stream, a, n, args, params)
+
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
         try:
@@ -813,6 +884,7 @@ def run_ours(args):
                "refinement_iterations": report.iterations,
                "gmres_iterations": report.inner_iterations,
                "factor_ms": report.factor_ms, "refine_ms": report.refine_ms,
+               "mixed_sweep": sweep,
                "fp64_cholesky": chol, "ooc_cholesky": ooc, "batched": batched,
                "cholesky_mixed": chol_mixed,
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,

@@ -111,6 +111,18 @@ __global__ void diag_mul_k(int n, int nrhs, const double *__restrict__ d, double
   for (int r = 0; r < nrhs; r++) X[i + (long)r * ldx] *= di;
 }
 
+// out(i, r) := (To) in(perm[i], r): a row permutation (the composed row
+// interchanges of an LU) and a conversion in one pass
+template <typename Ti, typename To>
+__global__ void gather_rows_k(int n, int nrhs, const int *__restrict__ perm,
+                              const Ti *__restrict__ in, long ldi, To *__restrict__ out,
+                              long ldo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long src = perm[i];
+  for (int r = 0; r < nrhs; r++) out[i + (long)r * ldo] = (To)in[src + (long)r * ldi];
+}
+
 constexpr int kRows = 256;
 
 // partial[s][i] = sum over j in slice s of op(A)(i, j) * X(j, r) for NR columns
@@ -222,6 +234,20 @@ extern "C" size_t pla_k_residual_work(int n, int ncols, int nrhs) {
   int nr = nrhs <= 1 ? 1 : nrhs <= 2 ? 2 : nrhs <= 4 ? 4 : nrhs <= 8 ? 8 : 16;
   (void)ncols;
   return (size_t)slices * nr * n * sizeof(double);
+}
+
+extern "C" int pla_k_gather_rows(int dt_out, int n, int nrhs, const int *perm, const double *in,
+                                  long ldi, void *out, long ldo, cudaStream_t s) {
+  if (n <= 0 || nrhs <= 0) return 0;
+  const int g = (n + 255) / 256;
+  if (dt_out == MPI_FLOAT)
+    gather_rows_k<double, float><<<g, 256, 0, s>>>(n, nrhs, perm, in, ldi, (float *)out, ldo);
+  else if (dt_out == MPI_DOUBLE)
+    gather_rows_k<double, double><<<g, 256, 0, s>>>(n, nrhs, perm, in, ldi, (double *)out, ldo);
+  else
+    return (int)cudaErrorInvalidValue;
+  pla_k_count(1);
+  return (int)cudaGetLastError();
 }
 
 extern "C" int pla_k_residual(int n, int ncols, int nrhs, const double *A, long lda,

@@ -224,6 +224,177 @@ trsv_ticket_k(int n, int nblk, const T *A, long lda, bool lower_op, bool trans, 
   }
 }
 
+// The same solve for up to NR right-hand sides (fp32): X := inv(op(A)) B, B
+// and X n x nrhs.  Every tile of A is loaded once, as above, and multiplied
+// into NR accumulators per thread, so A is read once for all the columns;
+// the reduction buffers and the block of right-hand sides for every column
+// are in dynamic shared memory (Ds TB x TB | red NR x 8 x TB | xs NR x TB |
+// part 2 x NR x TB), so a block row costs the single-column number of
+// barriers.
+template <int NR>
+__global__ void __launch_bounds__(THREADS)
+trsv_ticket_nr_k(int n, int nblk, int nrhs, const float *A, long lda, bool lower_op, bool trans,
+                 const float *Dinv, long ldd, const float *B, long ldb, float *X, long ldx,
+                 int *ticket, int *flags, int *status, bool vec_ok) {
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  float *Ds = reinterpret_cast<float *>(dyn_smem);
+  float *red = Ds + TB * TB;
+  float *xs = red + NR * 8 * TB;
+  float *part = xs + NR * TB;
+  __shared__ int s_blk, s_bad;
+  const int r = threadIdx.x % TB, half = threadIdx.x / TB;
+  const int rg = threadIdx.x & 31, cg = threadIdx.x >> 5;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_blk = atomicAdd(ticket, 1);
+      s_bad = 0;
+    }
+    __syncthreads();
+    const int q = s_blk;
+    if (q >= nblk) return;
+    const int i = lower_op ? q : nblk - 1 - q;
+    const long r0 = (long)i * TB;
+    const int nbi = min(TB, n - (int)r0);
+    float acc4[NR][4], acc[NR];
+#pragma unroll
+    for (int k = 0; k < NR; k++) {
+      acc[k] = 0.f;
+#pragma unroll
+      for (int e = 0; e < 4; e++) acc4[k][e] = 0.f;
+    }
+    for (int u = threadIdx.x; u < TB * TB / 4; u += THREADS) {
+      const int c = u / (TB / 4), r4 = (u % (TB / 4)) * 4;
+      cp_async16(&Ds[c * TB + r4], Dinv + (r0 + r4) + (long)c * ldd);
+    }
+    cp_async_commit();
+    for (int s = 0; s < q; s++) {
+      const int j = lower_op ? s : nblk - 1 - s;
+      const long c0 = (long)j * TB;
+      const int nbj = min(TB, n - (int)c0);
+      const bool full = nbi == TB && nbj == TB && vec_ok;
+      float4 v[16];
+      if (full) {
+        const float *base = trans ? A + (r0 + r) * lda + c0 + 64 * half
+                                  : A + (r0 + 4 * rg) + (c0 + 16 * cg) * lda;
+        const long step = trans ? 4 : lda;
+#pragma unroll
+        for (int u = 0; u < 16; u++) v[u] = *reinterpret_cast<const float4 *>(base + u * step);
+      }
+      if (threadIdx.x == 0) {
+        long spins = 0;
+        while (ld_acquire(&flags[j]) == 0) {
+          if (++spins > kSpin || *(volatile int *)status != PLA_K_OK) {
+            atomicCAS(status, PLA_K_OK, PLA_K_TIMEOUT);
+            s_bad = 1;
+            break;
+          }
+          __nanosleep(32);
+        }
+      }
+      __syncthreads();
+      if (s_bad) return;
+      for (int t = threadIdx.x; t < NR * TB; t += THREADS) {
+        const int k = t / TB, c = t % TB;
+        xs[t] = k < nrhs && c < nbj ? __ldcg(&X[c0 + c + (long)k * ldx]) : 0.f;
+      }
+      __syncthreads();
+      if (full && !trans) {
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+#pragma unroll
+          for (int k = 0; k < NR; k++) {
+            const float xv = xs[k * TB + 16 * cg + u];
+            acc4[k][0] += v[u].x * xv;
+            acc4[k][1] += v[u].y * xv;
+            acc4[k][2] += v[u].z * xv;
+            acc4[k][3] += v[u].w * xv;
+          }
+        }
+      } else if (full) {
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+          const int c = 64 * half + 4 * u;
+#pragma unroll
+          for (int k = 0; k < NR; k++) {
+            const float *xk = xs + k * TB + c;
+            acc[k] += v[u].x * xk[0] + v[u].y * xk[1] + v[u].z * xk[2] + v[u].w * xk[3];
+          }
+        }
+      } else if (r < nbi) {
+        if (!trans) {
+          for (int c = half; c < nbj; c += 2) {
+            const float a = A[(r0 + r) + (c0 + c) * lda];
+#pragma unroll
+            for (int k = 0; k < NR; k++) acc[k] += a * xs[k * TB + c];
+          }
+        } else {
+          const int cb = half * (TB / 2), ce = min(cb + TB / 2, nbj);
+          const float *col = A + (r0 + r) * lda + c0;
+          for (int c = cb; c < ce; c++) {
+            const float a = col[c];
+#pragma unroll
+            for (int k = 0; k < NR; k++) acc[k] += a * xs[k * TB + c];
+          }
+        }
+      }
+      __syncthreads();
+    }
+    // reduce the 8 column groups and the two halves, then y = b - sum
+#pragma unroll
+    for (int k = 0; k < NR; k++) {
+#pragma unroll
+      for (int e = 0; e < 4; e++) red[(k * 8 + cg) * TB + 4 * rg + e] = acc4[k][e];
+      part[(half * NR + k) * TB + r] = acc[k];
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < NR * TB; t += THREADS) {
+      const int k = t / TB, row = t % TB;
+      float sacc = part[k * TB + row] + part[(NR + k) * TB + row];
+#pragma unroll
+      for (int g = 0; g < 8; g++) sacc += red[(k * 8 + g) * TB + row];
+      xs[t] = row < nbi && k < nrhs ? B[r0 + row + (long)k * ldb] - sacc : 0.f;
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // x_i = inv(D_i) y for every column, with the inverse block from shared memory
+    {
+      float y4[NR][4];
+#pragma unroll
+      for (int k = 0; k < NR; k++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) y4[k][e] = 0.f;
+#pragma unroll
+      for (int u = 0; u < 16; u++) {
+        const float4 d = *reinterpret_cast<const float4 *>(&Ds[(16 * cg + u) * TB + 4 * rg]);
+#pragma unroll
+        for (int k = 0; k < NR; k++) {
+          const float xv = xs[k * TB + 16 * cg + u];
+          y4[k][0] += d.x * xv;
+          y4[k][1] += d.y * xv;
+          y4[k][2] += d.z * xv;
+          y4[k][3] += d.w * xv;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < NR; k++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) red[(k * 8 + cg) * TB + 4 * rg + e] = y4[k][e];
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < NR * TB; t += THREADS) {
+      const int k = t / TB, row = t % TB;
+      if (k >= nrhs || row >= nbi) continue;
+      float y = 0.f;
+#pragma unroll
+      for (int g = 0; g < 8; g++) y += red[(k * 8 + g) * TB + row];
+      X[r0 + row + (long)k * ldx] = y;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) st_release(&flags[i], 1);
+  }
+}
+
 // The FP64 form: 64 x 64 blocks (a 64 x 64 FP64 inverse is 32 KB), each tile
 // read as 8 independent 16-byte loads per thread.  No transpose: thread
 // (rg, cg) owns rows 2rg, 2rg+1 and columns 8cg .. 8cg+7; transpose: thread
@@ -407,6 +578,34 @@ int ticket_solve(char uplo, char trans, int n, const void *A, long lda, const vo
   return (int)cudaGetLastError();
 }
 
+template <int NR>
+int ticket_solve_nr(char uplo, char trans, int n, int nrhs, const float *A, long lda,
+                    const float *Dinv, long ldd, const float *B, long ldb, float *X, long ldx,
+                    int *status, cudaStream_t s) {
+  const bool tr = trans != 'N', lower_op = (uplo == 'L') != tr;
+  const int nblk = (n + TB - 1) / TB;
+  int *fl = flags_for(nblk);
+  if (!fl) return (int)cudaErrorMemoryAllocation;
+  cudaError_t e = cudaMemsetAsync(fl, 0, (size_t)(nblk + 8) * sizeof(int), s);
+  if (e) return (int)e;
+  if (!g_sms) {
+    int d;
+    cudaGetDevice(&d);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, d);
+  }
+  if (ldd % TB || (uintptr_t)Dinv % 16) return (int)cudaErrorMisalignedAddress;
+  const bool vec_ok = lda % 4 == 0 && (uintptr_t)A % 16 == 0;
+  const int grid = nblk < g_sms ? nblk : g_sms;
+  const size_t dyn = ((size_t)TB * TB + (size_t)NR * 8 * TB + (size_t)NR * TB + 2 * NR * TB) *
+                     sizeof(float);
+  cudaFuncSetAttribute(trsv_ticket_nr_k<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)dyn);
+  trsv_ticket_nr_k<NR><<<grid, THREADS, dyn, s>>>(n, nblk, nrhs, A, lda, lower_op, tr, Dinv, ldd,
+                                                  B, ldb, X, ldx, fl + nblk, fl, status, vec_ok);
+  pla_k_count(1);
+  return (int)cudaGetLastError();
+}
+
 int ticket_solve64(char uplo, char trans, int n, const void *A, long lda, const void *Dinv,
                    long ldd, const void *b, void *x, int *status, cudaStream_t s) {
   const bool tr = trans != 'N', lower_op = (uplo == 'L') != tr;
@@ -452,6 +651,22 @@ extern "C" int pla_k_trsv_ticket(int dt, char uplo, char trans, int n, const voi
   if (dt == MPI_FLOAT)
     return ticket_solve<float>(uplo, trans, n, A, lda, Dinv, ldd, b, x, status, s);
   if (dt == MPI_DOUBLE) return ticket_solve64(uplo, trans, n, A, lda, Dinv, ldd, b, x, status, s);
+  return (int)cudaErrorInvalidValue;
+}
+
+// X := inv(op(A)) B for nrhs <= 16 fp32 right-hand sides in one launch (B and
+// X may be the same array); Dinv as for pla_k_trsv_ticket
+extern "C" int pla_k_trsv_ticket_multi(char uplo, char trans, int n, int nrhs, const float *A,
+                                       long lda, const float *Dinv, long ldd, const float *B,
+                                       long ldb, float *X, long ldx, int *status,
+                                       cudaStream_t s) {
+  if (n <= 0 || nrhs <= 0) return 0;
+  if (nrhs <= 4) return ticket_solve_nr<4>(uplo, trans, n, nrhs, A, lda, Dinv, ldd, B, ldb, X,
+                                           ldx, status, s);
+  if (nrhs <= 8) return ticket_solve_nr<8>(uplo, trans, n, nrhs, A, lda, Dinv, ldd, B, ldb, X,
+                                           ldx, status, s);
+  if (nrhs <= 16) return ticket_solve_nr<16>(uplo, trans, n, nrhs, A, lda, Dinv, ldd, B, ldb, X,
+                                             ldx, status, s);
   return (int)cudaErrorInvalidValue;
 }
 

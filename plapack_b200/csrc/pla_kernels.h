@@ -157,7 +157,16 @@ int pla_k_trsv_inv_blocks(int dt, char uplo, char trans, char diag, int n, const
 int pla_k_trsv_ticket(int dt, char uplo, char trans, int n, const void *A, long lda,
                       const void *Dinv, long ldd, const void *b, void *x, int *status,
                       cudaStream_t s);
+/* the same for up to 16 fp32 right-hand sides (n x nrhs, ldb / ldx) in one
+ * launch: A read once for all of them; B and X may be the same array */
+int pla_k_trsv_ticket_multi(char uplo, char trans, int n, int nrhs, const float *A, long lda,
+                            const float *Dinv, long ldd, const float *B, long ldb, float *X,
+                            long ldx, int *status, cudaStream_t s);
 void pla_trsv_release(void);
+/* out (dt_out = MPI_FLOAT or MPI_DOUBLE, n x nrhs, ldo) := rows perm[0..n) of
+ * the FP64 in (ldi): a composed row permutation and a conversion in one pass */
+int pla_k_gather_rows(int dt_out, int n, int nrhs, const int *perm, const double *in, long ldi,
+                      void *out, long ldo, cudaStream_t s);
 size_t pla_k_residual_work(int n, int ncols, int nrhs);
 int pla_k_residual(int n, int ncols, int nrhs, const double *A, long lda, const double *X,
                    long ldx, const double *B, long ldb, double *R, long ldr, int abs_rows,

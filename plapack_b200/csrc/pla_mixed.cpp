@@ -63,6 +63,7 @@ struct Factor {
   double *a64 = nullptr;  // FP64 factors (FP64)
   double *dsc = nullptr;  // d = diag(A)^-1/2 when the factors are those of D A D
   int *piv = nullptr;
+  int *perm = nullptr;    // LU: row i of P v is v[perm[i]] (the pivots composed)
   int *status = nullptr;  // [status, info, zero_info]
   // inverses of the 128 x 128 diagonal blocks of the two triangular factors
   float *dinv1 = nullptr, *dinv2 = nullptr;
@@ -70,6 +71,32 @@ struct Factor {
 };
 
 constexpr int kSlotDinv = 13;
+constexpr int kSlotPerm = 30;
+
+// The row interchanges of an LU composed into one permutation, once per
+// factorization: the refinement applies P to every preconditioned vector, and
+// a gather is one parallel pass where the interchanges in sequence are n
+// dependent swaps per column.
+int prepare_perm(Factor &F) {
+  F.perm = nullptr;
+  if (F.kind != 0) return PLA_SUCCESS;
+  const int n = F.n;
+  std::vector<int> piv(n), perm(n);
+  PLA_CUDA(d2h(piv.data(), F.piv, (size_t)n * sizeof(int)));
+  for (int i = 0; i < n; i++) perm[i] = i;
+  for (int i = 0; i < n; i++) {
+    const int p = i + piv[i];
+    if (p < 0 || p >= n) PLA_FAIL("pivot outside the matrix");
+    std::swap(perm[i], perm[p]);
+  }
+  int *d = (int *)scratch(kSlotPerm, (size_t)n * sizeof(int));
+  if (!d) PLA_FAIL("cannot allocate the permutation");
+  PLA_CUDA(cudaMemcpyAsync(d, perm.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice,
+                           stream()));
+  PLA_CUDA(cudaStreamSynchronize(stream()));  // perm is a host temporary
+  F.perm = d;
+  return PLA_SUCCESS;
+}
 
 // the per-factor data of the single-launch triangular solves
 int prepare_solves(Factor &F) {
@@ -260,9 +287,12 @@ int precond(const Factor &F, const double *v, long ldv, double *out, long ldo, i
             float *t32) {
   const int n = F.n;
   if (F.prec == PLA_B200_PREC_FP64) {
-    K(pla_k_copy(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, nrhs, v, ldv, out, ldo, stream()));
+    if (F.kind == 0 && F.perm)
+      K(pla_k_gather_rows(MPI_DOUBLE, n, nrhs, F.perm, v, ldv, out, ldo, stream()));
+    else
+      K(pla_k_copy(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, nrhs, v, ldv, out, ldo, stream()));
     if (F.kind == 0) {
-      K(pla_k_laswp_rows(MPI_DOUBLE, out, ldo, nrhs, n, F.piv, stream()));
+      if (!F.perm) K(pla_k_laswp_rows(MPI_DOUBLE, out, ldo, nrhs, n, F.piv, stream()));
       const char *f = (const char *)F.a64;
       K(tri_solve(MPI_DOUBLE, 'L', 'N', 'U', n, nrhs, f, F.ld, (char *)out, ldo));
       K(tri_solve(MPI_DOUBLE, 'U', 'N', 'N', n, nrhs, f, F.ld, (char *)out, ldo));
@@ -277,10 +307,12 @@ int precond(const Factor &F, const double *v, long ldv, double *out, long ldo, i
     K(pla_k_copy(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, nrhs, v, ldv, out, ldo, stream()));
     K(pla_k_diag_mul(n, nrhs, F.dsc, out, ldo, stream()));
     K(pla_k_convert(MPI_DOUBLE, out, ldo, MPI_FLOAT, t32, n, n, nrhs, stream()));
+  } else if (F.kind == 0 && F.perm) {
+    K(pla_k_gather_rows(MPI_FLOAT, n, nrhs, F.perm, v, ldv, t32, n, stream()));
   } else {
     K(pla_k_convert(MPI_DOUBLE, v, ldv, MPI_FLOAT, t32, n, n, nrhs, stream()));
   }
-  if (F.kind == 0) K(pla_k_laswp_rows(MPI_FLOAT, t32, n, nrhs, n, F.piv, stream()));
+  if (F.kind == 0 && !F.perm) K(pla_k_laswp_rows(MPI_FLOAT, t32, n, nrhs, n, F.piv, stream()));
   const char u1 = 'L', t1 = 'N', d1 = F.kind == 0 ? 'U' : 'N';
   const char u2 = F.kind == 0 ? 'U' : 'L', t2 = F.kind == 0 ? 'N' : 'T', d2 = 'N';
   if (nrhs <= 2 && F.dinv1) {
@@ -291,6 +323,12 @@ int precond(const Factor &F, const double *v, long ldv, double *out, long ldo, i
       K(pla_k_trsv_ticket(MPI_FLOAT, u2, t2, n, F.a, F.ld, F.dinv2, F.ldd, col, col, F.status,
                           stream()));
     }
+  } else if (nrhs <= 16 && F.dinv1) {
+    // all the columns in one launch per triangle: the factors are read once
+    K(pla_k_trsv_ticket_multi(u1, t1, n, nrhs, F.a, F.ld, F.dinv1, F.ldd, t32, n, t32, n,
+                              F.status, stream()));
+    K(pla_k_trsv_ticket_multi(u2, t2, n, nrhs, F.a, F.ld, F.dinv2, F.ldd, t32, n, t32, n,
+                              F.status, stream()));
   } else {
     K(pla_k_trsv_blocked(MPI_FLOAT, u1, t1, d1, n, nrhs, F.a, F.ld, t32, n, stream()));
     K(pla_k_trsv_blocked(MPI_FLOAT, u2, t2, d2, n, nrhs, F.a, F.ld, t32, n, stream()));
@@ -406,6 +444,140 @@ int gmres(const Factor &F, const double *A, long lda, const double *r, double *d
     K(pla_k_gemv(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, j, 1.0, V, n, tmp, 0.0, d, stream()));
   }
   *iters += j;
+  return PLA_SUCCESS;
+}
+
+// out[i] := ||x_i||_2 for the columns x_i (n each): one launch per column,
+// one read-back for all
+int col_norms(int n, const std::vector<const double *> &x, double *tmp, std::vector<double> &out) {
+  for (size_t i = 0; i < x.size(); i++)
+    K(pla_k_gemv(MPI_DOUBLE, PLA_TRANSPOSE, n, 1, 1.0, x[i], n, x[i], 0.0, tmp + i, stream()));
+  out.assign(x.size(), 0.0);
+  if (x.empty()) return PLA_SUCCESS;
+  PLA_CUDA(cudaMemcpyAsync(out.data(), tmp, x.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                           stream()));
+  PLA_CUDA(cudaStreamSynchronize(stream()));
+  for (double &v : out) v = std::sqrt(v);
+  return PLA_SUCCESS;
+}
+
+// Restarted-GMRES corrections for nrhs columns at once, D(:, s) ~= A^{-1}
+// R(:, s).  The columns run in lockstep: one residual launch forms A v_j for
+// all of them and one preconditioner application solves with the factors for
+// all of them, so A (8.6 GB at n = 32768) and the factors are read once per
+// iteration rather than once per column.  The orthogonalisation (CGS2, its
+// coefficients read back in one copy per pass), the Givens rotations and the
+// convergence test are per column; a column that has converged takes no
+// further part.  V holds column s's basis at V + s (restart + 1) n, W is n x
+// nrhs, tmp at least (restart + 1) nrhs doubles.
+int gmres_block(const Factor &F, const double *A, long lda, const double *R, double *D, int nrhs,
+                int restart, double tau, double *V, double *W, double *tmp, float *t32,
+                double *work, int *iters) {
+  const int n = F.n, m = restart;
+  const long ldv = (long)n * (m + 1);
+  auto vcol = [&](int s, int j) { return V + (long)s * ldv + (long)j * n; };
+  int rc = precond(F, R, n, V, ldv, nrhs, t32);  // z_s = M^{-1} r_s into v_0 of every column
+  if (rc) return rc;
+  K(pla_k_fill(MPI_DOUBLE, n, nrhs, D, n, 0.0, stream()));
+  std::vector<const double *> cols(nrhs);
+  for (int s = 0; s < nrhs; s++) cols[s] = vcol(s, 0);
+  std::vector<double> beta;
+  rc = col_norms(n, cols, tmp, beta);
+  if (rc) return rc;
+  const size_t hm = (size_t)(m + 1) * m;
+  std::vector<double> H(hm * nrhs, 0.0), cs((size_t)m * nrhs), sn((size_t)m * nrhs),
+      g((size_t)(m + 1) * nrhs, 0.0);
+  std::vector<char> active(nrhs);
+  std::vector<int> jend(nrhs, 0);
+  int nact = 0;
+  for (int s = 0; s < nrhs; s++) {
+    active[s] = beta[s] > 0;
+    nact += active[s];
+    g[(size_t)s * (m + 1)] = beta[s];
+    if (active[s]) K(pla_k_scal(MPI_DOUBLE, n, 1, 1.0 / beta[s], vcol(s, 0), n, stream()));
+  }
+  std::vector<double> hp((size_t)(m + 1) * nrhs), hsum((size_t)(m + 1) * nrhs);
+  for (int j = 0; j < m && nact > 0; j++) {
+    // W = A [v_j of every column]; v_{j+1} = M^{-1} W
+    K(pla_k_residual(n, n, nrhs, A, lda, vcol(0, j), ldv, nullptr, n, W, n, 0, work, stream()));
+    rc = precond(F, W, n, vcol(0, j + 1), ldv, nrhs, t32);
+    if (rc) return rc;
+    // CGS2 against v_0 .. v_j, per active column
+    std::fill(hsum.begin(), hsum.end(), 0.0);
+    for (int pass = 0; pass < 2; pass++) {
+      for (int s = 0; s < nrhs; s++)
+        if (active[s])
+          K(pla_k_gemv(MPI_DOUBLE, PLA_TRANSPOSE, n, j + 1, 1.0, vcol(s, 0), n, vcol(s, j + 1),
+                       0.0, tmp + (size_t)s * (m + 1), stream()));
+      PLA_CUDA(cudaMemcpyAsync(hp.data(), tmp, hp.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                               stream()));
+      PLA_CUDA(cudaStreamSynchronize(stream()));
+      for (int s = 0; s < nrhs; s++) {
+        if (!active[s]) continue;
+        // tmp still holds the coefficients on the device
+        K(pla_k_gemv(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, j + 1, -1.0, vcol(s, 0), n,
+                     tmp + (size_t)s * (m + 1), 1.0, vcol(s, j + 1), stream()));
+        for (int i = 0; i <= j; i++) hsum[(size_t)s * (m + 1) + i] += hp[(size_t)s * (m + 1) + i];
+      }
+    }
+    cols.clear();
+    std::vector<int> who;
+    for (int s = 0; s < nrhs; s++)
+      if (active[s]) {
+        cols.push_back(vcol(s, j + 1));
+        who.push_back(s);
+      }
+    std::vector<double> hn;
+    rc = col_norms(n, cols, tmp, hn);
+    if (rc) return rc;
+    for (size_t q = 0; q < who.size(); q++) {
+      const int s = who[q];
+      double *Hs = H.data() + hm * s, *gs = g.data() + (size_t)s * (m + 1);
+      double *css = cs.data() + (size_t)s * m, *sns = sn.data() + (size_t)s * m;
+      for (int i = 0; i <= j; i++) Hs[i + (size_t)j * (m + 1)] = hsum[(size_t)s * (m + 1) + i];
+      Hs[j + 1 + (size_t)j * (m + 1)] = hn[q];
+      if (hn[q] > 0) K(pla_k_scal(MPI_DOUBLE, n, 1, 1.0 / hn[q], vcol(s, j + 1), n, stream()));
+      for (int i = 0; i < j; i++) {
+        const double a = Hs[i + (size_t)j * (m + 1)], b = Hs[i + 1 + (size_t)j * (m + 1)];
+        Hs[i + (size_t)j * (m + 1)] = css[i] * a + sns[i] * b;
+        Hs[i + 1 + (size_t)j * (m + 1)] = -sns[i] * a + css[i] * b;
+      }
+      const double a = Hs[j + (size_t)j * (m + 1)], b = Hs[j + 1 + (size_t)j * (m + 1)];
+      const double rr = std::hypot(a, b);
+      css[j] = rr > 0 ? a / rr : 1.0;
+      sns[j] = rr > 0 ? b / rr : 0.0;
+      Hs[j + (size_t)j * (m + 1)] = rr;
+      Hs[j + 1 + (size_t)j * (m + 1)] = 0.0;
+      gs[j + 1] = -sns[j] * gs[j];
+      gs[j] = css[j] * gs[j];
+      jend[s] = j + 1;
+      if (std::fabs(gs[j + 1]) <= tau * beta[s] || hn[q] == 0) {
+        active[s] = 0;
+        nact--;
+      }
+    }
+  }
+  // y_s = H_s \ g_s; D(:, s) = V_s y_s
+  std::vector<double> y((size_t)(m + 1) * nrhs, 0.0);
+  for (int s = 0; s < nrhs; s++) {
+    const int js = jend[s];
+    if (js == 0) continue;
+    const double *Hs = H.data() + hm * s, *gs = g.data() + (size_t)s * (m + 1);
+    double *ys = y.data() + (size_t)s * (m + 1);
+    for (int i = js - 1; i >= 0; i--) {
+      double t = gs[i];
+      for (int c = i + 1; c < js; c++) t -= Hs[i + (size_t)c * (m + 1)] * ys[c];
+      ys[i] = t / Hs[i + (size_t)i * (m + 1)];
+    }
+    *iters += js;
+  }
+  PLA_CUDA(cudaMemcpyAsync(tmp, y.data(), y.size() * sizeof(double), cudaMemcpyHostToDevice,
+                           stream()));
+  for (int s = 0; s < nrhs; s++)
+    if (jend[s] > 0)
+      K(pla_k_gemv(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, jend[s], 1.0, vcol(s, 0), n,
+                   tmp + (size_t)s * (m + 1), 0.0, D + (long)s * n, stream()));
+  PLA_CUDA(cudaStreamSynchronize(stream()));  // y must stay alive until copied
   return PLA_SUCCESS;
 }
 
@@ -659,8 +831,10 @@ int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
                                                        (size_t)n * sizeof(double)) + 256);
   double *V = nullptr, *w = nullptr;
   if (p.refinement == PLA_B200_IR_GMRES) {
-    V = (double *)scratch(kSlotV, (size_t)n * (p.gmres_restart + 2) * sizeof(double));
-    w = V + (size_t)n * (p.gmres_restart + 1);
+    // one basis per right-hand side (they run in lockstep), then W
+    V = (double *)scratch(kSlotV, (size_t)n * ((size_t)(p.gmres_restart + 1) * nrhs + nrhs) *
+                                      sizeof(double));
+    w = V + (size_t)n * (p.gmres_restart + 1) * nrhs;
   }
   if (!t32b || !work || (p.refinement == PLA_B200_IR_GMRES && !V))
     PLA_FAIL("cannot allocate the refinement workspace");
@@ -752,6 +926,7 @@ int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
       int rc0 = prepare_solves(F);
       if (rc0) return rc0;
     }
+    PK(prepare_perm(F));
     if (!have_x) {  // start from x = M^{-1} b
       int rc = precond(F, Bsave, n, X, n, nrhs, t32b);
       if (rc) return rc;
@@ -784,12 +959,14 @@ int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
         stalled = true;
         break;
       }
-      if (p.refinement == PLA_B200_IR_GMRES) {
-        for (int j = 0; j < nrhs; j++) {
-          rc = gmres(F, Ad, lda, R + (long)j * n, Dv + (long)j * n, p.gmres_restart, 1e-8, V, w,
-                     tmp, t32b, work, &r.inner_iterations);
-          if (rc) return rc;
-        }
+      if (p.refinement == PLA_B200_IR_GMRES && nrhs == 1) {
+        rc = gmres(F, Ad, lda, R, Dv, p.gmres_restart, 1e-8, V, w, tmp, t32b, work,
+                   &r.inner_iterations);
+        if (rc) return rc;
+      } else if (p.refinement == PLA_B200_IR_GMRES) {
+        rc = gmres_block(F, Ad, lda, R, Dv, nrhs, p.gmres_restart, 1e-8, V, w, tmp, t32b, work,
+                         &r.inner_iterations);
+        if (rc) return rc;
       } else {
         rc = precond(F, R, n, Dv, n, nrhs, t32b);
         if (rc) return rc;

@@ -455,3 +455,54 @@ def test_streamed_solve_small_order_copies_first(env):
     assert rc == 0 and rep.converged == 1
     assert backward_error(A, s.get(b), B) <= n * 2.0 ** -53
     s.free(a, b)
+
+
+@pytest.mark.parametrize("uplo,trans,diag", [("L", "N", "U"), ("U", "N", "N"), ("L", "N", "N"),
+                                             ("L", "T", "N")])
+@pytest.mark.parametrize("n,ld,nrhs", [(3001, 3008, 16), (2048, 2048, 3), (1500, 1501, 8)])
+def test_trsv_ticket_multi(env, uplo, trans, diag, n, ld, nrhs):
+    """The single-launch solve for several fp32 right-hand sides (the GMRES-IR
+    preconditioner of a multi-rhs solve) against an FP64 solve of the same
+    data: every triangle and transpose the preconditioner uses, ragged orders,
+    a leading dimension that rules out the vector loads, and in-place use."""
+    s, torch, pla = env
+    lib = s.lib
+    for name, args in (("pla_k_trsv_inv_blocks", [ctypes.c_int, ctypes.c_char, ctypes.c_char,
+                                                  ctypes.c_char, ctypes.c_int, ctypes.c_void_p,
+                                                  ctypes.c_long, ctypes.c_void_p, ctypes.c_long,
+                                                  ctypes.c_void_p]),
+                       ("pla_k_trsv_ticket_multi", [ctypes.c_char, ctypes.c_char, ctypes.c_int,
+                                                    ctypes.c_int, ctypes.c_void_p, ctypes.c_long,
+                                                    ctypes.c_void_p, ctypes.c_long,
+                                                    ctypes.c_void_p, ctypes.c_long,
+                                                    ctypes.c_void_p, ctypes.c_long,
+                                                    ctypes.c_void_p, ctypes.c_void_p])):
+        getattr(lib, name).argtypes = args
+        getattr(lib, name).restype = ctypes.c_int
+    g = torch.Generator(device="cuda").manual_seed(n + nrhs)
+    M = torch.randn(n, n, device="cuda", generator=g, dtype=torch.float64) * (0.5 / n ** 0.5)
+    T = torch.tril(M, -1) if uplo == "L" else torch.triu(M, 1)
+    T.diagonal().copy_(1.0 + torch.rand(n, device="cuda", generator=g, dtype=torch.float64))
+    T32 = T.float()
+    # column-major n x n with leading dimension ld: row-major (n, ld) of the transpose
+    Acm = torch.zeros(n, ld, device="cuda", dtype=torch.float32)
+    Acm[:, :n] = T32.t()
+    ldd = (n + 127) // 128 * 128
+    dinv = torch.zeros(128, ldd, device="cuda", dtype=torch.float32)
+    st = torch.zeros(4, dtype=torch.int32, device="cuda")
+    assert lib.pla_k_trsv_inv_blocks(pla.MPI_FLOAT, uplo.encode(), trans.encode(), diag.encode(), n,
+                                     Acm.data_ptr(), ld, dinv.data_ptr(), ldd, None) == 0
+    B = torch.randn(nrhs, n, device="cuda", generator=g, dtype=torch.float32)  # column-major n x nrhs
+    X = B.clone()
+    assert lib.pla_k_trsv_ticket_multi(uplo.encode(), trans.encode(), n, nrhs, Acm.data_ptr(), ld,
+                                       dinv.data_ptr(), ldd, X.data_ptr(), n, X.data_ptr(), n,
+                                       st.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    assert st[0].item() == 0
+    Td = T32.double()
+    if diag == "U":
+        Td.diagonal().fill_(1.0)
+    op = Td.t() if trans == "T" else Td
+    ref = torch.linalg.solve_triangular(op, B.double().t(), upper=(uplo == "U") != (trans == "T"))
+    err = (X.double().t() - ref).abs().max().item()
+    assert err <= 64 * n * np.finfo(np.float32).eps * ref.abs().max().item(), err
