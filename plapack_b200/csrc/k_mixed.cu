@@ -123,6 +123,54 @@ __global__ void gather_rows_k(int n, int nrhs, const int *__restrict__ perm,
   for (int r = 0; r < nrhs; r++) out[i + (long)r * ldo] = (To)in[src + (long)r * ldi];
 }
 
+// Batched helpers of the lockstep GMRES: column s's Krylov basis is
+// V + s * ldv (n x (m + 1), ld n); `active` has bit s set for the columns
+// still iterating.
+// out[s * ldo + c] := V_s(:, a0 + c) . V_s(:, b) for c < nc: one block per
+// (c, s), a fixed reduction order
+__global__ void __launch_bounds__(256)
+basis_dots_k(int n, const double *__restrict__ V, long ldv, int a0, int nc, int b,
+             unsigned active, double *__restrict__ out, int ldo) {
+  const int c = blockIdx.x, s = blockIdx.y;
+  if (!((active >> s) & 1u) || c >= nc) return;
+  const double *x = V + (long)s * ldv + (long)(a0 + c) * n, *y = V + (long)s * ldv + (long)b * n;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += 256) acc = fma(x[i], y[i], acc);
+  __shared__ double red[8];
+  for (int o = 16; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    acc = threadIdx.x < 8 ? red[threadIdx.x] : 0.0;
+    for (int o = 4; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (threadIdx.x == 0) out[s * ldo + c] = acc;
+  }
+}
+
+// V_s(:, b) -= V_s(:, 0:nc) h_s for the active columns, h_s = h + s * ldh
+__global__ void __launch_bounds__(256)
+basis_update_k(int n, double *__restrict__ V, long ldv, int nc, int b,
+               const double *__restrict__ h, int ldh, unsigned active) {
+  const int i = blockIdx.x * 256 + threadIdx.x, s = blockIdx.y;
+  if (i >= n || !((active >> s) & 1u)) return;
+  double *Vs = V + (long)s * ldv;
+  const double *hs = h + (long)s * ldh;
+  double acc = 0.0;
+  for (int c = 0; c < nc; c++) acc = fma(Vs[i + (long)c * n], hs[c], acc);
+  Vs[i + (long)b * n] -= acc;
+}
+
+struct ColScales {
+  double v[16];
+};
+// V_s(:, b) *= scale.v[s] for the active columns
+__global__ void basis_scale_k(int n, double *__restrict__ V, long ldv, int b, ColScales scale,
+                              unsigned active) {
+  const int i = blockIdx.x * 256 + threadIdx.x, s = blockIdx.y;
+  if (i >= n || !((active >> s) & 1u)) return;
+  V[(long)s * ldv + (long)b * n + i] *= scale.v[s];
+}
+
 constexpr int kRows = 256;
 
 // partial[s][i] = sum over j in slice s of op(A)(i, j) * X(j, r) for NR columns
@@ -234,6 +282,32 @@ extern "C" size_t pla_k_residual_work(int n, int ncols, int nrhs) {
   int nr = nrhs <= 1 ? 1 : nrhs <= 2 ? 2 : nrhs <= 4 ? 4 : nrhs <= 8 ? 8 : 16;
   (void)ncols;
   return (size_t)slices * nr * n * sizeof(double);
+}
+
+extern "C" int pla_k_basis_dots(int n, int nrhs, const double *V, long ldv, int a0, int nc, int b,
+                                 unsigned active, double *out, int ldo, cudaStream_t s) {
+  if (n <= 0 || nrhs <= 0 || nc <= 0 || nrhs > 16) return nrhs > 16 ? (int)cudaErrorInvalidValue : 0;
+  basis_dots_k<<<dim3(nc, nrhs), 256, 0, s>>>(n, V, ldv, a0, nc, b, active, out, ldo);
+  pla_k_count(1);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int pla_k_basis_update(int n, int nrhs, double *V, long ldv, int nc, int b,
+                                  const double *h, int ldh, unsigned active, cudaStream_t s) {
+  if (n <= 0 || nrhs <= 0 || nc <= 0 || nrhs > 16) return nrhs > 16 ? (int)cudaErrorInvalidValue : 0;
+  basis_update_k<<<dim3((n + 255) / 256, nrhs), 256, 0, s>>>(n, V, ldv, nc, b, h, ldh, active);
+  pla_k_count(1);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int pla_k_basis_scale(int n, int nrhs, double *V, long ldv, int b, const double *scale,
+                                 unsigned active, cudaStream_t s) {
+  if (n <= 0 || nrhs <= 0 || nrhs > 16) return nrhs > 16 ? (int)cudaErrorInvalidValue : 0;
+  ColScales sc{};
+  for (int i = 0; i < nrhs; i++) sc.v[i] = scale[i];
+  basis_scale_k<<<dim3((n + 255) / 256, nrhs), 256, 0, s>>>(n, V, ldv, b, sc, active);
+  pla_k_count(1);
+  return (int)cudaGetLastError();
 }
 
 extern "C" int pla_k_gather_rows(int dt_out, int n, int nrhs, const int *perm, const double *in,

@@ -167,6 +167,17 @@ void pla_trsv_release(void);
  * the FP64 in (ldi): a composed row permutation and a conversion in one pass */
 int pla_k_gather_rows(int dt_out, int n, int nrhs, const int *perm, const double *in, long ldi,
                       void *out, long ldo, cudaStream_t s);
+/* batched Krylov-basis operations for up to 16 columns, column s's basis at
+ * V + s ldv (ld n); bit s of `active` selects the columns:
+ *   dots:   out[s ldo + c] = V_s(:, a0 + c) . V_s(:, b), c < nc
+ *   update: V_s(:, b) -= V_s(:, 0:nc) h_s, h_s = h + s ldh (device)
+ *   scale:  V_s(:, b) *= scale[s] (host array) */
+int pla_k_basis_dots(int n, int nrhs, const double *V, long ldv, int a0, int nc, int b,
+                     unsigned active, double *out, int ldo, cudaStream_t s);
+int pla_k_basis_update(int n, int nrhs, double *V, long ldv, int nc, int b, const double *h,
+                       int ldh, unsigned active, cudaStream_t s);
+int pla_k_basis_scale(int n, int nrhs, double *V, long ldv, int b, const double *scale,
+                      unsigned active, cudaStream_t s);
 size_t pla_k_residual_work(int n, int ncols, int nrhs);
 int pla_k_residual(int n, int ncols, int nrhs, const double *A, long lda, const double *X,
                    long ldx, const double *B, long ldb, double *R, long ldr, int abs_rows,

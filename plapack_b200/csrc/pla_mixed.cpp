@@ -447,20 +447,6 @@ int gmres(const Factor &F, const double *A, long lda, const double *r, double *d
   return PLA_SUCCESS;
 }
 
-// out[i] := ||x_i||_2 for the columns x_i (n each): one launch per column,
-// one read-back for all
-int col_norms(int n, const std::vector<const double *> &x, double *tmp, std::vector<double> &out) {
-  for (size_t i = 0; i < x.size(); i++)
-    K(pla_k_gemv(MPI_DOUBLE, PLA_TRANSPOSE, n, 1, 1.0, x[i], n, x[i], 0.0, tmp + i, stream()));
-  out.assign(x.size(), 0.0);
-  if (x.empty()) return PLA_SUCCESS;
-  PLA_CUDA(cudaMemcpyAsync(out.data(), tmp, x.size() * sizeof(double), cudaMemcpyDeviceToHost,
-                           stream()));
-  PLA_CUDA(cudaStreamSynchronize(stream()));
-  for (double &v : out) v = std::sqrt(v);
-  return PLA_SUCCESS;
-}
-
 // Restarted-GMRES corrections for nrhs columns at once, D(:, s) ~= A^{-1}
 // R(:, s).  The columns run in lockstep: one residual launch forms A v_j for
 // all of them and one preconditioner application solves with the factors for
@@ -476,67 +462,61 @@ int gmres_block(const Factor &F, const double *A, long lda, const double *R, dou
   const int n = F.n, m = restart;
   const long ldv = (long)n * (m + 1);
   auto vcol = [&](int s, int j) { return V + (long)s * ldv + (long)j * n; };
+  const unsigned all = nrhs >= 32 ? ~0u : (1u << nrhs) - 1u;
   int rc = precond(F, R, n, V, ldv, nrhs, t32);  // z_s = M^{-1} r_s into v_0 of every column
   if (rc) return rc;
   K(pla_k_fill(MPI_DOUBLE, n, nrhs, D, n, 0.0, stream()));
-  std::vector<const double *> cols(nrhs);
-  for (int s = 0; s < nrhs; s++) cols[s] = vcol(s, 0);
-  std::vector<double> beta;
-  rc = col_norms(n, cols, tmp, beta);
-  if (rc) return rc;
+  std::vector<double> beta(nrhs), sc(nrhs);
+  K(pla_k_basis_dots(n, nrhs, V, ldv, 0, 1, 0, all, tmp, 1, stream()));
+  PLA_CUDA(cudaMemcpyAsync(beta.data(), tmp, nrhs * sizeof(double), cudaMemcpyDeviceToHost,
+                           stream()));
+  PLA_CUDA(cudaStreamSynchronize(stream()));
   const size_t hm = (size_t)(m + 1) * m;
   std::vector<double> H(hm * nrhs, 0.0), cs((size_t)m * nrhs), sn((size_t)m * nrhs),
       g((size_t)(m + 1) * nrhs, 0.0);
-  std::vector<char> active(nrhs);
   std::vector<int> jend(nrhs, 0);
-  int nact = 0;
+  unsigned active = 0;
   for (int s = 0; s < nrhs; s++) {
-    active[s] = beta[s] > 0;
-    nact += active[s];
+    beta[s] = std::sqrt(beta[s]);
     g[(size_t)s * (m + 1)] = beta[s];
-    if (active[s]) K(pla_k_scal(MPI_DOUBLE, n, 1, 1.0 / beta[s], vcol(s, 0), n, stream()));
+    if (beta[s] > 0) active |= 1u << s;
+    sc[s] = beta[s] > 0 ? 1.0 / beta[s] : 1.0;
   }
-  std::vector<double> hp((size_t)(m + 1) * nrhs), hsum((size_t)(m + 1) * nrhs);
-  for (int j = 0; j < m && nact > 0; j++) {
+  K(pla_k_basis_scale(n, nrhs, V, ldv, 0, sc.data(), active, stream()));
+  std::vector<double> hp((size_t)(m + 1) * nrhs), hsum((size_t)(m + 1) * nrhs), hn(nrhs);
+  for (int j = 0; j < m && active; j++) {
     // W = A [v_j of every column]; v_{j+1} = M^{-1} W
     K(pla_k_residual(n, n, nrhs, A, lda, vcol(0, j), ldv, nullptr, n, W, n, 0, work, stream()));
     rc = precond(F, W, n, vcol(0, j + 1), ldv, nrhs, t32);
     if (rc) return rc;
-    // CGS2 against v_0 .. v_j, per active column
+    // CGS2 against v_0 .. v_j: one launch for the coefficients of every
+    // active column, one read-back, one launch for the updates
     std::fill(hsum.begin(), hsum.end(), 0.0);
     for (int pass = 0; pass < 2; pass++) {
-      for (int s = 0; s < nrhs; s++)
-        if (active[s])
-          K(pla_k_gemv(MPI_DOUBLE, PLA_TRANSPOSE, n, j + 1, 1.0, vcol(s, 0), n, vcol(s, j + 1),
-                       0.0, tmp + (size_t)s * (m + 1), stream()));
+      K(pla_k_basis_dots(n, nrhs, V, ldv, 0, j + 1, j + 1, active, tmp, m + 1, stream()));
       PLA_CUDA(cudaMemcpyAsync(hp.data(), tmp, hp.size() * sizeof(double), cudaMemcpyDeviceToHost,
                                stream()));
       PLA_CUDA(cudaStreamSynchronize(stream()));
-      for (int s = 0; s < nrhs; s++) {
-        if (!active[s]) continue;
-        // tmp still holds the coefficients on the device
-        K(pla_k_gemv(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, j + 1, -1.0, vcol(s, 0), n,
-                     tmp + (size_t)s * (m + 1), 1.0, vcol(s, j + 1), stream()));
-        for (int i = 0; i <= j; i++) hsum[(size_t)s * (m + 1) + i] += hp[(size_t)s * (m + 1) + i];
-      }
+      // tmp still holds the coefficients on the device
+      K(pla_k_basis_update(n, nrhs, V, ldv, j + 1, j + 1, tmp, m + 1, active, stream()));
+      for (int s = 0; s < nrhs; s++)
+        if ((active >> s) & 1u)
+          for (int i = 0; i <= j; i++) hsum[(size_t)s * (m + 1) + i] += hp[(size_t)s * (m + 1) + i];
     }
-    cols.clear();
-    std::vector<int> who;
-    for (int s = 0; s < nrhs; s++)
-      if (active[s]) {
-        cols.push_back(vcol(s, j + 1));
-        who.push_back(s);
-      }
-    std::vector<double> hn;
-    rc = col_norms(n, cols, tmp, hn);
-    if (rc) return rc;
-    for (size_t q = 0; q < who.size(); q++) {
-      const int s = who[q];
+    K(pla_k_basis_dots(n, nrhs, V, ldv, j + 1, 1, j + 1, active, tmp, 1, stream()));
+    PLA_CUDA(cudaMemcpyAsync(hn.data(), tmp, nrhs * sizeof(double), cudaMemcpyDeviceToHost,
+                             stream()));
+    PLA_CUDA(cudaStreamSynchronize(stream()));
+    unsigned next = active;
+    for (int s = 0; s < nrhs; s++) {
+      sc[s] = 1.0;
+      if (!((active >> s) & 1u)) continue;
+      const double h1 = std::sqrt(hn[s]);
       double *Hs = H.data() + hm * s, *gs = g.data() + (size_t)s * (m + 1);
       double *css = cs.data() + (size_t)s * m, *sns = sn.data() + (size_t)s * m;
       for (int i = 0; i <= j; i++) Hs[i + (size_t)j * (m + 1)] = hsum[(size_t)s * (m + 1) + i];
-      Hs[j + 1 + (size_t)j * (m + 1)] = hn[q];
-      if (hn[q] > 0) K(pla_k_scal(MPI_DOUBLE, n, 1, 1.0 / hn[q], vcol(s, j + 1), n, stream()));
+      Hs[j + 1 + (size_t)j * (m + 1)] = h1;
+      if (h1 > 0) sc[s] = 1.0 / h1;
       for (int i = 0; i < j; i++) {
         const double a = Hs[i + (size_t)j * (m + 1)], b = Hs[i + 1 + (size_t)j * (m + 1)];
         Hs[i + (size_t)j * (m + 1)] = css[i] * a + sns[i] * b;
@@ -551,11 +531,10 @@ int gmres_block(const Factor &F, const double *A, long lda, const double *R, dou
       gs[j + 1] = -sns[j] * gs[j];
       gs[j] = css[j] * gs[j];
       jend[s] = j + 1;
-      if (std::fabs(gs[j + 1]) <= tau * beta[s] || hn[q] == 0) {
-        active[s] = 0;
-        nact--;
-      }
+      if (std::fabs(gs[j + 1]) <= tau * beta[s] || h1 == 0) next &= ~(1u << s);
     }
+    K(pla_k_basis_scale(n, nrhs, V, ldv, j + 1, sc.data(), active, stream()));
+    active = next;
   }
   // y_s = H_s \ g_s; D(:, s) = V_s y_s
   std::vector<double> y((size_t)(m + 1) * nrhs, 0.0);
