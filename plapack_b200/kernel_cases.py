@@ -164,6 +164,31 @@ def case_trsv(torch, lib, a):
             "algorithmic_bytes": byt, "gbs": byt / t / 1e9}
 
 
+def case_trsv_multi(torch, lib, a):
+    """pla_k_trsv_ticket_multi: --k right-hand sides (at most 16) in one launch."""
+    n, nrhs = a.n, min(a.k, 16)
+    ld = (n + 31) // 32 * 32
+    M = torch.randn(n, ld, device="cuda") * 0.01
+    M.diagonal()[:n] += 1.0
+    ldd = (n + 127) // 128 * 128
+    Dinv = torch.zeros(128, ldd, device="cuda")
+    B = torch.randn(nrhs, n, device="cuda")
+    X = torch.empty_like(B)
+    st = torch.zeros(4, dtype=torch.int32, device="cuda")
+    inv = _fn(lib, "pla_k_trsv_inv_blocks", [i32, ch, ch, ch, i32, vp, lg, vp, lg, vp])
+    assert inv(pla.MPI_FLOAT, b"L", b"N", b"U", n, M.data_ptr(), ld, Dinv.data_ptr(), ldd, None) == 0
+    g = _fn(lib, "pla_k_trsv_ticket_multi", [ch, ch, i32, i32, vp, lg, vp, lg, vp, lg, vp, lg, vp,
+                                             vp])
+    t = _time(torch, lambda: g(b"L", b"N", n, nrhs, M.data_ptr(), ld, Dinv.data_ptr(), ldd,
+                               B.data_ptr(), n, X.data_ptr(), n, st.data_ptr(), None),
+              a.warmup, a.reps)
+    assert st[0].item() == 0
+    byt = 4.0 * n * n / 2 + 2 * 4.0 * n * nrhs
+    return {"case": f"single-launch unit-lower triangular solve, n={n}, {nrhs} rhs (fp32 factor)",
+            "s": t, "algorithmic_bytes": byt, "gbs": byt / t / 1e9,
+            "gflops": 2.0 * n * n / 2 * nrhs / t / 1e9}
+
+
 def case_residual(torch, lib, a):
     n = a.n
     A = torch.randn(n, n, dtype=torch.float64, device="cuda")
