@@ -189,6 +189,35 @@ def case_trsv_multi(torch, lib, a):
             "gflops": 2.0 * n * n / 2 * nrhs / t / 1e9}
 
 
+def case_basis(torch, lib, a):
+    """The lockstep GMRES's batched basis kernels at --n rows, --k columns (at
+    most 16) and --count basis vectors: CGS coefficients, update, norms, scale."""
+    n, nrhs, j = a.n, min(a.k, 16), min(a.count, 30)
+    m = 30
+    ldv = n * (m + 1)
+    V = torch.randn(nrhs, m + 1, n, dtype=torch.float64, device="cuda")
+    tmp = torch.zeros(nrhs * (m + 1), dtype=torch.float64, device="cuda")
+    dots = _fn(lib, "pla_k_basis_dots", [i32, i32, vp, lg, i32, i32, i32, ctypes.c_uint, vp, i32,
+                                         vp])
+    upd = _fn(lib, "pla_k_basis_update", [i32, i32, vp, lg, i32, i32, vp, i32, ctypes.c_uint, vp])
+    scl = _fn(lib, "pla_k_basis_scale", [i32, i32, vp, lg, i32, ctypes.POINTER(ctypes.c_double),
+                                         ctypes.c_uint, vp])
+    active = (1 << nrhs) - 1
+    scales = (ctypes.c_double * 16)(*([0.5] * 16))
+
+    def one_pass():
+        dots(n, nrhs, V.data_ptr(), ldv, 0, j, j, active, tmp.data_ptr(), m + 1, None)
+        upd(n, nrhs, V.data_ptr(), ldv, j, j, tmp.data_ptr(), m + 1, active, None)
+        dots(n, nrhs, V.data_ptr(), ldv, j, 1, j, active, tmp.data_ptr(), 1, None)
+        return scl(n, nrhs, V.data_ptr(), ldv, j, scales, active, None)
+
+    t = _time(torch, one_pass, a.warmup, a.reps)
+    byt = 8.0 * n * nrhs * (2 * (j + 1) + j + 3)   # dots, update (read j, r/w one), norms, scale
+    return {"case": f"GMRES basis kernels, n={n}, {nrhs} columns, {j} basis vectors: one CGS "
+                    "pass + norms + scale", "s": t, "algorithmic_bytes": byt,
+            "gbs": byt / t / 1e9}
+
+
 def case_residual(torch, lib, a):
     n = a.n
     A = torch.randn(n, n, dtype=torch.float64, device="cuda")
