@@ -454,7 +454,8 @@ def run_mixed_sweep(torch, pla, lib, s, device, stream, a, n, args, params):
                                              5: "fp8"}.get(rep.precision_used),
                           "factorizations": rep.factorizations,
                           "converged": rep.converged, "iterations": rep.iterations,
-                          "gmres_iterations": rep.inner_iterations})
+                          "gmres_iterations": rep.inner_iterations,
+                          "factor_ms": rep.factor_ms, "refine_ms": rep.refine_ms})
         out.append(entry)
         s.free(bo, piv)
         del T, X, Bm, Bc, Xh, R

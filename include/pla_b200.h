@@ -81,13 +81,13 @@ typedef struct {
   int max_iterations;   /* outer refinement steps (default 50)              */
   int gmres_restart;    /* inner GMRES iterations per step (default 30)     */
   int nb;               /* block size of the low-precision factorization; 0 = nb_alg */
-  int escalate;         /* 1 (default): when the refinement stagnates (less than
-                           a halving of the backward error twice in a row, a
-                           non-finite iterate, max_iterations reached) or the
-                           low-precision Cholesky breaks down, refactor one
-                           precision higher (FP8 -> BF16, BF16/FP16 -> FP32
-                           -> FP64) and
-                           continue from the current iterate                 */
+  int escalate;         /* 1 (default): when the refinement stagnates (a GMRES-IR
+                           step, or two LU-IR steps in a row, that fail to halve
+                           the backward error; a non-finite iterate;
+                           max_iterations reached) or the low-precision
+                           Cholesky breaks down, refactor one precision higher
+                           (FP8 -> BF16 -> FP64; FP16 -> FP64; FP32 -> FP64)
+                           and continue from the current iterate             */
   double tol;           /* target backward error; <= 0 selects n * 2^-53    */
 } PLA_Mixed_params;
 

@@ -277,7 +277,9 @@ int factor_fp64(Factor &F, const double *A, long lda, int *info) {
   F.a64 = (double *)scratch(kSlotA64, (size_t)F.ld * n * sizeof(double));
   if (!F.a64) PLA_FAIL("cannot allocate the FP64 factors");
   K(pla_k_copy(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, n, A, lda, F.a64, F.ld, stream()));
-  const int nb = 128;
+  // the block size the FP64 loops run fastest at (512-wide DMMA updates at
+  // large n); the low-precision nb does not carry over
+  const int nb = n >= 8192 ? 512 : 128;
   if (F.kind == 0) return lu_on_device(MPI_DOUBLE, n, n, (char *)F.a64, F.ld, F.piv, nb, info);
   return chol_on_device(MPI_DOUBLE, n, (char *)F.a64, F.ld, nb, info);
 }
@@ -759,12 +761,18 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
   return PLA_SUCCESS;
 }
 
-// the next precision up when the refinement stagnates (0: none left)
+// the next precision up when the refinement stagnates (0: none left).  BF16
+// and FP16 go straight to FP64: fp32 has no tensor-core path of fp32
+// accuracy, and the FP64 factorization on the DMMA pipe is the faster of the
+// two here (n = 32768 LU: 0.8 s FP64 against 1.1 s fp32; n = 49152
+// Cholesky: 1.6 s against 1.7 s), besides needing a step or two of
+// refinement where fp32 factors at kappa = 1e10 needed over a hundred GMRES
+// iterations.  FP32 factors stay available on request.
 int escalated(int prec) {
   switch (prec) {
     case PLA_B200_PREC_FP8: return PLA_B200_PREC_BF16;
     case PLA_B200_PREC_BF16:
-    case PLA_B200_PREC_FP16: return PLA_B200_PREC_FP32;
+    case PLA_B200_PREC_FP16:
     case PLA_B200_PREC_FP32: return PLA_B200_PREC_FP64;
     default: return 0;
   }
@@ -913,6 +921,11 @@ int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
     }
     std::vector<double> eta;
     double prev = std::numeric_limits<double>::infinity();
+    // A GMRES-IR step that fails to halve the backward error has run a full
+    // restart cycle without converging: at that rate the remaining steps cost
+    // more than refactoring one precision up, so one such step escalates.
+    // Classic LU-IR steps are cheap (one residual and one solve) and get two.
+    const int slow_limit = p.refinement == PLA_B200_IR_GMRES ? 1 : 2;
     int slow = 0, it = 0;
     bool stalled = false;
     for (;; it++) {
@@ -934,7 +947,7 @@ int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
       }
       slow = worst > 0.5 * prev ? slow + 1 : 0;
       prev = worst;
-      if (it >= p.max_iterations || (p.escalate && slow >= 2)) {
+      if (it >= p.max_iterations || (p.escalate && slow >= slow_limit)) {
         stalled = true;
         break;
       }

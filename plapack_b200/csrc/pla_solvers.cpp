@@ -282,7 +282,7 @@ int trsm_right_lower_t(int dt, int b, int rest, const char *L11, long lda, char 
 int chol_device(int dt, int n, char *A, long lda, int nb, Status *st) {
   const int es = dt == MPI_DOUBLE ? 8 : 4;
   auto at = [&](long i, long j) { return A + (i + j * lda) * es; };
-  nb = std::min(nb, 2 * kTri);  // a block column of up to 256, factored in steps of <= 128
+  nb = std::min(nb, 4 * kTri);  // a block column of up to 512, factored in steps of <= 128
   PLA_Phase_times &ph = state().phases;
   const bool la = n >= 4 * nb;
   cudaStream_t s0 = stream(), s1 = la ? lookahead_stream() : s0;

@@ -148,6 +148,29 @@ def test_chol_golden(pla_session, golden, restated):
         s.free(a)
 
 
+@pytest.mark.parametrize("n,nb", [(2600, 512), (2100, 384)])
+def test_chol_wide_block_columns(pla_session, restated, n, nb):
+    """Block columns of 384 and 512 (factored in 128-column steps, with the
+    lookahead on) against the restated PLA_Chol at the same nb_alg, and the
+    failing column of an indefinite matrix."""
+    from plapack_b200 import pla
+    s = pla_session
+    rng = np.random.default_rng(nb)
+    G = rng.standard_normal((n, n))
+    A = np.asfortranarray(G @ G.T / n + np.eye(n))
+    s.set_nb_alg(nb)
+    a = s.matrix(n, n)
+    s.put(a, A)
+    assert pla.check(s.lib.PLA_Chol(pla.PLA_LOWER_TRIANGULAR, a), "PLA_Chol") == 0
+    Lo, info = restated.chol_blocked(A, nb)
+    assert info == 0
+    assert np.abs(np.tril(s.get(a)) - np.tril(Lo)).max() <= tol_factor(A, Lo)
+    A[n - 700, n - 700] = -1.0                 # indefinite at 1-based column n - 699
+    s.put(a, A)
+    assert s.lib.PLA_Chol(pla.PLA_LOWER_TRIANGULAR, a) == restated.chol_blocked(A, nb)[1]
+    s.free(a)
+
+
 def test_general_and_pos_def_solve_golden(pla_session, golden, restated):
     from plapack_b200 import pla
     manifest, arrays = golden
