@@ -124,51 +124,63 @@ trsm_right_k(int b, int nrows, T alpha, const T *Tg, long ldt, T *B, long ldb, b
   }
 }
 
-// Cholesky of the b x b lower block: column k gets a(k:b,k) -= A(k:b,0:k) a(k,0:k)'
-// (dgemv), fails when a(k,k) <= 0, then a(k,k) = sqrt and the column below is
-// scaled by the reciprocal.  Only the lower triangle is read or written.
+// Cholesky of the b x b lower block (SOLVERS/Cholesky/PLA_Local_chol.c:114-138):
+// column k fails when a(k,k) <= 0, then a(k,k) = sqrt and the column below is
+// scaled by the reciprocal.  The reference's column k is left-looking,
+// a(k:b,k) -= A(k:b,0:k) a(k,0:k)' as one dgemv; here the same products are
+// applied right-looking, step l subtracting l(i,l) l(j,l) from every a(i,j)
+// with l < j <= i.  Each element receives the same fma in the same order
+// (l = 0, 1, ...), so the result is bitwise that of the left-looking loop,
+// but a step is independent per element: the left-looking form serialised
+// each thread on a chain of k dependent shared-memory loads and took 219 us
+// for b = 128 (FP64).  Thread t owns row k+1 + (t mod 128) of the trailing
+// block and every second of its columns.  Only the lower triangle is read or
+// written.
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 potrf_lower_k(int b, T *A, long lda, int *status, int *info, int base) {
+  static_assert(kThreads == 2 * kMaxTri, "two threads per row of the block");
   extern __shared__ __align__(16) unsigned char sm[];
-  __shared__ int s_fail;
+  __shared__ T colk[kMaxTri];  // column k of L, scaled
   if (*status != PLA_K_OK) return;
   T *S = (T *)sm;  // ld = b
-  for (int t = threadIdx.x; t < b * b; t += kThreads) {
+  const int tid = threadIdx.x, half = tid / kMaxTri, ti = tid % kMaxTri;
+  for (int t = tid; t < b * b; t += kThreads) {
     int i = t % b, j = t / b;
     S[t] = i >= j ? A[i + (long)j * lda] : T(0);
   }
-  if (threadIdx.x == 0) s_fail = 0;
   __syncthreads();
+  int fail = 0;
   for (int k = 0; k < b; k++) {
-    for (int i = k + threadIdx.x; i < b; i += kThreads) {
-      T y = S[i + k * b];
-      for (int l = 0; l < k; l++) y = fma(-S[k + l * b], S[i + l * b], y);
-      S[i + k * b] = y;
+    const T d = S[k + k * b];  // every thread reads it: the test below is uniform
+    if (d <= T(0)) {
+      fail = k + 1;
+      break;
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      T d = S[k + k * b];
-      if (d <= T(0)) {
-        s_fail = k + 1;
-      } else {
-        S[k + k * b] = sqrt(d);
-      }
+    const T dk = sqrt(d);
+    const int i = k + 1 + ti;
+    if (half == 0 && i < b) {  // one thread per row scales column k
+      const T l = S[i + k * b] * (T(1) / dk);
+      S[i + k * b] = l;
+      colk[i] = l;
     }
-    __syncthreads();
-    if (s_fail) break;
-    const T inv = T(1) / S[k + k * b];
-    for (int i = k + 1 + threadIdx.x; i < b; i += kThreads) S[i + k * b] *= inv;
-    __syncthreads();
+    __syncthreads();  // d read by all; column k scaled
+    if (tid == 0) S[k + k * b] = dk;
+    if (i < b) {
+      const T lik = colk[i];
+      for (int j = k + 1 + half; j <= i; j += 2)
+        S[i + (long)j * b] = fma(-colk[j], lik, S[i + (long)j * b]);
+    }
+    __syncthreads();  // the trailing block updated; colk free again
   }
-  if (s_fail) {
-    if (threadIdx.x == 0) {
-      *info = base + s_fail;
+  if (fail) {
+    if (tid == 0) {
+      *info = base + fail;
       *status = PLA_K_NOT_SPD;
     }
     return;  // the reference leaves A11 unwritten on failure (PLA_Chol.c:181-185)
   }
-  for (int t = threadIdx.x; t < b * b; t += kThreads) {
+  for (int t = tid; t < b * b; t += kThreads) {
     int i = t % b, j = t / b;
     if (i >= j) A[i + (long)j * lda] = S[t];
   }

@@ -12,6 +12,9 @@ bytes or flops and the rate they imply.
     python -m plapack_b200.kernel_cases trsv --n 32768
     python -m plapack_b200.kernel_cases residual --n 32768
     python -m plapack_b200.kernel_cases batched --count 2000
+    python -m plapack_b200.kernel_cases potrf --k 128 --dtype f64
+    python -m plapack_b200.kernel_cases trsm_small --side R --m 32768 --k 128 --dtype f64
+    python -m plapack_b200.kernel_cases sgemm --m 32768 --n 224 --k 32
 
 The cases mirror the calls the solvers make (the trailing update of one LU
 step, one 32-column sub-panel, the row interchanges of one panel, the
@@ -235,6 +238,87 @@ def case_residual(torch, lib, a):
             "gbs": byt / t / 1e9}
 
 
+def case_potrf(torch, lib, a):
+    """pla_k_potrf_lower on one --k x --k diagonal block (k <= 128): the
+    Cholesky's diagonal factorization, one CTA, latency-bound."""
+    b = a.k
+    dt = pla.MPI_DOUBLE if a.dtype == "f64" else pla.MPI_FLOAT
+    tdt = torch.float64 if a.dtype == "f64" else torch.float32
+    G = torch.randn(b, b, dtype=torch.float64, device="cuda")
+    A0 = (G @ G.t() / b + torch.eye(b, dtype=torch.float64, device="cuda")).to(tdt)
+    A = A0.clone()
+    st = torch.zeros(4, dtype=torch.int32, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    g = _fn(lib, "pla_k_potrf_lower", [i32, i32, vp, lg, vp, vp, i32, vp])
+
+    def launch():
+        A.copy_(A0)
+        return g(dt, b, A.data_ptr(), b, st.data_ptr(), info.data_ptr(), 0, None)
+
+    t = _time(torch, launch, a.warmup, a.reps)
+    assert st[0].item() == 0 and info.item() == 0
+    flops = b ** 3 / 3.0
+    return {"case": f"diagonal block Cholesky {b} x {b} ({a.dtype}), copy of the block included",
+            "s": t, "flops": flops, "gflops": flops / t / 1e9}
+
+
+def case_trsm_small(torch, lib, a):
+    """pla_k_trsm_small as the solvers call it: --side L solves the --k x --n
+    block to the right of a unit-lower --k x --k diagonal block (the LU's
+    sub-panel and U12 solves); --side R solves the --m x --k block column
+    below a lower --k x --k block, A21 inv(L11)' (the Cholesky)."""
+    dt = pla.MPI_DOUBLE if a.dtype == "f64" else pla.MPI_FLOAT
+    tdt = torch.float64 if a.dtype == "f64" else torch.float32
+    es = 8 if a.dtype == "f64" else 4
+    b = a.k
+    L = torch.randn(b, b, dtype=tdt, device="cuda") * 0.05      # column-major b x b
+    L.diagonal().add_(1.0)
+    st = torch.zeros(4, dtype=torch.int32, device="cuda")
+    g = _fn(lib, "pla_k_trsm_small", [i32, ch, ch, ch, ch, i32, i32, f64, vp, lg, vp, lg, vp, vp])
+    if a.side == "L":
+        other = a.n
+        B0 = torch.randn(other, b, dtype=tdt, device="cuda")       # column-major b x other
+        args = (b"L", b"L", b"N", b"U")
+        what = f"unit-lower {b} x {b} solve of a {b} x {other} block (left)"
+        ldb = b
+    else:
+        other = a.m
+        B0 = torch.randn(b, other, dtype=tdt, device="cuda")       # column-major other x b
+        args = (b"R", b"L", b"T", b"N")
+        what = f"A21 inv(L11)' for a {other} x {b} block column (right, lower, transposed)"
+        ldb = other
+    B = B0.clone()
+
+    def launch():
+        B.copy_(B0)
+        return g(dt, *args, b, other, 1.0, L.data_ptr(), b, B.data_ptr(), ldb, st.data_ptr(), None)
+
+    t = _time(torch, launch, a.warmup, a.reps)
+    assert st[0].item() == 0
+    flops = float(b) * b * other
+    byt = 2.0 * b * other * es
+    return {"case": f"{what} ({a.dtype}), copy of the block included", "s": t, "flops": flops,
+            "gflops": flops / t / 1e9, "algorithmic_bytes": byt, "gbs": byt / t / 1e9}
+
+
+def case_sgemm(torch, lib, a):
+    """pla_k_gemm in fp32 as the mixed LU's sub-panel update calls it:
+    C (m x n) -= A (m x k) B (k x n), k = 32."""
+    m, n, k = a.m, a.n, a.k
+    A = torch.randn(k, m, device="cuda")
+    B = torch.randn(n, k, device="cuda")
+    C = torch.randn(n, m, device="cuda")
+    g = _fn(lib, "pla_k_gemm", [i32, i32, i32, i32, i32, i32, f64, vp, lg, vp, lg, f64, vp, lg,
+                                i32, vp, vp])
+    t = _time(torch, lambda: g(pla.MPI_FLOAT, pla.PLA_NO_TRANSPOSE, pla.PLA_NO_TRANSPOSE, m, n, k,
+                               -1.0, A.data_ptr(), m, B.data_ptr(), k, 1.0, C.data_ptr(), m, 0,
+                               None, None), a.warmup, a.reps)
+    flops = 2.0 * m * n * k
+    byt = 4.0 * (2.0 * m * n + m * k + k * n)
+    return {"case": f"fp32 update C -= A B, {m} x {n} x {k}", "s": t,
+            "tflops": flops / t / 1e12, "algorithmic_bytes": byt, "gbs": byt / t / 1e9}
+
+
 def case_batched(torch, lib, a):
     sys.path.insert(0, __import__("os").path.dirname(__import__("os").path.dirname(
         __import__("os").path.abspath(__file__))))
@@ -274,6 +358,7 @@ def main(argv=None):
     p.add_argument("--warmup", type=int, default=2)
     p.add_argument("--reps", type=int, default=3)
     p.add_argument("--ctas", type=int, default=0, help="panel: CTA cap (0: one per SM)")
+    p.add_argument("--side", choices=["L", "R"], default="L", help="trsm_small: side")
     a = p.parse_args(argv)
     import torch
     torch.cuda.set_device(0)

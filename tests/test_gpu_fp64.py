@@ -345,3 +345,50 @@ def test_trsv_single_launch(pla_session, dtype, n):
                                unit_diagonal=diag == pla.PLA_UNIT_DIAG)
         assert np.abs(got - ref).max() <= 64 * n * eps * np.abs(ref).max(), (uplo, trans, diag)
         s.free(a, x)
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+@pytest.mark.parametrize("b", [1, 7, 64, 100, 128])
+def test_potrf_diagonal_block(pla_session, dt, b):
+    """pla_k_potrf_lower, the Cholesky's diagonal-block kernel, against
+    LAPACK's Cholesky; the strict upper triangle is never written; a block
+    that is not positive definite at column c reports base + c and
+    PLA_K_NOT_SPD and leaves the block unwritten (PLA_Chol.c:181-185)."""
+    import torch
+    from plapack_b200 import pla
+    lib = pla_session.lib
+    f = lib.pla_k_potrf_lower
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p,
+                  ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    f.restype = ctypes.c_int
+    mpi = pla.MPI_DOUBLE if dt == np.float64 else pla.MPI_FLOAT
+    rng = np.random.default_rng(b)
+    G = rng.standard_normal((b, b))
+    A = (G @ G.T / b + np.eye(b)).astype(dt)
+    A[np.triu_indices(b, 1)] = 7.0               # the upper triangle must stay as it is
+    lda = b + 3
+    buf = np.full((b, lda), -1.0, dtype=dt)      # column-major b x b, leading dimension lda
+    buf[:, :b] = A.T
+    a = torch.from_numpy(buf).cuda()
+    st = torch.zeros(4, dtype=torch.int32, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert f(mpi, b, a.data_ptr(), lda, st.data_ptr(), info.data_ptr(), 0, None) == 0
+    torch.cuda.synchronize()
+    out = a.cpu().numpy()[:, :b].T
+    assert int(st[0]) == 0 and int(info[0]) == 0
+    Lr = np.linalg.cholesky(np.tril(A).astype(np.float64) + np.tril(A, -1).T)
+    eps = np.finfo(dt).eps
+    assert np.abs(np.tril(out) - Lr).max() <= 8 * b * eps * np.abs(Lr).max()
+    assert np.array_equal(np.triu(out, 1), np.triu(A, 1))
+    assert np.all(a.cpu().numpy()[:, b:] == -1.0)
+    if b < 7:
+        return
+    c = b // 2                                   # make column c + 1 (1-based) fail
+    A2 = A.copy()
+    A2[c, c] = -1.0
+    buf[:, :b] = A2.T
+    a = torch.from_numpy(buf).cuda()
+    assert f(mpi, b, a.data_ptr(), lda, st.data_ptr(), info.data_ptr(), 500, None) == 0
+    torch.cuda.synchronize()
+    assert int(info[0]) == 500 + c + 1 and int(st[0]) != 0
+    assert np.array_equal(a.cpu().numpy()[:, :b].T, A2)
