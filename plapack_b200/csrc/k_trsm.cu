@@ -128,62 +128,120 @@ trsm_right_k(int b, int nrows, T alpha, const T *Tg, long ldt, T *B, long ldb, b
 // column k fails when a(k,k) <= 0, then a(k,k) = sqrt and the column below is
 // scaled by the reciprocal.  The reference's column k is left-looking,
 // a(k:b,k) -= A(k:b,0:k) a(k,0:k)' as one dgemv; here the same products are
-// applied right-looking, step l subtracting l(i,l) l(j,l) from every a(i,j)
-// with l < j <= i.  Each element receives the same fma in the same order
-// (l = 0, 1, ...), so the result is bitwise that of the left-looking loop,
-// but a step is independent per element: the left-looking form serialised
-// each thread on a chain of k dependent shared-memory loads and took 219 us
-// for b = 128 (FP64).  Thread t owns row k+1 + (t mod 128) of the trailing
-// block and every second of its columns.  Only the lower triangle is read or
-// written.
+// applied right-looking, step k subtracting l(j,k) l(i,k) from every a(i,j)
+// with k < j <= i.  Each element receives the same fma in the same order
+// (k = 0, 1, ...), so the result is bitwise that of the left-looking loop.
+//
+// The block lives in registers: thread (tx, ty) of a 16 x 16 grid holds the
+// 8 x 8 elements (tx + 16p, ty + 16q), lower triangle only.  Per column one
+// barrier: the owners of column k (ty = k mod 16) leave its raw values and
+// the diagonal in shared memory (two slots by parity), every thread reads
+// the diagonal, takes the square root and the reciprocal, scales the column
+// values it needs itself (the same multiply the owners keep), and updates its
+// elements; tiles wholly left of or above column k are skipped.  The
+// left-looking form serialised each thread on a chain of dependent
+// shared-memory loads and took 219 us for b = 128 (FP64).
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 potrf_lower_k(int b, T *A, long lda, int *status, int *info, int base) {
-  static_assert(kThreads == 2 * kMaxTri, "two threads per row of the block");
-  extern __shared__ __align__(16) unsigned char sm[];
-  __shared__ T colk[kMaxTri];  // column k of L, scaled
+  static_assert(kThreads == 256 && kMaxTri == 128, "a 16 x 16 grid of 8 x 8 register tiles");
+  __shared__ T col[2][kMaxTri];  // column k before scaling (rows >= k), by parity of k
   if (*status != PLA_K_OK) return;
-  T *S = (T *)sm;  // ld = b
-  const int tid = threadIdx.x, half = tid / kMaxTri, ti = tid % kMaxTri;
-  for (int t = tid; t < b * b; t += kThreads) {
-    int i = t % b, j = t / b;
-    S[t] = i >= j ? A[i + (long)j * lda] : T(0);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  T a[8][8];
+#pragma unroll
+  for (int p = 0; p < 8; p++)
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int i = tx + 16 * p, j = ty + 16 * q;
+      a[p][q] = (i < b && i >= j) ? A[i + (long)j * lda] : T(0);
+    }
+  if (ty == 0) {
+#pragma unroll
+    for (int p = 0; p < 8; p++)
+      if (tx + 16 * p < b) col[0][tx + 16 * p] = a[p][0];
   }
   __syncthreads();
   int fail = 0;
-  for (int k = 0; k < b; k++) {
-    const T d = S[k + k * b];  // every thread reads it: the test below is uniform
-    if (d <= T(0)) {
-      fail = k + 1;
-      break;
+#pragma unroll
+  for (int q = 0; q < 8; q++) {  // columns 16q .. 16q + 15
+    for (int kk = 0; kk < 16; kk++) {
+      const int k = 16 * q + kk;
+      if (k >= b) break;
+      const int par = k & 1;
+      const T d = col[par][k];  // the same value in every thread: the test is uniform
+      if (d <= T(0)) {
+        fail = k + 1;
+        break;
+      }
+      const T dk = sqrt(d);
+      const T inv = T(1) / dk;
+      T li[8], lj[8];
+#pragma unroll
+      for (int p = 0; p < 8; p++) {
+        li[p] = lj[p] = T(0);
+        if (16 * p + 15 <= k) continue;
+        const int i = tx + 16 * p, j = ty + 16 * p;
+        if (i > k && i < b) li[p] = col[par][i] * inv;
+        if (j > k && j < b) lj[p] = col[par][j] * inv;
+      }
+      if (ty == kk) {  // the owners keep column k of L
+#pragma unroll
+        for (int p = 0; p < 8; p++) {
+          const int i = tx + 16 * p;
+          if (i == k) a[p][q] = dk;
+          else if (i > k) a[p][q] = li[p];
+        }
+      }
+      // Tiles wholly at or left of column k are skipped (a test uniform over
+      // the block); only the tile holding column k tests j > k, and only the
+      // diagonal tiles i >= j.  Rows at or past b are never written back, so
+      // they take part without a test.
+#pragma unroll
+      for (int p = 0; p < 8; p++) {
+        if (16 * p + 15 <= k) continue;
+#pragma unroll
+        for (int qq = 0; qq <= p; qq++) {
+          if (16 * qq + 15 <= k) continue;
+          bool ok = qq < p || tx >= ty;
+          if (16 * qq <= k) ok = ok && ty + 16 * qq > k;
+          if (ok) a[p][qq] = fma(-lj[qq], li[p], a[p][qq]);
+        }
+      }
+      // column k + 1 before scaling, and its diagonal, for the next step
+      if (k + 1 < b) {
+        if (kk < 15) {
+          if (ty == kk + 1) {
+#pragma unroll
+            for (int p = 0; p < 8; p++)
+              if (tx + 16 * p > k && tx + 16 * p < b) col[par ^ 1][tx + 16 * p] = a[p][q];
+          }
+        } else if (q + 1 < 8) {
+          if (ty == 0) {
+#pragma unroll
+            for (int p = 0; p < 8; p++)
+              if (tx + 16 * p > k && tx + 16 * p < b) col[par ^ 1][tx + 16 * p] = a[p][q + 1];
+          }
+        }
+      }
+      __syncthreads();
     }
-    const T dk = sqrt(d);
-    const int i = k + 1 + ti;
-    if (half == 0 && i < b) {  // one thread per row scales column k
-      const T l = S[i + k * b] * (T(1) / dk);
-      S[i + k * b] = l;
-      colk[i] = l;
-    }
-    __syncthreads();  // d read by all; column k scaled
-    if (tid == 0) S[k + k * b] = dk;
-    if (i < b) {
-      const T lik = colk[i];
-      for (int j = k + 1 + half; j <= i; j += 2)
-        S[i + (long)j * b] = fma(-colk[j], lik, S[i + (long)j * b]);
-    }
-    __syncthreads();  // the trailing block updated; colk free again
+    if (fail) break;
   }
   if (fail) {
-    if (tid == 0) {
+    if (threadIdx.x == 0) {
       *info = base + fail;
       *status = PLA_K_NOT_SPD;
     }
     return;  // the reference leaves A11 unwritten on failure (PLA_Chol.c:181-185)
   }
-  for (int t = tid; t < b * b; t += kThreads) {
-    int i = t % b, j = t / b;
-    if (i >= j) A[i + (long)j * lda] = S[t];
-  }
+#pragma unroll
+  for (int p = 0; p < 8; p++)
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int i = tx + 16 * p, j = ty + 16 * q;
+      if (i < b && i >= j) A[i + (long)j * lda] = a[p][q];
+    }
 }
 
 int g_sms = 0;
@@ -242,13 +300,9 @@ extern "C" int pla_k_potrf_lower(int dt, int b, void *A, long lda, int *status, 
   if (b <= 0) return 0;
   if (b > kMaxTri) return (int)cudaErrorInvalidValue;
   if (dt == MPI_DOUBLE) {
-    size_t sm = (size_t)b * b * sizeof(double);
-    cudaFuncSetAttribute(potrf_lower_k<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    potrf_lower_k<double><<<1, kThreads, sm, s>>>(b, (double *)A, lda, status, info, base);
+    potrf_lower_k<double><<<1, kThreads, 0, s>>>(b, (double *)A, lda, status, info, base);
   } else if (dt == MPI_FLOAT) {
-    size_t sm = (size_t)b * b * sizeof(float);
-    cudaFuncSetAttribute(potrf_lower_k<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    potrf_lower_k<float><<<1, kThreads, sm, s>>>(b, (float *)A, lda, status, info, base);
+    potrf_lower_k<float><<<1, kThreads, 0, s>>>(b, (float *)A, lda, status, info, base);
   } else {
     return (int)cudaErrorInvalidValue;
   }
