@@ -258,6 +258,26 @@ def test_kappa_1e10_escalates_to_fp64_backward_error(env, prec):
     assert fwd <= 1e10 * n * 2.0 ** -53, fwd
 
 
+@pytest.mark.parametrize("refinement,max_steps", [(1, 2), (2, 1)])
+def test_stagnation_rule_per_refinement(env, refinement, max_steps):
+    """How many non-halving steps escalate: one GMRES-IR step (a whole restart
+    cycle), two classic LU-IR steps.  kappa = 1e10 stagnates at once with fp16
+    factors, so the fp16 attempt ends after max_steps corrections and FP64
+    factors finish the solve."""
+    s, torch, pla = env
+    n = 1024
+    A = c3_matrix(n, 1e10, 17)
+    B = A @ np.random.default_rng(18).standard_normal((n, 1))
+    rc, X, rep = solve_mixed_params(s, pla, A, B, "lu", precision=2, refinement=refinement)
+    assert rc == 0 and rep.converged == 1
+    assert rep.precision_used == pla.PLA_B200_PREC_FP64 and rep.factorizations == 2
+    # the fp16 attempt takes at most max_steps corrections, FP64 factors a few
+    assert rep.iterations <= max_steps + 3, rep.iterations
+    if refinement == 2:  # one restart cycle of fp16 GMRES (30), then short FP64 cycles
+        assert rep.inner_iterations <= 30 + 10, rep.inner_iterations
+    assert backward_error(A, X, B) <= n * 2.0 ** -53
+
+
 def test_no_escalation_reports_stagnation(env):
     s, torch, pla = env
     n = 1024
