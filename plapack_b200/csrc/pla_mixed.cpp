@@ -581,8 +581,19 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
   const int kprec = F.prec == PLA_B200_PREC_BF16 ? PLA_K_BF16 : PLA_K_FP16;
   const int esz = f8 ? 1 : 2;
   const int nsteps = (n + nb - 1) / nb;
-  const int gcols = std::max(nb, (n / 8 + nb - 1) / nb * nb);  // about 8 groups
-  const int ngroups = (n + gcols - 1) / gcols;
+  // Groups of about n / 8 columns; the first is split into 4 nb, 4 nb and
+  // the rest, so the first steps start after a few milliseconds of copying
+  // rather than after an eighth of the whole copy.  Boundaries are multiples
+  // of nb.
+  const int gcols = std::max(nb, (n / 8 + nb - 1) / nb * nb);
+  std::vector<int> gb{0};
+  if (gcols >= 16 * nb) {
+    gb.push_back(4 * nb);
+    gb.push_back(8 * nb);
+  }
+  for (int c = gcols; c < n; c += gcols) gb.push_back(c);
+  gb.push_back(n);
+  const int ngroups = (int)gb.size() - 1;
   const int tiles = (n + 127) / 128 + 1;
   // per-step storage
   std::vector<size_t> loff(nsteps);
@@ -623,7 +634,7 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
 
   // 1. the copies and conversions, group by group, on the copy stream
   for (int g = 0; g < ngroups; g++) {
-    const long c0 = (long)g * gcols, nc = std::min<long>(gcols, n - c0);
+    const long c0 = gb[g], nc = gb[g + 1] - gb[g];
     PLA_CUDA(cudaMemcpy2DAsync(Ad + c0 * lda, lda * sizeof(double), Ah + c0 * ldh,
                                ldh * sizeof(double), (size_t)n * sizeof(double), nc,
                                cudaMemcpyHostToDevice, sc));
@@ -714,11 +725,13 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
     if (k > 0) PLA_CUDA(cudaStreamWaitEvent(s0, ev_panel, 0));
     if (k >= 2) PLA_CUDA(cudaEventSynchronize(thr[(k - 2) % 4]));
     // groups through the one holding block k+1 must take part now
-    const int need = (int)((std::min<long>(n, (long)(k + 2) * nb) + gcols - 1) / gcols);
+    const int upto = (int)std::min<long>(n, (long)(k + 2) * nb);
+    int need = 0;
+    while (gb[need] < upto) need++;
     const int was = known;
     PK(poll(need));
     for (int g = was; g < known; g++) {  // replay the steps a new group missed
-      const int g0 = g * gcols, g1 = std::min(n, g0 + gcols);
+      const int g0 = gb[g], g1 = gb[g + 1];
       for (int s2 = applied[g]; s2 < k; s2++) {
         const int c0 = std::max(g0, (s2 + 1) * nb);
         PK(prep(s2, c0, g1));
@@ -726,7 +739,7 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
       }
       applied[g] = k;
     }
-    const int kc = std::min(n, known * gcols);  // columns that take part
+    const int kc = gb[known];  // columns that take part
     if (rest > 0) {
       PK(prep(k, k0 + b, kc));
       const int b2 = std::min(nb, rest);

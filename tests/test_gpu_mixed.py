@@ -425,7 +425,7 @@ def test_fp8_lu_ir(env):
     assert backward_error(A, X, B) <= n * 2.0 ** -53
 
 
-@pytest.mark.parametrize("prec,nb", [(2, 256), (5, 128)])
+@pytest.mark.parametrize("prec,nb", [(2, 256), (5, 128), (2, 64)])   # 64: split first group
 def test_streamed_solve_from_host(env, prec, nb):
     """PLA_General_solve_mixed_host copies A from host memory while the
     factorization runs: FP64 backward error, A copied into the device object,
