@@ -800,7 +800,8 @@ def run_ours(args):
                                       ("panel_ms", "trsm_ms", "update_ms", "solve_ms")},
                 "backward_error": (rc.abs().max() / (s_inf * x.abs().max() + bs.abs().max())).item()}
         # ---- out-of-core Cholesky (PLA_OOC_Chol) of the same S from a file in host memory ----
-        if not args.skip_ooc:
+        # one GPU only: N replicas would each keep an 8.6 GB file in the host's memory
+        if not args.skip_ooc and world == 1:
             ooc = run_ooc_chol(torch, pla, lib, s, device, S, a, n, args, chol["chol_factor_s"])
         del S, bs, xs, rc
         torch.cuda.empty_cache()
