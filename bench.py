@@ -824,11 +824,19 @@ def run_ours(args):
     # ---- end to end: host buffers in, host solution out ----
     e2e = None
     if not args.skip_e2e:
-        Th = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+        # page-locked host buffers (8.6 GB per rank); should the host refuse to
+        # lock that much (N replicas on one node), pageable memory still works:
+        # the copy of A then completes before the factorization starts
+        try:
+            Th = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+            pinned = True
+        except RuntimeError:
+            Th = torch.empty((n, n), dtype=torch.float64)
+            pinned = False
         Th.copy_(T)
-        bh = torch.empty((n, 1), dtype=torch.float64, pin_memory=True)
+        bh = torch.empty((n, 1), dtype=torch.float64, pin_memory=pinned)
         bh.copy_(b)
-        xh = torch.empty((n, 1), dtype=torch.float64, pin_memory=True)
+        xh = torch.empty((n, 1), dtype=torch.float64, pin_memory=pinned)
         NT = pla.PLA_NO_TRANSPOSE
 
         def e2e_step():
@@ -854,6 +862,7 @@ def run_ours(args):
                "path": "PLA_Obj_set_local_contents (b, pinned host) -> "
                        "PLA_General_solve_mixed_host (A from pinned host, copied during the "
                        "factorization) -> PLA_Obj_get_local_contents",
+               "pinned": max_over_ranks(0.0 if pinned else 1.0) == 0.0,
                "factor_ms": report.factor_ms, "refine_ms": report.refine_ms}
         del Th
 
