@@ -16,10 +16,13 @@ solution read back through PLA_Obj_get_local_contents, every step.
 
 --impl reference times the upstream PLAPACK (compiled from its sources into
 oracle/_ref, linked to a threaded OpenBLAS) on the host cores: PLA_General_solve
-on a bounded sample of the same matrix family, scaled to n = 32768 by n^3.
+on the n = 32768 system of the same family itself (minutes per solve, so
+--ref-steps solves, default 1, whatever --steps asks; the line reports the
+count it timed).  `cpu_baseline` of this arm is the same measurement.
 
 Under torchrun (--gpus N > 1) every rank solves its own system (replicas; the
-path has no data exchange) and rank 0 prints the max over ranks.
+single large solve has no data exchange) and rank 0 prints the max over ranks;
+the batched sub-arm shards its instances across the ranks instead.
 """
 from __future__ import annotations
 
@@ -38,12 +41,14 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from plapack_b200.workloads import (batched_backward_error, batched_orders,  # noqa: E402
+                                    batched_workload, c3_device, c3_host, spd_device)
+
 METRIC = "n=32768 solve time: mixed-prec LU-IR vs FP64 LU, same B200, both at FP64 bkwd err"
 # DRAM bytes (read + write) of one tensor-core update launch as a fraction of
-# its algorithmic bytes: 486.5 MB measured against 545.3 MB for the
-# M = N = 8192, K = 256 launch captured by ncu
-# (profiles/tc_update_k_fp16_fp8_8192_k256.md).  Below 1 because the last C
-# tiles written are still dirty in L2 when the launch ends.
+# its algorithmic bytes: 486.5 MB measured by ncu against 545.3 MB for an
+# M = N = 8192, K = 256 fp16 launch.  Below 1 because the last C tiles written
+# are still dirty in L2 when the launch ends.
 TC_UPDATE_TRAFFIC_RATIO = 486.5 / 545.3
 
 
@@ -75,43 +80,9 @@ def parse():
     p.add_argument("--skip-chol-mixed", action="store_true",
                    help="skip the fp8 / bf16 Cholesky-IR at --chol-n")
     p.add_argument("--chol-n", type=int, default=49152)
-    p.add_argument("--cpu-seconds", type=float, default=12.0,
-                   help="target length of one reference sample on the host")
+    p.add_argument("--ref-steps", type=int, default=1,
+                   help="timed upstream solves at n on the host (reference arm and cpu_baseline)")
     return p.parse_args()
-
-
-# ----------------------------------------------------------------- inputs ---
-def c3_device(n, kappa, seed, torch, device):
-    """Column-major A = U diag(sigma) V' as the memory of a row-major tensor T
-    (T = A'), built by 16 seeded Householder reflections of diag(sigma)."""
-    g = torch.Generator(device=device).manual_seed(seed)
-    sigma = kappa ** (-torch.arange(n, dtype=torch.float64, device=device) / max(n - 1, 1))
-    T = torch.diag(sigma)
-    for _ in range(8):                      # T <- H T
-        v = torch.randn(n, dtype=torch.float64, device=device, generator=g)
-        w = v @ T
-        T.addr_(v, w, alpha=-2.0 / float(v @ v))
-    for _ in range(8):                      # T <- T H
-        v = torch.randn(n, dtype=torch.float64, device=device, generator=g)
-        w = T @ v
-        T.addr_(w, v, alpha=-2.0 / float(v @ v))
-    x = torch.randn(n, 1, dtype=torch.float64, device=device, generator=g)
-    b = T.t() @ x                            # b = A x_true
-    return T, x, b
-
-
-def c3_host(n, kappa, seed):
-    rng = np.random.default_rng(seed)
-    sigma = kappa ** (-np.arange(n) / max(n - 1, 1))
-    A = np.diag(sigma)
-    for _ in range(8):
-        v = rng.standard_normal(n)
-        A -= (2.0 / (v @ v)) * np.outer(v, v @ A)
-    for _ in range(8):
-        v = rng.standard_normal(n)
-        A -= (2.0 / (v @ v)) * np.outer(A @ v, v)
-    x = rng.standard_normal((n, 1))
-    return np.asfortranarray(A), x, A @ x
 
 
 # --------------------------------------------------------------- helpers ---
@@ -202,42 +173,47 @@ def cpu_cores():
 
 
 # ----------------------------------------------------- reference (CPU) arm ---
-def reference_sample(n_full, kappa, target_s, steps=1, warmup=0):
-    """Time the upstream PLA_General_solve on the host cores on a bounded sample
-    and scale its time to n_full by n^3.  Returns (seconds at n_full, info)."""
+def reference_solve(n, kappa, steps=1, seed=12, warmup_n=2048):
+    """Time the upstream PLA_General_solve (PLA_LU + PLA_Trsv, nb_alg = 128,
+    error checking off, OpenBLAS on every host core) on the n x n system of
+    the headline family itself, bracketed by MPI_Wtime around the call as
+    TEST/test_lu.c:136-142 brackets PLA_LU.  One warm-up solve at warmup_n
+    first (thread pool, page faults), then `steps` timed solves at n.
+    Returns the contract's cpu_baseline dict (value = median seconds)."""
     cores = cpu_cores()
     os.environ.setdefault("OPENBLAS_NUM_THREADS", str(cores))
+    threads = int(os.environ["OPENBLAS_NUM_THREADS"])
     from oracle import oracle as orc
     ref = orc.Reference("openblas", nb_distr=128, nb_alg=128, error_checking=0)
-    # probe the rate on a small case, then size the sample to ~target_s
-    A, _, b = c3_host(2048, kappa, 11)
-    t0 = time.perf_counter()
+    A, _, b = c3_host(warmup_n, kappa, 11)
     ref.general_solve(A, b)
-    rate = (2 / 3 * 2048 ** 3) / max(time.perf_counter() - t0, 1e-3)
-    n_s = int((target_s * rate * 1.5) ** (1 / 3)) // 512 * 512
-    n_s = max(2048, min(n_s, n_full))
-    A, x_true, b = c3_host(n_s, kappa, 12)
-    times = []
-    for i in range(warmup + steps):
-        t0 = time.perf_counter()
+    t0 = time.perf_counter()
+    A, x_true, b = c3_host(n, kappa, seed)
+    gen_s = time.perf_counter() - t0
+    times, X = [], None
+    for _ in range(max(1, steps)):
         _, X, _, ret, t_inner = ref.general_solve(A, b)
-        wall = time.perf_counter() - t0
-        if i >= warmup:
-            times.append(t_inner if t_inner > 0 else wall)
+        times.append(t_inner)
     t = statistics.median(times)
-    scaled = t * (n_full / n_s) ** 3
-    resid = b - A @ X
-    eta = float(np.abs(resid).max() / (np.abs(A).sum(axis=1).max() * np.abs(X).max() + np.abs(b).max()))
-    info = {"value": scaled, "unit": "s", "cores": int(os.environ["OPENBLAS_NUM_THREADS"]),
-            "kind": "reference",
-            "sample": (f"upstream PLA_General_solve (PLA_LU nb_alg=128 + PLA_Trsv, FP64, 1x1 "
-                       f"template, OpenBLAS 0.3.15, {os.environ['OPENBLAS_NUM_THREADS']} threads) "
-                       f"on the same matrix family at n={n_s}: {t:.3f} s, scaled by "
-                       f"(32768/{n_s})^3; backward error {eta:.2e}")}
-    return scaled, info
+    a_inf = float(np.abs(A).sum(axis=1).max())
+    eta = float(np.abs(b - A @ X).max() / (a_inf * np.abs(X).max() + np.abs(b).max()))
+    fwd = float(np.abs(X - x_true).max() / np.abs(x_true).max())
+    return {"value": t, "unit": "s", "cores": threads, "kind": "reference",
+            "steps": len(times), "warmup": 1,
+            "sample": (f"the full workload, not a sample: upstream PLA_General_solve (PLA_LU "
+                       f"nb_alg=128 + PLA_Trsv, FP64, 1x1 template, error checking off, "
+                       f"OpenBLAS 0.3.15 with {threads} threads) on the n={n}, "
+                       f"kappa={kappa:g} system, {len(times)} timed solve(s) after one "
+                       f"warm-up at n={warmup_n}; backward error {eta:.2e}, forward error "
+                       f"{fwd:.2e}; matrix built in {gen_s:.1f} s (untimed)"),
+            "backward_error": eta, "forward_error": fwd, "solve_seconds": times}
 
 
 def run_reference(args):
+    """The reference arm: rank 0 solves the headline system on the host cores
+    with the upstream PLAPACK; other ranks exit at once.  A solve at n = 32768
+    takes minutes, so the arm times --ref-steps solves (default 1) whatever
+    --steps asks, and reports the count it actually timed."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -246,11 +222,11 @@ def run_reference(args):
         print(json.dumps({"impl": "reference",
                           "unavailable": "oracle/_ref/libplapack_ref_openblas.so is not built"}))
         return 0
-    per_step = max(3.0, args.cpu_seconds / 2)
-    value, info = reference_sample(args.n, args.kappa, per_step, steps=args.steps,
-                                   warmup=min(args.warmup, 1))
+    info = reference_solve(args.n, args.kappa, steps=args.ref_steps)
+    value = info["value"]
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s",
-           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+           "n_gpus": args.gpus, "steps": info["steps"], "warmup": info["warmup"],
+           "steps_requested": args.steps, "warmup_requested": args.warmup,
            "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded C3 family)",
            "config": {"workload": f"general solve n={args.n}, kappa={args.kappa:g}, 1 rhs",
@@ -262,142 +238,88 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------- our arm ---
-def batched_workload(torch, pla, device, dtype, count, seed):
-    """Independent instances, n log-uniform in [8, 512], even-numbered ones LU
-    on i.i.d. uniform[-1, 1] matrices, odd-numbered ones Cholesky on
-    G G'/n + I (G standard normal), 1-4 right-hand sides each.  Matrices of
-    one order share a tensor; `A0`/`B0` keep copies to restore them."""
-    rng = np.random.default_rng(seed)
-    ns = np.round(np.exp(rng.uniform(np.log(8), np.log(512), count))).astype(int)
-    nrhs = rng.integers(1, 5, count)
-    kinds = np.arange(count) % 2
-    gen = torch.Generator(device=device)
-    gen.manual_seed(seed)
-    es = 8 if dtype == torch.float64 else 4
-    arr = (pla.BatchInstance * count)()
-    groups = []
-    piv = torch.zeros(int(ns.sum()), dtype=torch.int32, device=device)
-    poff = np.concatenate([[0], np.cumsum(ns)[:-1]])
-    flops = 0.0
-    for n in np.unique(ns):
-        n = int(n)
-        idx = np.nonzero(ns == n)[0]
-        lu = idx[kinds[idx] == 0]
-        ch = idx[kinds[idx] == 1]
-        A = torch.empty((len(idx), n, n), dtype=dtype, device=device)
-        if len(lu):
-            A[:len(lu)] = torch.rand((len(lu), n, n), generator=gen, device=device,
-                                     dtype=torch.float64).mul_(2).sub_(1).to(dtype)
-        if len(ch):
-            G = torch.randn((len(ch), n, n), generator=gen, device=device, dtype=torch.float64)
-            S = torch.bmm(G, G.transpose(1, 2)).div_(n)
-            S.diagonal(dim1=1, dim2=2).add_(1.0)
-            A[len(lu):] = S.to(dtype)
-            del G, S
-        B = torch.randn((len(idx), 4, n), generator=gen, device=device,
-                        dtype=torch.float64).to(dtype)
-        order = np.concatenate([lu, ch])
-        for j, k in enumerate(order):
-            k = int(k)
-            arr[k].n, arr[k].nrhs, arr[k].kind = n, int(nrhs[k]), int(kinds[k])
-            arr[k].A = int(A.data_ptr() + j * n * n * es)
-            arr[k].B = int(B.data_ptr() + j * 4 * n * es)
-            arr[k].pivots = ctypes.cast(int(piv.data_ptr() + int(poff[k]) * 4),
-                                        ctypes.POINTER(ctypes.c_int))
-            flops += (2.0 / 3.0 if kinds[k] == 0 else 1.0 / 3.0) * n ** 3 + 2.0 * n * n * nrhs[k]
-        groups.append({"n": n, "order": order, "A": A, "B": B,
-                       "A0": A.clone(), "B0": B.clone()})
-    return arr, groups, piv, flops
-
-
-def batched_backward_error(torch, groups, nrhs_of):
-    """max over instances of ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf),
-    A and b the pristine inputs, x the solution left in B (in float64)."""
-    worst = 0.0
-    for gr in groups:
-        A0 = gr["A0"].double()                 # row-major storage = A' of the column-major A
-        X = gr["B"].double()                   # [cnt, 4, n]: column c of instance j is X[j, c]
-        B0 = gr["B0"].double()
-        R = B0 - torch.bmm(X, A0)              # (A x)' = x' A'
-        mask = torch.tensor([[c < nrhs_of[int(k)] for c in range(4)] for k in gr["order"]],
-                            device=X.device)
-        a_inf = A0.abs().sum(dim=1).max(dim=1).values   # max row sum of A = max col sum of A'
-        num = R.abs().amax(dim=2)
-        den = a_inf[:, None] * X.abs().amax(dim=2) + B0.abs().amax(dim=2)
-        eta = torch.where(mask, num / den, torch.zeros_like(num))
-        worst = max(worst, float(eta.max()))
-    return worst
-
-
-def run_batched(torch, pla, lib, device, stream, dtype, steps, warmup, count=20000, seed=3):
-    arr, groups, piv, flops = batched_workload(torch, pla, device, dtype, count, seed)
-    nrhs_of = [arr[k].nrhs for k in range(count)]
+def run_batched(torch, pla, lib, device, stream, dtype, steps, warmup, dist, count=20000,
+                seed=3):
+    """The batched workload, sharded by instance over the ranks (shard.partition:
+    flop-balanced, the same on every rank); each rank factors and solves its
+    share with one PLA_Batch_plan, the info words are gathered at the end.
+    Time = max over ranks of the device time of one execute."""
+    from plapack_b200 import shard
+    world = dist.get_world_size() if dist is not None else 1
+    rank = dist.get_rank() if dist is not None else 0
+    ns, nrhs, kinds = batched_orders(count, seed)
+    parts = shard.partition(ns.tolist(), kinds.tolist(), nrhs.tolist(), world)
+    total_flops = sum(shard.instance_flops(int(a), int(k), int(r))
+                      for a, k, r in zip(ns, kinds, nrhs))
+    arr, groups, piv, flops, ids = batched_workload(torch, pla, device, dtype, count, seed,
+                                                    select=parts[rank])
     dt = pla.MPI_DOUBLE if dtype == torch.float64 else pla.MPI_FLOAT
-    info = torch.full((count,), -1, dtype=torch.int32, device=device)
+    info = torch.full((max(1, len(ids)),), -1, dtype=torch.int32, device=device)
 
     def restore():
         for gr in groups:
             gr["A"].copy_(gr["A0"])
             gr["B"].copy_(gr["B0"])
 
+    def sync():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    plan = ctypes.c_void_p()
-    pla.check(lib.PLA_Batch_plan_create(dt, count, arr, ctypes.c_void_p(info.data_ptr()), 1,
-                                        ctypes.byref(plan)), "PLA_Batch_plan_create")
-    plan_s = time.perf_counter() - t0
+    share = shard.RankBatch(lib, dt, arr, info.data_ptr(), autotune=1)
+    plan_s = max_over_ranks(time.perf_counter() - t0)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     times = []
     for it in range(warmup + steps):
         restore()
-        torch.cuda.synchronize()
+        sync()
         e0.record(stream)
-        pla.check(lib.PLA_Batch_plan_execute(plan), "PLA_Batch_plan_execute")
+        share.execute()
         e1.record(stream)
         torch.cuda.synchronize()
         if it >= warmup:
             times.append(e0.elapsed_time(e1) / 1e3)
-    bad = int((info != 0).sum())
-    eta = batched_backward_error(torch, groups, nrhs_of)
-    lib.PLA_Batch_plan_free(ctypes.byref(plan))
+    batched_s = max_over_ranks(sum(times) / len(times))
+    info_all = shard.gather_info(ids.tolist(), info[:len(ids)].cpu().tolist(), count, dist)
+    bad = sum(1 for v in info_all if v != 0)
+    eta = max_over_ranks(batched_backward_error(torch, groups, nrhs))
+    share.free()
     # the per-instance launch loop of the plain kernels, same instances
     restore()
     torch.cuda.synchronize()
-    pla.check(lib.PLA_Batched_factor_solve_loop(dt, count, arr), "loop warm-up")
+    if len(ids):
+        pla.check(lib.PLA_Batched_factor_solve_loop(dt, len(ids), arr), "loop warm-up")
     restore()
-    torch.cuda.synchronize()
+    sync()
     e0.record(stream)
-    pla.check(lib.PLA_Batched_factor_solve_loop(dt, count, arr), "PLA_Batched_factor_solve_loop")
+    if len(ids):
+        pla.check(lib.PLA_Batched_factor_solve_loop(dt, len(ids), arr),
+                  "PLA_Batched_factor_solve_loop")
     e1.record(stream)
     torch.cuda.synchronize()
-    loop_s = e0.elapsed_time(e1) / 1e3
-    loop_eta = batched_backward_error(torch, groups, nrhs_of)
-    batched_s = sum(times) / len(times)
+    loop_s = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    loop_eta = max_over_ranks(batched_backward_error(torch, groups, nrhs))
     del groups, piv
     torch.cuda.empty_cache()
     return {"workload": f"{count} instances, n log-uniform [8, 512], half LU half Cholesky, "
                         "1-4 rhs", "dtype": "f64" if dtype == torch.float64 else "f32",
+            "ranks": world, "sharding": "by instance, flop-balanced (shard.partition); "
+                                        "info words gathered once",
+            "instances_this_rank": len(ids), "flops_this_rank": flops,
             "batched_s": batched_s, "loop_s": loop_s, "speedup_vs_loop": loop_s / batched_s,
-            "gflops": flops / batched_s / 1e9, "loop_gflops": flops / loop_s / 1e9,
+            "gflops": total_flops / batched_s / 1e9, "loop_gflops": total_flops / loop_s / 1e9,
             "plan_create_s": plan_s, "instances_failed": bad,
             "backward_error_max": eta, "loop_backward_error_max": loop_eta}
-
-
-def spd_device(n, kappa, seed, torch, device):
-    """A = Q diag(lambda) Q' with lambda log-uniform in [1/kappa, 1] and Q a
-    product of 8 Householder reflectors with seeded Gaussian vectors."""
-    g = torch.Generator(device=device).manual_seed(seed)
-    u = torch.rand(n, dtype=torch.float64, device=device, generator=g)
-    lam = torch.exp(u * -np.log(kappa))
-    lam[0], lam[-1] = 1.0, 1.0 / kappa
-    A = torch.diag(lam)
-    for _ in range(8):                      # A <- H A H
-        v = torch.randn(n, dtype=torch.float64, device=device, generator=g)
-        c = -2.0 / float(v @ v)
-        A.addr_(v, v @ A, alpha=c)
-        A.addr_(A @ v, v, alpha=c)
-    A.add_(A.t().clone()).mul_(0.5)
-    return A
 
 
 def run_mixed_sweep(torch, pla, lib, s, device, stream, a, n, args, params):
@@ -810,8 +732,8 @@ def run_ours(args):
     # ---- batched factor-and-solve: one persistent graph launch vs a launch loop ----
     batched = None
     if not args.skip_batched:
-        batched = [run_batched(torch, pla, lib, device, stream, dt, args.steps, args.warmup,
-                               count=args.batch_count, seed=3 + 1000 * rank)
+        batched = [run_batched(torch, pla, lib, device, stream, dt, args.steps, args.warmup, dist,
+                               count=args.batch_count, seed=3)
                    for dt in (torch.float64, torch.float32)]
 
     # ---- mixed-precision Cholesky-IR: fp8 E4M3 vs bf16 trailing updates ----
@@ -876,7 +798,7 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
         try:
-            _, cpu = reference_sample(n, args.kappa, args.cpu_seconds)
+            cpu = reference_solve(n, args.kappa, steps=args.ref_steps)
         except Exception as exc:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "s", "cores": cpu_cores(), "kind": "reference",
                    "sample": f"unavailable: {exc}"}

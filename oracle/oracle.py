@@ -44,12 +44,16 @@ def _ptr(a: np.ndarray):
 
 
 def build(reference_root: str | None = None) -> None:
-    """Build liboracle.so, and the compiled reference when its sources exist."""
+    """Build liboracle.so, and the compiled reference when its sources exist.
+
+    The reference tree is the Makefile's REFERENCE (overridden by the
+    argument or the PLA_REFERENCE_ROOT environment variable); where it is
+    absent, as on a machine that only runs the prebuilt files, the
+    `ref-if-present` target does nothing."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    root = reference_root or "/root/reference"
-    if os.path.isdir(root):
-        subprocess.run(["make", "-s", "-j8", "-C", HERE, f"REFERENCE={root}",
-                        "ref", "ref-openblas"], check=True)
+    root = reference_root or os.environ.get("PLA_REFERENCE_ROOT")
+    extra = [f"REFERENCE={root}"] if root else []
+    subprocess.run(["make", "-s", "-j8", "-C", HERE, *extra, "ref-if-present"], check=True)
 
 
 class Restated:

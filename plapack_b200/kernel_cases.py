@@ -320,12 +320,10 @@ def case_sgemm(torch, lib, a):
 
 
 def case_batched(torch, lib, a):
-    sys.path.insert(0, __import__("os").path.dirname(__import__("os").path.dirname(
-        __import__("os").path.abspath(__file__))))
-    import bench  # the bench's workload generator: n log-uniform in [8, 512], LU and Cholesky
+    from .workloads import batched_workload  # n log-uniform in [8, 512], LU and Cholesky
     dtype = torch.float64 if a.dtype == "f64" else torch.float32
-    arr, groups, piv, flops = bench.batched_workload(torch, pla, torch.device("cuda", 0), dtype,
-                                                     a.count, 3)
+    arr, groups, piv, flops, _ = batched_workload(torch, pla, torch.device("cuda", 0), dtype,
+                                                  a.count, 3)
     info = torch.zeros(a.count, dtype=torch.int32, device="cuda")
     dt = pla.MPI_DOUBLE if a.dtype == "f64" else pla.MPI_FLOAT
     plan = ctypes.c_void_p()

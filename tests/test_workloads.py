@@ -18,8 +18,8 @@ sys.path.insert(0, ROOT)
 
 @pytest.fixture(scope="module")
 def bench():
-    import bench as b
-    return b
+    from plapack_b200 import workloads
+    return workloads
 
 
 @pytest.mark.parametrize("kappa", [1e2, 1e6, 1e10])
