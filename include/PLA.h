@@ -10,8 +10,9 @@
  * lives in device memory (PLA_Obj_local_buffer returns a device pointer).
  *
  * Differences a caller may notice, all deliberate:
- *   - no MPI is needed: when no <mpi.h> was included first, the MPI handle
- *     types below are plain ints and MPI_COMM_WORLD names the single rank;
+ *   - no MPI is needed: without an MPI header the MPI handle names below are
+ *     plain int codes and MPI_COMM_WORLD names the single rank; with one, the
+ *     caller's own MPI handles are translated at each call (pla_mpi_compat.h);
  *   - fatal errors never call exit(): PLA_Abort records the message and the
  *     failing call returns PLA_ERROR (see PLA_Last_error in pla_b200.h);
  *   - fill and extract go through PLA_API_axpy_* or PLA_Obj_set/get_local_contents
@@ -26,22 +27,51 @@
 extern "C" {
 #endif
 
-/* ---- MPI handle types (single-rank stand-ins when no MPI is present) ---- */
-#ifndef MPI_VERSION
-typedef int MPI_Datatype;
-typedef int MPI_Comm;
-#ifndef MPI_COMM_NULL
-#define MPI_COMM_NULL   0
-#define MPI_COMM_WORLD  1
+/* ---- MPI -------------------------------------------------------------------
+ * The library needs no MPI: one process drives one GPU on a 1x1 template.  Its
+ * entry points take datatype and communicator CODES, plain ints with the
+ * values below (PLA_B200_Datatype, PLA_B200_Comm).
+ *  - Without an MPI header, the MPI_* names are those codes, so a caller
+ *    writes MPI_DOUBLE or MPI_COMM_WORLD as it would against the reference.
+ *  - With an MPI header -- included before this one, or found on the include
+ *    path, as the reference's INCLUDE/PLA.h:14 includes <mpi.h> -- MPI_* are
+ *    that MPI's own handles (ints in MPICH, pointers in Open MPI).  The entry
+ *    points that take or return a datatype or a communicator are then macros
+ *    over the inline translators at the end of this header
+ *    (pla_mpi_compat.h), which map the caller's handles to the codes and back.
+ *    Define PLA_B200_NO_MPI to keep MPI out even when <mpi.h> is reachable. */
+#if !defined(PLA_B200_NO_MPI) && !defined(MPI_VERSION) && !defined(MPI_DOUBLE) && \
+    defined(__has_include)
+#if __has_include(<mpi.h>)
+#include <mpi.h>
 #endif
-#ifndef MPI_INT
-#define MPI_CHAR            1
-#define MPI_INT             3
-#define MPI_FLOAT           4
-#define MPI_DOUBLE          5
-#define MPI_COMPLEX         6
-#define MPI_DOUBLE_COMPLEX  7
 #endif
+#if !defined(PLA_B200_NO_MPI) && (defined(MPI_VERSION) || defined(MPI_DOUBLE))
+#define PLA_B200_WITH_MPI 1
+#endif
+
+typedef int PLA_B200_Datatype; /* datatype code */
+typedef int PLA_B200_Comm;     /* communicator code */
+#define PLA_B200_DT_CHAR           1
+#define PLA_B200_DT_INT            3
+#define PLA_B200_DT_FLOAT          4
+#define PLA_B200_DT_DOUBLE         5
+#define PLA_B200_DT_COMPLEX        6
+#define PLA_B200_DT_DOUBLE_COMPLEX 7
+#define PLA_B200_COMM_NULL         0
+#define PLA_B200_COMM_WORLD        1
+
+#ifndef PLA_B200_WITH_MPI
+typedef PLA_B200_Datatype MPI_Datatype;
+typedef PLA_B200_Comm MPI_Comm;
+#define MPI_COMM_NULL       PLA_B200_COMM_NULL
+#define MPI_COMM_WORLD      PLA_B200_COMM_WORLD
+#define MPI_CHAR            PLA_B200_DT_CHAR
+#define MPI_INT             PLA_B200_DT_INT
+#define MPI_FLOAT           PLA_B200_DT_FLOAT
+#define MPI_DOUBLE          PLA_B200_DT_DOUBLE
+#define MPI_COMPLEX         PLA_B200_DT_COMPLEX
+#define MPI_DOUBLE_COMPLEX  PLA_B200_DT_DOUBLE_COMPLEX
 #endif
 
 /* ---- constants: same names and values as INCLUDE/PLA_define.h:11-101 ---- */
@@ -134,13 +164,13 @@ typedef struct PLA_Obj_view_struct *PLA_Obj;
 typedef struct PLA_Template_struct *PLA_Template;
 
 /* ---- library and template (TEMPLATE/PLA_Init.c, TEMPLATE/PLA_Temp.c) ---- */
-int PLA_Init(MPI_Comm comm);                                  /* PLA_Init.c:85 */
+int PLA_Init(PLA_B200_Comm comm);                                  /* PLA_Init.c:85 */
 int PLA_Finalize(void);                                       /* PLA_Init.c:132 */
 int PLA_Initialized(int *initialized);                        /* PLA_Init.c:113 */
-int PLA_Comm_1D_to_2D(MPI_Comm comm1d, int nprows, int npcols,
-                      MPI_Comm *comm2d);                      /* PLA_Init.c:20 */
-int PLA_Comm_1D_to_2D_ratio(MPI_Comm comm1d, float ratio,
-                            MPI_Comm *comm2d);                /* PLA_Init.c:38 */
+int PLA_Comm_1D_to_2D(PLA_B200_Comm comm1d, int nprows, int npcols,
+                      PLA_B200_Comm *comm2d);                      /* PLA_Init.c:20 */
+int PLA_Comm_1D_to_2D_ratio(PLA_B200_Comm comm1d, float ratio,
+                            PLA_B200_Comm *comm2d);                /* PLA_Init.c:38 */
 int PLA_Temp_create(int nb, int zero_or_one, PLA_Template *templ); /* PLA_Temp.c:19 */
 int PLA_Temp_free(PLA_Template *templ);                       /* PLA_Temp.c:136 */
 int PLA_Temp_nb(PLA_Template templ, int *nb);                 /* PLA_Temp.c:176 */
@@ -159,15 +189,15 @@ int PLA_Abort(char *message, int line, char *file);
 int PLA_Warning(char *message);
 
 /* ---- object creation (OBJ/PLA_Obj.c) ---------------------------------- */
-int PLA_Matrix_create(MPI_Datatype datatype, int length, int width,
+int PLA_Matrix_create(PLA_B200_Datatype datatype, int length, int width,
                       PLA_Template templ, int align_row, int align_col,
                       PLA_Obj *new_obj);                      /* PLA_Obj.c:323 */
-int PLA_Mvector_create(MPI_Datatype datatype, int length, int width,
+int PLA_Mvector_create(PLA_B200_Datatype datatype, int length, int width,
                        PLA_Template templ, int align, PLA_Obj *new_obj); /* :149 */
-int PLA_Mscalar_create(MPI_Datatype datatype, int owner_row, int owner_col,
+int PLA_Mscalar_create(PLA_B200_Datatype datatype, int owner_row, int owner_col,
                        int length, int width, PLA_Template templ,
                        PLA_Obj *new_obj);                     /* PLA_Obj.c:497 */
-int PLA_Pmvector_create(MPI_Datatype datatype, int project_onto, int owner,
+int PLA_Pmvector_create(PLA_B200_Datatype datatype, int project_onto, int owner,
                         int length, int width, PLA_Template templ, int align,
                         PLA_Obj *new_obj);                    /* PLA_Obj.c:740 */
 int PLA_Matrix_create_conf_to(PLA_Obj obj, PLA_Obj *new_obj);
@@ -196,7 +226,7 @@ int PLA_Obj_view_swap(PLA_Obj *obj1, PLA_Obj *obj2);
 
 /* ---- inquiry (OBJ/PLA_Obj.c:831-1436) ------------------------------------ */
 int PLA_Obj_objtype(PLA_Obj obj, int *objtype);
-int PLA_Obj_datatype(PLA_Obj obj, MPI_Datatype *datatype);
+int PLA_Obj_datatype(PLA_Obj obj, PLA_B200_Datatype *datatype);
 int PLA_Obj_template(PLA_Obj obj, PLA_Template *templ);
 int PLA_Obj_global_length(PLA_Obj obj, int *length);
 int PLA_Obj_global_width(PLA_Obj obj, int *width);
@@ -218,7 +248,7 @@ int PLA_Obj_set_to_zero(PLA_Obj obj);
 int PLA_Obj_set_to_one(PLA_Obj obj);
 int PLA_Obj_set_to_minus_one(PLA_Obj obj);
 int PLA_Obj_set_to_identity(PLA_Obj obj);
-int PLA_Obj_set(PLA_Obj obj, MPI_Datatype datatype, void *value);
+int PLA_Obj_set(PLA_Obj obj, PLA_B200_Datatype datatype, void *value);
 int PLA_Obj_get_local_contents(PLA_Obj obj, int trans, int *rows_in_buf,
                                int *cols_in_buf, void *buf, int ldim_buf,
                                int stride_buf);
@@ -265,14 +295,14 @@ int PLA_Max_size_malloced(void);                     /* OBJ/PLA_Memory.c:100 */
 /* an out-of-core matrix keeps its data in a file (column-major, leading
  * dimension local_ldim elements); PLA_Copy moves blocks between its views and
  * in-core objects.  Errors return PLA_ERROR where the reference aborts. */
-int PLA_OOC_Matrix_create_without_fd(MPI_Datatype datatype, int global_length,
+int PLA_OOC_Matrix_create_without_fd(PLA_B200_Datatype datatype, int global_length,
                                      int global_width, PLA_Template templ,
                                      int global_align_row, int global_align_col,
                                      PLA_Obj *new_obj);   /* OBJ/PLA_Obj_ooc.c:50 */
 int PLA_Obj_attach_fd(PLA_Obj obj, int fd, int local_ldim,
                       int user_buffer);       /* OBJ/PLA_Obj_management.c:146 */
-int PLA_File_create(char *filename, MPI_Datatype datatype, int size, int *fd); /* IO/PLA_File.c:25 */
-int PLA_File_open(char *filename, MPI_Datatype datatype, int size, int *fd);   /* :47 */
+int PLA_File_create(char *filename, PLA_B200_Datatype datatype, int size, int *fd); /* IO/PLA_File.c:25 */
+int PLA_File_open(char *filename, PLA_B200_Datatype datatype, int size, int *fd);   /* :47 */
 int PLA_File_close(int fd);                          /* IO/PLA_File.c:61 */
 int PLA_File_unlink(char *filename);                 /* IO/PLA_File.c:72 */
 int PLA_File_stats_start(void);                      /* IO/PLA_File_stats.c:21 */
@@ -306,7 +336,7 @@ int PLA_Gemv(int trans, PLA_Obj alpha, PLA_Obj A, PLA_Obj x, PLA_Obj beta,
 int PLA_Iamax(PLA_Obj x, PLA_Obj k, PLA_Obj xmax);   /* BLAS1/PLA_Iamax.c:37 */
 int PLA_Axpy(PLA_Obj alpha, PLA_Obj x, PLA_Obj y);   /* BLAS1/PLA_Axpy.c:13 */
 int PLA_Nrm2(PLA_Obj x, PLA_Obj alpha);              /* BLAS1/PLA_Nrm2.c:13 */
-int PLA_Shift(PLA_Obj obj, MPI_Datatype datatype, void *value); /* UTIL/PLA_Shift.c:15 */
+int PLA_Shift(PLA_Obj obj, PLA_B200_Datatype datatype, void *value); /* UTIL/PLA_Shift.c:15 */
 int PLA_Syrk_perform_local_part(int uplo, PLA_Obj alpha, PLA_Obj X,
                                 PLA_Obj X_trans, PLA_Obj beta,
                                 PLA_Obj A);  /* BLAS3/PLA_Syrk_perform_local_part.c:13 */
@@ -337,5 +367,9 @@ int PLA_Local_chol(int uplo, PLA_Obj A);   /* SOLVERS/Cholesky/PLA_Local_chol.c:
 #endif
 
 #include "pla_b200.h"
+
+#ifdef PLA_B200_WITH_MPI
+#include "pla_mpi_compat.h"
+#endif
 
 #endif /* PLA_B200_PLA_H */

@@ -124,8 +124,10 @@ int PLA_General_solve_mixed_host(PLA_Obj A, const void *A_host, int ldh, PLA_Obj
  * column-major, lda >= m, w <= m) in place with partial pivoting, the column
  * loop PLA_LU runs on each panel: pivots[j] receives the reference's offset
  * encoding (row j was swapped with row j + pivots[j]), the swaps cover the
- * panel's own columns only.  *status (device int, 0 on entry) is set to 1 if
- * a bounded wait in the kernel gave up.
+ * panel's own columns only.  status points to two device ints, both 0 on
+ * entry: status[0] is set to 1 if a bounded wait in the kernel gave up,
+ * status[1] to the 1-based column of the first exact zero pivot (the
+ * factorization still completes, dividing by that zero, as PLA_LU does).
  * For callers that cannot let the library call cudaMalloc -- programs whose
  * GPU memory belongs to another allocator, or services that forbid allocation
  * while running: the kernel's workspace is a fixed array of about 667 KB in
@@ -133,10 +135,14 @@ int PLA_General_solve_mixed_host(PLA_Obj A, const void *A_host, int ldh, PLA_Obj
  * process exits, instead of memory the library allocates.  Limit: w <= 128
  * (larger panels return PLA_ERROR with a message in PLA_Last_error).
  * The call is asynchronous on `stream` (a cudaStream_t, NULL for the default
- * stream).  The first call on a device looks up the array's device address;
- * make that first call before any stream capture.  All calls share the one
- * array, so calls whose kernels overlap on the GPU race. */
-int PLA_B200_lu_panel_noalloc(MPI_Datatype datatype, int m, int w, void *A, int lda, int *pivots,
+ * stream).  The first call on a device, and the first after the device's
+ * context was replaced (cudaDeviceReset), looks up the array's device address
+ * and queues a clear of the array; make that call before any stream capture.
+ * The array is cleared again once every 2^24 panel launches.  All calls share
+ * the one array, so calls whose kernels overlap on the GPU (other streams,
+ * other host threads) race: serialise them on one stream or synchronise
+ * between them. */
+int PLA_B200_lu_panel_noalloc(PLA_B200_Datatype datatype, int m, int w, void *A, int lda, int *pivots,
                               int *status, void *stream);
 
 /* ---- batched factor-and-solve ------------------------------------------------
@@ -159,16 +165,16 @@ typedef struct PLA_Batch_plan_struct *PLA_Batch_plan;
 /* Sort and bucket the instances, optionally autotune the schedule on a
  * synthetic sample of the same sizes, upload the descriptors and capture the
  * launch in a CUDA graph.  The instances' buffers must stay valid. */
-int PLA_Batch_plan_create(MPI_Datatype datatype, int count, const PLA_Batch_instance *instances,
+int PLA_Batch_plan_create(PLA_B200_Datatype datatype, int count, const PLA_Batch_instance *instances,
                           int *info, int autotune, PLA_Batch_plan *plan);
 int PLA_Batch_plan_execute(PLA_Batch_plan plan);
 int PLA_Batch_plan_free(PLA_Batch_plan *plan);
 /* create + execute + free, without autotuning */
-int PLA_Batched_factor_solve(MPI_Datatype datatype, int count,
+int PLA_Batched_factor_solve(PLA_B200_Datatype datatype, int count,
                              const PLA_Batch_instance *instances, int *info);
 /* the same work as a loop of per-instance launches of the single-matrix
  * kernels (the baseline the batched launch is measured against) */
-int PLA_Batched_factor_solve_loop(MPI_Datatype datatype, int count,
+int PLA_Batched_factor_solve_loop(PLA_B200_Datatype datatype, int count,
                                   const PLA_Batch_instance *instances);
 
 /* The counters of PLA_File_stats_start/stop: bytes and seconds of the file

@@ -31,6 +31,8 @@
 // published values are bitwise those the CTA stores later), and then updates
 // its remaining columns while the other CTAs publish.  Every wait is bounded;
 // on timeout the kernel records PLA_K_TIMEOUT and exits.
+#include <cuda.h>
+
 #include <atomic>
 #include <climits>
 #include <cstdio>
@@ -142,11 +144,15 @@ __device__ __forceinline__ void block_argmax(K &v, int &i, K *sv, int *si) {
 //   rec  [2][P][NW + 1]  pivot key of each CTA's candidate, then its row index
 //   crow [2][P][w][NW]   each candidate's row
 //   trow [2][w][NW]      the diagonal row, published by its owner
+//
+// spin_limit bounds every poll (kSpinLimit in production).  mute_cta >= 0
+// makes that CTA skip its stores of published words, so every wait on them
+// runs out: the test of the timeout path uses it with a small spin_limit.
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 1)
 panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *status,
            int *zero_info, int row_base, unsigned seq, unsigned long long *rec,
-           unsigned long long *crow, unsigned long long *trow) {
+           unsigned long long *crow, unsigned long long *trow, long spin_limit, int mute_cta) {
   constexpr int NW = (int)(sizeof(T) / 4), NR = NW + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   using K = typename KeyOf<T>::K;
@@ -155,6 +161,7 @@ panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *sta
   __shared__ int s_p, s_q;
 
   const int P = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+  const bool mute = b == mute_cta;
   const int row0 = b * R;
   const int row1 = min(row0 + R, r);
   const int nrows = max(row1 - row0, 0);
@@ -196,13 +203,13 @@ panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *sta
       const T e = E(li, c);
       return (pend && c > col) ? fma(E(li, col - 1), -u[c], e) : e;
     };
-    if (bidx != INT_MAX)
+    if (bidx != INT_MAX && !mute)
       for (int c = tid; c < w; c += kThreads)
         put<T>(crow + (((long)par * P + b) * w + c) * NW, row_val(bidx - row0, c), tag);
-    if (col >= row0 && col < row1)
+    if (col >= row0 && col < row1 && !mute)
       for (int c = tid; c < w; c += kThreads)
         put<T>(trow + ((long)par * w + c) * NW, row_val(col - row0, c), tag);
-    if (tid == 0) {
+    if (tid == 0 && !mute) {
       unsigned long long *rp = rec + ((long)par * P + b) * NR;
       const bool none = bidx == INT_MAX;  // no candidate: every entry is NaN
       const K kv = none ? K(0) : best;
@@ -248,7 +255,7 @@ panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *sta
             else all = false;
           }
         if (all) break;
-        if (spins > kSpinLimit || *(volatile int *)status != PLA_K_OK) {
+        if (spins > spin_limit || *(volatile int *)status != PLA_K_OK) {
           ok = false;
           break;
         }
@@ -293,7 +300,7 @@ panel_lu_k(T *A, long lda, int r, int w, int R, int use_smem, int *piv, int *sta
       for (long spins = 0;; spins++) {
         v = ld_relaxed64(src);
         if ((unsigned)(v >> 32) == tag) break;
-        if (spins > kSpinLimit || *(volatile int *)status != PLA_K_OK) {
+        if (spins > spin_limit || *(volatile int *)status != PLA_K_OK) {
           ok = false;
           break;
         }
@@ -364,8 +371,13 @@ Layout layout(int P, int w) {
   return l;
 }
 
-// launch sequence number for the tags: never 0 in its low 24 bits, so no tag
-// matches a zeroed word
+// Launch sequence number for the tags: never 0 in its low 24 bits, so no tag
+// matches a zeroed word.  A tag carries only those 24 bits, so once the
+// sequence has wrapped a word left by a launch 2^24 launches earlier (with a
+// larger grid or width than any launch since) could carry a current tag.  The
+// bits above 24 number the epoch: every workspace is cleared before its first
+// launch of each epoch (and before its first launch at all), so a word a
+// reader accepts was written in the current epoch, that is by this launch.
 std::atomic<unsigned> g_seq{0};
 unsigned next_seq() {
   unsigned v;
@@ -373,10 +385,13 @@ unsigned next_seq() {
   while ((v & 0xffffffu) == 0);
   return v;
 }
+constexpr unsigned kNoEpoch = 0xffffffffu;  // a workspace never cleared
+inline unsigned epoch_of(unsigned seq) { return seq >> 24; }
 
 struct Workspace {
   void *ptr = nullptr;
   size_t bytes = 0;
+  unsigned epoch = kNoEpoch;  // epoch it was last cleared in
 };
 Workspace g_ws;
 
@@ -385,10 +400,15 @@ void *workspace(size_t bytes) {
   if (g_ws.ptr) cudaFree(g_ws.ptr);
   g_ws.ptr = nullptr;
   g_ws.bytes = 0;
+  g_ws.epoch = kNoEpoch;
   if (cudaMalloc(&g_ws.ptr, bytes) != cudaSuccess) return nullptr;
   g_ws.bytes = bytes;
   return g_ws.ptr;
 }
+
+// spin limit and muted CTA of the next launch (test hook; see panel_lu_k)
+long g_test_spin_limit = 0;
+int g_test_mute_cta = -1;
 
 int g_sms = 0, g_smem_optin = 0;
 
@@ -423,9 +443,18 @@ int launch(int r, int w, void *A, long lda, int *piv, int *status, int *zero_inf
   if (!ws) return (int)cudaErrorMemoryAllocation;
   unsigned long long *rec = ws, *crow = ws + lay.off_crow, *trow = ws + lay.off_trow;
   unsigned seq = next_seq();
+  if (g_ws.epoch != epoch_of(seq)) {
+    cudaError_t ce = cudaMemsetAsync(g_ws.ptr, 0, g_ws.bytes, s);
+    if (ce != cudaSuccess) return (int)ce;
+    g_ws.epoch = epoch_of(seq);
+  }
+  long spin_limit = g_test_spin_limit > 0 ? g_test_spin_limit : kSpinLimit;
+  int mute_cta = g_test_mute_cta;
+  g_test_spin_limit = 0;
+  g_test_mute_cta = -1;
   T *Ap = (T *)A;
-  void *args[] = {&Ap, &lda, &r, &w, &R, &use_smem, &piv, &status, &zero_info, &row_base, &seq,
-                  &rec, &crow, &trow};
+  void *args[] = {&Ap,      &lda, &r,   &w,    &R,    &use_smem,   &piv,     &status,
+                  &zero_info, &row_base, &seq, &rec, &crow, &trow, &spin_limit, &mute_cta};
   cudaError_t e =
       cudaLaunchCooperativeKernel((void *)panel_lu_k<T>, dim3(P), dim3(kThreads), args, dyn, s);
   pla_k_count(1);
@@ -450,10 +479,26 @@ extern "C" int pla_k_lu_panel(int dt, int r, int w, void *A, long lda, int *piv,
   return pla_k_lu_panel_ex(dt, r, w, A, lda, piv, status, zero_info, row_base, 0, s);
 }
 
+// Test hooks, not part of the public interface: read or move the launch
+// sequence (to make the tag wrap), and give the next panel launch a spin limit
+// and a CTA that publishes nothing (to make its waits run out).
+extern "C" unsigned pla_k_panel_sequence(void) { return g_seq.load(); }
+extern "C" void pla_k_panel_set_sequence(unsigned v) { g_seq.store(v); }
+extern "C" void pla_k_panel_test_timeout(long spin_limit, int mute_cta) {
+  g_test_spin_limit = spin_limit;
+  g_test_mute_cta = mute_cta;
+}
+
+namespace {
+void release_noalloc();
+}
+
 extern "C" void pla_kernels_release(void) {
   if (g_ws.ptr) cudaFree(g_ws.ptr);
   g_ws.ptr = nullptr;
   g_ws.bytes = 0;
+  g_ws.epoch = kNoEpoch;
+  release_noalloc();
 }
 
 // ---------------------------------------------------------------------------
@@ -484,29 +529,74 @@ static __device__ __align__(256) unsigned char g_panel_scratch[kNoAllocBytes];
 
 namespace {
 
+// Per device: the array's device address, the context it was looked up in,
+// and the sequence epoch the array was last cleared in.
+struct NoAllocSlot {
+  void *addr = nullptr;
+  unsigned long long ctx_id = 0;
+  unsigned epoch = kNoEpoch;
+};
 std::mutex g_noalloc_mu;
-void *g_noalloc_addr[128] = {};
+NoAllocSlot g_noalloc[128];
 
-// The array's device address on the current device, looked up once per
-// device (the host-side name of the array is only a stand-in).
-int noalloc_scratch(char **out) {
+void release_noalloc() {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  for (auto &s : g_noalloc) s = NoAllocSlot{};
+}
+
+// The array's device address on the current device (the host-side name of
+// the array is only a stand-in), looked up on the first call in each context:
+// after cudaDeviceReset the device has a new primary context, the module is
+// loaded again and the old address is stale, so the cache is keyed by the
+// context's unique id.  *clear is set when the array must be zeroed before
+// the launch with sequence `seq` (a new context, or a new sequence epoch).
+int noalloc_scratch(unsigned seq, char **out, bool *clear) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return (int)e;
   if (dev < 0 || dev >= 128) return (int)cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_panel_scratch);
-    if (e != cudaSuccess) return (int)e;
-    g_noalloc_addr[dev] = p;
+  // driver entry points resolved at run time: the library does not link libcuda
+  using GetCurrent = CUresult (*)(CUcontext *);
+  using GetId = CUresult (*)(CUcontext, unsigned long long *);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  if (!get_current || !get_id) {
+    void *p1 = nullptr, *p2 = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p1, cudaEnableDefault, &q1) != cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &p2, cudaEnableDefault, &q2) != cudaSuccess ||
+        q2 != cudaDriverEntryPointSuccess)
+      return (int)cudaErrorSymbolNotFound;
+    get_current = (GetCurrent)p1;
+    get_id = (GetId)p2;
   }
-  *out = (char *)g_noalloc_addr[dev];
+  auto context_id = [](unsigned long long *id) -> bool {
+    CUcontext ctx = nullptr;
+    return get_current(&ctx) == CUDA_SUCCESS && ctx && get_id(ctx, id) == CUDA_SUCCESS;
+  };
+  unsigned long long id = 0;
+  const bool known = context_id(&id);  // false before the runtime's first use of the device
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  NoAllocSlot &s = g_noalloc[dev];
+  if (!known || !s.addr || s.ctx_id != id) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_panel_scratch);  // loads the module if needed
+    if (e != cudaSuccess) return (int)e;
+    if (!context_id(&id)) return (int)cudaErrorDeviceUninitialized;
+    s.addr = p;
+    s.ctx_id = id;
+    s.epoch = kNoEpoch;
+  }
+  *clear = s.epoch != epoch_of(seq);
+  s.epoch = epoch_of(seq);
+  *out = (char *)s.addr;
   return 0;
 }
 
 template <typename T>
-int launch_noalloc(int r, int w, T *A, long lda, int *piv, int *status, cudaStream_t s) {
+int launch_noalloc(int r, int w, T *A, long lda, int *piv, int *status, int *zero_info,
+                   cudaStream_t s) {
   int dev = 0, sms = 0, optin = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return (int)e;
@@ -527,20 +617,27 @@ int launch_noalloc(int r, int w, T *A, long lda, int *piv, int *status, cudaStre
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, panel_lu_k<T>, kThreads, dyn);
   if (per_sm * sms < P) return (int)cudaErrorCooperativeLaunchTooLarge;
-  char *ws = nullptr;
-  int rc = noalloc_scratch(&ws);
-  if (rc) return rc;
-  // Nothing in the array needs clearing: every word a call reads carries the
-  // call's own tag, so what earlier calls left there is never taken for data.
   const Layout lay = layout<T>(P, w);
   if (lay.words * sizeof(unsigned long long) > kNoAllocBytes) return (int)cudaErrorInvalidValue;
+  unsigned seq = next_seq();
+  char *ws = nullptr;
+  bool clear = false;
+  int rc = noalloc_scratch(seq, &ws, &clear);
+  if (rc) return rc;
+  // Every word a call reads carries the call's own tag, so what earlier calls
+  // left in the array is never taken for data -- within one sequence epoch.
+  // The array is zeroed at the first call of each epoch and of each context.
+  if (clear) {
+    e = cudaMemsetAsync(ws, 0, kNoAllocBytes, s);
+    if (e != cudaSuccess) return (int)e;
+  }
   unsigned long long *wsw = (unsigned long long *)ws;
   unsigned long long *rec = wsw, *crow = wsw + lay.off_crow, *trow = wsw + lay.off_trow;
-  unsigned seq = next_seq();
-  int *zero_info = nullptr;
   int row_base = 0;
-  void *args[] = {&A,   &lda,      &r,        &w,   &R,   &use_smem, &piv,
-                  &status, &zero_info, &row_base, &seq, &rec, &crow,  &trow};
+  long spin_limit = kSpinLimit;
+  int mute_cta = -1;
+  void *args[] = {&A,      &lda,      &r,    &w,   &R,    &use_smem, &piv,       &status,
+                  &zero_info, &row_base, &seq, &rec, &crow, &trow,     &spin_limit, &mute_cta};
   e = cudaLaunchCooperativeKernel((void *)panel_lu_k<T>, dim3(P), dim3(kThreads), args, dyn, s);
   pla_k_count(1);
   return (int)e;
@@ -568,9 +665,10 @@ extern "C" int PLA_B200_lu_panel_noalloc(MPI_Datatype datatype, int m, int w, vo
   if (!A || !pivots || !status)
     return pla::fail("PLA_B200_lu_panel_noalloc: null pointer", __LINE__, __FILE__);
   cudaStream_t s = (cudaStream_t)stream;
+  // status[1] receives the first exact zero pivot
   int e = datatype == MPI_DOUBLE
-              ? launch_noalloc<double>(m, w, (double *)A, lda, pivots, status, s)
-              : launch_noalloc<float>(m, w, (float *)A, lda, pivots, status, s);
+              ? launch_noalloc<double>(m, w, (double *)A, lda, pivots, status, status + 1, s)
+              : launch_noalloc<float>(m, w, (float *)A, lda, pivots, status, status + 1, s);
   if (e) return pla::cuda_fail((cudaError_t)e, __LINE__, __FILE__);
   return PLA_SUCCESS;
 }

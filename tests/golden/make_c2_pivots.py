@@ -9,8 +9,7 @@ seed-1 i.i.d. N(0,1) matrix
 once with the restated netlib BLAS (the bit-reproducible build the golden
 fixtures come from) and once with OpenBLAS 0.3.15, and writes per case
 
-    tests/golden/c2/lu_n<n>_<blas>.npz   pivots (int32, PLAPACK offsets),
-                                          diag(U), column norms of the factor
+    tests/golden/c2/lu_n<n>_<blas>.npz   pivots (int32, PLAPACK offsets)
     tests/golden/c2/manifest.json        SHA-256 of the pivot vector and of
                                           diag(U), ||factor||_F, sum log|u_ii|,
                                           min/max |u_ii|, seconds
@@ -65,8 +64,7 @@ def run_case(n: int, blas: str, nb: int) -> dict:
     d = np.ascontiguousarray(np.diagonal(A))
     colnorm = np.sqrt(np.einsum("ij,ij->j", A, A))
     os.makedirs(OUT, exist_ok=True)
-    np.savez_compressed(os.path.join(OUT, f"lu_n{n}_{blas}.npz"), pivots=piv, diag_u=d,
-                        col_norms=colnorm)
+    np.savez_compressed(os.path.join(OUT, f"lu_n{n}_{blas}.npz"), pivots=piv)
     return {"n": n, "blas": blas, "nb_alg": nb, "nb_distr": nb, "ret": int(r),
             "seconds": t.value,
             "threads": int(os.environ.get("OPENBLAS_NUM_THREADS", "1")) if blas != "netlib" else 1,

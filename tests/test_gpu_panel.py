@@ -121,3 +121,38 @@ def test_panel_ties_zero_and_nan_columns(env, dt, case):
     # the columns before the zero or NaN column are finite and match
     good = {"ties": w, "zero": 5, "nan": 9}[case]
     check_factors(LU[:, :good], ref[:, :good], A[:, :good], w)
+
+
+def test_panel_wait_runs_out_and_the_next_call_succeeds(env):
+    """The timeout path of the panel's exchange: one CTA publishes nothing and
+    every poll is limited to a few hundred tries, so every CTA gives up.  The
+    launch must return with status PLA_K_TIMEOUT (1), and the next panel on
+    the same stream must run normally and match the oracle."""
+    s, torch, pla, rs = env
+    lib = s.lib
+    lib.pla_k_panel_test_timeout.argtypes = [ctypes.c_long, ctypes.c_int]
+    lib.pla_k_panel_test_timeout.restype = None
+    rng = np.random.default_rng(77)
+    r, w = 4096, 32
+    A = rng.standard_normal((r, w))
+    a = torch.from_numpy(np.ascontiguousarray(A.T)).cuda()
+    piv = torch.zeros(w, dtype=torch.int32, device="cuda")
+    status = torch.zeros(4, dtype=torch.int32, device="cuda")
+    lib.pla_k_panel_test_timeout(300, 1)           # CTA 1 of 4 or more stays silent
+    rc = lib.pla_k_lu_panel_ex(pla.MPI_DOUBLE, r, w, a.data_ptr(), r, piv.data_ptr(),
+                               status.data_ptr(), None, 0, 4, None)
+    assert rc == 0
+    torch.cuda.synchronize()
+    assert int(status[0].item()) == 1              # PLA_K_TIMEOUT
+    # the hook applies to one launch only: the same panel again, fresh status
+    a = torch.from_numpy(np.ascontiguousarray(A.T)).cuda()
+    status.zero_()
+    rc = lib.pla_k_lu_panel_ex(pla.MPI_DOUBLE, r, w, a.data_ptr(), r, piv.data_ptr(),
+                               status.data_ptr(), None, 0, 4, None)
+    assert rc == 0
+    torch.cuda.synchronize()
+    assert int(status[0].item()) == 0
+    LUo, pivo = rs.lu_unblocked(A)
+    assert np.array_equal(piv.cpu().numpy(), pivo)
+    LU = a.cpu().numpy().T
+    assert np.abs(LU - LUo).max() <= 4 * r * 2.0 ** -52 * np.abs(LUo).max()
