@@ -63,6 +63,8 @@ def parse():
     p.add_argument("--precision", choices=["fp16", "bf16", "fp32"], default="fp16")
     p.add_argument("--refinement", choices=["gmres", "lu"], default="gmres")
     p.add_argument("--nb", type=int, default=256, help="block size of the mixed factorization")
+    p.add_argument("--panel-pivoting", choices=["tournament", "partial"], default="tournament",
+                   help="pivoting of the mixed LU's fp32 panels")
     p.add_argument("--nb-fp64", type=int, default=512,
                    help="nb_alg of the FP64 LU (512: K = 512 trailing updates); the Cholesky "
                         "caps it at 256")
@@ -541,6 +543,8 @@ def run_ours(args):
     params.precision = prec
     params.refinement = pla.PLA_B200_IR_GMRES if args.refinement == "gmres" else pla.PLA_B200_IR_LU
     params.nb = args.nb
+    params.panel_pivoting = (pla.PLA_B200_PIVOT_TOURNAMENT if args.panel_pivoting == "tournament"
+                             else pla.PLA_B200_PIVOT_PARTIAL)
     report = pla.MixedReport()
 
     def mixed_step():
@@ -813,6 +817,7 @@ def run_ours(args):
                                       f"{args.precision} factors + {args.refinement.upper()}-IR",
                           "n": n, "nrhs": 1, "kappa": args.kappa, "precision": args.precision,
                           "refinement": args.refinement, "nb": args.nb, "nb_fp64": args.nb_fp64,
+                          "panel_pivoting": args.panel_pivoting,
                           "l2": "inputs larger than L2 (8.6 GB FP64 matrix)",
                           "parallelism": f"replicas x{world}"},
                "fp64_lu_solve_s": fp64_s, "fp64_phase_ms_per_step": fp64_detail,

@@ -74,6 +74,13 @@ long PLA_B200_kernel_launches(void);
                                     refines with M^-1 = D (L L')^-1 D */
 #define PLA_B200_IR_LU       1   /* classic iterative refinement             */
 #define PLA_B200_IR_GMRES    2   /* GMRES-IR                                 */
+/* pivoting of the low-precision LU's fp32 panels (the FP64 PLA_LU always uses
+ * the reference's partial pivoting) */
+#define PLA_B200_PIVOT_PARTIAL    0 /* one pivot search over the panel per column */
+#define PLA_B200_PIVOT_TOURNAMENT 1 /* tournament pivoting (CALU): each block of
+                                       rows picks its pivot candidates on its own,
+                                       the candidate sets meet in a reduction tree;
+                                       the pivots differ from partial pivoting's */
 
 typedef struct {
   int precision;        /* PLA_B200_PREC_*                                  */
@@ -89,6 +96,8 @@ typedef struct {
                            (FP8 -> BF16 -> FP64; FP16 -> FP64; FP32 -> FP64)
                            and continue from the current iterate             */
   double tol;           /* target backward error; <= 0 selects n * 2^-53    */
+  int panel_pivoting;   /* PLA_B200_PIVOT_* of the fp32 LU panels (default
+                           TOURNAMENT)                                       */
 } PLA_Mixed_params;
 
 typedef struct {

@@ -97,6 +97,15 @@ class Restated:
         getattr(self.lib, f"oracle_{self._dt(A)}lu_linpack")(m, n, nb, _ptr(A), m, _ptr(piv))
         return A, piv
 
+    def slu_tournament(self, A: np.ndarray, max_ctas: int):
+        """Model of the library's own tournament-pivoted fp32 panel (no
+        reference counterpart): pivots and L \\ U of the r x w float32 panel."""
+        A = np.asfortranarray(A.astype(np.float32, copy=True))
+        r, w = A.shape
+        piv = np.zeros(w, dtype=np.int32)
+        self.lib.oracle_slu_tournament(r, w, max_ctas, _ptr(A), r, _ptr(piv))
+        return A, piv
+
     def chol_blocked(self, A: np.ndarray, nb: int):
         A = np.asfortranarray(A.copy())
         n = A.shape[0]

@@ -272,3 +272,160 @@ void oracle_fill_drand48(long seed, long count, double *out) {
 
 DEFINE_ORACLE(double, d)
 DEFINE_ORACLE(float, s)
+
+/* ---------------------------------------------------------------------------
+ * Model of the library's OWN tournament-pivoted fp32 panel (the mixed LU's
+ * sub-panels, plapack_b200/csrc/k_tslu.cu).  It has no counterpart in the
+ * reference -- whose panel is partial pivoting -- and is here only so the GPU
+ * test can check that kernel bit for bit: the same tree (leaf row blocks of R
+ * rows, passes of at most 512 candidate rows carrying the rows kept, sets of
+ * 16 merged per node), the same candidate order (|x| as bits + 2, NaN 1,
+ * then the smaller row), the same arithmetic (l = x * (1/u), fmaf(-l, u, x);
+ * inv(U11) by back substitution per column, the rows below as (row) inv(U11)
+ * accumulated with fmaf) in the same order.
+ * r x w panel (w <= 32), column-major A (lda), P leaf blocks.  Pivots in the
+ * reference's offset encoding; A overwritten by L \ U under them.
+ * ------------------------------------------------------------------------- */
+#define TS_W 32
+#define TS_CAND 512
+#define TS_GROUP 16
+
+static unsigned long long ts_key(float x, int row) {
+  unsigned b;
+  unsigned k;
+  memcpy(&b, &x, 4);
+  b &= 0x7fffffffu;
+  k = b > 0x7f800000u ? 1u : b + 2u;
+  return ((unsigned long long)k << 32) | (0xffffffffu - (unsigned)row);
+}
+
+/* partial-pivoting LU of the candidate rows ids (entries < 0 empty); keeps
+ * min(live, w) rows in keep[] in pivot order, their factored rows in rows[] */
+static int ts_select(const float *A, int lda, int w, const int *ids, int cnt, int *keep,
+                     float *rows) {
+  static float v[TS_CAND][TS_W];
+  int live[TS_CAND], i, j, c, nlive = 0, k;
+  for (i = 0; i < cnt; i++) {
+    live[i] = ids[i] >= 0;
+    nlive += live[i];
+    for (c = 0; c < TS_W; c++) v[i][c] = (live[i] && c < w) ? A[IDX(ids[i], c, lda)] : 0.f;
+  }
+  k = nlive < w ? nlive : w;
+  for (j = 0; j < k; j++) {
+    unsigned long long best = 0;
+    int bi = -1;
+    float u[TS_W], inv;
+    for (i = 0; i < cnt; i++)
+      if (live[i]) {
+        unsigned long long kk = ts_key(v[i][j], ids[i]);
+        if (kk > best) { best = kk; bi = i; }
+      }
+    for (c = 0; c < TS_W; c++) u[c] = v[bi][c];
+    live[bi] = 0;
+    keep[j] = ids[bi];
+    if (rows)
+      for (c = 0; c < w; c++) rows[j * TS_W + c] = v[bi][c];
+    inv = 1.0f / u[j];
+    for (i = 0; i < cnt; i++)
+      if (live[i]) {
+        float l = v[i][j] * inv;
+        v[i][j] = l;
+        for (c = j + 1; c < TS_W; c++) v[i][c] = fmaf(-l, u[c], v[i][c]);
+      }
+  }
+  return k;
+}
+
+void oracle_slu_tournament(int r, int w, int max_ctas, float *A, int lda, int *piv) {
+  int P = max_ctas, R, b, nsets, level_off = 0, i, j, c;
+  int maxP = (r + 2 * TS_W - 1) / (2 * TS_W);
+  int *slots, ids[TS_CAND], keep[TS_W], kept, root_done = 0;
+  static float rows[TS_W * TS_W], stage[TS_W * TS_W], uinv[TS_W * TS_W];
+  int e_pos[2 * TS_W], e_row[2 * TS_W], ne;
+  if (P > maxP) P = maxP;
+  if (P < 1) P = 1;
+  R = (r + P - 1) / P;
+  P = (r + R - 1) / R;
+  slots = (int *)malloc(sizeof(int) * 2 * (size_t)P * TS_W);
+  /* leaves */
+  for (b = 0; b < P; b++) {
+    int row0 = b * R, row1 = row0 + R < r ? row0 + R : r, next = row0;
+    kept = 0;
+    for (;;) {
+      int take = row1 - next < TS_CAND - kept ? row1 - next : TS_CAND - kept, cnt, last;
+      for (i = 0; i < kept; i++) ids[i] = keep[i];
+      for (i = 0; i < take; i++) ids[kept + i] = next + i;
+      next += take;
+      last = next >= row1;
+      cnt = kept + take;
+      if (last && P > 1 && cnt <= w) {
+        for (i = 0; i < TS_W; i++) keep[i] = i < cnt ? ids[i] : -1;
+        kept = cnt;
+      } else {
+        kept = ts_select(A, lda, w, ids, cnt, keep, (last && P == 1) ? rows : NULL);
+      }
+      if (last) break;
+    }
+    for (i = 0; i < TS_W; i++) slots[(size_t)b * TS_W + i] = i < kept ? keep[i] : -1;
+  }
+  root_done = P == 1;
+  nsets = P;
+  while (!root_done) {
+    int ngroups = (nsets + TS_GROUP - 1) / TS_GROUP, g;
+    for (g = 0; g < ngroups; g++) {
+      int gsize = nsets - g * TS_GROUP < TS_GROUP ? nsets - g * TS_GROUP : TS_GROUP;
+      int cnt = gsize * TS_W;
+      for (i = 0; i < cnt; i++) ids[i] = slots[(size_t)(level_off + g * TS_GROUP) * TS_W + i];
+      kept = ts_select(A, lda, w, ids, cnt, keep, ngroups == 1 ? rows : NULL);
+      for (i = 0; i < TS_W; i++)
+        slots[(size_t)(level_off + nsets + g) * TS_W + i] = i < kept ? keep[i] : -1;
+    }
+    level_off += nsets;
+    nsets = ngroups;
+    root_done = nsets == 1;
+  }
+  /* the interchanges as sequential swaps */
+  ne = w;
+  for (i = 0; i < w; i++) { e_pos[i] = i; e_row[i] = i; }
+  for (j = 0; j < w; j++)
+    if (keep[j] >= w) { e_pos[ne] = keep[j]; e_row[ne] = keep[j]; ne++; }
+  for (j = 0; j < w; j++) {
+    int e = 0;
+    while (e_row[e] != keep[j]) e++;
+    piv[j] = e_pos[e] - j;
+    e_row[e] = e_row[j];
+    e_row[j] = keep[j];
+  }
+  for (j = 0; j < w; j++)
+    for (c = 0; c < w; c++) stage[j * TS_W + c] = A[IDX(j, c, lda)];
+  /* inv(U11), column by column: U y = e_c by back substitution */
+  for (c = 0; c < TS_W; c++) {
+    float y[TS_W];
+    int q;
+    for (i = 0; i < TS_W; i++) y[i] = 0.f;
+    if (c < w)
+      for (i = c; i >= 0; i--) {
+        float acc = i == c ? 1.f : 0.f;
+        for (q = i + 1; q <= c; q++) acc = fmaf(-rows[i * TS_W + q], y[q], acc);
+        y[i] = acc * (1.0f / rows[i * TS_W + i]);
+      }
+    for (i = 0; i < TS_W; i++) uinv[i * TS_W + c] = y[i];
+  }
+  /* the panel without further pivoting: row i >= w := (source row) inv(U11) */
+  for (i = w; i < r; i++) {
+    float b2[TS_W], x[TS_W];
+    int q = -1, e, k2;
+    for (e = w; e < ne; e++)
+      if (e_pos[e] == i && e_row[e] != e_pos[e]) q = e_row[e];
+    for (c = 0; c < TS_W; c++) {
+      b2[c] = c < w ? (q >= 0 ? stage[q * TS_W + c] : A[IDX(i, c, lda)]) : 0.f;
+      x[c] = 0.f;
+    }
+    for (k2 = 0; k2 < TS_W; k2++)
+      for (c = k2; c < TS_W; c++) x[c] = fmaf(b2[k2], uinv[k2 * TS_W + c], x[c]);
+    for (c = 0; c < w; c++) A[IDX(i, c, lda)] = x[c];
+  }
+  for (i = 0; i < w; i++)
+    for (c = 0; c < w; c++) A[IDX(i, c, lda)] = rows[i * TS_W + c];
+  free(slots);
+}

@@ -499,6 +499,7 @@ extern "C" void pla_kernels_release(void) {
   g_ws.bytes = 0;
   g_ws.epoch = kNoEpoch;
   release_noalloc();
+  pla_tslu_release();
 }
 
 // ---------------------------------------------------------------------------

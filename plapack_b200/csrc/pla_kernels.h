@@ -45,6 +45,14 @@ int pla_k_lu_panel_ex(int dt, int r, int w, void *A, long lda, int *piv, int *st
 int pla_k_lu_panel(int dt, int r, int w, void *A, long lda, int *piv, int *status,
                    int *zero_info, int row_base, cudaStream_t s);
 
+/* ---- tournament-pivoted LU of an r x w fp32 panel, w <= 32 (k_tslu.cu): the
+ * pivots (offset encoding) to piv, the panel overwritten by L \ U under them;
+ * zero_info as above.  One launch sequence at a time (its workspace and
+ * counters are shared). */
+int pla_k_lu_panel_tslu(int r, int w, float *A, long lda, int *piv, int *zero_info,
+                        int row_base, int max_ctas, cudaStream_t s);
+void pla_tslu_release(void);
+
 /* ---- row interchanges: for i in [0, npiv): swap rows i and i + piv[i] of the
  * block whose row 0 is A (rows relative to A), in columns [c0, c1) and
  * [c2, c3). */

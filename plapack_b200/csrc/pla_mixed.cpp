@@ -32,7 +32,7 @@ int chol_on_device(int dt, int n, char *A, long lda, int nb, int *info_host);
 int trsm_device(int dt, char side, char uplo, char trans, char diag, int nt, int other,
                 double alpha, const char *T, long ldt, char *B, long ldb);
 int panel_lu(int dt, int r, int b, char *P, long lda, int *piv, int *status, int *zero_info,
-             int row_base, int max_ctas);
+             int row_base, int max_ctas, int pivoting);
 }
 
 namespace {
@@ -59,6 +59,7 @@ long round_up(long v, long m) { return (v + m - 1) / m * m; }
 
 struct Factor {
   int n = 0, ld = 0, prec = 0, kind = 0;  // kind 0 = LU, 1 = Cholesky
+  int pivoting = PLA_B200_PIVOT_PARTIAL;   // of the fp32 LU panels
   float *a = nullptr;     // fp32 factors (BF16, FP16, FP32)
   double *a64 = nullptr;  // FP64 factors (FP64)
   double *dsc = nullptr;  // d = diag(A)^-1/2 when the factors are those of D A D
@@ -184,7 +185,8 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
         PLA_CUDA(cudaStreamWaitEvent(s0, ev_panel, 0));
       } else {
         PhaseTimer t(&ph.panel_ms);
-        K(panel_lu(MPI_FLOAT, n - k, b, (char *)at(k, k), ld, F.piv + k, &st[0], &st[2], k, 0));
+        K(panel_lu(MPI_FLOAT, n - k, b, (char *)at(k, k), ld, F.piv + k, &st[0], &st[2], k, 0,
+                   F.pivoting));
       }
       {
         PhaseTimer t(&ph.swap_ms);
@@ -250,7 +252,7 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
           OnStream on(s1);
           PhaseTimer t(&ph.panel_ms);
           K(panel_lu(MPI_FLOAT, n - k2, b2, (char *)at(k2, k2), ld, F.piv + k2, &st[0], &st[2],
-                     k2, lookahead_ctas(MPI_FLOAT)));
+                     k2, lookahead_ctas(MPI_FLOAT), F.pivoting));
         }
         PLA_CUDA(cudaEventRecord(ev_panel, s1));
         ready = k2;
@@ -716,7 +718,8 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
   PK(poll(1));
   {
     PhaseTimer t(&ph.panel_ms);
-    K(panel_lu(MPI_FLOAT, n, std::min(nb, n), (char *)at(0, 0), ld, F.piv, &st[0], &st[2], 0, 0));
+    K(panel_lu(MPI_FLOAT, n, std::min(nb, n), (char *)at(0, 0), ld, F.piv, &st[0], &st[2], 0, 0,
+               F.pivoting));
   }
   PK(post_panel(0));
   std::vector<int> applied(ngroups, 0);  // steps already applied to each group
@@ -752,7 +755,7 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
           {
             PhaseTimer t(&ph.panel_ms);
             K(panel_lu(MPI_FLOAT, n - k0 - b, b2, (char *)at(k0 + b, k0 + b), ld, F.piv + k0 + b,
-                       &st[0], &st[2], k0 + b, lookahead_ctas(MPI_FLOAT)));
+                       &st[0], &st[2], k0 + b, lookahead_ctas(MPI_FLOAT), F.pivoting));
           }
           PK(post_panel(k + 1));
         }
@@ -805,6 +808,8 @@ int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
   if (p.gmres_restart <= 0) p.gmres_restart = 30;
   if (p.precision < PLA_B200_PREC_BF16 || p.precision > PLA_B200_PREC_FP8)
     PLA_FAIL("unknown precision");
+  if (p.panel_pivoting != PLA_B200_PIVOT_PARTIAL && p.panel_pivoting != PLA_B200_PIVOT_TOURNAMENT)
+    PLA_FAIL("unknown panel pivoting");
   const int n = A->length, nrhs = B->width;
   if (n == 0 || nrhs == 0) {
     if (rep) *rep = PLA_Mixed_report{1, 0, 0, 0, 0.0, 0.0, 0.0, p.precision, 0};
@@ -873,6 +878,7 @@ int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
     F.ld = (int)ldf;
     F.prec = prec;
     F.kind = kind;
+    F.pivoting = p.panel_pivoting;
     F.piv = piv;
     F.status = status;
     PLA_CUDA(cudaMemsetAsync(status, 0, 64, stream()));
@@ -1005,6 +1011,7 @@ void PLA_Mixed_params_default(PLA_Mixed_params *p) {
   p->nb = 0;
   p->escalate = 1;
   p->tol = 0.0;
+  p->panel_pivoting = PLA_B200_PIVOT_TOURNAMENT;
 }
 
 int PLA_General_solve_mixed(PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *params,

@@ -152,17 +152,24 @@ namespace pla {
 // rank-kSub update.  Pivot choices are those of the column-by-column loop;
 // only the rounding order of the panel's trailing columns differs.
 int panel_lu(int dt, int r, int b, char *P, long lda, int *piv, int *status, int *zero_info,
-             int row_base, int max_ctas) {
+             int row_base, int max_ctas, int pivoting) {
   constexpr int kSub = 32;
   const int es = dt == MPI_DOUBLE ? 8 : 4;
   auto at = [&](long i, long j) { return P + (i + j * lda) * es; };
-  if (b <= kSub)
-    return pla_k_lu_panel_ex(dt, r, b, P, lda, piv, status, zero_info, row_base, max_ctas,
-                             stream());
+  // one sub-panel of width sb at (s, s): partial pivoting (the reference's
+  // column loop, one exchange round per column), or -- fp32 only, for the
+  // mixed LU whose pivots need not be the reference's -- tournament pivoting
+  auto factor = [&](int s, int sb) -> int {
+    if (pivoting == PLA_B200_PIVOT_TOURNAMENT && dt == MPI_FLOAT)
+      return pla_k_lu_panel_tslu(r - s, sb, (float *)at(s, s), lda, piv + s, zero_info,
+                                 row_base + s, max_ctas, stream());
+    return pla_k_lu_panel_ex(dt, r - s, sb, at(s, s), lda, piv + s, status, zero_info,
+                             row_base + s, max_ctas, stream());
+  };
+  if (b <= kSub) return factor(0, b);
   for (int s = 0; s < b; s += kSub) {
     const int sb = std::min(kSub, b - s), rest = b - s - sb;
-    int e = pla_k_lu_panel_ex(dt, r - s, sb, at(s, s), lda, piv + s, status, zero_info,
-                              row_base + s, max_ctas, stream());
+    int e = factor(s, sb);
     if (e) return e;
     e = pla_k_laswp(dt, at(s, 0), lda, sb, piv + s, 0, s, s + sb, b, stream());
     if (e) return e;
@@ -219,7 +226,8 @@ int lu_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, Status 
       PLA_CUDA(cudaStreamWaitEvent(s0, ev_panel, 0));
     } else {
       PhaseTimer t(&ph.panel_ms);
-      K(panel_lu(dt, r, b, at(k, k), lda, piv + k, &st->status, &st->zero_info, k, 0));
+      K(panel_lu(dt, r, b, at(k, k), lda, piv + k, &st->status, &st->zero_info, k, 0,
+                   PLA_B200_PIVOT_PARTIAL));
     }
     {
       PhaseTimer t(&ph.swap_ms);
@@ -241,7 +249,7 @@ int lu_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, Status 
         OnStream on(s1);
         PhaseTimer t(&ph.panel_ms);
         K(panel_lu(dt, m - k2, b2, at(k2, k2), lda, piv + k2, &st->status, &st->zero_info, k2,
-                   lookahead_ctas(dt)));
+                   lookahead_ctas(dt), PLA_B200_PIVOT_PARTIAL));
       }
       PLA_CUDA(cudaEventRecord(ev_panel, s1));
       ready = k2;

@@ -133,6 +133,25 @@ def case_panel(torch, lib, a):
             "gbs": 2.0 * r * w * es / t / 1e9}
 
 
+def case_tslu(torch, lib, a):
+    """The tournament-pivoted fp32 panel (select + apply launches)."""
+    r, w = a.m, a.k
+    A0 = torch.randn(w, r, dtype=torch.float32, device="cuda")
+    A = A0.clone()
+    piv = torch.zeros(w, dtype=torch.int32, device="cuda")
+    g = _fn(lib, "pla_k_lu_panel_tslu", [i32, i32, vp, lg, vp, vp, i32, i32, vp])
+
+    def launch():
+        A.copy_(A0)
+        return g(r, w, A.data_ptr(), r, piv.data_ptr(), None, 0, a.ctas, None)
+
+    t = _time(torch, launch, a.warmup, a.reps)
+    return {"case": f"tournament panel LU {r} x {w} (f32), at most {a.ctas or 'one per SM'} "
+                    f"CTAs, copy of the panel included", "s": t,
+            "us_per_column": t / w * 1e6, "bytes_read_written": 2.0 * r * w * 4,
+            "gbs": 2.0 * r * w * 4 / t / 1e9}
+
+
 def case_laswp(torch, lib, a):
     m, n, npiv = a.m, a.n, a.k
     A = torch.randn(n, m, dtype=torch.float64, device="cuda")

@@ -37,6 +37,7 @@ PLA_ERROR = -1000
 PLA_B200_PREC_BF16, PLA_B200_PREC_FP16, PLA_B200_PREC_FP32, PLA_B200_PREC_FP64 = 1, 2, 3, 4
 PLA_B200_PREC_FP8 = 5
 PLA_B200_IR_LU, PLA_B200_IR_GMRES = 1, 2
+PLA_B200_PIVOT_PARTIAL, PLA_B200_PIVOT_TOURNAMENT = 0, 1
 
 _DT = {np.dtype(np.float64): MPI_DOUBLE, np.dtype(np.float32): MPI_FLOAT,
        np.dtype(np.int32): MPI_INT}
@@ -56,7 +57,8 @@ class PhaseTimes(ctypes.Structure):
 
 class MixedParams(ctypes.Structure):
     _fields_ = [("precision", _i), ("refinement", _i), ("max_iterations", _i),
-                ("gmres_restart", _i), ("nb", _i), ("escalate", _i), ("tol", _d)]
+                ("gmres_restart", _i), ("nb", _i), ("escalate", _i), ("tol", _d),
+                ("panel_pivoting", _i)]
 
 
 class MixedReport(ctypes.Structure):

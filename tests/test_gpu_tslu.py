@@ -1,0 +1,132 @@
+"""Tournament-pivoted fp32 panel (the mixed LU's sub-panels) against its CPU model.
+
+pla_k_lu_panel_tslu factors an r x w fp32 panel (w <= 32) with tournament
+pivoting: every block of rows picks w candidate rows by partial pivoting on
+its own, the candidate sets are merged up a tree, the root's rows become the
+pivots, and the rest of the panel is solved against their U.  The reference
+has no such panel (its pivots are partial pivoting's), so the check is twofold:
+- bit for bit against the oracle's C model of the same tree and arithmetic
+  (oracle_slu_tournament): pivots and factors identical, NaN where it has NaN;
+- as an LU: P A = L U to fp32 rounding, |L| bounded, pivots a valid
+  sequence of interchanges.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def env():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    torch.cuda.set_device(0)
+    from plapack_b200 import pla
+    s = pla.Session(nb_distr=128, nb_alg=128)
+    lib = s.lib
+    lib.pla_k_lu_panel_tslu.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                        ctypes.c_long, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    lib.pla_k_lu_panel_tslu.restype = ctypes.c_int
+    yield s, torch, pla, orc.Restated()
+    s.close()
+
+
+def run_tslu(env, A, ld, max_ctas, row_base=0):
+    s, torch, pla, _ = env
+    r, w = A.shape
+    buf = np.zeros((w, ld), dtype=np.float32)   # column-major r x w, leading dimension ld
+    buf[:, :r] = A.T
+    a = torch.from_numpy(buf).cuda()
+    piv = torch.full((w,), -7, dtype=torch.int32, device="cuda")
+    zinfo = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rc = s.lib.pla_k_lu_panel_tslu(r, w, a.data_ptr(), ld, piv.data_ptr(), zinfo.data_ptr(),
+                                   row_base, max_ctas, None)
+    assert rc == 0
+    torch.cuda.synchronize()
+    out = a.cpu().numpy()
+    assert np.array_equal(out[:, r:], buf[:, r:])   # rows past r untouched
+    return out[:, :r].T, piv.cpu().numpy(), int(zinfo.item())
+
+
+CASES = [(1000, 32, 4), (5000, 32, 72), (32768, 32, 72), (32768, 32, 148), (300, 17, 3),
+         (64, 32, 1), (100, 32, 2), (1500, 32, 148), (2000, 8, 16), (40, 32, 148),
+         (33, 32, 1), (9000, 32, 1)]
+
+
+@pytest.mark.parametrize("r,w,ctas", CASES)
+def test_tslu_matches_its_model_bit_for_bit(env, r, w, ctas):
+    rs = env[3]
+    A = np.random.default_rng(r * 7 + w).standard_normal((r, w)).astype(np.float32)
+    LU, piv, zinfo = run_tslu(env, A, r + 3, ctas)
+    LUo, pivo = rs.slu_tournament(A, ctas)
+    assert np.array_equal(piv, pivo)
+    assert np.array_equal(LU, LUo)
+    assert zinfo == 0
+
+
+@pytest.mark.parametrize("r,w,ctas", [(4096, 32, 72), (777, 20, 8)])
+def test_tslu_is_an_lu_factorization(env, r, w, ctas):
+    A = np.random.default_rng(5).standard_normal((r, w)).astype(np.float32)
+    LU, piv, _ = run_tslu(env, A, r, ctas)
+    assert np.all(piv >= 0) and np.all(np.arange(w) + piv < r)
+    perm = np.arange(r)
+    for j in range(w):
+        p = j + piv[j]
+        perm[[j, p]] = perm[[p, j]]
+    L = np.tril(LU.astype(np.float64), -1)[:, :w] + np.eye(r, w)
+    U = np.triu(LU[:w].astype(np.float64))
+    res = np.abs(A[perm].astype(np.float64) - L @ U).max() / np.abs(A).max()
+    assert res < 16 * w * 2.0 ** -24
+    assert np.abs(L).max() < 8.0                   # tournament growth stays small here
+
+
+def test_tslu_ties_zero_and_nan_columns(env):
+    """Equal candidates in different blocks (the smaller row wins), an exactly
+    zero column (first zero pivot reported, 1-based + row_base, as the
+    partial-pivoting panel does) and a NaN: all as the model has them."""
+    rs = env[3]
+    r, w = 3000, 32
+    A = np.random.default_rng(9).standard_normal((r, w)).astype(np.float32)
+    A[:, 0] = np.where(np.arange(r) % 2, 1.0, -1.0)    # every |a| equal in column 0
+    A[:, 5] = 0.0
+    A[17, 9] = np.nan
+    LU, piv, zinfo = run_tslu(env, A, r, 72, row_base=100)
+    LUo, pivo = rs.slu_tournament(A, 72)
+    assert piv[0] == 0                               # row 0 is the first of the maximal rows
+    assert np.array_equal(piv, pivo)
+    assert np.array_equal(LU, LUo, equal_nan=True)
+    assert zinfo == 100 + 6
+
+
+def test_mixed_solve_with_either_panel_pivoting(env):
+    """The fp16 mixed LU-IR solve reaches FP64 backward error with tournament
+    (the default) and with partial pivoting of its fp32 panels."""
+    s, torch, pla, _ = env
+    lib = s.lib
+    n = 3000
+    rng = np.random.default_rng(12)
+    M = np.asfortranarray(rng.standard_normal((n, n)))
+    B = M @ rng.standard_normal((n, 1))
+    for pivoting in (pla.PLA_B200_PIVOT_TOURNAMENT, pla.PLA_B200_PIVOT_PARTIAL):
+        m, b = s.matrix(n, n), s.matrix(n, 1)
+        s.set(m, M)
+        s.set(b, B)
+        prm, rep = pla.MixedParams(), pla.MixedReport()
+        lib.PLA_Mixed_params_default(ctypes.byref(prm))
+        assert prm.panel_pivoting == pla.PLA_B200_PIVOT_TOURNAMENT
+        prm.panel_pivoting = pivoting
+        prm.nb = 256
+        pla.check(lib.PLA_General_solve_mixed(m, b, ctypes.byref(prm), ctypes.byref(rep)),
+                  "PLA_General_solve_mixed")
+        X = s.get(b)
+        eta = np.abs(B - M @ X).max() / (np.abs(M).sum(axis=1).max() * np.abs(X).max() +
+                                         np.abs(B).max())
+        assert rep.converged == 1 and eta <= n * 2.0 ** -53, (pivoting, eta)
+        assert rep.precision_used == pla.PLA_B200_PREC_FP16
+        s.free(m, b)

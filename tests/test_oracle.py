@@ -174,3 +174,22 @@ def test_linpack_restatement_matches_compiled_reference(restated):
         assert np.array_equal(ps, pr)
         assert np.array_equal(np.triu(LUs), np.triu(LUr))
     ref.set_nb_alg(64)
+
+
+def test_tournament_panel_model_is_an_lu(restated):
+    """The C model of the library's tournament-pivoted fp32 panel (checked bit
+    for bit against the GPU kernel in test_gpu_tslu.py) is itself an LU with
+    interchanges: P A = L U to fp32 rounding, whatever the tree's shape."""
+    for r, w, ctas in [(1000, 32, 1), (1000, 32, 4), (5000, 32, 72), (300, 17, 3), (64, 32, 1)]:
+        A = np.random.default_rng(r + w).standard_normal((r, w)).astype(np.float32)
+        LU, piv = restated.slu_tournament(A, ctas)
+        perm = np.arange(r)
+        for j in range(w):
+            p = j + piv[j]
+            assert j <= p < r
+            perm[[j, p]] = perm[[p, j]]
+        L = np.tril(LU.astype(np.float64), -1)[:, :w] + np.eye(r, w)
+        U = np.triu(LU[:w].astype(np.float64))
+        assert np.abs(A[perm] - L @ U).max() <= 16 * w * 2.0 ** -24 * np.abs(A).max()
+        # the first pivot is the largest |a| of column 0 (smallest row on ties)
+        assert perm[0] == int(np.argmax(np.abs(A[:, 0])))
