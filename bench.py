@@ -50,6 +50,9 @@ METRIC = "n=32768 solve time: mixed-prec LU-IR vs FP64 LU, same B200, both at FP
 # M = N = 8192, K = 256 fp16 launch.  Below 1 because the last C tiles written
 # are still dirty in L2 when the launch ends.
 TC_UPDATE_TRAFFIC_RATIO = 486.5 / 545.3
+# DRAM bytes (read + write) of the panel phase per n = 32768 step: filled in
+# from the ncu capture of the tournament panel kernels (None until measured).
+PANEL_TRAFFIC_PER_STEP = None
 
 
 def parse():
@@ -176,26 +179,40 @@ def cpu_cores():
 
 # ----------------------------------------------------- reference (CPU) arm ---
 def reference_solve(n, kappa, steps=1, seed=12, warmup_n=2048):
-    """Time the upstream PLA_General_solve (PLA_LU + PLA_Trsv, nb_alg = 128,
-    error checking off, OpenBLAS on every host core) on the n x n system of
-    the headline family itself, bracketed by MPI_Wtime around the call as
-    TEST/test_lu.c:136-142 brackets PLA_LU.  One warm-up solve at warmup_n
-    first (thread pool, page faults), then `steps` timed solves at n.
+    """Time the upstream PLA_General_solve (PLA_LU nb_alg = 128, then the
+    triangular solves; error checking off, OpenBLAS on every host core) on
+    the n x n system of the headline family itself, bracketed by MPI_Wtime
+    around the call as TEST/test_lu.c:136-142 brackets PLA_LU.  One warm-up
+    solve at warmup_n first (thread pool, page faults), then `steps` timed
+    solves at n.
+
+    The right-hand side goes in as two columns, b and a zero column, so that
+    PLA_General_solve takes its PLA_Trsm branch (SOLVERS/LU/PLA_General.c):
+    with one column it calls PLA_Trsv, whose upper-triangular solve splits
+    views at byte offsets computed in 32-bit ints (OBJ/PLA_Obj.c:2284-2285,
+    left_global_width * local_ldim * typesize), which overflow once
+    n * n * 8 >= 2^31 -- it crashes at n = 16384 and returns NaN at 32768.
+    The extra zero column adds 2 n^2 flops to 2/3 n^3.
     Returns the contract's cpu_baseline dict (value = median seconds)."""
     cores = cpu_cores()
     os.environ.setdefault("OPENBLAS_NUM_THREADS", str(cores))
     threads = int(os.environ["OPENBLAS_NUM_THREADS"])
     from oracle import oracle as orc
     ref = orc.Reference("openblas", nb_distr=128, nb_alg=128, error_checking=0)
+
+    def rhs2(b):
+        return np.asfortranarray(np.hstack([b, np.zeros_like(b)]))
+
     A, _, b = c3_host(warmup_n, kappa, 11)
-    ref.general_solve(A, b)
+    ref.general_solve(A, rhs2(b))
     t0 = time.perf_counter()
     A, x_true, b = c3_host(n, kappa, seed)
     gen_s = time.perf_counter() - t0
     times, X = [], None
     for _ in range(max(1, steps)):
-        _, X, _, ret, t_inner = ref.general_solve(A, b)
+        _, X, _, ret, t_inner = ref.general_solve(A, rhs2(b))
         times.append(t_inner)
+    X = X[:, :1]
     t = statistics.median(times)
     a_inf = float(np.abs(A).sum(axis=1).max())
     eta = float(np.abs(b - A @ X).max() / (a_inf * np.abs(X).max() + np.abs(b).max()))
@@ -203,11 +220,13 @@ def reference_solve(n, kappa, steps=1, seed=12, warmup_n=2048):
     return {"value": t, "unit": "s", "cores": threads, "kind": "reference",
             "steps": len(times), "warmup": 1,
             "sample": (f"the full workload, not a sample: upstream PLA_General_solve (PLA_LU "
-                       f"nb_alg=128 + PLA_Trsv, FP64, 1x1 template, error checking off, "
+                       f"nb_alg=128 + PLA_Trsm, FP64, 1x1 template, error checking off, "
                        f"OpenBLAS 0.3.15 with {threads} threads) on the n={n}, "
-                       f"kappa={kappa:g} system, {len(times)} timed solve(s) after one "
-                       f"warm-up at n={warmup_n}; backward error {eta:.2e}, forward error "
-                       f"{fwd:.2e}; matrix built in {gen_s:.1f} s (untimed)"),
+                       f"kappa={kappa:g} system (b plus a zero column: the one-column "
+                       f"PLA_Trsv path overflows 32-bit view offsets at this n), "
+                       f"{len(times)} timed solve(s) after one warm-up at n={warmup_n}; "
+                       f"backward error {eta:.2e}, forward error {fwd:.2e}; matrix built in "
+                       f"{gen_s:.1f} s (untimed)"),
             "backward_error": eta, "forward_error": fwd, "solve_seconds": times}
 
 
@@ -597,27 +616,73 @@ def run_ours(args):
     eta = (r.abs().max() / (a_inf * x.abs().max() + b.abs().max())).item()
     fwd = ((x - x_true).abs().max() / x_true.abs().max()).item()
 
-    # tensor-core update roofline: algorithmic bytes (fp32 C read + write,
-    # fp16 L and U read) over the update kernels' own event-timed duration
+    # ---- roofline of every phase of the step, the largest share first ----
+    # Algorithmic bytes per step, by phase (n = order, nb = block, 32-column
+    # sub-panels, r = rows of a panel, rest = trailing columns):
+    #   panel   each sub-panel read and written, 2 r_s 32 4, plus its update of
+    #           the panel's columns to its right, 2 (r_s - 32) right 4
+    #   update  the fp32 trailing matrix read and written, 8 rest^2, and the
+    #           fp16 L and U' panels read, 2 rest nb 2
+    #   trsm    U12 (nb x rest) read and written, 8 nb rest
+    #   convert the fp32 L and U12 read and their fp16 packs written, 6 (2 rest nb)
+    #   swap    nb interchanges across the other n - nb columns, 16 (n - nb) nb
+    #   refine  per GMRES iteration and per outer step: the FP64 matrix read
+    #           once (8 n^2) and both fp32 triangles once (4 n^2)
     nb = args.nb
-    steps_bytes = 0.0
+    by = {"panel": 0.0, "update": 0.0, "trsm": 0.0, "convert": 0.0, "swap": 0.0}
+    update_launch_bytes = 0.0
     for k in range(0, n, nb):
-        rest = n - k - min(nb, n - k)
+        b = min(nb, n - k)
+        r = n - k
+        rest = r - b
+        for s0 in range(0, b, 32):
+            sb = min(32, b - s0)
+            by["panel"] += 2.0 * (r - s0) * sb * 4 + 2.0 * max(r - s0 - sb, 0) * (b - s0 - sb) * 4
+        by["swap"] += 16.0 * (n - b) * b
         if rest > 0:
-            steps_bytes += rest * rest * 8.0 + 2.0 * rest * nb * 2.0
-    algo_bytes = steps_bytes * args.steps
+            by["update"] += rest * rest * 8.0 + 2.0 * rest * nb * 2.0
+            by["trsm"] += 8.0 * b * rest
+            by["convert"] += 6.0 * 2 * rest * b
+    iters = report.inner_iterations + report.iterations
+    by["refine"] = iters * 12.0 * n * n
     peak, peak_src = measured_peaks()
-    achieved = algo_bytes / (ph.update_ms / 1e3) / 1e9 if ph.update_ms > 0 else None
-    per_launch = steps_bytes / max(1, ph.update_launches // max(1, args.steps))
-    roofline = {"bound": "hbm", "kernel": "tc_update_k (tcgen05 fp16 trailing update)",
-                "achieved": achieved, "peak": peak, "peak_source": peak_src, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None,
-                "traffic": (per_launch * TC_UPDATE_TRAFFIC_RATIO) if TC_UPDATE_TRAFFIC_RATIO else None,
-                "algorithmic_bytes_per_launch": per_launch,
-                "update_ms_per_step": ph.update_ms / args.steps,
+    ms = {"panel": ph.panel_ms / args.steps, "update": ph.update_ms / args.steps,
+          "trsm": ph.trsm_ms / args.steps, "convert": ph.convert_ms / args.steps,
+          "swap": ph.swap_ms / args.steps, "refine": report.refine_ms}
+    kernels = {
+        "panel": "tslu_select_k + tslu_apply_k (tournament-pivoted fp32 sub-panels), laswp_k, "
+                 "trsm_left_k, sgemm_k (updates inside the panel); on the lookahead stream",
+        "update": "tc_update_k (tcgen05 fp16 trailing update, TMA reduce-add into fp32)",
+        "trsm": "trsm_left_k / sgemm_k (U12 = inv(L11) A12)",
+        "convert": "pack_rows_k, convert_k (fp32 -> fp16 operand packs)",
+        "swap": "laswp_k (row interchanges outside the panel)",
+        "refine": "gemv_slices_k + gemv_reduce_k (FP64 residual), trsv_ticket_k (fp32 factors), "
+                  "basis kernels (GMRES)"}
+    step_ms = mixed_s * 1e3
+    phases = []
+    for key in sorted(ms, key=lambda q: -ms[q]):
+        ach = by[key] / (ms[key] / 1e3) / 1e9 if ms[key] > 0 else None
+        phases.append({"phase": key, "kernels": kernels[key], "ms_per_step": ms[key],
+                       "share_of_step": ms[key] / step_ms if step_ms else None,
+                       "algorithmic_bytes_per_step": by[key], "achieved_gbs": ach,
+                       "frac": (ach / peak) if ach else None})
+    top = phases[0]
+    upd_launches = max(1, ph.update_launches // max(1, args.steps))
+    update_launch_bytes = by["update"] / upd_launches
+    roofline = {"bound": "hbm", "kernel": top["kernels"], "phase": top["phase"],
+                "achieved": top["achieved_gbs"], "peak": peak, "peak_source": peak_src,
+                "unit": "GB/s", "frac": top["frac"],
+                "traffic": (PANEL_TRAFFIC_PER_STEP if top["phase"] == "panel" else
+                            update_launch_bytes * TC_UPDATE_TRAFFIC_RATIO
+                            if top["phase"] == "update" else None),
+                "traffic_note": ("DRAM bytes per step of the panel phase, scaled from one ncu "
+                                 "capture of tslu_select_k + tslu_apply_k" if
+                                 top["phase"] == "panel" else
+                                 "DRAM bytes of one tc_update_k launch (ncu)"),
+                "phases": phases,
                 "update_launches_per_step": ph.update_launches / args.steps,
-                "phase_ms_per_step": {k: getattr(ph, k) / args.steps for k in
-                                      ("panel_ms", "swap_ms", "trsm_ms", "convert_ms", "update_ms")}}
+                "update_algorithmic_bytes_per_launch": update_launch_bytes,
+                "update_traffic_per_launch": update_launch_bytes * TC_UPDATE_TRAFFIC_RATIO}
 
     # ---- FP64 LU arm (PLA_General_solve), restoring A every step ----
     fp64_s = None

@@ -22,7 +22,7 @@
 //                  L11 \ U11, every other row i gets (P A)_i inv(U11),
 //                  reading a displaced row from the copy.
 //
-// A CTA factors at most kMaxCand candidate rows per pass (two per thread);
+// A CTA factors at most kMaxCand candidate rows per pass (kRows per thread);
 // taller blocks run several passes, carrying the w rows kept so far.  No
 // kernel here waits on another CTA, so none can hang; the counters a group
 // used are reset by the CTA that finished it.  The column loop is not
@@ -39,8 +39,12 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kW = 32;                  // sub-panel width (columns)
-constexpr int kMaxCand = 2 * kThreads;  // candidate rows one pass factors
-constexpr int kGroup = kMaxCand / kW;   // candidate sets merged per tree node (16)
+// Candidate rows per thread.  Each tree level costs w column steps, each
+// step's time grows with the rows a thread updates: measured at 32768 x 32 on
+// 72 CTAs, 2 rows (3 levels) took 92 us, 4 rows (2 levels) 99 us.
+constexpr int kRows = 2;
+constexpr int kMaxCand = kRows * kThreads;  // candidate rows one pass factors
+constexpr int kGroup = kMaxCand / kW;       // candidate sets merged per tree node (16)
 
 // Candidate order: larger |value| first (bits(|x|) + 2; NaN 1; 0 = none), then
 // the smaller row.
@@ -78,20 +82,20 @@ __device__ __forceinline__ unsigned long long warp_max_key(unsigned long long x)
 // `root`, sm.rows row j = the kept row j's factored values (row j of
 // L11 \ U11).  All threads call it.
 //
-// Each thread holds two candidate rows in registers, shifted left by one
-// column after every step, so the current column is always v[h][0] and every
-// index is static.  The multipliers shifted out go to `hist` (needed only for
-// the rows the root keeps).  One barrier per column: every warp posts its
-// best candidate (row, reciprocal pivot) before it, every thread picks the
-// same winner after it.
+// Each thread holds kRows candidate rows in registers (slots tid + h kThreads),
+// shifted left by one column after every step, so the current column is
+// always v[h][0] and every index is static.  The multipliers shifted out go
+// to `hist` (needed only for the rows the root keeps).  One barrier per
+// column: every warp posts its best candidate (row, reciprocal pivot) before
+// it, every thread picks the same winner after it.
 __device__ __forceinline__ int select_rows(const float *__restrict__ A, long lda, int w, int cnt,
                                            SelectSmem &sm, float *hist, bool root) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  float v[2][kW];
-  int id[2];
-  bool live[2];
+  float v[kRows][kW];
+  int id[kRows];
+  bool live[kRows];
 #pragma unroll
-  for (int h = 0; h < 2; h++) {
+  for (int h = 0; h < kRows; h++) {
     const int s = tid + h * kThreads;
     id[h] = s < cnt ? sm.ids[s] : -1;
     live[h] = id[h] >= 0;
@@ -99,32 +103,32 @@ __device__ __forceinline__ int select_rows(const float *__restrict__ A, long lda
     for (int c = 0; c < kW; c++)
       v[h][c] = (live[h] && c < w) ? A[(long)id[h] + (long)c * lda] : 0.f;
   }
-  const int nlive = __syncthreads_count(live[0]) + __syncthreads_count(live[1]);
+  int nlive = 0;
+#pragma unroll
+  for (int h = 0; h < kRows; h++) nlive += __syncthreads_count(live[h]);
   const int k = nlive < w ? nlive : w;
   for (int j = 0; j < k; j++) {
     const int par = j & 1;
-    unsigned long long key[2];
+    unsigned long long mine = 0;
+    int mh = 0;
 #pragma unroll
-    for (int h = 0; h < 2; h++)
-      key[h] = live[h] ? ((unsigned long long)cand_key(v[h][0]) << 32) |
-                             (0xffffffffu - (unsigned)id[h])
-                       : 0ull;
-    const int mh = key[1] > key[0];
-    const unsigned long long mine = mh ? key[1] : key[0];
+    for (int h = 0; h < kRows; h++) {
+      const unsigned long long key =
+          live[h] ? ((unsigned long long)cand_key(v[h][0]) << 32) | (0xffffffffu - (unsigned)id[h])
+                  : 0ull;
+      if (key > mine) { mine = key; mh = h; }
+    }
     const unsigned long long best = warp_max_key(mine);
     if (best != 0 && mine == best) {
       float4 *dst = reinterpret_cast<float4 *>(sm.wrow[par][warp]);
-      if (mh) {
 #pragma unroll
-        for (int q = 0; q < kW / 4; q++)
-          dst[q] = make_float4(v[1][4 * q], v[1][4 * q + 1], v[1][4 * q + 2], v[1][4 * q + 3]);
-        sm.winv[par][warp] = 1.0f / v[1][0];
-      } else {
+      for (int h = 0; h < kRows; h++)
+        if (h == mh) {
 #pragma unroll
-        for (int q = 0; q < kW / 4; q++)
-          dst[q] = make_float4(v[0][4 * q], v[0][4 * q + 1], v[0][4 * q + 2], v[0][4 * q + 3]);
-        sm.winv[par][warp] = 1.0f / v[0][0];
-      }
+          for (int q = 0; q < kW / 4; q++)
+            dst[q] = make_float4(v[h][4 * q], v[h][4 * q + 1], v[h][4 * q + 2], v[h][4 * q + 3]);
+          sm.winv[par][warp] = 1.0f / v[h][0];
+        }
       sm.wslot[par][warp] = tid + mh * kThreads;
     }
     if (lane == 0) sm.wkey[par][warp] = best;
@@ -148,7 +152,7 @@ __device__ __forceinline__ int select_rows(const float *__restrict__ A, long lda
     }
     const float inv = sm.winv[par][gw];
 #pragma unroll
-    for (int h = 0; h < 2; h++)
+    for (int h = 0; h < kRows; h++)
       if (live[h] && id[h] == gr) live[h] = false;
     if (tid == 0) {
       sm.keep[j] = gr;
@@ -156,7 +160,7 @@ __device__ __forceinline__ int select_rows(const float *__restrict__ A, long lda
     }
     if (root && tid < w - j) sm.rows[j * kW + j + tid] = sm.wrow[par][gw][tid];  // U part
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
+    for (int h = 0; h < kRows; h++) {
       const float l = v[h][0] * inv;
       if (live[h]) {
         hist[j * kMaxCand + tid + h * kThreads] = l;
