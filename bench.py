@@ -631,18 +631,19 @@ def run_ours(args):
     nb = args.nb
     by = {"panel": 0.0, "update": 0.0, "trsm": 0.0, "convert": 0.0, "swap": 0.0}
     update_launch_bytes = 0.0
-    for k in range(0, n, nb):
-        b = min(nb, n - k)
-        r = n - k
-        rest = r - b
-        for s0 in range(0, b, 32):
-            sb = min(32, b - s0)
-            by["panel"] += 2.0 * (r - s0) * sb * 4 + 2.0 * max(r - s0 - sb, 0) * (b - s0 - sb) * 4
-        by["swap"] += 16.0 * (n - b) * b
+    for k0 in range(0, n, nb):
+        bw = min(nb, n - k0)
+        rows = n - k0
+        rest = rows - bw
+        for s0 in range(0, bw, 32):
+            sb = min(32, bw - s0)
+            by["panel"] += (2.0 * (rows - s0) * sb * 4
+                            + 2.0 * max(rows - s0 - sb, 0) * (bw - s0 - sb) * 4)
+        by["swap"] += 16.0 * (n - bw) * bw
         if rest > 0:
             by["update"] += rest * rest * 8.0 + 2.0 * rest * nb * 2.0
-            by["trsm"] += 8.0 * b * rest
-            by["convert"] += 6.0 * 2 * rest * b
+            by["trsm"] += 8.0 * bw * rest
+            by["convert"] += 6.0 * 2 * rest * bw
     iters = report.inner_iterations + report.iterations
     by["refine"] = iters * 12.0 * n * n
     peak, peak_src = measured_peaks()

@@ -381,6 +381,10 @@ double dot(int n, const double *x, const double *y, double *tmp) {
   return h;
 }
 
+// GMRES iterations after which a cycle that has not reduced its residual
+// tenfold is cut short (see gmres)
+constexpr int kSlowCycle = 16;
+
 // one restarted-GMRES correction: d ~= A^{-1} r (d, r fp64 columns)
 int gmres(const Factor &F, const double *A, long lda, const double *r, double *d, int restart,
           double tau, double *V, double *w, double *tmp, float *t32, double *work, int *iters) {
@@ -432,6 +436,15 @@ int gmres(const Factor &F, const double *A, long lda, const double *r, double *d
     g[j + 1] = -sn[j] * g[j];
     g[j] = cs[j] * g[j];
     if (std::fabs(g[j + 1]) <= tau * beta || hn == 0) {
+      j++;
+      break;
+    }
+    // kSlowCycle iterations without a tenfold reduction of the preconditioned
+    // residual: these factors are too far from A for the cycle to converge
+    // (kappa times their precision is large).  Stop here, keep the partial
+    // correction, and let the caller's stagnation test escalate instead of
+    // running out the restart.
+    if (j + 1 >= kSlowCycle && std::fabs(g[j + 1]) > 0.1 * beta) {
       j++;
       break;
     }
@@ -536,6 +549,8 @@ int gmres_block(const Factor &F, const double *A, long lda, const double *R, dou
       gs[j] = css[j] * gs[j];
       jend[s] = j + 1;
       if (std::fabs(gs[j + 1]) <= tau * beta[s] || h1 == 0) next &= ~(1u << s);
+      // a column as slow as the single-column cycle's cut-off stops too
+      if (j + 1 >= kSlowCycle && std::fabs(gs[j + 1]) > 0.1 * beta[s]) next &= ~(1u << s);
     }
     K(pla_k_basis_scale(n, nrhs, V, ldv, j + 1, sc.data(), active, stream()));
     active = next;
