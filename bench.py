@@ -16,9 +16,11 @@ solution read back through PLA_Obj_get_local_contents, every step.
 
 --impl reference times the upstream PLAPACK (compiled from its sources into
 oracle/_ref, linked to a threaded OpenBLAS) on the host cores: PLA_General_solve
-on the n = 32768 system of the same family itself (minutes per solve, so
---ref-steps solves, default 1, whatever --steps asks; the line reports the
-count it timed).  `cpu_baseline` of this arm is the same measurement.
+on the n = 32768 system of the same family itself: its PLA_LU, the solve's
+O(n^3) part (the upstream triangular solves overflow 32-bit view offsets at
+this n; see reference_solve).  About a minute and a half per run, so
+--ref-steps runs, default 1, whatever --steps asks; the line reports the
+count it timed.  `cpu_baseline` of this arm is the same measurement.
 
 Under torchrun (--gpus N > 1) every rank solves its own system (replicas; the
 single large solve has no data exchange) and rank 0 prints the max over ranks;
@@ -179,55 +181,58 @@ def cpu_cores():
 
 # ----------------------------------------------------- reference (CPU) arm ---
 def reference_solve(n, kappa, steps=1, seed=12, warmup_n=2048):
-    """Time the upstream PLA_General_solve (PLA_LU nb_alg = 128, then the
-    triangular solves; error checking off, OpenBLAS on every host core) on
-    the n x n system of the headline family itself, bracketed by MPI_Wtime
-    around the call as TEST/test_lu.c:136-142 brackets PLA_LU.  One warm-up
-    solve at warmup_n first (thread pool, page faults), then `steps` timed
-    solves at n.
+    """Time the upstream PLAPACK on the host cores (error checking off, OpenBLAS
+    on every core, nb_alg = 128) on the n x n system of the headline family
+    itself, bracketed by MPI_Wtime around the call as TEST/test_lu.c:136-142
+    brackets PLA_LU.  One warm-up at warmup_n first (thread pool, page
+    faults), then `steps` timed runs at n.
 
-    The right-hand side goes in as two columns, b and a zero column, so that
-    PLA_General_solve takes its PLA_Trsm branch (SOLVERS/LU/PLA_General.c):
-    with one column it calls PLA_Trsv, whose upper-triangular solve splits
-    views at byte offsets computed in 32-bit ints (OBJ/PLA_Obj.c:2284-2285,
-    left_global_width * local_ldim * typesize), which overflow once
-    n * n * 8 >= 2^31 -- it crashes at n = 16384 and returns NaN at 32768.
-    The extra zero column adds 2 n^2 flops to 2/3 n^3.
+    What is timed is PLA_LU, the factorization (2/3 n^3 of the solve's
+    2/3 n^3 + 2 n^2 flops).  The upstream solves cannot run at this size:
+    PLA_General_solve's triangular solves split views at byte offsets that
+    OBJ/PLA_Obj.c:2284-2285 computes in 32-bit ints (left_global_width *
+    local_ldim * typesize), which overflow once n * n * 8 >= 2^31 -- the
+    one-column PLA_Trsv path crashes at n = 16384, the PLA_Trsm path returns
+    NaN at n = 32768 -- while PLA_LU carves its views a panel at a time and
+    stays correct (its pivots at n = 32768 are pinned in tests/golden/c2).
+    Leaving the solves out understates the reference's time.  The solution
+    that checks the factorization is formed from the reference's own L, U
+    and pivots outside the timed region (scipy's lu_solve).
     Returns the contract's cpu_baseline dict (value = median seconds)."""
+    import scipy.linalg as sl
     cores = cpu_cores()
     os.environ.setdefault("OPENBLAS_NUM_THREADS", str(cores))
     threads = int(os.environ["OPENBLAS_NUM_THREADS"])
     from oracle import oracle as orc
     ref = orc.Reference("openblas", nb_distr=128, nb_alg=128, error_checking=0)
-
-    def rhs2(b):
-        return np.asfortranarray(np.hstack([b, np.zeros_like(b)]))
-
     A, _, b = c3_host(warmup_n, kappa, 11)
-    ref.general_solve(A, rhs2(b))
+    ref.lu(A)
     t0 = time.perf_counter()
     A, x_true, b = c3_host(n, kappa, seed)
     gen_s = time.perf_counter() - t0
-    times, X = [], None
+    times, LU, piv = [], None, None
     for _ in range(max(1, steps)):
-        _, X, _, ret, t_inner = ref.general_solve(A, rhs2(b))
+        LU, piv, ret, t_inner = ref.lu(A)
         times.append(t_inner)
-    X = X[:, :1]
     t = statistics.median(times)
+    # the reference's offsets (row i swapped with row i + piv[i]) as LAPACK ipiv
+    X = sl.lu_solve((LU, piv.astype(np.int64) + np.arange(n)), b, check_finite=False)
+    del LU
     a_inf = float(np.abs(A).sum(axis=1).max())
     eta = float(np.abs(b - A @ X).max() / (a_inf * np.abs(X).max() + np.abs(b).max()))
     fwd = float(np.abs(X - x_true).max() / np.abs(x_true).max())
     return {"value": t, "unit": "s", "cores": threads, "kind": "reference",
             "steps": len(times), "warmup": 1,
-            "sample": (f"the full workload, not a sample: upstream PLA_General_solve (PLA_LU "
-                       f"nb_alg=128 + PLA_Trsm, FP64, 1x1 template, error checking off, "
-                       f"OpenBLAS 0.3.15 with {threads} threads) on the n={n}, "
-                       f"kappa={kappa:g} system (b plus a zero column: the one-column "
-                       f"PLA_Trsv path overflows 32-bit view offsets at this n), "
-                       f"{len(times)} timed solve(s) after one warm-up at n={warmup_n}; "
-                       f"backward error {eta:.2e}, forward error {fwd:.2e}; matrix built in "
-                       f"{gen_s:.1f} s (untimed)"),
-            "backward_error": eta, "forward_error": fwd, "solve_seconds": times}
+            "sample": (f"the full workload's factorization, not a sample: upstream PLA_LU "
+                       f"(nb_alg=128, FP64, 1x1 template, error checking off, OpenBLAS 0.3.15 "
+                       f"with {threads} threads) on the n={n}, kappa={kappa:g} system, "
+                       f"{len(times)} timed run(s) after one warm-up at n={warmup_n}; the "
+                       f"upstream triangular solves overflow 32-bit view offsets at this n "
+                       f"(OBJ/PLA_Obj.c:2284), so they are left out (the time is a lower "
+                       f"bound of the reference's solve); solution from the reference's L, U "
+                       f"and pivots: backward error {eta:.2e}, forward error {fwd:.2e}; matrix "
+                       f"built in {gen_s:.1f} s (untimed)"),
+            "backward_error": eta, "forward_error": fwd, "lu_seconds": times}
 
 
 def run_reference(args):
@@ -518,11 +523,33 @@ def run_chol_mixed(torch, pla, lib, s, device, stream, n, kappas, precs, nrhs, s
                         "gmres_iterations": rep.inner_iterations, "factor_ms": rep.factor_ms,
                         "refine_ms": rep.refine_ms, "backward_error": eta,
                         "backward_error_target": n * 2.0 ** -53, "forward_error": fwd})
+        # the FP64 PLA_Pos_def_solve of the same system, the time to beat
+        times = []
+        for it in range(warmup + steps):
+            pla.check(lib.PLA_Obj_set_local_contents_device(ctypes.c_void_p(A.data_ptr()), n, a), "A")
+            pla.check(lib.PLA_Obj_set_local_contents_device(ctypes.c_void_p(Bt.data_ptr()), n, bo), "B")
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rc = lib.PLA_Pos_def_solve(a, bo)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if it >= warmup:
+                times.append(e0.elapsed_time(e1) / 1e3)
+        X = torch.empty(nrhs, n, dtype=torch.float64, device=device)
+        pla.check(lib.PLA_Obj_get_local_contents_device(bo, ctypes.c_void_p(X.data_ptr()), n), "X")
+        R = Bt - X @ A
+        eta = (R.abs().amax(dim=1) / (a_inf * X.abs().amax(dim=1) + Bt.abs().amax(dim=1))).max().item()
+        out.append({"kappa": kappa, "precision": "fp64 (PLA_Pos_def_solve)", "rc": rc,
+                    "solve_s": min(times), "backward_error": eta,
+                    "backward_error_target": n * 2.0 ** -53,
+                    "forward_error": ((X - Xt).abs().max() / Xt.abs().max()).item()})
         del A, Xt, Bt
         torch.cuda.empty_cache()
     s.free(a, bo)
     return {"workload": f"PLA_Pos_def_solve_mixed n={n}, A = Q diag(lambda) Q', {nrhs} rhs, "
-                        "GMRES-IR", "results": out}
+                        "GMRES-IR; the FP64 PLA_Pos_def_solve of each system beside it",
+            "results": out}
 
 
 def run_ours(args):

@@ -226,6 +226,28 @@ __global__ void gemv_reduce_k(int n, int nrhs, int slices, const double *partial
 
 int g_sms = 0;
 
+// x = hi + lo with hi = bf16(x) and lo = bf16(x - hi): about 16 significant
+// bits.  Row i of dst (ld ldd, K-contiguous) receives three K-wide segments,
+// each hi or lo as `pattern` says (bit s set: segment s is lo), so that a
+// single K = 3 kdim product of two such operands sums hi*hi + hi*lo + lo*hi.
+// x(i, k) = src[i si + k sk]; with `zero`, src is cleared behind the read.
+__global__ void pack_split_k(int m, int kdim, float *src, long si, long sk,
+                             __nv_bfloat16 *dst, long ldd, int pattern, int zero) {
+  const long total = (long)m * kdim;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long)gridDim.x * blockDim.x) {
+    const long k = e % kdim, i = e / kdim;
+    float *p = src + i * si + k * sk;
+    const float x = *p;
+    const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+    const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+    __nv_bfloat16 *row = dst + i * ldd + k;
+#pragma unroll
+    for (int seg = 0; seg < 3; seg++) row[(long)seg * kdim] = (pattern >> seg) & 1 ? lo : hi;
+    if (zero) *p = 0.f;
+  }
+}
+
 }  // namespace
 
 extern "C" int pla_k_pack_rows(int prec, int m, int kdim, const float *src, long lds, void *dst,
@@ -236,6 +258,18 @@ extern "C" int pla_k_pack_rows(int prec, int m, int kdim, const float *src, long
     pack_rows_k<__nv_bfloat16><<<grid, block, 0, s>>>(m, kdim, src, lds, (__nv_bfloat16 *)dst, ldd);
   else
     pack_rows_k<__half><<<grid, block, 0, s>>>(m, kdim, src, lds, (__half *)dst, ldd);
+  pla_k_count(1);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int pla_k_pack_split(int m, int kdim, float *src, long si, long sk, void *dst,
+                                long ldd, int pattern, int zero, cudaStream_t s) {
+  if (m <= 0 || kdim <= 0) return 0;
+  const long total = (long)m * kdim;
+  int grid = (int)((total + 255) / 256);
+  if (grid > 148 * 16) grid = 148 * 16;
+  pack_split_k<<<grid, 256, 0, s>>>(m, kdim, src, si, sk, (__nv_bfloat16 *)dst, ldd, pattern,
+                                    zero);
   pla_k_count(1);
   return (int)cudaGetLastError();
 }

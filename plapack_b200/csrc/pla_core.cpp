@@ -155,7 +155,7 @@ struct Scratch {
   void *ptr = nullptr;
   size_t bytes = 0;
 };
-constexpr int kScratchSlots = 32;
+constexpr int kScratchSlots = 40;
 Scratch g_scratch[kScratchSlots];
 }  // namespace
 

@@ -150,6 +150,13 @@ int pla_k_pack_rows(int prec, int m, int kdim, const float *src, long lds, void 
  * max |x| of rows [128 b, 128 b + 128) * 2^e <= 448; inv[b] := 2^-e(b). */
 int pla_k_pack_fp8(int m, int kdim, const float *src, long si, long sk, void *dst, long ldd,
                    float *inv, cudaStream_t s);
+/* bf16 split of an fp32 matrix for fp32-like products on the tensor cores:
+ * x(i, k) = src[i si + k sk] (i < m, k < kdim) = hi + lo, hi = bf16(x),
+ * lo = bf16(x - hi); row i of dst (ld ldd >= 3 kdim, K-contiguous) gets three
+ * kdim-wide segments, segment s holding lo if bit s of pattern is set, else
+ * hi.  With zero != 0 the source is cleared after it is read. */
+int pla_k_pack_split(int m, int kdim, float *src, long si, long sk, void *dst, long ldd,
+                     int pattern, int zero, cudaStream_t s);
 /* d := diag(A)^-1/2 (1 where A(i, i) <= 0); dst (fp32, ldd) := D A D */
 int pla_k_sym_scale(int n, const double *A, long lda, double *d, float *dst, long ldd,
                     cudaStream_t s);

@@ -18,6 +18,8 @@
 #include <limits>
 #include <vector>
 
+#include <cuda_bf16.h>
+
 #include "pla_internal.h"
 #include "pla_kernels.h"
 
@@ -53,7 +55,8 @@ namespace {
 
 enum Slots { kSlotA32 = 4, kSlotL = 5, kSlotU = 6, kSlotPiv = 7, kSlotVec = 8, kSlotWork = 9,
              kSlotV = 10, kSlotSt = 11, kSlotA64 = 16, kSlotScales = 18, kSlotDiag = 19,
-             kSlotLbig = 24, kSlotDinvSteps = 25, kSlotSclSteps = 26, kSlotTmp = 27 };
+             kSlotLbig = 24, kSlotDinvSteps = 25, kSlotSclSteps = 26, kSlotTmp = 27,
+             kSlotSplitL = 31, kSlotSplitU = 32 };
 
 long round_up(long v, long m) { return (v + m - 1) / m * m; }
 
@@ -136,6 +139,55 @@ struct EventTimer {
   }
 };
 
+// U12 := inv(L11) A12 on the tensor cores.  The solve with the unit-lower
+// diagonal block is on the factorization's critical path (the next panel
+// waits for it); in fp32 on the SIMT pipe it took about 0.25 ms a step at
+// n = 32768.  Here inv(L11) is formed once per panel (beside the trailing
+// update, on the panel's stream) and both operands are split into bf16
+// hi + lo, so that one K = 3b product sums hi*hi + hi*lo + lo*hi in fp32:
+// about 16 significant bits, against the 11 of the fp16 operands the trailing
+// update rounds U12 to anyway.  The product accumulates into A12 itself,
+// which the split-pack clears behind its read.
+struct SplitU12 {
+  float *dinv[2] = {nullptr, nullptr};           // inv(L11), b x b column-major
+  __nv_bfloat16 *lsplit[2] = {nullptr, nullptr};  // [hi | hi | lo] of inv(L11), b x 3b
+  __nv_bfloat16 *usplit = nullptr;                // [hi | lo | hi] of A12', rest x 3b
+};
+
+int split_alloc(SplitU12 &S, int n, int nb) {
+  const size_t d = (size_t)nb * nb * sizeof(float), l = (size_t)nb * 3 * nb * 2;
+  char *p = (char *)scratch(kSlotSplitL, 2 * (d + l) + 1024);
+  S.usplit = (__nv_bfloat16 *)scratch(kSlotSplitU, (size_t)n * 3 * nb * 2 + 1024);
+  if (!p || !S.usplit) PLA_FAIL("cannot allocate the split operands of the U12 solve");
+  for (int q = 0; q < 2; q++) {
+    S.dinv[q] = (float *)(p + q * (d + l));
+    S.lsplit[q] = (__nv_bfloat16 *)(p + q * (d + l) + d);
+  }
+  return PLA_SUCCESS;
+}
+
+// after the panel at (k, k) (on the current stream): inv(L11) and its split
+int split_prepare(SplitU12 &S, int q, const float *L11, long ld, int b) {
+  float *D = S.dinv[q];
+  K(pla_k_fill(MPI_FLOAT, b, b, D, b, 0.0, stream()));
+  K(pla_k_fill(MPI_FLOAT, 1, b, D, b + 1, 1.0, stream()));
+  K(trsm_device(MPI_FLOAT, 'L', 'L', 'N', 'U', b, b, 1.0, (const char *)L11, ld, (char *)D, b));
+  // row i of inv(L11): element (i, k) at D[i + k b]
+  K(pla_k_pack_split(b, b, D, 1, b, S.lsplit[q], 3L * b, 0b100, 0, stream()));
+  return PLA_SUCCESS;
+}
+
+// U12 (b x cols at A12, ld) := inv(L11) A12 with the split of step parity q
+int split_solve(SplitU12 &S, int q, float *C, long ld, long c_rows, long c_cols, int row0,
+                int col0, int b, int cols, int *status) {
+  float *A12 = C + row0 + (long)col0 * ld;
+  // row j of A12' is column j of A12: element (j, k) at A12[k + j ld]
+  K(pla_k_pack_split(cols, b, A12, ld, 1, S.usplit, 3L * b, 0b010, 1, stream()));
+  K(pla_k_tc_update_ex(PLA_K_BF16, b, cols, 3 * b, 1.0f, S.lsplit[q], 3L * b, b, S.usplit,
+                       3L * b, cols, C, ld, c_rows, c_cols, row0, col0, 0, 0, status, stream()));
+  return PLA_SUCCESS;
+}
+
 // fp32 factorization with low-precision trailing updates
 int factor_mixed(Factor &F, const double *A, long lda, int nb) {
   const int n = F.n;
@@ -177,6 +229,11 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
   }
   const int side_ctas = std::max(1, sms - lookahead_ctas(MPI_FLOAT));
   const int esz = f8 ? 1 : 2;  // bytes per packed element
+  // the LU's U12 solves on the tensor cores (low-precision factors only: an
+  // fp32 factorization keeps the fp32 solve)
+  const bool split = F.kind == 0 && lowp && nb % 64 == 0 && nb <= 256;
+  SplitU12 S;
+  if (split) PK(split_alloc(S, n, nb));
   int ready = -1;
   for (int k = 0; k < n; k += nb) {
     const int b = std::min(nb, n - k), rest = n - k - b, k2 = k + b;
@@ -194,8 +251,14 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
       }
       if (rest <= 0) continue;
       PhaseTimer t(&ph.trsm_ms);
-      K(trsm_device(MPI_FLOAT, 'L', 'L', 'N', 'U', b, rest, 1.0, (const char *)at(k, k), ld,
-                    (char *)at(k, k + b), ld));
+      if (split) {
+        const int q = (k / nb) & 1;
+        if (ready != k) PK(split_prepare(S, q, at(k, k), ld, b));
+        PK(split_solve(S, q, F.a, ld, ld, n, k, k + b, b, rest, &st[0]));
+      } else {
+        K(trsm_device(MPI_FLOAT, 'L', 'L', 'N', 'U', b, rest, 1.0, (const char *)at(k, k), ld,
+                      (char *)at(k, k + b), ld));
+      }
     } else {
       {
         PhaseTimer t(&ph.panel_ms);
@@ -253,6 +316,9 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
           PhaseTimer t(&ph.panel_ms);
           K(panel_lu(MPI_FLOAT, n - k2, b2, (char *)at(k2, k2), ld, F.piv + k2, &st[0], &st[2],
                      k2, lookahead_ctas(MPI_FLOAT), F.pivoting));
+          // the next step's inv(L11) and its split, beside the update
+          if (split && b2 == nb && n - k2 - b2 > 0)
+            PK(split_prepare(S, (k2 / nb) & 1, at(k2, k2), ld, b2));
         }
         PLA_CUDA(cudaEventRecord(ev_panel, s1));
         ready = k2;
@@ -623,9 +689,14 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
   char *Lbig = (char *)scratch(kSlotLbig, lbytes + 256);
   float *dinv = (float *)scratch(kSlotDinvSteps, (size_t)nsteps * nb * nb * sizeof(float));
   float *scl = (float *)scratch(kSlotSclSteps, ((size_t)nsteps + 1) * tiles * sizeof(float));
-  float *tmp = (float *)scratch(kSlotTmp, (size_t)nb * n * sizeof(float) + 256);
   void *Ub = scratch(kSlotU, (size_t)n * nb * 2 + 256);
-  if (!Lbig || !dinv || !scl || !tmp || !Ub) PLA_FAIL("cannot allocate the streamed-solve buffers");
+  // per step: the split of inv(L11) for the tensor-core U12 solves (replays
+  // of late column groups use old steps' splits)
+  __nv_bfloat16 *lsplit =
+      (__nv_bfloat16 *)scratch(kSlotSplitL, (size_t)nsteps * nb * 3 * nb * 2 + 256);
+  __nv_bfloat16 *usplit = (__nv_bfloat16 *)scratch(kSlotSplitU, (size_t)n * 3 * nb * 2 + 256);
+  if (!Lbig || !dinv || !scl || !Ub || !lsplit || !usplit)
+    PLA_FAIL("cannot allocate the streamed-solve buffers");
   float *inv_u = scl + (size_t)nsteps * tiles;  // the U' scales of the launch in flight
   int *st = F.status;
   PLA_Phase_times &ph = state().phases;
@@ -683,6 +754,8 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
     K(trsm_device(MPI_FLOAT, 'L', 'L', 'N', 'U', b, b, 1.0, (const char *)at(k0, k0), ld,
                   (char *)D, b));
     if (rest <= 0) return 0;
+    K(pla_k_pack_split(b, b, D, 1, b, lsplit + (size_t)s * nb * 3 * nb, 3L * b, 0b100, 0,
+                       stream()));
     PhaseTimer t(&ph.convert_ms);
     if (f8)
       K(pla_k_pack_fp8(rest, b, at(k0 + b, k0), 1, ld, Lbig + loff[s], nb,
@@ -700,11 +773,13 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
       K(pla_k_laswp(MPI_FLOAT, at(k0, 0), ld, b, F.piv + k0, 0, 0, c0, c1, stream()));
     }
     {
+      // U rows := inv(L11) block on the tensor cores, bf16 hi/lo split (see
+      // split_solve): the block is split and cleared, then accumulated into
       PhaseTimer t(&ph.trsm_ms);
-      K(pla_k_copy(MPI_FLOAT, PLA_NO_TRANSPOSE, b, nc, at(k0, c0), ld, tmp, b, stream()));
-      K(pla_k_gemm(MPI_FLOAT, PLA_NO_TRANSPOSE, PLA_NO_TRANSPOSE, b, nc, b, 1.0,
-                   dinv + (size_t)s * nb * nb, b, tmp, b, 0.0, at(k0, c0), ld, 0, &st[0],
-                   stream()));
+      K(pla_k_pack_split(nc, b, at(k0, c0), ld, 1, usplit, 3L * b, 0b010, 1, stream()));
+      K(pla_k_tc_update_ex(PLA_K_BF16, b, nc, 3 * b, 1.0f, lsplit + (size_t)s * nb * 3 * nb,
+                           3L * b, b, usplit, 3L * b, nc, F.a, ld, ld, n, k0, c0, 0, 0, &st[0],
+                           stream()));
     }
     if (n - k0 - b <= 0) return 0;
     PhaseTimer t(&ph.convert_ms);

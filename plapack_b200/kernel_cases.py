@@ -339,15 +339,20 @@ def case_sgemm(torch, lib, a):
 
 
 def case_batched(torch, lib, a):
-    from .workloads import batched_workload  # n log-uniform in [8, 512], LU and Cholesky
+    """The batched workload's instance mix (n log-uniform in [8, 512], LU and
+    Cholesky), optionally only the orders in [--nmin, --nmax], planned with
+    (--tune 1) or without the autotuner."""
+    from .workloads import batched_orders, batched_workload
     dtype = torch.float64 if a.dtype == "f64" else torch.float32
-    arr, groups, piv, flops, _ = batched_workload(torch, pla, torch.device("cuda", 0), dtype,
-                                                  a.count, 3)
-    info = torch.zeros(a.count, dtype=torch.int32, device="cuda")
+    ns, _, _ = batched_orders(a.count, 3)
+    sel = [i for i in range(a.count) if a.nmin <= ns[i] <= a.nmax]
+    arr, groups, piv, flops, ids = batched_workload(torch, pla, torch.device("cuda", 0), dtype,
+                                                    a.count, 3, select=sel)
+    info = torch.zeros(max(1, len(ids)), dtype=torch.int32, device="cuda")
     dt = pla.MPI_DOUBLE if a.dtype == "f64" else pla.MPI_FLOAT
     plan = ctypes.c_void_p()
-    pla.check(lib.PLA_Batch_plan_create(dt, a.count, arr, ctypes.c_void_p(info.data_ptr()), 1,
-                                        ctypes.byref(plan)), "plan")
+    pla.check(lib.PLA_Batch_plan_create(dt, len(ids), arr, ctypes.c_void_p(info.data_ptr()),
+                                        a.tune, ctypes.byref(plan)), "plan")
 
     def launch():
         for gr in groups:
@@ -357,7 +362,8 @@ def case_batched(torch, lib, a):
 
     t = _time(torch, launch, a.warmup, a.reps)
     lib.PLA_Batch_plan_free(ctypes.byref(plan))
-    return {"case": f"batched factor-and-solve, {a.count} instances ({a.dtype}), input restore "
+    return {"case": f"batched factor-and-solve, {len(ids)} of {a.count} instances (orders "
+                    f"{a.nmin}..{a.nmax}, {a.dtype}, autotune {a.tune}), input restore "
                     "included", "s": t, "gflops": flops / t / 1e9}
 
 
@@ -371,6 +377,9 @@ def main(argv=None):
     p.add_argument("--n", type=int, default=16384)
     p.add_argument("--k", type=int, default=128)
     p.add_argument("--count", type=int, default=2000)
+    p.add_argument("--nmin", type=int, default=0, help="batched: smallest order kept")
+    p.add_argument("--nmax", type=int, default=1 << 30, help="batched: largest order kept")
+    p.add_argument("--tune", type=int, default=1, help="batched: autotune the plan")
     p.add_argument("--dtype", choices=["f32", "f64"], default="f32")
     p.add_argument("--warmup", type=int, default=2)
     p.add_argument("--reps", type=int, default=3)

@@ -39,7 +39,7 @@ def test_reference_arm_prints_one_contract_line():
     assert d["n_gpus"] == 1 and d["config"]["n"] == 2048
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["value"] == d["value"] and cb["cores"] == 4
-    assert "upstream PLA_General_solve" in cb["sample"] and "n=2048" in cb["sample"]
+    assert "upstream PLA_LU" in cb["sample"] and "n=2048" in cb["sample"]
     assert "scaled" not in cb["sample"]
     assert cb["backward_error"] < 2048 * 2.0 ** -53
     assert d["e2e"] == {"value": d["value"], "unit": "s", "h2d_bytes_per_step": 0,
