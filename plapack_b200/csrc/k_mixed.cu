@@ -392,3 +392,134 @@ extern "C" int pla_k_residual(int n, int ncols, int nrhs, const double *A, long 
   pla_k_count(2);
   return (int)cudaGetLastError();
 }
+
+// ---------------------------------------------------------------------------
+// D := inv(L) for a unit-lower-triangular n x n fp32 L (n = 32, 64, 128 or
+// 256), in one CTA of 1024 threads:
+//   1. the n / 32 diagonal 32 x 32 blocks, one warp each: lane c forward-
+//      substitutes column c of the block's inverse (x_c = 1, x_i = -sum_{c <=
+//      j < i} L(i, j) x_j), the block and the columns in shared memory;
+//   2. doubling: with D11 = inv(L11) and D22 = inv(L22) known for the two
+//      h x h halves of a 2h block, D21 = -D22 (L21 D11), two h x h products
+//      per pair, h = 32, 64, 128 (products in 32-wide K tiles through shared
+//      memory, a 4 x 4 register tile per thread).
+// D (ldd) receives the whole lower triangle, unit diagonal included; the
+// strictly upper part is set to zero.  T: n * n / 2 floats of scratch.
+namespace {
+constexpr int kInvThreads = 1024;
+// dynamic shared memory: the diagonal blocks and their inverses in phase 1,
+// the product tiles in phase 2
+constexpr size_t kInvSmem = 2 * 8 * 32 * 33 * sizeof(float);
+
+// the products of one doubling level: for every pair p of h-blocks starting
+// at row q = 2 h p, T_p = L21 D11 (step 0), then D21 = -D22 T_p (step 1)
+__device__ void inv_products(int n, int h, const float *L, long ldl, float *D, long ldd,
+                             float *T, float *sA, float *sB) {
+  const int npairs = n / (2 * h), tid = threadIdx.x;
+  const int tiles = (h / 4) * (h / 4);  // 4 x 4 output tiles per product
+  for (int step = 0; step < 2; step++) {
+    for (int p0 = 0; p0 < npairs; p0++) {
+      const int q = 2 * h * p0;
+      const float *Aop = step == 0 ? L + (q + h) + (long)q * ldl : D + (q + h) + (long)(q + h) * ldd;
+      const long lda = step == 0 ? ldl : ldd;
+      const float *Bop = step == 0 ? D + q + (long)q * ldd : T + (long)p0 * h * h;
+      const long ldb = step == 0 ? ldd : h;
+      float *Cop = step == 0 ? T + (long)p0 * h * h : D + (q + h) + (long)q * ldd;
+      const long ldc = step == 0 ? h : ldd;
+      const float alpha = step == 0 ? 1.f : -1.f;
+      float acc[4][4];
+      const int t = tid < tiles ? tid : 0;
+      const int i0 = (t % (h / 4)) * 4, j0 = (t / (h / 4)) * 4;
+#pragma unroll
+      for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) acc[r][c] = 0.f;
+      for (int k0 = 0; k0 < h; k0 += 32) {
+        // stage A[:, k0 .. k0 + 32] (h x 32) and B[k0 .. k0 + 32, :] (32 x h)
+        for (int e = tid; e < h * 32; e += kInvThreads) {
+          const int i = e % h, k = e / h;
+          sA[i + k * h] = Aop[i + (long)(k0 + k) * lda];
+          const int kk = e % 32, j = e / 32;
+          sB[kk + j * 32] = Bop[(k0 + kk) + (long)j * ldb];
+        }
+        __syncthreads();
+        if (tid < tiles)
+          for (int k = 0; k < 32; k++) {
+            float a[4], b[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) a[r] = sA[(i0 + r) + k * h];
+#pragma unroll
+            for (int c = 0; c < 4; c++) b[c] = sB[k + (j0 + c) * 32];
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+#pragma unroll
+              for (int c = 0; c < 4; c++) acc[r][c] = fmaf(a[r], b[c], acc[r][c]);
+          }
+        __syncthreads();
+      }
+      if (tid < tiles)
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+          for (int c = 0; c < 4; c++) Cop[(i0 + r) + (long)(j0 + c) * ldc] = alpha * acc[r][c];
+      __syncthreads();
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kInvThreads, 1)
+trtri_unit_lower_k(int n, const float *__restrict__ L, long ldl, float *D, long ldd, float *T) {
+  extern __shared__ __align__(16) float inv_smem[];
+  auto blk = reinterpret_cast<float(*)[32][33]>(inv_smem);
+  auto xs = reinterpret_cast<float(*)[32][33]>(inv_smem + 8 * 32 * 33);
+  float *sA = inv_smem, *sB = inv_smem + 128 * 32;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // the off-diagonal blocks start at zero (the lower ones are computed below)
+  for (long e = tid; e < (long)n * n; e += kInvThreads) {
+    const int i = (int)(e % n), j = (int)(e / n);
+    if (i / 32 != j / 32) D[i + (long)j * ldd] = 0.f;
+  }
+  // 1. diagonal blocks
+  const int nb32 = n / 32;
+  if (warp < nb32) {
+    const int q = warp * 32;
+    for (int j = 0; j < 32; j++) blk[warp][lane][j] = L[(q + lane) + (long)(q + j) * ldl];
+    __syncwarp();
+    // column `lane` of the block's inverse: x_i for i >= lane
+    for (int i = 0; i < 32; i++) {
+      float x;
+      if (i < lane) x = 0.f;
+      else if (i == lane) x = 1.f;
+      else {
+        float s = 0.f;
+        for (int j = lane; j < i; j++) s = fmaf(blk[warp][i][j], xs[warp][j][lane], s);
+        x = -s;
+      }
+      xs[warp][i][lane] = x;
+    }
+    __syncwarp();
+    for (int i = 0; i < 32; i++) D[(q + i) + (long)(q + lane) * ldd] = xs[warp][i][lane];
+  }
+  __syncthreads();
+  // 2. doubling
+  for (int h = 32; h < n; h *= 2) {
+    inv_products(n, h, L, ldl, D, ldd, T, sA, sB);
+    __syncthreads();
+  }
+}
+}  // namespace
+
+extern "C" int pla_k_trtri_unit_lower(int n, const float *L, long ldl, float *D, long ldd,
+                                      float *work, cudaStream_t s) {
+  if (n <= 0) return 0;
+  if (n % 32 || n > 256 || (n & (n - 1))) return (int)cudaErrorInvalidValue;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(trtri_unit_lower_k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kInvSmem);
+    attr = true;
+  }
+  trtri_unit_lower_k<<<1, kInvThreads, kInvSmem, s>>>(n, L, ldl, D, ldd, work);
+  pla_k_count(1);
+  return (int)cudaGetLastError();
+}

@@ -157,6 +157,10 @@ int pla_k_pack_fp8(int m, int kdim, const float *src, long si, long sk, void *ds
  * hi.  With zero != 0 the source is cleared after it is read. */
 int pla_k_pack_split(int m, int kdim, float *src, long si, long sk, void *dst, long ldd,
                      int pattern, int zero, cudaStream_t s);
+/* D (ldd) := inv(L) for a unit-lower-triangular fp32 L (n x n, n = 32, 64,
+ * 128 or 256), in one CTA; work: n * n / 2 floats of scratch */
+int pla_k_trtri_unit_lower(int n, const float *L, long ldl, float *D, long ldd, float *work,
+                           cudaStream_t s);
 /* d := diag(A)^-1/2 (1 where A(i, i) <= 0); dst (fp32, ldd) := D A D */
 int pla_k_sym_scale(int n, const double *A, long lda, double *d, float *dst, long ldd,
                     cudaStream_t s);

@@ -152,13 +152,32 @@ struct SplitU12 {
   float *dinv[2] = {nullptr, nullptr};           // inv(L11), b x b column-major
   __nv_bfloat16 *lsplit[2] = {nullptr, nullptr};  // [hi | hi | lo] of inv(L11), b x 3b
   __nv_bfloat16 *usplit = nullptr;                // [hi | lo | hi] of A12', rest x 3b
+  float *work = nullptr;                          // the inverse kernel's products
 };
+
+constexpr int kSlotInvWork = 12;
+
+// inv(L11) of a unit-lower b x b block: one CTA (pla_k_trtri_unit_lower) when b
+// is a power of two from 32 to 256, else the blocked triangular solve on I.
+// The inverse sits on the panel chain of the factorization; the blocked solve
+// took about 0.16 ms a step at b = 256.
+int unit_lower_inverse(const float *L11, long ld, int b, float *D, float *work) {
+  if (b >= 32 && b <= 256 && (b & (b - 1)) == 0 && work) {
+    K(pla_k_trtri_unit_lower(b, L11, ld, D, b, work, stream()));
+    return PLA_SUCCESS;
+  }
+  K(pla_k_fill(MPI_FLOAT, b, b, D, b, 0.0, stream()));
+  K(pla_k_fill(MPI_FLOAT, 1, b, D, b + 1, 1.0, stream()));
+  K(trsm_device(MPI_FLOAT, 'L', 'L', 'N', 'U', b, b, 1.0, (const char *)L11, ld, (char *)D, b));
+  return PLA_SUCCESS;
+}
 
 int split_alloc(SplitU12 &S, int n, int nb) {
   const size_t d = (size_t)nb * nb * sizeof(float), l = (size_t)nb * 3 * nb * 2;
   char *p = (char *)scratch(kSlotSplitL, 2 * (d + l) + 1024);
   S.usplit = (__nv_bfloat16 *)scratch(kSlotSplitU, (size_t)n * 3 * nb * 2 + 1024);
-  if (!p || !S.usplit) PLA_FAIL("cannot allocate the split operands of the U12 solve");
+  S.work = (float *)scratch(kSlotInvWork, (size_t)nb * nb * sizeof(float) / 2 + 1024);
+  if (!p || !S.usplit || !S.work) PLA_FAIL("cannot allocate the split operands of the U12 solve");
   for (int q = 0; q < 2; q++) {
     S.dinv[q] = (float *)(p + q * (d + l));
     S.lsplit[q] = (__nv_bfloat16 *)(p + q * (d + l) + d);
@@ -169,9 +188,7 @@ int split_alloc(SplitU12 &S, int n, int nb) {
 // after the panel at (k, k) (on the current stream): inv(L11) and its split
 int split_prepare(SplitU12 &S, int q, const float *L11, long ld, int b) {
   float *D = S.dinv[q];
-  K(pla_k_fill(MPI_FLOAT, b, b, D, b, 0.0, stream()));
-  K(pla_k_fill(MPI_FLOAT, 1, b, D, b + 1, 1.0, stream()));
-  K(trsm_device(MPI_FLOAT, 'L', 'L', 'N', 'U', b, b, 1.0, (const char *)L11, ld, (char *)D, b));
+  PK(unit_lower_inverse(L11, ld, b, D, S.work));
   // row i of inv(L11): element (i, k) at D[i + k b]
   K(pla_k_pack_split(b, b, D, 1, b, S.lsplit[q], 3L * b, 0b100, 0, stream()));
   return PLA_SUCCESS;
@@ -695,7 +712,8 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
   __nv_bfloat16 *lsplit =
       (__nv_bfloat16 *)scratch(kSlotSplitL, (size_t)nsteps * nb * 3 * nb * 2 + 256);
   __nv_bfloat16 *usplit = (__nv_bfloat16 *)scratch(kSlotSplitU, (size_t)n * 3 * nb * 2 + 256);
-  if (!Lbig || !dinv || !scl || !Ub || !lsplit || !usplit)
+  float *inv_work = (float *)scratch(kSlotInvWork, (size_t)nb * nb * sizeof(float) / 2 + 1024);
+  if (!Lbig || !dinv || !scl || !Ub || !lsplit || !usplit || !inv_work)
     PLA_FAIL("cannot allocate the streamed-solve buffers");
   float *inv_u = scl + (size_t)nsteps * tiles;  // the U' scales of the launch in flight
   int *st = F.status;
@@ -749,10 +767,7 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
   auto post_panel = [&](int s) -> int {
     const int k0 = s * nb, b = std::min(nb, n - k0), rest = n - k0 - b;
     float *D = dinv + (size_t)s * nb * nb;
-    K(pla_k_fill(MPI_FLOAT, b, b, D, b, 0.0, stream()));
-    K(pla_k_fill(MPI_FLOAT, 1, b, D, b + 1, 1.0, stream()));
-    K(trsm_device(MPI_FLOAT, 'L', 'L', 'N', 'U', b, b, 1.0, (const char *)at(k0, k0), ld,
-                  (char *)D, b));
+    PK(unit_lower_inverse(at(k0, k0), ld, b, D, inv_work));
     if (rest <= 0) return 0;
     K(pla_k_pack_split(b, b, D, 1, b, lsplit + (size_t)s * nb * 3 * nb, 3L * b, 0b100, 0,
                        stream()));

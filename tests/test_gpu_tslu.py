@@ -130,3 +130,32 @@ def test_mixed_solve_with_either_panel_pivoting(env):
         assert rep.converged == 1 and eta <= n * 2.0 ** -53, (pivoting, eta)
         assert rep.precision_used == pla.PLA_B200_PREC_FP16
         s.free(m, b)
+
+
+@pytest.mark.parametrize("n", [32, 64, 128, 256])
+def test_unit_lower_inverse_one_cta(env, n):
+    """inv(L11) of the mixed LU's unit-lower diagonal block (pla_k_trtri_unit_lower:
+    diagonal 32 x 32 blocks by warps, then doubling): equal to the inverse to
+    fp32 rounding, unit diagonal, strictly upper part zero."""
+    import scipy.linalg as sl
+    s, torch, pla, _ = env
+    lib = s.lib
+    lib.pla_k_trtri_unit_lower.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_long,
+                                           ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p,
+                                           ctypes.c_void_p]
+    lib.pla_k_trtri_unit_lower.restype = ctypes.c_int
+    rng = np.random.default_rng(n)
+    ld = n + 5
+    L = sl.lu(rng.standard_normal((n, n)))[1]         # a unit-lower factor of a pivoted LU
+    Lbuf = np.zeros((n, ld), dtype=np.float32)      # column-major n x n, leading dimension ld
+    Lbuf[:, :n] = L.T
+    tL = torch.from_numpy(Lbuf).cuda()
+    tD = torch.full((n, n), 7.0, dtype=torch.float32, device="cuda")
+    work = torch.zeros(n * n, dtype=torch.float32, device="cuda")
+    assert lib.pla_k_trtri_unit_lower(n, tL.data_ptr(), ld, tD.data_ptr(), n, work.data_ptr(),
+                                      None) == 0
+    torch.cuda.synchronize()
+    D = tD.cpu().numpy().T.astype(np.float64)
+    assert np.all(np.triu(D, 1) == 0.0) and np.all(np.diag(D) == 1.0)
+    Dref = np.linalg.inv(L.astype(np.float32).astype(np.float64))
+    assert np.abs(D - Dref).max() <= 64 * n * 2.0 ** -24 * np.abs(Dref).max()
