@@ -652,7 +652,8 @@ def run_ours(args):
     #           fp16 L and U' panels read, 2 rest nb 2
     #   trsm    U12 (nb x rest) read and written, 8 nb rest
     #   convert the fp32 L and U12 read and their fp16 packs written, 6 (2 rest nb)
-    #   swap    nb interchanges across the other n - nb columns, 16 (n - nb) nb
+    #   swap    each interchange that moves rows (pivot offset != 0, counted on
+    #           the device) across the other n - nb columns, 16 (n - nb) each
     #   refine  per GMRES iteration and per outer step: the FP64 matrix read
     #           once (8 n^2) and both fp32 triangles once (4 n^2)
     nb = args.nb
@@ -666,11 +667,11 @@ def run_ours(args):
             sb = min(32, bw - s0)
             by["panel"] += (2.0 * (rows - s0) * sb * 4
                             + 2.0 * max(rows - s0 - sb, 0) * (bw - s0 - sb) * 4)
-        by["swap"] += 16.0 * (n - bw) * bw
         if rest > 0:
             by["update"] += rest * rest * 8.0 + 2.0 * rest * nb * 2.0
             by["trsm"] += 8.0 * bw * rest
             by["convert"] += 6.0 * 2 * rest * bw
+    by["swap"] = 16.0 * (n - nb) * ph.interchanges / args.steps
     iters = report.inner_iterations + report.iterations
     by["refine"] = iters * 12.0 * n * n
     peak, peak_src = measured_peaks()
@@ -709,6 +710,7 @@ def run_ours(args):
                                  "DRAM bytes of one tc_update_k launch (ncu)"),
                 "phases": phases,
                 "update_launches_per_step": ph.update_launches / args.steps,
+                "interchanges_per_step": ph.interchanges / args.steps,
                 "update_algorithmic_bytes_per_launch": update_launch_bytes,
                 "update_traffic_per_launch": update_launch_bytes * TC_UPDATE_TRAFFIC_RATIO}
 

@@ -43,6 +43,10 @@ typedef struct {
   double refine_ms;  /* residuals and corrections of iterative refinement */
   double convert_ms; /* precision conversions and operand packing         */
   int update_launches; /* trailing-update kernels timed in update_ms      */
+  long long interchanges; /* LU row interchanges that moved rows (pivot
+                             offset != 0), summed over the factorizations
+                             timed; each costs a read and a write of two
+                             elements in every column outside its panel   */
 } PLA_Phase_times;
 /* Phase timing uses CUDA events recorded on the library stream without
  * synchronizing; the times are collected when PLA_B200_phase_times is

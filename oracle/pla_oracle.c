@@ -283,7 +283,8 @@ DEFINE_ORACLE(float, s)
  * then the smaller row), the same arithmetic (l = x * (1/u), fmaf(-l, u, x);
  * inv(U11) by back substitution per column, the rows below as (row) inv(U11)
  * accumulated with fmaf) in the same order.
- * r x w panel (w <= 32), column-major A (lda), P leaf blocks.  Pivots in the
+ * r x w panel (w <= 32), column-major A (lda), P = min(max_ctas, ceil(r / 512))
+ * leaf blocks of R = ceil(r / P) rows.  Pivots in the
  * reference's offset encoding; A overwritten by L \ U under them.
  * ------------------------------------------------------------------------- */
 #define TS_W 32
@@ -338,7 +339,7 @@ static int ts_select(const float *A, int lda, int w, const int *ids, int cnt, in
 
 void oracle_slu_tournament(int r, int w, int max_ctas, float *A, int lda, int *piv) {
   int P = max_ctas, R, b, nsets, level_off = 0, i, j, c;
-  int maxP = (r + 2 * TS_W - 1) / (2 * TS_W);
+  int maxP = (r + TS_CAND - 1) / TS_CAND;
   int *slots, ids[TS_CAND], keep[TS_W], kept, root_done = 0;
   static float rows[TS_W * TS_W], stage[TS_W * TS_W], uinv[TS_W * TS_W];
   int e_pos[2 * TS_W], e_row[2 * TS_W], ne;

@@ -190,6 +190,16 @@ __global__ void laswp_k(T *A, long lda, int npiv, const int *piv, int c0, int c1
   }
 }
 
+// number of non-trivial interchanges (piv[i] != 0) in a pivot vector, added
+// to *ctr: one atomic per warp
+__global__ void count_interchanges_k(int npiv, const int *piv, unsigned long long *ctr) {
+  unsigned c = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npiv; i += gridDim.x * blockDim.x)
+    c += piv[i] != 0;
+  for (int o = 16; o; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(ctr, (unsigned long long)c);
+}
+
 template <typename T>
 __global__ void row_abs_sums_k(int m, int n, const T *A, long lda, double *rs) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -437,6 +447,14 @@ int pla_k_laswp(int dt, void *A, long lda, int npiv, const int *piv, int c0, int
   if (dt == MPI_DOUBLE) laswp_k<double><<<g, 128, sh, s>>>((double *)A, lda, npiv, piv, c0, c1, c2, c3);
   else if (dt == MPI_FLOAT) laswp_k<float><<<g, 128, sh, s>>>((float *)A, lda, npiv, piv, c0, c1, c2, c3);
   else return (int)cudaErrorInvalidValue;
+  return status();
+}
+
+int pla_k_count_interchanges(int npiv, const int *piv, unsigned long long *ctr,
+                              cudaStream_t s) {
+  if (npiv <= 0) return 0;
+  int g = (npiv + 255) / 256;
+  count_interchanges_k<<<g < 148 ? g : 148, 256, 0, s>>>(npiv, piv, ctr);
   return status();
 }
 

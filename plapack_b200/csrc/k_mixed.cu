@@ -394,132 +394,150 @@ extern "C" int pla_k_residual(int n, int ncols, int nrhs, const double *A, long 
 }
 
 // ---------------------------------------------------------------------------
-// D := inv(L) for a unit-lower-triangular n x n fp32 L (n = 32, 64, 128 or
-// 256), in one CTA of 1024 threads:
-//   1. the n / 32 diagonal 32 x 32 blocks, one warp each: lane c forward-
-//      substitutes column c of the block's inverse (x_c = 1, x_i = -sum_{c <=
-//      j < i} L(i, j) x_j), the block and the columns in shared memory;
-//   2. doubling: with D11 = inv(L11) and D22 = inv(L22) known for the two
-//      h x h halves of a 2h block, D21 = -D22 (L21 D11), two h x h products
-//      per pair, h = 32, 64, 128 (products in 32-wide K tiles through shared
-//      memory, a 4 x 4 register tile per thread).
-// D (ldd) receives the whole lower triangle, unit diagonal included; the
-// strictly upper part is set to zero.  T: n * n / 2 floats of scratch.
+// D := inv(L) for a unit-lower-triangular n x n fp32 L (n a multiple of 32, at
+// most 256), by block columns: X = inv(L) solves L X = I, and block column j
+// of X (32 columns) depends only on L's blocks from block row j down, so the
+// block columns are independent.  CTA (j, h) computes columns 32 j + 16 h ..
+// + 15 of X:
+//   1. L's lower triangle from block row j down is staged in shared memory
+//      (one load of everything the CTA reads); warp w inverts the diagonal
+//      block j + w in place (lane c: column c by right-looking substitution,
+//      the column in registers);
+//   2. X_jj = inv(L_jj), then for every block row i > j: S = sum_{j <= k < i}
+//      L_ik X_kj (the k range split in four quarters over warp pairs, the
+//      partial sums added in a fixed order), X_ij = -inv(L_ii) S;
+//   3. the CTA's columns of D written: zero above block row j and above the
+//      diagonal, one on it.
+// The longest chain (block column 0) is n / 32 - 1 block rows of small
+// products out of shared memory, against a serial doubling over the whole
+// triangle in one CTA before.
 namespace {
-constexpr int kInvThreads = 1024;
-// dynamic shared memory: the diagonal blocks and their inverses in phase 1,
-// the product tiles in phase 2
-constexpr size_t kInvSmem = 2 * 8 * 32 * 33 * sizeof(float);
-
-// the products of one doubling level: for every pair p of h-blocks starting
-// at row q = 2 h p, T_p = L21 D11 (step 0), then D21 = -D22 T_p (step 1)
-__device__ void inv_products(int n, int h, const float *L, long ldl, float *D, long ldd,
-                             float *T, float *sA, float *sB) {
-  const int npairs = n / (2 * h), tid = threadIdx.x;
-  const int tiles = (h / 4) * (h / 4);  // 4 x 4 output tiles per product
-  for (int step = 0; step < 2; step++) {
-    for (int p0 = 0; p0 < npairs; p0++) {
-      const int q = 2 * h * p0;
-      const float *Aop = step == 0 ? L + (q + h) + (long)q * ldl : D + (q + h) + (long)(q + h) * ldd;
-      const long lda = step == 0 ? ldl : ldd;
-      const float *Bop = step == 0 ? D + q + (long)q * ldd : T + (long)p0 * h * h;
-      const long ldb = step == 0 ? ldd : h;
-      float *Cop = step == 0 ? T + (long)p0 * h * h : D + (q + h) + (long)q * ldd;
-      const long ldc = step == 0 ? h : ldd;
-      const float alpha = step == 0 ? 1.f : -1.f;
-      float acc[4][4];
-      const int t = tid < tiles ? tid : 0;
-      const int i0 = (t % (h / 4)) * 4, j0 = (t / (h / 4)) * 4;
-#pragma unroll
-      for (int r = 0; r < 4; r++)
-#pragma unroll
-        for (int c = 0; c < 4; c++) acc[r][c] = 0.f;
-      for (int k0 = 0; k0 < h; k0 += 32) {
-        // stage A[:, k0 .. k0 + 32] (h x 32) and B[k0 .. k0 + 32, :] (32 x h)
-        for (int e = tid; e < h * 32; e += kInvThreads) {
-          const int i = e % h, k = e / h;
-          sA[i + k * h] = Aop[i + (long)(k0 + k) * lda];
-          const int kk = e % 32, j = e / 32;
-          sB[kk + j * 32] = Bop[(k0 + kk) + (long)j * ldb];
-        }
-        __syncthreads();
-        if (tid < tiles)
-          for (int k = 0; k < 32; k++) {
-            float a[4], b[4];
-#pragma unroll
-            for (int r = 0; r < 4; r++) a[r] = sA[(i0 + r) + k * h];
-#pragma unroll
-            for (int c = 0; c < 4; c++) b[c] = sB[k + (j0 + c) * 32];
-#pragma unroll
-            for (int r = 0; r < 4; r++)
-#pragma unroll
-              for (int c = 0; c < 4; c++) acc[r][c] = fmaf(a[r], b[c], acc[r][c]);
-          }
-        __syncthreads();
-      }
-      if (tid < tiles)
-#pragma unroll
-        for (int r = 0; r < 4; r++)
-#pragma unroll
-          for (int c = 0; c < 4; c++) Cop[(i0 + r) + (long)(j0 + c) * ldc] = alpha * acc[r][c];
-      __syncthreads();
-    }
-  }
+constexpr int kInvThreads = 256;
+constexpr int kInvCols = 16;         // columns of X per CTA
+constexpr int kBlkStride = 32 * 33;  // one 32 x 32 block, column-major, columns padded to 33
+__host__ __device__ constexpr int inv_tri_blocks(int nb) { return nb * (nb + 1) / 2; }
+constexpr size_t inv_smem_bytes(int nblk) {
+  return ((size_t)inv_tri_blocks(nblk) * kBlkStride + (size_t)nblk * 32 * kInvCols +
+          4 * 32 * kInvCols + 32 * kInvCols) * sizeof(float);
 }
 
 __global__ void __launch_bounds__(kInvThreads, 1)
-trtri_unit_lower_k(int n, const float *__restrict__ L, long ldl, float *D, long ldd, float *T) {
+trtri_unit_lower_k(int n, const float *__restrict__ L, long ldl, float *__restrict__ D,
+                   long ldd) {
   extern __shared__ __align__(16) float inv_smem[];
-  auto blk = reinterpret_cast<float(*)[32][33]>(inv_smem);
-  auto xs = reinterpret_cast<float(*)[32][33]>(inv_smem + 8 * 32 * 33);
-  float *sA = inv_smem, *sB = inv_smem + 128 * 32;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  // the off-diagonal blocks start at zero (the lower ones are computed below)
-  for (long e = tid; e < (long)n * n; e += kInvThreads) {
-    const int i = (int)(e % n), j = (int)(e / n);
-    if (i / 32 != j / 32) D[i + (long)j * ldd] = 0.f;
-  }
-  // 1. diagonal blocks
-  const int nb32 = n / 32;
-  if (warp < nb32) {
-    const int q = warp * 32;
-    for (int j = 0; j < 32; j++) blk[warp][lane][j] = L[(q + lane) + (long)(q + j) * ldl];
-    __syncwarp();
-    // column `lane` of the block's inverse: x_i for i >= lane
-    for (int i = 0; i < 32; i++) {
-      float x;
-      if (i < lane) x = 0.f;
-      else if (i == lane) x = 1.f;
-      else {
-        float s = 0.f;
-        for (int j = lane; j < i; j++) s = fmaf(blk[warp][i][j], xs[warp][j][lane], s);
-        x = -s;
+  const int nblk = n / 32, j = blockIdx.x >> 1, h = blockIdx.x & 1;
+  const int nb = nblk - j;  // block rows from j down
+  // block (I, K) of the staged triangle (rows and columns relative to 32 j,
+  // K <= I < nb) at (I (I + 1) / 2 + K) kBlkStride, element (r, k) at k 33 + r
+  float *sL = inv_smem;
+  float *sX = sL + (size_t)inv_tri_blocks(nb) * kBlkStride;  // X rows from 32 j, row-major
+  float *part = sX + (size_t)nb * 32 * kInvCols;             // [quarter][column][row]
+  float *sS = part + 4 * 32 * kInvCols;                       // S, row-major
+
+  // 1. stage, then invert the diagonal blocks in place
+  for (int I = 0; I < nb; I++)
+    for (int K = 0; K <= I; K++) {
+      float *dst = sL + (I * (I + 1) / 2 + K) * kBlkStride;
+      const float *src = L + 32 * (j + I) + (long)(32 * (j + K)) * ldl;
+#pragma unroll
+      for (int q = 0; q < 1024 / kInvThreads; q++) {
+        const int e = tid + q * kInvThreads, k = e >> 5, r = e & 31;
+        dst[k * 33 + r] = src[r + (long)k * ldl];
       }
-      xs[warp][i][lane] = x;
+    }
+  __syncthreads();
+  if (warp < nb) {
+    float *blk = sL + (warp * (warp + 1) / 2 + warp) * kBlkStride;
+    float acc[32];
+#pragma unroll
+    for (int i = 0; i < 32; i++) acc[i] = i == lane ? 1.f : 0.f;
+#pragma unroll
+    for (int c = 0; c < 32; c++) {  // acc_i -= L(i, c) x_c for i > c, x_c = acc_c final
+      const float x = acc[c];
+#pragma unroll
+      for (int i = c + 1; i < 32; i++) acc[i] = fmaf(-blk[c * 33 + i], x, acc[i]);
     }
     __syncwarp();
-    for (int i = 0; i < 32; i++) D[(q + i) + (long)(q + lane) * ldd] = xs[warp][i][lane];
+#pragma unroll
+    for (int i = 0; i < 32; i++) blk[lane * 33 + i] = i < lane ? 0.f : acc[i];
   }
   __syncthreads();
-  // 2. doubling
-  for (int h = 32; h < n; h *= 2) {
-    inv_products(n, h, L, ldl, D, ldd, T, sA, sB);
+
+  // 2. block rows of X, from the diagonal down
+  for (int e = tid; e < 32 * kInvCols; e += kInvThreads) {
+    const int r = e / kInvCols, c = e % kInvCols;
+    sX[e] = sL[(kInvCols * h + c) * 33 + r];  // X_jj = inv(L_jj), this CTA's columns
+  }
+  __syncthreads();
+  const int g = warp >> 1, ch = warp & 1;  // quarter of the k range, half of the columns
+  for (int I = 1; I < nb; I++) {
+    const float *row = sL + (I * (I + 1) / 2) * kBlkStride;  // block (I, 0)
+    float acc[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) acc[q] = 0.f;
+    const int k0 = g * 8 * I, k1 = k0 + 8 * I;
+    for (int k = k0; k < k1; k++) {
+      const float a = row[(k >> 5) * kBlkStride + (k & 31) * 33 + lane];
+      const float4 b0 = *reinterpret_cast<const float4 *>(sX + k * kInvCols + 8 * ch);
+      const float4 b1 = *reinterpret_cast<const float4 *>(sX + k * kInvCols + 8 * ch + 4);
+      acc[0] = fmaf(a, b0.x, acc[0]);
+      acc[1] = fmaf(a, b0.y, acc[1]);
+      acc[2] = fmaf(a, b0.z, acc[2]);
+      acc[3] = fmaf(a, b0.w, acc[3]);
+      acc[4] = fmaf(a, b1.x, acc[4]);
+      acc[5] = fmaf(a, b1.y, acc[5]);
+      acc[6] = fmaf(a, b1.z, acc[6]);
+      acc[7] = fmaf(a, b1.w, acc[7]);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) part[(g * kInvCols + 8 * ch + q) * 32 + lane] = acc[q];
     __syncthreads();
+    for (int e = tid; e < 32 * kInvCols; e += kInvThreads) {
+      const int r = e & 31, c = e >> 5;
+      const int o = c * 32 + r;
+      sS[r * kInvCols + c] = ((part[o] + part[512 + o]) + part[1024 + o]) + part[1536 + o];
+    }
+    __syncthreads();
+    {  // X_I = -inv(L_II) S: row `lane`, columns 2 warp and 2 warp + 1
+      const float *dI = sL + (I * (I + 1) / 2 + I) * kBlkStride;
+      float x0 = 0.f, x1 = 0.f;
+#pragma unroll 8
+      for (int k = 0; k < 32; k++) {
+        const float a = dI[k * 33 + lane];
+        const float2 s = *reinterpret_cast<const float2 *>(sS + k * kInvCols + 2 * warp);
+        x0 = fmaf(a, s.x, x0);
+        x1 = fmaf(a, s.y, x1);
+      }
+      sX[(32 * I + lane) * kInvCols + 2 * warp] = -x0;
+      sX[(32 * I + lane) * kInvCols + 2 * warp + 1] = -x1;
+    }
+    __syncthreads();
+  }
+
+  // 3. this CTA's columns of D
+  for (int e = tid; e < n * kInvCols; e += kInvThreads) {
+    const int r = e % n, c = e / n;
+    const int col = 32 * j + kInvCols * h + c, rr = r - 32 * j, cc = col - 32 * j;
+    const float v = rr < cc ? 0.f : rr == cc ? 1.f : sX[rr * kInvCols + c];
+    D[r + (long)col * ldd] = v;
   }
 }
 }  // namespace
 
 extern "C" int pla_k_trtri_unit_lower(int n, const float *L, long ldl, float *D, long ldd,
                                       float *work, cudaStream_t s) {
+  (void)work;  // no scratch: every intermediate stays in shared memory
   if (n <= 0) return 0;
-  if (n % 32 || n > 256 || (n & (n - 1))) return (int)cudaErrorInvalidValue;
+  if (n % 32 || n > 256) return (int)cudaErrorInvalidValue;
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(trtri_unit_lower_k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)kInvSmem);
+                         (int)inv_smem_bytes(8));
     attr = true;
   }
-  trtri_unit_lower_k<<<1, kInvThreads, kInvSmem, s>>>(n, L, ldl, D, ldd, work);
+  const int nblk = n / 32;
+  trtri_unit_lower_k<<<2 * nblk, kInvThreads, inv_smem_bytes(nblk), s>>>(n, L, ldl, D, ldd);
   pla_k_count(1);
   return (int)cudaGetLastError();
 }

@@ -76,38 +76,17 @@ __device__ __forceinline__ unsigned long long warp_max_key(unsigned long long x)
   return ((unsigned long long)hi << 32) | lo;
 }
 
-// LU with partial pivoting of the candidate rows ids[0..cnt) (entries < 0 are
-// empty) of the column-major panel A (w columns), cnt <= kMaxCand.  Keeps
-// k = min(candidates, w) rows: sm.keep[j] = the row chosen as pivot j; with
-// `root`, sm.rows row j = the kept row j's factored values (row j of
-// L11 \ U11).  All threads call it.
-//
-// Each thread holds kRows candidate rows in registers (slots tid + h kThreads),
-// shifted left by one column after every step, so the current column is
-// always v[h][0] and every index is static.  The multipliers shifted out go
-// to `hist` (needed only for the rows the root keeps).  One barrier per
-// column: every warp posts its best candidate (row, reciprocal pivot) before
-// it, every thread picks the same winner after it.
-__device__ __forceinline__ int select_rows(const float *__restrict__ A, long lda, int w, int cnt,
-                                           SelectSmem &sm, float *hist, bool root) {
+// Column steps j0 .. j1-1 of select_rows on a window of WIN columns: at step
+// j the columns still to be eliminated sit at positions 0 .. w-1-j of v, so
+// a window of WIN >= w - j positions carries every value that matters; the
+// positions past it are never read again.  The arithmetic on each element is
+// that of the full-width step, in the same order.
+template <int WIN>
+__device__ __forceinline__ void column_steps(int j0, int j1, int w, float (&v)[kRows][kW],
+                                             const int (&id)[kRows], bool (&live)[kRows],
+                                             SelectSmem &sm, float *hist, bool root) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  float v[kRows][kW];
-  int id[kRows];
-  bool live[kRows];
-#pragma unroll
-  for (int h = 0; h < kRows; h++) {
-    const int s = tid + h * kThreads;
-    id[h] = s < cnt ? sm.ids[s] : -1;
-    live[h] = id[h] >= 0;
-#pragma unroll
-    for (int c = 0; c < kW; c++)
-      v[h][c] = (live[h] && c < w) ? A[(long)id[h] + (long)c * lda] : 0.f;
-  }
-  int nlive = 0;
-#pragma unroll
-  for (int h = 0; h < kRows; h++) nlive += __syncthreads_count(live[h]);
-  const int k = nlive < w ? nlive : w;
-  for (int j = 0; j < k; j++) {
+  for (int j = j0; j < j1; j++) {
     const int par = j & 1;
     unsigned long long mine = 0;
     int mh = 0;
@@ -125,7 +104,7 @@ __device__ __forceinline__ int select_rows(const float *__restrict__ A, long lda
       for (int h = 0; h < kRows; h++)
         if (h == mh) {
 #pragma unroll
-          for (int q = 0; q < kW / 4; q++)
+          for (int q = 0; q < WIN / 4; q++)
             dst[q] = make_float4(v[h][4 * q], v[h][4 * q + 1], v[h][4 * q + 2], v[h][4 * q + 3]);
           sm.winv[par][warp] = 1.0f / v[h][0];
         }
@@ -138,11 +117,11 @@ __device__ __forceinline__ int select_rows(const float *__restrict__ A, long lda
     const unsigned long long g = warp_max_key(e);
     const int gw = __ffs(__ballot_sync(0xffffffffu, e == g)) - 1;
     const int gr = (int)(0xffffffffu - (unsigned)g);
-    float u[kW];
+    float u[WIN];
     {
       const float4 *src = reinterpret_cast<const float4 *>(sm.wrow[par][gw]);
 #pragma unroll
-      for (int q = 0; q < kW / 4; q++) {
+      for (int q = 0; q < WIN / 4; q++) {
         const float4 f = src[q];
         u[4 * q] = f.x;
         u[4 * q + 1] = f.y;
@@ -165,11 +144,51 @@ __device__ __forceinline__ int select_rows(const float *__restrict__ A, long lda
       if (live[h]) {
         hist[j * kMaxCand + tid + h * kThreads] = l;
 #pragma unroll
-        for (int c = 1; c < kW; c++) v[h][c - 1] = fmaf(-l, u[c], v[h][c]);
-        v[h][kW - 1] = 0.f;
+        for (int c = 1; c < WIN; c++) v[h][c - 1] = fmaf(-l, u[c], v[h][c]);
+        v[h][WIN - 1] = 0.f;
       }
     }
   }
+}
+
+// LU with partial pivoting of the candidate rows ids[0..cnt) (entries < 0 are
+// empty) of the column-major panel A (w columns), cnt <= kMaxCand.  Keeps
+// k = min(candidates, w) rows: sm.keep[j] = the row chosen as pivot j; with
+// `root`, sm.rows row j = the kept row j's factored values (row j of
+// L11 \ U11).  All threads call it.
+//
+// Each thread holds kRows candidate rows in registers (slots tid + h kThreads),
+// shifted left by one column after every step, so the current column is
+// always v[h][0] and every index is static.  The multipliers shifted out go
+// to `hist` (needed only for the rows the root keeps).  One barrier per
+// column: every warp posts its best candidate (row, reciprocal pivot) before
+// it, every thread picks the same winner after it.  Steps 8 q .. 8 q + 7 run
+// on a window of 32 - 8 q columns (column_steps), so the multiply-adds follow
+// the shrinking trailing part instead of all 32 positions.
+__device__ __forceinline__ int select_rows(const float *__restrict__ A, long lda, int w, int cnt,
+                                           SelectSmem &sm, float *hist, bool root) {
+  const int tid = threadIdx.x;
+  float v[kRows][kW];
+  int id[kRows];
+  bool live[kRows];
+#pragma unroll
+  for (int h = 0; h < kRows; h++) {
+    const int s = tid + h * kThreads;
+    id[h] = s < cnt ? sm.ids[s] : -1;
+    live[h] = id[h] >= 0;
+#pragma unroll
+    for (int c = 0; c < kW; c++)
+      v[h][c] = (live[h] && c < w) ? A[(long)id[h] + (long)c * lda] : 0.f;
+  }
+  int nlive = 0;
+#pragma unroll
+  for (int h = 0; h < kRows; h++) nlive += __syncthreads_count(live[h]);
+  const int k = nlive < w ? nlive : w;
+  static_assert(kW == 32, "the windows below assume 32-column sub-panels");
+  column_steps<32>(0, min(k, 8), w, v, id, live, sm, hist, root);
+  column_steps<24>(8, min(k, 16), w, v, id, live, sm, hist, root);
+  column_steps<16>(16, min(k, 24), w, v, id, live, sm, hist, root);
+  column_steps<8>(24, k, w, v, id, live, sm, hist, root);
   __syncthreads();  // keep[] complete; ids[] and wrow[] free for the caller
   if (root)  // the multipliers of the kept rows: row j's columns left of j
     for (int i = tid; i < k * kW; i += kThreads) {
@@ -405,8 +424,11 @@ extern "C" int pla_k_lu_panel_tslu(int r, int w, float *A, long lda, int *piv, i
   }
   int P = g_tsms;
   if (max_ctas > 0 && P > max_ctas) P = max_ctas;
-  // at least two candidate sets' worth of rows per CTA, so leaves choose
-  const int maxP = (r + 2 * kW - 1) / (2 * kW);
+  // no more leaves than it takes to give each one pass (kMaxCand rows): every
+  // tree level costs w dependent column steps whatever the leaves' heights,
+  // and fewer, fuller leaves need fewer levels (r <= 512: the root alone;
+  // r <= 16 kMaxCand: one merge)
+  const int maxP = (r + kMaxCand - 1) / kMaxCand;
   if (P > maxP) P = maxP;
   if (P < 1) P = 1;
   const int R = (r + P - 1) / P;

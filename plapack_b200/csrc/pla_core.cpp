@@ -225,7 +225,40 @@ PhaseTimer::~PhaseTimer() {
   g_pending.push_back({acc, e0, e1});
 }
 
+namespace {
+unsigned long long *g_interchanges = nullptr;  // device counter, phase timing only
+bool g_interchanges_pending = false;
+}  // namespace
+
+void count_interchanges(int npiv, const int *piv) {
+  if (!state().phase_timing || npiv <= 0) return;
+  if (!g_interchanges) {
+    if (cudaMalloc(&g_interchanges, sizeof(unsigned long long)) != cudaSuccess) {
+      g_interchanges = nullptr;
+      return;
+    }
+    cudaMemsetAsync(g_interchanges, 0, sizeof(unsigned long long), stream());
+  }
+  if (pla_k_count_interchanges(npiv, piv, g_interchanges, stream()) == 0)
+    g_interchanges_pending = true;
+}
+
+void release_interchange_counter() {
+  if (g_interchanges) cudaFree(g_interchanges);
+  g_interchanges = nullptr;
+  g_interchanges_pending = false;
+}
+
 void resolve_phases() {
+  if (g_interchanges_pending) {
+    unsigned long long v = 0;
+    cudaStream_t s = stream();
+    if (cudaMemcpyAsync(&v, g_interchanges, sizeof v, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+        cudaStreamSynchronize(s) == cudaSuccess)
+      state().phases.interchanges += (long long)v;
+    cudaMemsetAsync(g_interchanges, 0, sizeof(unsigned long long), s);
+    g_interchanges_pending = false;
+  }
   for (Pending &p : g_pending) {
     cudaEventSynchronize(p.b);
     float ms = 0.f;
@@ -381,6 +414,7 @@ int PLA_Finalize(void) {
   cudaStreamSynchronize(stream());
   release_scratch();
   release_ooc();
+  release_interchange_counter();
   pla_kernels_release();
   for (cudaStream_t *st : {&s.la_stream, &s.copy_stream})
     if (*st) {

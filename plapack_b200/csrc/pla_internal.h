@@ -147,6 +147,10 @@ struct PhaseTimer {
   ~PhaseTimer();
 };
 void resolve_phases();
+// with phase timing on: add the non-trivial interchanges of piv[0..npiv) to
+// PLA_Phase_times.interchanges (a device count, read when the times are)
+void count_interchanges(int npiv, const int *piv);
+void release_interchange_counter();
 
 }  // namespace pla
 

@@ -52,12 +52,19 @@ int pla_k_lu_panel(int dt, int r, int w, void *A, long lda, int *piv, int *statu
 int pla_k_lu_panel_tslu(int r, int w, float *A, long lda, int *piv, int *zero_info,
                         int row_base, int max_ctas, cudaStream_t s);
 void pla_tslu_release(void);
+/* the mixed / FP64 LU's blocked r x b panel factorization (32-column
+ * sub-panels, pivoting PLA_B200_PIVOT_*) on stream s (0: the library stream) */
+int pla_k_panel_lu_blocked(int dt, int r, int b, void *P, long lda, int *piv, int *zero_info,
+                           int max_ctas, int pivoting, cudaStream_t s);
 
 /* ---- row interchanges: for i in [0, npiv): swap rows i and i + piv[i] of the
  * block whose row 0 is A (rows relative to A), in columns [c0, c1) and
  * [c2, c3). */
 int pla_k_laswp(int dt, void *A, long lda, int npiv, const int *piv, int c0, int c1, int c2,
                 int c3, cudaStream_t s);
+// adds the number of non-trivial interchanges (piv[i] != 0) of piv[0..npiv) to *ctr
+int pla_k_count_interchanges(int npiv, const int *piv, unsigned long long *ctr,
+                              cudaStream_t s);
 /* apply a host pivot vector to m x n B in sequence (device pivots) */
 int pla_k_laswp_rows(int dt, void *B, long ldb, int ncols, int npiv, const int *piv,
                      cudaStream_t s);
@@ -157,8 +164,9 @@ int pla_k_pack_fp8(int m, int kdim, const float *src, long si, long sk, void *ds
  * hi.  With zero != 0 the source is cleared after it is read. */
 int pla_k_pack_split(int m, int kdim, float *src, long si, long sk, void *dst, long ldd,
                      int pattern, int zero, cudaStream_t s);
-/* D (ldd) := inv(L) for a unit-lower-triangular fp32 L (n x n, n = 32, 64,
- * 128 or 256), in one CTA; work: n * n / 2 floats of scratch */
+/* D (ldd) := inv(L) for a unit-lower-triangular fp32 L (n x n, n a multiple
+ * of 32 up to 256; only L's strictly lower part is read), one launch of
+ * n / 16 CTAs; work is not used (kept for the interface) */
 int pla_k_trtri_unit_lower(int n, const float *L, long ldl, float *D, long ldd, float *work,
                            cudaStream_t s);
 /* d := diag(A)^-1/2 (1 where A(i, i) <= 0); dst (fp32, ldd) := D A D */

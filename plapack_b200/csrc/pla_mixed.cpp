@@ -152,18 +152,15 @@ struct SplitU12 {
   float *dinv[2] = {nullptr, nullptr};           // inv(L11), b x b column-major
   __nv_bfloat16 *lsplit[2] = {nullptr, nullptr};  // [hi | hi | lo] of inv(L11), b x 3b
   __nv_bfloat16 *usplit = nullptr;                // [hi | lo | hi] of A12', rest x 3b
-  float *work = nullptr;                          // the inverse kernel's products
 };
 
-constexpr int kSlotInvWork = 12;
-
-// inv(L11) of a unit-lower b x b block: one CTA (pla_k_trtri_unit_lower) when b
-// is a power of two from 32 to 256, else the blocked triangular solve on I.
-// The inverse sits on the panel chain of the factorization; the blocked solve
-// took about 0.16 ms a step at b = 256.
-int unit_lower_inverse(const float *L11, long ld, int b, float *D, float *work) {
-  if (b >= 32 && b <= 256 && (b & (b - 1)) == 0 && work) {
-    K(pla_k_trtri_unit_lower(b, L11, ld, D, b, work, stream()));
+// inv(L11) of a unit-lower b x b block: pla_k_trtri_unit_lower (independent
+// block columns, one launch) when b is a multiple of 32 up to 256, else the
+// blocked triangular solve on I.  The inverse sits on the panel chain of the
+// factorization; the blocked solve took about 0.16 ms a step at b = 256.
+int unit_lower_inverse(const float *L11, long ld, int b, float *D) {
+  if (b >= 32 && b <= 256 && b % 32 == 0) {
+    K(pla_k_trtri_unit_lower(b, L11, ld, D, b, nullptr, stream()));
     return PLA_SUCCESS;
   }
   K(pla_k_fill(MPI_FLOAT, b, b, D, b, 0.0, stream()));
@@ -176,8 +173,7 @@ int split_alloc(SplitU12 &S, int n, int nb) {
   const size_t d = (size_t)nb * nb * sizeof(float), l = (size_t)nb * 3 * nb * 2;
   char *p = (char *)scratch(kSlotSplitL, 2 * (d + l) + 1024);
   S.usplit = (__nv_bfloat16 *)scratch(kSlotSplitU, (size_t)n * 3 * nb * 2 + 1024);
-  S.work = (float *)scratch(kSlotInvWork, (size_t)nb * nb * sizeof(float) / 2 + 1024);
-  if (!p || !S.usplit || !S.work) PLA_FAIL("cannot allocate the split operands of the U12 solve");
+  if (!p || !S.usplit) PLA_FAIL("cannot allocate the split operands of the U12 solve");
   for (int q = 0; q < 2; q++) {
     S.dinv[q] = (float *)(p + q * (d + l));
     S.lsplit[q] = (__nv_bfloat16 *)(p + q * (d + l) + d);
@@ -188,7 +184,7 @@ int split_alloc(SplitU12 &S, int n, int nb) {
 // after the panel at (k, k) (on the current stream): inv(L11) and its split
 int split_prepare(SplitU12 &S, int q, const float *L11, long ld, int b) {
   float *D = S.dinv[q];
-  PK(unit_lower_inverse(L11, ld, b, D, S.work));
+  PK(unit_lower_inverse(L11, ld, b, D));
   // row i of inv(L11): element (i, k) at D[i + k b]
   K(pla_k_pack_split(b, b, D, 1, b, S.lsplit[q], 3L * b, 0b100, 0, stream()));
   return PLA_SUCCESS;
@@ -351,6 +347,7 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
                    ld, at(k + b, k), ld, 1.0, at(k + b, k + b), ld, 'L', &st[0], stream()));
     }
   }
+  if (F.kind == 0) count_interchanges(n, F.piv);
   return PLA_SUCCESS;
 }
 
@@ -712,8 +709,7 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
   __nv_bfloat16 *lsplit =
       (__nv_bfloat16 *)scratch(kSlotSplitL, (size_t)nsteps * nb * 3 * nb * 2 + 256);
   __nv_bfloat16 *usplit = (__nv_bfloat16 *)scratch(kSlotSplitU, (size_t)n * 3 * nb * 2 + 256);
-  float *inv_work = (float *)scratch(kSlotInvWork, (size_t)nb * nb * sizeof(float) / 2 + 1024);
-  if (!Lbig || !dinv || !scl || !Ub || !lsplit || !usplit || !inv_work)
+  if (!Lbig || !dinv || !scl || !Ub || !lsplit || !usplit)
     PLA_FAIL("cannot allocate the streamed-solve buffers");
   float *inv_u = scl + (size_t)nsteps * tiles;  // the U' scales of the launch in flight
   int *st = F.status;
@@ -767,7 +763,7 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
   auto post_panel = [&](int s) -> int {
     const int k0 = s * nb, b = std::min(nb, n - k0), rest = n - k0 - b;
     float *D = dinv + (size_t)s * nb * nb;
-    PK(unit_lower_inverse(at(k0, k0), ld, b, D, inv_work));
+    PK(unit_lower_inverse(at(k0, k0), ld, b, D));
     if (rest <= 0) return 0;
     K(pla_k_pack_split(b, b, D, 1, b, lsplit + (size_t)s * nb * 3 * nb, 3L * b, 0b100, 0,
                        stream()));
@@ -878,6 +874,7 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
     PhaseTimer t(&ph.swap_ms);
     K(pla_k_laswp(MPI_FLOAT, at(k0, 0), ld, b, F.piv + k0, 0, k0, 0, 0, stream()));
   }
+  count_interchanges(n, F.piv);
   PLA_CUDA(cudaStreamSynchronize(s0));
   return PLA_SUCCESS;
 }

@@ -150,7 +150,11 @@ namespace pla {
 // memory; after each sub-panel its pivots are applied to the panel's other
 // columns and the columns to its right get the unit-lower solve and the
 // rank-kSub update.  Pivot choices are those of the column-by-column loop;
-// only the rounding order of the panel's trailing columns differs.
+// only the rounding order of the panel's trailing columns differs.  (Tournament
+// pivoting of the sub-panels with their interchanges and U12 solve done in
+// the tournament kernels themselves, two launches fewer per sub-panel, was
+// measured slower inside the solve: 233 against 225 ms at n = 32768, that
+// work then sitting on the root CTA of the critical path.)
 int panel_lu(int dt, int r, int b, char *P, long lda, int *piv, int *status, int *zero_info,
              int row_base, int max_ctas, int pivoting) {
   constexpr int kSub = 32;
@@ -187,6 +191,20 @@ int panel_lu(int dt, int r, int b, char *P, long lda, int *piv, int *status, int
   return 0;
 }
 }  // namespace pla
+
+// The blocked panel factorization alone (panel_lu: the r x b panel at P,
+// pivots to piv, first exact zero pivot to zero_info), queued on stream s
+// (0: the library stream), for timing and tests.
+extern "C" int pla_k_panel_lu_blocked(int dt, int r, int b, void *P, long lda, int *piv,
+                                      int *zero_info, int max_ctas, int pivoting,
+                                      cudaStream_t s) {
+  if (dt != MPI_FLOAT && dt != MPI_DOUBLE) return (int)cudaErrorInvalidValue;
+  OnStream on(s);
+  int *st = (int *)scratch(0, 4 * sizeof(int));
+  if (!st) return (int)cudaErrorMemoryAllocation;
+  cudaMemsetAsync(st, 0, 4 * sizeof(int), stream());
+  return panel_lu(dt, r, b, (char *)P, lda, piv, st, zero_info, 0, max_ctas, pivoting);
+}
 
 namespace {
 
@@ -382,6 +400,7 @@ int lu_on_device(int dt, int m, int n, char *A, long lda, int *piv, int nb, int 
   PLA_CUDA(cudaMemsetAsync(st, 0, sizeof(Status), stream()));
   int r = lu_device(dt, m, n, A, lda, piv, nb, st, left_swaps);
   if (r) return r;
+  count_interchanges(std::min(m, n), piv);
   Status h{};
   PLA_CUDA(cudaMemcpyAsync(&h, st, sizeof h, cudaMemcpyDeviceToHost, stream()));
   r = finish("lu");

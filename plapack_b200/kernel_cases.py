@@ -15,6 +15,8 @@ bytes or flops and the rate they imply.
     python -m plapack_b200.kernel_cases potrf --k 128 --dtype f64
     python -m plapack_b200.kernel_cases trsm_small --side R --m 32768 --k 128 --dtype f64
     python -m plapack_b200.kernel_cases sgemm --m 32768 --n 224 --k 32
+    python -m plapack_b200.kernel_cases panel_blocked --m 32768 --n 256 --ctas 72
+    python -m plapack_b200.kernel_cases trtri --m 32768 --k 256
 
 The cases mirror the calls the solvers make (the trailing update of one LU
 step, one 32-column sub-panel, the row interchanges of one panel, the
@@ -150,6 +152,43 @@ def case_tslu(torch, lib, a):
                     f"CTAs, copy of the panel included", "s": t,
             "us_per_column": t / w * 1e6, "bytes_read_written": 2.0 * r * w * 4,
             "gbs": 2.0 * r * w * 4 / t / 1e9}
+
+
+def case_panel_blocked(torch, lib, a):
+    """The mixed LU's whole r x b fp32 panel (--m x --n): 32-column sub-panels
+    with tournament pivoting, each followed by its row interchanges,
+    triangular solve and rank-32 update (pla_k_panel_lu_blocked)."""
+    r, b = a.m, a.n
+    st = torch.cuda.Stream()
+    A0 = torch.randn(b, r, dtype=torch.float32, device="cuda")
+    A = A0.clone()
+    piv = torch.zeros(b, dtype=torch.int32, device="cuda")
+    g = _fn(lib, "pla_k_panel_lu_blocked", [i32, i32, i32, vp, lg, vp, vp, i32, i32, vp])
+
+    def launch():
+        A.copy_(A0)
+        return g(pla.MPI_FLOAT, r, b, A.data_ptr(), r, piv.data_ptr(), None, a.ctas, 1,
+                 st.cuda_stream)
+
+    with torch.cuda.stream(st):
+        t = _time(torch, launch, a.warmup, a.reps)
+    return {"case": f"blocked tournament panel {r} x {b} (f32), 32-column sub-panels, at most "
+                    f"{a.ctas or 'one per SM'} CTAs, copy of the panel included",
+            "s": t, "us_per_subpanel": t / ((b + 31) // 32) * 1e6}
+
+
+def case_trtri(torch, lib, a):
+    """inv(L11) of the mixed LU's unit-lower diagonal block (n = --k), L11 at
+    the top of an --m-row column-major panel as the factorization has it."""
+    n, ld = a.k, max(a.m, a.k)
+    P = torch.randn(n, ld, dtype=torch.float32, device="cuda") * (1.0 / n)
+    D = torch.empty(n, n, dtype=torch.float32, device="cuda")
+    g = _fn(lib, "pla_k_trtri_unit_lower", [i32, vp, lg, vp, lg, vp, vp])
+    t = _time(torch, lambda: g(n, P.data_ptr(), ld, D.data_ptr(), n, None, None), a.warmup,
+              a.reps)
+    flops = n ** 3 / 3.0
+    return {"case": f"unit-lower triangular inverse, n={n} (f32), leading dimension {ld}",
+            "s": t, "us": t * 1e6, "gflops": flops / t / 1e9}
 
 
 def case_laswp(torch, lib, a):

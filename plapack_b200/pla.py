@@ -52,7 +52,8 @@ _pi, _pobj = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_void_p)
 class PhaseTimes(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in
                 ("total_ms", "panel_ms", "swap_ms", "trsm_ms", "update_ms", "solve_ms", "refine_ms",
-                 "convert_ms")] + [("update_launches", ctypes.c_int)]
+                 "convert_ms")] + [("update_launches", ctypes.c_int),
+                                   ("interchanges", ctypes.c_longlong)]
 
 
 class MixedParams(ctypes.Structure):

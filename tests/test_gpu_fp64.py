@@ -392,3 +392,23 @@ def test_potrf_diagonal_block(pla_session, dt, b):
     torch.cuda.synchronize()
     assert int(info[0]) == 500 + c + 1 and int(st[0]) != 0
     assert np.array_equal(a.cpu().numpy()[:, :b].T, A2)
+
+
+def test_phase_times_count_interchanges(pla_session):
+    """With phase timing on, PLA_Phase_times.interchanges counts the LU's row
+    interchanges that moved rows (pivot offset != 0), summed over calls."""
+    from plapack_b200 import pla
+    lib = pla_session.lib
+    A = np.asfortranarray(np.random.default_rng(4).standard_normal((700, 700)))
+    lib.PLA_B200_set_phase_timing(1)
+    try:
+        lib.PLA_B200_reset_phase_times()
+        _, piv1, _ = pla_lu(pla_session, A, 64)
+        _, piv2, _ = pla_lu(pla_session, np.asfortranarray(np.eye(700)), 64)
+        ph = pla.PhaseTimes()
+        lib.PLA_B200_phase_times(ctypes.byref(ph))
+    finally:
+        lib.PLA_B200_set_phase_timing(0)
+    assert np.count_nonzero(piv2) == 0
+    assert ph.interchanges == np.count_nonzero(piv1) > 600
+    assert ph.update_launches > 0

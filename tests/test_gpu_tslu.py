@@ -132,11 +132,12 @@ def test_mixed_solve_with_either_panel_pivoting(env):
         s.free(m, b)
 
 
-@pytest.mark.parametrize("n", [32, 64, 128, 256])
-def test_unit_lower_inverse_one_cta(env, n):
+@pytest.mark.parametrize("n", [32, 64, 96, 128, 160, 224, 256])
+def test_unit_lower_inverse(env, n):
     """inv(L11) of the mixed LU's unit-lower diagonal block (pla_k_trtri_unit_lower:
-    diagonal 32 x 32 blocks by warps, then doubling): equal to the inverse to
-    fp32 rounding, unit diagonal, strictly upper part zero."""
+    independent 32-column block columns, diagonal blocks inverted by warps):
+    equal to the inverse to fp32 rounding, unit diagonal, strictly upper part
+    zero; only L's strictly lower part is read (the upper part holds U)."""
     import scipy.linalg as sl
     s, torch, pla, _ = env
     lib = s.lib
@@ -148,12 +149,10 @@ def test_unit_lower_inverse_one_cta(env, n):
     ld = n + 5
     L = sl.lu(rng.standard_normal((n, n)))[1]         # a unit-lower factor of a pivoted LU
     Lbuf = np.zeros((n, ld), dtype=np.float32)      # column-major n x n, leading dimension ld
-    Lbuf[:, :n] = L.T
+    Lbuf[:, :n] = (L + np.triu(rng.standard_normal((n, n)), 0) * 1e3).T   # U above, ignored
     tL = torch.from_numpy(Lbuf).cuda()
     tD = torch.full((n, n), 7.0, dtype=torch.float32, device="cuda")
-    work = torch.zeros(n * n, dtype=torch.float32, device="cuda")
-    assert lib.pla_k_trtri_unit_lower(n, tL.data_ptr(), ld, tD.data_ptr(), n, work.data_ptr(),
-                                      None) == 0
+    assert lib.pla_k_trtri_unit_lower(n, tL.data_ptr(), ld, tD.data_ptr(), n, None, None) == 0
     torch.cuda.synchronize()
     D = tD.cpu().numpy().T.astype(np.float64)
     assert np.all(np.triu(D, 1) == 0.0) and np.all(np.diag(D) == 1.0)
