@@ -56,6 +56,9 @@ TC_UPDATE_TRAFFIC_RATIO = 486.5 / 545.3
 # from the ncu capture of the tournament panel kernels (None until measured).
 PANEL_TRAFFIC_PER_STEP = None
 
+# PLA_B200_PREC_* codes as the JSON line names them
+PREC_NAMES = {1: "bf16", 2: "fp16", 3: "fp32", 4: "fp64", 5: "fp8", 6: "bf16x6"}
+
 
 def parse():
     p = argparse.ArgumentParser(description=__doc__.split("\n")[0])
@@ -65,7 +68,7 @@ def parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--n", type=int, default=32768)
     p.add_argument("--kappa", type=float, default=1e6)
-    p.add_argument("--precision", choices=["fp16", "bf16", "fp32"], default="fp16")
+    p.add_argument("--precision", choices=["fp16", "bf16", "bf16x6", "fp32"], default="fp16")
     p.add_argument("--refinement", choices=["gmres", "lu"], default="gmres")
     p.add_argument("--nb", type=int, default=256, help="block size of the mixed factorization")
     p.add_argument("--panel-pivoting", choices=["tournament", "partial"], default="tournament",
@@ -398,8 +401,7 @@ def run_mixed_sweep(torch, pla, lib, s, device, stream, a, n, args, params):
                  f"PLA_General_solve_mixed ({args.precision}, {args.refinement.upper()}-IR)",
                  "solve_s": t, "backward_error_max": eta, "forward_error_rhs0": fwd}
         if not fp64:
-            entry.update({"precision_used": {1: "bf16", 2: "fp16", 3: "fp32", 4: "fp64",
-                                             5: "fp8"}.get(rep.precision_used),
+            entry.update({"precision_used": PREC_NAMES.get(rep.precision_used),
                           "factorizations": rep.factorizations,
                           "converged": rep.converged, "iterations": rep.iterations,
                           "gmres_iterations": rep.inner_iterations,
@@ -517,8 +519,7 @@ def run_chol_mixed(torch, pla, lib, s, device, stream, n, kappas, precs, nrhs, s
             eta = (R.abs().amax(dim=1) / (a_inf * X.abs().amax(dim=1) + Bt.abs().amax(dim=1))).max().item()
             fwd = ((X - Xt).abs().max() / Xt.abs().max()).item()
             out.append({"kappa": kappa, "precision": name, "rc": rc, "solve_s": min(times),
-                        "precision_used": {1: "bf16", 2: "fp16", 3: "fp32", 4: "fp64",
-                                           5: "fp8"}.get(rep.precision_used),
+                        "precision_used": PREC_NAMES.get(rep.precision_used),
                         "factorizations": rep.factorizations, "iterations": rep.iterations,
                         "gmres_iterations": rep.inner_iterations, "factor_ms": rep.factor_ms,
                         "refine_ms": rep.refine_ms, "backward_error": eta,
@@ -583,7 +584,7 @@ def run_ours(args):
     check(lib.PLA_Obj_set_local_contents_device(ctypes.c_void_p(T.data_ptr()), n, a), "fill A")
 
     prec = {"fp16": pla.PLA_B200_PREC_FP16, "bf16": pla.PLA_B200_PREC_BF16,
-            "fp32": pla.PLA_B200_PREC_FP32}[args.precision]
+            "bf16x6": pla.PLA_B200_PREC_BF16X6, "fp32": pla.PLA_B200_PREC_FP32}[args.precision]
     params = pla.MixedParams()
     lib.PLA_Mixed_params_default(ctypes.byref(params))
     params.precision = prec
@@ -840,7 +841,8 @@ def run_ours(args):
     if not args.skip_chol_mixed:
         chol_mixed = run_chol_mixed(torch, pla, lib, s, device, stream, args.chol_n, (1e3, 1e7),
                                     (("fp8", pla.PLA_B200_PREC_FP8),
-                                     ("bf16", pla.PLA_B200_PREC_BF16)), 8, 1, 1)
+                                     ("bf16", pla.PLA_B200_PREC_BF16),
+                                     ("bf16x6", pla.PLA_B200_PREC_BF16X6)), 8, 1, 1)
 
     # ---- end to end: host buffers in, host solution out ----
     e2e = None

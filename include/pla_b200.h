@@ -76,6 +76,11 @@ long PLA_B200_kernel_launches(void);
                                     scale per 128-row tile, fp32 accumulate; the
                                     Cholesky factors D A D, D = diag(A)^-1/2, and
                                     refines with M^-1 = D (L L')^-1 D */
+#define PLA_B200_PREC_BF16X6 6   /* trailing update on the tensor cores with both
+                                    operands split three ways into bf16 (x = p0 +
+                                    p1 + p2) and six of the nine part products
+                                    summed in fp32: fp32-level factors at about
+                                    six times the bf16 tensor work */
 #define PLA_B200_IR_LU       1   /* classic iterative refinement             */
 #define PLA_B200_IR_GMRES    2   /* GMRES-IR                                 */
 /* pivoting of the low-precision LU's fp32 panels (the FP64 PLA_LU always uses
@@ -97,8 +102,13 @@ typedef struct {
                            the backward error; a non-finite iterate;
                            max_iterations reached) or the low-precision
                            Cholesky breaks down, refactor one precision higher
-                           (FP8 -> BF16 -> FP64; FP16 -> FP64; FP32 -> FP64)
-                           and continue from the current iterate             */
+                           (FP8 -> BF16 -> BF16X6 -> FP64; FP16 -> BF16X6 ->
+                           FP64; FP32 -> FP64) and continue from the current
+                           iterate.  Right after a low-precision factorization,
+                           a diagonal range of its factors (max / min |u_ii|,
+                           squared for a Cholesky factor) above 1e4 over the
+                           precision's unit roundoff escalates one level at
+                           once, without refining                           */
   double tol;           /* target backward error; <= 0 selects n * 2^-53    */
   int panel_pivoting;   /* PLA_B200_PIVOT_* of the fp32 LU panels (default
                            TOURNAMENT)                                       */

@@ -226,25 +226,95 @@ __global__ void gemv_reduce_k(int n, int nrhs, int slices, const double *partial
 
 int g_sms = 0;
 
-// x = hi + lo with hi = bf16(x) and lo = bf16(x - hi): about 16 significant
-// bits.  Row i of dst (ld ldd, K-contiguous) receives three K-wide segments,
-// each hi or lo as `pattern` says (bit s set: segment s is lo), so that a
-// single K = 3 kdim product of two such operands sums hi*hi + hi*lo + lo*hi.
-// x(i, k) = src[i si + k sk]; with `zero`, src is cleared behind the read.
+// x = p0 + p1 + p2 with p0 = bf16(x), p1 = bf16(x - p0), p2 = bf16(x - p0 -
+// p1) (each difference exact in fp32): p0 + p1 carries about 16 significant
+// bits, p0 + p1 + p2 all 24.  Row i of dst (ld ldd, K-contiguous) receives
+// nseg K-wide segments, segment s holding part (code >> 2 s) & 3, so that a
+// single K = nseg kdim product of two such operands sums the chosen part
+// products: [p0 p0 p1] x [p0 p1 p0] gives p0 p0 + p0 p1 + p1 p0 (bf16 x 3),
+// [p0 p0 p1 p0 p1 p2] x [p0 p1 p0 p2 p1 p0] adds p0 p2 + p1 p1 + p2 p0 (bf16 x
+// 6, the terms left out below 2^-24 relative).  x(i, k) = src[i si + k sk];
+// with `zero`, src is cleared behind the read.
+__device__ __forceinline__ void split_parts(float x, __nv_bfloat16 (&p)[3]) {
+  p[0] = __float2bfloat16_rn(x);
+  const float r1 = x - __bfloat162float(p[0]);
+  p[1] = __float2bfloat16_rn(r1);
+  p[2] = __float2bfloat16_rn(r1 - __bfloat162float(p[1]));
+}
+
 __global__ void pack_split_k(int m, int kdim, float *src, long si, long sk,
-                             __nv_bfloat16 *dst, long ldd, int pattern, int zero) {
+                             __nv_bfloat16 *dst, long ldd, int nseg, unsigned code, int zero) {
   const long total = (long)m * kdim;
   for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (long)gridDim.x * blockDim.x) {
     const long k = e % kdim, i = e / kdim;
     float *p = src + i * si + k * sk;
-    const float x = *p;
-    const __nv_bfloat16 hi = __float2bfloat16_rn(x);
-    const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+    __nv_bfloat16 part[3];
+    split_parts(*p, part);
     __nv_bfloat16 *row = dst + i * ldd + k;
-#pragma unroll
-    for (int seg = 0; seg < 3; seg++) row[(long)seg * kdim] = (pattern >> seg) & 1 ? lo : hi;
+    for (int seg = 0; seg < nseg; seg++) row[(long)seg * kdim] = part[(code >> (2 * seg)) & 3];
     if (zero) *p = 0.f;
+  }
+}
+
+// the same for a column-major source (element (i, k) at src[i + k lds]),
+// transposed through shared memory so that both the reads and the writes
+// are coalesced
+__global__ void pack_split_rows_k(int m, int kdim, const float *src, long lds,
+                                  __nv_bfloat16 *dst, long ldd, int nseg, unsigned code) {
+  __shared__ float tile[32][33];
+  const int i0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + threadIdx.x, k = k0 + r;
+    tile[r][threadIdx.x] = (i < m && k < kdim) ? src[i + (long)k * lds] : 0.f;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + r, k = k0 + threadIdx.x;
+    if (i < m && k < kdim) {
+      __nv_bfloat16 part[3];
+      split_parts(tile[threadIdx.x][r], part);
+      __nv_bfloat16 *row = dst + (long)i * ldd + k;
+      for (int seg = 0; seg < nseg; seg++) row[(long)seg * kdim] = part[(code >> (2 * seg)) & 3];
+    }
+  }
+}
+
+// out[0] = max_i |A(i, i)|, out[1] = min_i |A(i, i)| (NaN for a NaN diagonal
+// entry), one CTA; the factor's diagonal range, a cheap bound from below on
+// its condition number
+__global__ void __launch_bounds__(1024) diag_range_k(int n, const float *A, long lda, float *out) {
+  __shared__ float smax[32], smin[32];
+  float hi = 0.f, lo = __int_as_float(0x7f800000);
+  bool nan = false;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float a = fabsf(A[i + (long)i * lda]);
+    nan |= a != a;
+    hi = fmaxf(hi, a);
+    lo = fminf(lo, a);
+  }
+  nan = __syncthreads_or(nan);
+  for (int o = 16; o; o >>= 1) {
+    hi = fmaxf(hi, __shfl_down_sync(0xffffffffu, hi, o));
+    lo = fminf(lo, __shfl_down_sync(0xffffffffu, lo, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    smax[threadIdx.x >> 5] = hi;
+    smin[threadIdx.x >> 5] = lo;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int nw = blockDim.x >> 5;
+    hi = threadIdx.x < nw ? smax[threadIdx.x] : 0.f;
+    lo = threadIdx.x < nw ? smin[threadIdx.x] : __int_as_float(0x7f800000);
+    for (int o = 16; o; o >>= 1) {
+      hi = fmaxf(hi, __shfl_down_sync(0xffffffffu, hi, o));
+      lo = fminf(lo, __shfl_down_sync(0xffffffffu, lo, o));
+    }
+    if (threadIdx.x == 0) {
+      out[0] = nan ? __int_as_float(0x7fc00000) : hi;
+      out[1] = nan ? __int_as_float(0x7fc00000) : lo;
+    }
   }
 }
 
@@ -262,14 +332,38 @@ extern "C" int pla_k_pack_rows(int prec, int m, int kdim, const float *src, long
   return (int)cudaGetLastError();
 }
 
+extern "C" int pla_k_pack_split_ex(int m, int kdim, float *src, long si, long sk, void *dst,
+                                   long ldd, int nseg, unsigned code, int zero, cudaStream_t s) {
+  if (m <= 0 || kdim <= 0) return 0;
+  if (nseg < 1 || nseg > 8) return (int)cudaErrorInvalidValue;
+  for (int seg = 0; seg < nseg; seg++)
+    if (((code >> (2 * seg)) & 3) > 2) return (int)cudaErrorInvalidValue;
+  if (si == 1 && !zero) {  // column-major source: the transposing form
+    dim3 grid((m + 31) / 32, (kdim + 31) / 32), block(32, 8);
+    pack_split_rows_k<<<grid, block, 0, s>>>(m, kdim, src, sk, (__nv_bfloat16 *)dst, ldd, nseg,
+                                             code);
+  } else {
+    const long total = (long)m * kdim;
+    int grid = (int)((total + 255) / 256);
+    if (grid > 148 * 16) grid = 148 * 16;
+    pack_split_k<<<grid, 256, 0, s>>>(m, kdim, src, si, sk, (__nv_bfloat16 *)dst, ldd, nseg,
+                                      code, zero);
+  }
+  pla_k_count(1);
+  return (int)cudaGetLastError();
+}
+
+// three segments of hi (part 0) or lo (part 1): bit s of pattern set = lo
 extern "C" int pla_k_pack_split(int m, int kdim, float *src, long si, long sk, void *dst,
                                 long ldd, int pattern, int zero, cudaStream_t s) {
-  if (m <= 0 || kdim <= 0) return 0;
-  const long total = (long)m * kdim;
-  int grid = (int)((total + 255) / 256);
-  if (grid > 148 * 16) grid = 148 * 16;
-  pack_split_k<<<grid, 256, 0, s>>>(m, kdim, src, si, sk, (__nv_bfloat16 *)dst, ldd, pattern,
-                                    zero);
+  unsigned code = 0;
+  for (int seg = 0; seg < 3; seg++) code |= (unsigned)((pattern >> seg) & 1) << (2 * seg);
+  return pla_k_pack_split_ex(m, kdim, src, si, sk, dst, ldd, 3, code, zero, s);
+}
+
+extern "C" int pla_k_diag_range(int n, const float *A, long lda, float *out, cudaStream_t s) {
+  if (n <= 0) return 0;
+  diag_range_k<<<1, 1024, 0, s>>>(n, A, lda, out);
   pla_k_count(1);
   return (int)cudaGetLastError();
 }

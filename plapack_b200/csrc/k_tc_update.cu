@@ -174,13 +174,26 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Tile t of the walk: bands of `band` tile rows, each band walked column by
+// column.  band = tiles_m is the plain column-major walk; a narrower band
+// keeps the L rows of the tiles in flight few enough to stay in L2 while the
+// band's columns pass (long K: the split operands of the bf16 x 6 update).
+__device__ __forceinline__ void tile_coords(int t, int tiles_m, int tiles_n, int band, int &tm,
+                                            int &tn) {
+  const int span = band * tiles_n;
+  const int b = t / span, w = t - b * span;
+  const int rows = min(band, tiles_m - b * band);
+  tm = b * band + w % rows;
+  tn = w / rows;
+}
+
 // F8: E4M3 operands with one power-of-two scale per 128-row tile of L and of
 // U (inv_l, inv_u); a K chunk is then 128 elements (still 128 bytes per row)
 template <bool F8>
 __global__ void __launch_bounds__(THREADS, 1)
 tc_update_k(const __grid_constant__ CUtensorMap mapL, const __grid_constant__ CUtensorMap mapU,
             const __grid_constant__ CUtensorMap mapC, int M, int N, int kchunks, int row0,
-            int col0, float alpha, uint32_t idesc, int lower, const float *inv_l,
+            int col0, float alpha, uint32_t idesc, int lower, int band, const float *inv_l,
             const float *inv_u, int *status) {
   constexpr int KE = F8 ? 128 : KBOX;  // elements per K chunk
   extern __shared__ uint8_t smem_raw[];
@@ -232,7 +245,8 @@ tc_update_k(const __grid_constant__ CUtensorMap mapL, const __grid_constant__ CU
       int issued_ph[kStages];
       for (int s = 0; s < kStages; s++) issued_ph[s] = -1;
       for (int t = blockIdx.x; t < ntiles && !s_abort; t += gridDim.x) {
-        const int tm = t % tiles_m, tn = t / tiles_m;
+        int tm, tn;
+        tile_coords(t, tiles_m, tiles_n, band, tm, tn);
         if (skip(tm, tn)) continue;
         for (int kc = 0; kc < kchunks && !s_abort; kc++) {
           if (!mbar_wait(&empty[stage], ph ^ 1)) {
@@ -260,7 +274,8 @@ tc_update_k(const __grid_constant__ CUtensorMap mapL, const __grid_constant__ CU
       uint32_t ph = 0;
       bool issued = false;
       for (int t = blockIdx.x; t < ntiles && !s_abort; t += gridDim.x) {
-        const int tm = t % tiles_m, tn = t / tiles_m;
+        int tm, tn;
+        tile_coords(t, tiles_m, tiles_n, band, tm, tn);
         if (skip(tm, tn)) continue;
         const int ab = count & 1;
         if (!mbar_wait(&acc_empty[ab], ((count >> 1) & 1) ^ 1)) {
@@ -313,7 +328,8 @@ tc_update_k(const __grid_constant__ CUtensorMap mapL, const __grid_constant__ CU
     const bool elected = threadIdx.x == 64;
     int count = 0, chunk = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-      const int tm = t % tiles_m, tn = t / tiles_m;
+      int tm, tn;
+        tile_coords(t, tiles_m, tiles_n, band, tm, tn);
       if (skip(tm, tn)) continue;
       const int ab = count & 1;
       if (!mbar_wait(&acc_full[ab], (count >> 1) & 1)) fail();
@@ -386,7 +402,7 @@ int g_sms = 0;
 
 template <bool F8>
 int launch(const CUtensorMap &mL, const CUtensorMap &mU, const CUtensorMap &mC, int M, int N,
-           int kchunks, int row0, int col0, float alpha, uint32_t idesc, int lower,
+           int kchunks, int row0, int col0, float alpha, uint32_t idesc, int lower, int band,
            const float *inv_l, const float *inv_u, int max_ctas, int *status, cudaStream_t s) {
   if (!g_sms) {
     int dev = 0;
@@ -397,8 +413,10 @@ int launch(const CUtensorMap &mL, const CUtensorMap &mU, const CUtensorMap &mC, 
   const long tiles = (long)((M + TM - 1) / TM) * ((N + TN - 1) / TN);
   const int cap = max_ctas > 0 && max_ctas < g_sms ? max_ctas : g_sms;
   const int grid = (int)(tiles < cap ? tiles : cap);
+  const int tiles_m = (M + TM - 1) / TM;
+  if (band <= 0 || band > tiles_m) band = tiles_m;
   tc_update_k<F8><<<grid, THREADS, SMEM_BYTES, s>>>(mL, mU, mC, M, N, kchunks, row0, col0, alpha,
-                                                    idesc, lower, inv_l, inv_u, status);
+                                                    idesc, lower, band, inv_l, inv_u, status);
   pla_k_count(1);
   return (int)cudaGetLastError();
 }
@@ -432,7 +450,10 @@ extern "C" int pla_k_tc_update_ex(int prec, int M, int N, int K, float alpha, co
   const uint32_t ab = prec == PLA_K_BF16 ? 1u : 0u;
   const uint32_t idesc = (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)(TN >> 3) << 17) |
                          ((uint32_t)(TM >> 4) << 24);
-  return launch<false>(mL, mU, mC, M, N, K / KBOX, row0, col0, alpha, idesc, lower, nullptr,
+  // K past 512 (split operands): bands of 32 tile rows, so that the L rows
+  // in flight (32 x 128 rows x 2K bytes) stay in L2 across the band's columns
+  const int band = K > 512 ? 32 : 0;
+  return launch<false>(mL, mU, mC, M, N, K / KBOX, row0, col0, alpha, idesc, lower, band, nullptr,
                        nullptr, max_ctas, status, s);
 }
 
@@ -471,7 +492,7 @@ extern "C" int pla_k_tc_update_fp8_ex(int M, int N, int K, float alpha, const vo
   // instruction descriptor, kind::f8f6f4: fp32 accumulate, A and B both E4M3
   // (format 0), both K-major, N = 128, M = 128
   const uint32_t idesc = (1u << 4) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
-  return launch<true>(mL, mU, mC, M, N, K / 128, row0, col0, alpha, idesc, lower, inv_l, inv_u,
+  return launch<true>(mL, mU, mC, M, N, K / 128, row0, col0, alpha, idesc, lower, 0, inv_l, inv_u,
                       max_ctas, status, s);
 }
 

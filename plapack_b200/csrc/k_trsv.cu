@@ -31,20 +31,22 @@ __device__ __forceinline__ T opA(const T *A, long lda, bool trans, long i, long 
 // inverse of the TB x TB diagonal block `blockIdx.x` of op(A) into Dinv
 // (element (r, c) of block i at Dinv[i*TB + r + c*ldd]); TB = 128 for fp32,
 // 64 for FP64 (two TB x (TB + 1) blocks must fit in shared memory)
-template <typename T, int TB>
+// TA: the factor's element type; T: the inverse's (an fp32 factor may have
+// its inverse blocks in FP64, for solves carried out in FP64)
+template <typename TA, typename T, int TB>
 __global__ void __launch_bounds__(THREADS)
-tri_inv_blocks_k(int n, const T *A, long lda, bool lower_op, bool trans, bool unit, T *Dinv,
+tri_inv_blocks_k(int n, const TA *A, long lda, bool lower_op, bool trans, bool unit, T *Dinv,
                  long ldd) {
   extern __shared__ __align__(16) unsigned char sm[];
-  T *D = (T *)sm;                 // TB x TB, ld TB + 1
-  T *X = D + TB * (TB + 1);       // TB x TB, ld TB + 1
   constexpr int L = TB + 1, NT = THREADS / TB;  // NT threads per column
+  TA *D = (TA *)sm;               // TB x TB, ld TB + 1
+  T *X = (T *)(sm + ((size_t)TB * L * sizeof(TA) + 15) / 16 * 16);  // TB x TB, ld TB + 1
   const int blk = blockIdx.x, r0 = blk * TB, nb = min(TB, n - r0);
   for (int t = threadIdx.x; t < TB * TB; t += THREADS) {
     int i = t % TB, j = t / TB;
-    T v = T(0);
+    TA v = TA(0);
     if (i < nb && j < nb) v = opA(A, lda, trans, (long)r0 + i, (long)r0 + j);
-    if (i == j && (unit || i >= nb)) v = T(1);
+    if (i == j && (unit || i >= nb)) v = TA(1);
     D[i + j * L] = v;
     X[i + j * L] = i == j ? T(1) : T(0);
   }
@@ -234,16 +236,34 @@ trsv_ticket_k(int n, int nblk, const T *A, long lda, bool lower_op, bool trans, 
 // single-column number of barriers.  Groups of 4 keep each chain's serial
 // step (the last tile, the reduction and the inverse block, per column) short:
 // at n = 32768, 16 columns as one chain took 2.73 ms, as four chains 1.81 ms.
-template <int NR>
+// T: the right-hand sides' and the arithmetic's type, float or double (the
+// factor A is fp32 either way; Dinv is of type T)
+template <typename T>
+struct Four {
+  T x, y, z, w;
+};
+template <typename T>
+__device__ __forceinline__ Four<T> ld_four(const T *p) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 f = *reinterpret_cast<const float4 *>(p);
+    return {f.x, f.y, f.z, f.w};
+  } else {
+    const double2 a = reinterpret_cast<const double2 *>(p)[0];
+    const double2 b = reinterpret_cast<const double2 *>(p)[1];
+    return {a.x, a.y, b.x, b.y};
+  }
+}
+
+template <int NR, typename T>
 __global__ void __launch_bounds__(THREADS)
 trsv_ticket_nr_k(int n, int nblk, int nrhs, const float *A, long lda, bool lower_op, bool trans,
-                 const float *Dinv, long ldd, const float *B, long ldb, float *X, long ldx,
+                 const T *Dinv, long ldd, const T *B, long ldb, T *X, long ldx,
                  int *ticket, int *flags, int *status, bool vec_ok) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
-  float *Ds = reinterpret_cast<float *>(dyn_smem);
-  float *red = Ds + TB * TB;
-  float *xs = red + NR * 8 * TB;
-  float *part = xs + NR * TB;
+  T *Ds = reinterpret_cast<T *>(dyn_smem);
+  T *red = Ds + TB * TB;
+  T *xs = red + NR * 8 * TB;
+  T *part = xs + NR * TB;
   __shared__ int s_blk, s_bad;
   const int r = threadIdx.x % TB, half = threadIdx.x / TB;
   const int rg = threadIdx.x & 31, cg = threadIdx.x >> 5;
@@ -266,16 +286,17 @@ trsv_ticket_nr_k(int n, int nblk, int nrhs, const float *A, long lda, bool lower
     const int i = lower_op ? q : nblk - 1 - q;
     const long r0 = (long)i * TB;
     const int nbi = min(TB, n - (int)r0);
-    float acc4[NR][4], acc[NR];
+    T acc4[NR][4], acc[NR];
 #pragma unroll
     for (int k = 0; k < NR; k++) {
-      acc[k] = 0.f;
+      acc[k] = T(0);
 #pragma unroll
-      for (int e = 0; e < 4; e++) acc4[k][e] = 0.f;
+      for (int e = 0; e < 4; e++) acc4[k][e] = T(0);
     }
-    for (int u = threadIdx.x; u < TB * TB / 4; u += THREADS) {
-      const int c = u / (TB / 4), r4 = (u % (TB / 4)) * 4;
-      cp_async16(&Ds[c * TB + r4], Dinv + (r0 + r4) + (long)c * ldd);
+    constexpr int kv = 16 / sizeof(T);  // elements per 16-byte copy
+    for (int u = threadIdx.x; u < TB * TB / kv; u += THREADS) {
+      const int c = u / (TB / kv), rk = (u % (TB / kv)) * kv;
+      cp_async16(&Ds[c * TB + rk], Dinv + (r0 + rk) + (long)c * ldd);
     }
     cp_async_commit();
     for (int s = 0; s < q; s++) {
@@ -306,7 +327,7 @@ trsv_ticket_nr_k(int n, int nblk, int nrhs, const float *A, long lda, bool lower
       if (s_bad) return;
       for (int t = threadIdx.x; t < NR * TB; t += THREADS) {
         const int k = t / TB, c = t % TB;
-        xs[t] = k < nrhs && c < nbj ? __ldcg(&X[c0 + c + (long)k * ldx]) : 0.f;
+        xs[t] = k < nrhs && c < nbj ? __ldcg(&X[c0 + c + (long)k * ldx]) : T(0);
       }
       __syncthreads();
       if (full && !trans) {
@@ -314,7 +335,7 @@ trsv_ticket_nr_k(int n, int nblk, int nrhs, const float *A, long lda, bool lower
         for (int u = 0; u < 16; u++) {
 #pragma unroll
           for (int k = 0; k < NR; k++) {
-            const float xv = xs[k * TB + 16 * cg + u];
+            const T xv = xs[k * TB + 16 * cg + u];
             acc4[k][0] += v[u].x * xv;
             acc4[k][1] += v[u].y * xv;
             acc4[k][2] += v[u].z * xv;
@@ -327,7 +348,7 @@ trsv_ticket_nr_k(int n, int nblk, int nrhs, const float *A, long lda, bool lower
           const int c = 64 * half + 4 * u;
 #pragma unroll
           for (int k = 0; k < NR; k++) {
-            const float *xk = xs + k * TB + c;
+            const T *xk = xs + k * TB + c;
             acc[k] += v[u].x * xk[0] + v[u].y * xk[1] + v[u].z * xk[2] + v[u].w * xk[3];
           }
         }
@@ -360,26 +381,26 @@ trsv_ticket_nr_k(int n, int nblk, int nrhs, const float *A, long lda, bool lower
     __syncthreads();
     for (int t = threadIdx.x; t < NR * TB; t += THREADS) {
       const int k = t / TB, row = t % TB;
-      float sacc = part[k * TB + row] + part[(NR + k) * TB + row];
+      T sacc = part[k * TB + row] + part[(NR + k) * TB + row];
 #pragma unroll
       for (int g = 0; g < 8; g++) sacc += red[(k * 8 + g) * TB + row];
-      xs[t] = row < nbi && k < nrhs ? B[r0 + row + (long)k * ldb] - sacc : 0.f;
+      xs[t] = row < nbi && k < nrhs ? B[r0 + row + (long)k * ldb] - sacc : T(0);
     }
     cp_async_wait_all();
     __syncthreads();
     // x_i = inv(D_i) y for every column, with the inverse block from shared memory
     {
-      float y4[NR][4];
+      T y4[NR][4];
 #pragma unroll
       for (int k = 0; k < NR; k++)
 #pragma unroll
-        for (int e = 0; e < 4; e++) y4[k][e] = 0.f;
+        for (int e = 0; e < 4; e++) y4[k][e] = T(0);
 #pragma unroll
       for (int u = 0; u < 16; u++) {
-        const float4 d = *reinterpret_cast<const float4 *>(&Ds[(16 * cg + u) * TB + 4 * rg]);
+        const Four<T> d = ld_four(&Ds[(16 * cg + u) * TB + 4 * rg]);
 #pragma unroll
         for (int k = 0; k < NR; k++) {
-          const float xv = xs[k * TB + 16 * cg + u];
+          const T xv = xs[k * TB + 16 * cg + u];
           y4[k][0] += d.x * xv;
           y4[k][1] += d.y * xv;
           y4[k][2] += d.z * xv;
@@ -395,7 +416,7 @@ trsv_ticket_nr_k(int n, int nblk, int nrhs, const float *A, long lda, bool lower
     for (int t = threadIdx.x; t < NR * TB; t += THREADS) {
       const int k = t / TB, row = t % TB;
       if (k >= nrhs || row >= nbi) continue;
-      float y = 0.f;
+      T y = T(0);
 #pragma unroll
       for (int g = 0; g < 8; g++) y += red[(k * 8 + g) * TB + row];
       X[r0 + row + (long)k * ldx] = y;
@@ -549,16 +570,17 @@ int *flags_for(int nblk) {
 
 int g_sms = 0;
 
-template <typename T, int TBK>
+template <typename TA, typename T, int TBK>
 int inv_blocks(char uplo, char trans, char diag, int n, const void *A, long lda, void *Dinv,
                long ldd, cudaStream_t s) {
   const bool tr = trans != 'N', lower_op = (uplo == 'L') != tr, unit = diag == 'U';
   const int nblk = (n + TBK - 1) / TBK;
-  size_t sm = (size_t)2 * TBK * (TBK + 1) * sizeof(T);
-  cudaFuncSetAttribute(tri_inv_blocks_k<T, TBK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)sm);
-  tri_inv_blocks_k<T, TBK><<<nblk, THREADS, sm, s>>>(n, (const T *)A, lda, lower_op, tr, unit,
-                                                     (T *)Dinv, ldd);
+  const size_t sm = ((size_t)TBK * (TBK + 1) * sizeof(TA) + 15) / 16 * 16 +
+                    (size_t)TBK * (TBK + 1) * sizeof(T);
+  cudaFuncSetAttribute(tri_inv_blocks_k<TA, T, TBK>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  tri_inv_blocks_k<TA, T, TBK><<<nblk, THREADS, sm, s>>>(n, (const TA *)A, lda, lower_op, tr,
+                                                         unit, (T *)Dinv, ldd);
   pla_k_count(1);
   return (int)cudaGetLastError();
 }
@@ -589,9 +611,9 @@ int ticket_solve(char uplo, char trans, int n, const void *A, long lda, const vo
   return (int)cudaGetLastError();
 }
 
-template <int NR>
+template <int NR, typename T>
 int ticket_solve_nr(char uplo, char trans, int n, int nrhs, const float *A, long lda,
-                    const float *Dinv, long ldd, const float *B, long ldb, float *X, long ldx,
+                    const T *Dinv, long ldd, const T *B, long ldb, T *X, long ldx,
                     int *status, cudaStream_t s) {
   const bool tr = trans != 'N', lower_op = (uplo == 'L') != tr;
   const int nblk = (n + TB - 1) / TB, groups = (nrhs + NR - 1) / NR;
@@ -608,16 +630,18 @@ int ticket_solve_nr(char uplo, char trans, int n, int nrhs, const float *A, long
   }
   if (ldd % TB || (uintptr_t)Dinv % 16) return (int)cudaErrorMisalignedAddress;
   const bool vec_ok = lda % 4 == 0 && (uintptr_t)A % 16 == 0;
-  int per = 2 * g_sms / groups;  // two CTAs per SM fit
+  // two CTAs per SM fit in fp32, one in FP64 (the ticket order needs no
+  // co-residency either way)
+  int per = (sizeof(T) == 4 ? 2 : 1) * g_sms / groups;
   if (per < 1) per = 1;
   const dim3 grid(nblk < per ? nblk : per, groups);
   const size_t dyn = ((size_t)TB * TB + (size_t)NR * 8 * TB + (size_t)NR * TB + 2 * NR * TB) *
-                     sizeof(float);
-  cudaFuncSetAttribute(trsv_ticket_nr_k<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                     sizeof(T);
+  cudaFuncSetAttribute(trsv_ticket_nr_k<NR, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)dyn);
-  trsv_ticket_nr_k<NR><<<grid, THREADS, dyn, s>>>(n, nblk, nrhs, A, lda, lower_op, tr, Dinv, ldd,
-                                                  B, ldb, X, ldx, fl + groups * nblk, fl, status,
-                                                  vec_ok);
+  trsv_ticket_nr_k<NR, T><<<grid, THREADS, dyn, s>>>(n, nblk, nrhs, A, lda, lower_op, tr, Dinv,
+                                                     ldd, B, ldb, X, ldx, fl + groups * nblk, fl,
+                                                     status, vec_ok);
   pla_k_count(1);
   return (int)cudaGetLastError();
 }
@@ -654,10 +678,20 @@ extern "C" int pla_k_trsv_inv_blocks(int dt, char uplo, char trans, char diag, i
                                      const void *A, long lda, void *Dinv, long ldd,
                                      cudaStream_t s) {
   if (n <= 0) return 0;
-  if (dt == MPI_FLOAT) return inv_blocks<float, TB>(uplo, trans, diag, n, A, lda, Dinv, ldd, s);
+  if (dt == MPI_FLOAT)
+    return inv_blocks<float, float, TB>(uplo, trans, diag, n, A, lda, Dinv, ldd, s);
   if (dt == MPI_DOUBLE)
-    return inv_blocks<double, TB64>(uplo, trans, diag, n, A, lda, Dinv, ldd, s);
+    return inv_blocks<double, double, TB64>(uplo, trans, diag, n, A, lda, Dinv, ldd, s);
   return (int)cudaErrorInvalidValue;
+}
+
+// FP64 inverses (128 x 128 blocks, ldd a multiple of 128) of an fp32 factor's
+// diagonal blocks, for pla_k_trsv_ticket_multi_f64
+extern "C" int pla_k_trsv_inv_blocks_f64(char uplo, char trans, char diag, int n,
+                                         const float *A, long lda, double *Dinv, long ldd,
+                                         cudaStream_t s) {
+  if (n <= 0) return 0;
+  return inv_blocks<float, double, TB>(uplo, trans, diag, n, A, lda, Dinv, ldd, s);
 }
 
 extern "C" int pla_k_trsv_ticket(int dt, char uplo, char trans, int n, const void *A, long lda,
@@ -678,7 +712,21 @@ extern "C" int pla_k_trsv_ticket_multi(char uplo, char trans, int n, int nrhs, c
                                        cudaStream_t s) {
   if (n <= 0 || nrhs <= 0) return 0;
   if (nrhs > 16) return (int)cudaErrorInvalidValue;
-  return ticket_solve_nr<4>(uplo, trans, n, nrhs, A, lda, Dinv, ldd, B, ldb, X, ldx, status, s);
+  return ticket_solve_nr<4, float>(uplo, trans, n, nrhs, A, lda, Dinv, ldd, B, ldb, X, ldx,
+                                   status, s);
+}
+
+// The same with FP64 right-hand sides and arithmetic on the fp32 factor
+// (the factor read once, 4 bytes an element): X := inv(op(A)) B for nrhs <=
+// 16, Dinv from pla_k_trsv_inv_blocks_f64
+extern "C" int pla_k_trsv_ticket_multi_f64(char uplo, char trans, int n, int nrhs,
+                                           const float *A, long lda, const double *Dinv,
+                                           long ldd, const double *B, long ldb, double *X,
+                                           long ldx, int *status, cudaStream_t s) {
+  if (n <= 0 || nrhs <= 0) return 0;
+  if (nrhs > 16) return (int)cudaErrorInvalidValue;
+  return ticket_solve_nr<4, double>(uplo, trans, n, nrhs, A, lda, Dinv, ldd, B, ldb, X, ldx,
+                                    status, s);
 }
 
 extern "C" void pla_trsv_release(void) {

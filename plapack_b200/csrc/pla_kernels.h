@@ -164,6 +164,14 @@ int pla_k_pack_fp8(int m, int kdim, const float *src, long si, long sk, void *ds
  * hi.  With zero != 0 the source is cleared after it is read. */
 int pla_k_pack_split(int m, int kdim, float *src, long si, long sk, void *dst, long ldd,
                      int pattern, int zero, cudaStream_t s);
+/* nseg K-wide segments per row, segment s holding part (code >> 2 s) & 3 of
+ * the three-way split x = p0 + p1 + p2 (p0 = bf16(x), p1 = bf16(x - p0), p2 =
+ * bf16(x - p0 - p1)); nseg <= 8 */
+int pla_k_pack_split_ex(int m, int kdim, float *src, long si, long sk, void *dst, long ldd,
+                        int nseg, unsigned code, int zero, cudaStream_t s);
+/* out[0] = max |A(i, i)|, out[1] = min |A(i, i)| over i < n (fp32, device); NaN in both
+ * when a diagonal entry is NaN */
+int pla_k_diag_range(int n, const float *A, long lda, float *out, cudaStream_t s);
 /* D (ldd) := inv(L) for a unit-lower-triangular fp32 L (n x n, n a multiple
  * of 32 up to 256; only L's strictly lower part is read), one launch of
  * n / 16 CTAs; work is not used (kept for the interface) */
@@ -189,6 +197,13 @@ int pla_k_trsv_ticket(int dt, char uplo, char trans, int n, const void *A, long 
 int pla_k_trsv_ticket_multi(char uplo, char trans, int n, int nrhs, const float *A, long lda,
                             const float *Dinv, long ldd, const float *B, long ldb, float *X,
                             long ldx, int *status, cudaStream_t s);
+/* FP64 right-hand sides and arithmetic on an fp32 triangle: the FP64 inverses of
+ * its 128 x 128 diagonal blocks, then X := inv(op(A)) B for nrhs <= 16 */
+int pla_k_trsv_inv_blocks_f64(char uplo, char trans, char diag, int n, const float *A, long lda,
+                              double *Dinv, long ldd, cudaStream_t s);
+int pla_k_trsv_ticket_multi_f64(char uplo, char trans, int n, int nrhs, const float *A, long lda,
+                                const double *Dinv, long ldd, const double *B, long ldb,
+                                double *X, long ldx, int *status, cudaStream_t s);
 void pla_trsv_release(void);
 /* out (dt_out = MPI_FLOAT or MPI_DOUBLE, n x nrhs, ldo) := rows perm[0..n) of
  * the FP64 in (ldi): a composed row permutation and a conversion in one pass */

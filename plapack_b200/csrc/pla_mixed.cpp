@@ -63,7 +63,7 @@ long round_up(long v, long m) { return (v + m - 1) / m * m; }
 struct Factor {
   int n = 0, ld = 0, prec = 0, kind = 0;  // kind 0 = LU, 1 = Cholesky
   int pivoting = PLA_B200_PIVOT_PARTIAL;   // of the fp32 LU panels
-  float *a = nullptr;     // fp32 factors (BF16, FP16, FP32)
+  float *a = nullptr;     // fp32 factors (BF16, FP16, FP32, BF16X6)
   double *a64 = nullptr;  // FP64 factors (FP64)
   double *dsc = nullptr;  // d = diag(A)^-1/2 when the factors are those of D A D
   int *piv = nullptr;
@@ -71,10 +71,15 @@ struct Factor {
   int *status = nullptr;  // [status, info, zero_info]
   // inverses of the 128 x 128 diagonal blocks of the two triangular factors
   float *dinv1 = nullptr, *dinv2 = nullptr;
+  // BF16X6: the same inverses in FP64, the solves with the fp32 factors then
+  // carried out in FP64 (fp32-level factors serve up to kappa near 2^24 times
+  // the refinement's reach, and an fp32 solve would round that away)
+  double *dinv1d = nullptr, *dinv2d = nullptr;
   long ldd = 0;
 };
 
 constexpr int kSlotDinv = 13;
+constexpr int kSlotDinv64 = 12;
 constexpr int kSlotPerm = 30;
 
 // The row interchanges of an LU composed into one permutation, once per
@@ -105,6 +110,17 @@ int prepare_perm(Factor &F) {
 // the per-factor data of the single-launch triangular solves
 int prepare_solves(Factor &F) {
   F.ldd = round_up(F.n, 128);
+  if (F.prec == PLA_B200_PREC_BF16X6) {
+    double *d = (double *)scratch(kSlotDinv64, (size_t)2 * F.ldd * 128 * sizeof(double));
+    if (!d) PLA_FAIL("cannot allocate the inverse diagonal blocks");
+    F.dinv1d = d;
+    F.dinv2d = d + F.ldd * 128;
+    const char u2 = F.kind == 0 ? 'U' : 'L', t2 = F.kind == 0 ? 'N' : 'T';
+    K(pla_k_trsv_inv_blocks_f64('L', 'N', F.kind == 0 ? 'U' : 'N', F.n, F.a, F.ld, F.dinv1d,
+                                F.ldd, stream()));
+    K(pla_k_trsv_inv_blocks_f64(u2, t2, 'N', F.n, F.a, F.ld, F.dinv2d, F.ldd, stream()));
+    return PLA_SUCCESS;
+  }
   float *d = (float *)scratch(kSlotDinv, (size_t)2 * F.ldd * 128 * sizeof(float));
   if (!d) PLA_FAIL("cannot allocate the inverse diagonal blocks");
   F.dinv1 = d;
@@ -147,11 +163,24 @@ struct EventTimer {
 // hi + lo, so that one K = 3b product sums hi*hi + hi*lo + lo*hi in fp32:
 // about 16 significant bits, against the 11 of the fp16 operands the trailing
 // update rounds U12 to anyway.  The product accumulates into A12 itself,
-// which the split-pack clears behind its read.
+// which the split-pack clears behind its read.  With bf16 x 6 factors both
+// operands are split three ways and the K = 6b product keeps fp32 accuracy.
+//
+// Segment codes of pla_k_pack_split_ex (two bits per K-wide segment, the part
+// of x = p0 + p1 + p2 it holds): the A operand and the B operand of a product
+// that sums p0 p1 + p1 p0 + p0 p0 (three segments) or p0 p2 + p1 p1 + p2 p0 +
+// p0 p1 + p1 p0 + p0 p0 (six).  The small part products come first: the
+// tensor core's fp32 accumulation truncates each addition relative to the
+// running sum, so the terms 2^-8 and 2^-16 below the leading ones are summed
+// before the leading ones make that sum large.
+constexpr unsigned kSplitA3 = 0x4, kSplitB3 = 0x1;      // [0 1 0] x [1 0 0]
+constexpr unsigned kSplitA6 = 0x124, kSplitB6 = 0x46;   // [0 1 2 0 1 0] x [2 1 0 1 0 0]
+
 struct SplitU12 {
+  int nseg = 3;                                   // 3: bf16 x 3, 6: bf16 x 6
   float *dinv[2] = {nullptr, nullptr};           // inv(L11), b x b column-major
-  __nv_bfloat16 *lsplit[2] = {nullptr, nullptr};  // [hi | hi | lo] of inv(L11), b x 3b
-  __nv_bfloat16 *usplit = nullptr;                // [hi | lo | hi] of A12', rest x 3b
+  __nv_bfloat16 *lsplit[2] = {nullptr, nullptr};  // A-operand split of inv(L11), b x nseg b
+  __nv_bfloat16 *usplit = nullptr;                // B-operand split of A12', rest x nseg b
 };
 
 // inv(L11) of a unit-lower b x b block: pla_k_trtri_unit_lower (independent
@@ -169,10 +198,11 @@ int unit_lower_inverse(const float *L11, long ld, int b, float *D) {
   return PLA_SUCCESS;
 }
 
-int split_alloc(SplitU12 &S, int n, int nb) {
-  const size_t d = (size_t)nb * nb * sizeof(float), l = (size_t)nb * 3 * nb * 2;
+int split_alloc(SplitU12 &S, int n, int nb, int nseg) {
+  S.nseg = nseg;
+  const size_t d = (size_t)nb * nb * sizeof(float), l = (size_t)nb * nseg * nb * 2;
   char *p = (char *)scratch(kSlotSplitL, 2 * (d + l) + 1024);
-  S.usplit = (__nv_bfloat16 *)scratch(kSlotSplitU, (size_t)n * 3 * nb * 2 + 1024);
+  S.usplit = (__nv_bfloat16 *)scratch(kSlotSplitU, (size_t)n * nseg * nb * 2 + 1024);
   if (!p || !S.usplit) PLA_FAIL("cannot allocate the split operands of the U12 solve");
   for (int q = 0; q < 2; q++) {
     S.dinv[q] = (float *)(p + q * (d + l));
@@ -186,7 +216,8 @@ int split_prepare(SplitU12 &S, int q, const float *L11, long ld, int b) {
   float *D = S.dinv[q];
   PK(unit_lower_inverse(L11, ld, b, D));
   // row i of inv(L11): element (i, k) at D[i + k b]
-  K(pla_k_pack_split(b, b, D, 1, b, S.lsplit[q], 3L * b, 0b100, 0, stream()));
+  K(pla_k_pack_split_ex(b, b, D, 1, b, S.lsplit[q], (long)S.nseg * b, S.nseg,
+                        S.nseg == 6 ? kSplitA6 : kSplitA3, 0, stream()));
   return PLA_SUCCESS;
 }
 
@@ -195,9 +226,11 @@ int split_solve(SplitU12 &S, int q, float *C, long ld, long c_rows, long c_cols,
                 int col0, int b, int cols, int *status) {
   float *A12 = C + row0 + (long)col0 * ld;
   // row j of A12' is column j of A12: element (j, k) at A12[k + j ld]
-  K(pla_k_pack_split(cols, b, A12, ld, 1, S.usplit, 3L * b, 0b010, 1, stream()));
-  K(pla_k_tc_update_ex(PLA_K_BF16, b, cols, 3 * b, 1.0f, S.lsplit[q], 3L * b, b, S.usplit,
-                       3L * b, cols, C, ld, c_rows, c_cols, row0, col0, 0, 0, status, stream()));
+  const long kk = (long)S.nseg * b;
+  K(pla_k_pack_split_ex(cols, b, A12, ld, 1, S.usplit, kk, S.nseg,
+                        S.nseg == 6 ? kSplitB6 : kSplitB3, 1, stream()));
+  K(pla_k_tc_update_ex(PLA_K_BF16, b, cols, (int)kk, 1.0f, S.lsplit[q], kk, b, S.usplit, kk,
+                       cols, C, ld, c_rows, c_cols, row0, col0, 0, 0, status, stream()));
   return PLA_SUCCESS;
 }
 
@@ -212,13 +245,19 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
     K(pla_k_convert(MPI_DOUBLE, A, lda, MPI_FLOAT, F.a, ld, n, n, stream()));
   const bool lowp = F.prec != PLA_B200_PREC_FP32;
   const bool f8 = F.prec == PLA_B200_PREC_FP8;
-  const int kprec = F.prec == PLA_B200_PREC_BF16 ? PLA_K_BF16 : PLA_K_FP16;
+  // bf16 x 6: each operand of the update split three ways into bf16, six
+  // K-wide segments per packed row, one K = 6b product of fp32 accuracy
+  const bool x6 = F.prec == PLA_B200_PREC_BF16X6;
+  const int nseg = x6 ? 6 : 1;
+  const int kprec =
+      F.prec == PLA_B200_PREC_BF16 || x6 ? PLA_K_BF16 : PLA_K_FP16;
   const int kmult = f8 ? 128 : 64;  // K granularity of the tensor-core update
+  const long ku = (long)nseg * nb;  // elements per packed operand row
   void *Lp = nullptr, *Up = nullptr;
   float *inv_l = nullptr, *inv_u = nullptr;
   if (lowp) {
-    Lp = scratch(kSlotL, (size_t)n * nb * 2 + 256);
-    Up = scratch(kSlotU, (size_t)n * nb * 2 + 256);
+    Lp = scratch(kSlotL, (size_t)n * ku * 2 + 256);
+    Up = scratch(kSlotU, (size_t)n * ku * 2 + 256);
     if (!Lp || !Up) PLA_FAIL("cannot allocate the low-precision panels");
     if (f8) {  // one scale per 128 rows of L and of U'
       const size_t tiles = (size_t)(n + 127) / 128 + 1;
@@ -246,7 +285,7 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
   // fp32 factorization keeps the fp32 solve)
   const bool split = F.kind == 0 && lowp && nb % 64 == 0 && nb <= 256;
   SplitU12 S;
-  if (split) PK(split_alloc(S, n, nb));
+  if (split) PK(split_alloc(S, n, nb, x6 ? 6 : 3));
   int ready = -1;
   for (int k = 0; k < n; k += nb) {
     const int b = std::min(nb, n - k), rest = n - k - b, k2 = k + b;
@@ -297,6 +336,16 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
             Uop = (const char *)Up;
             su = inv_u;
           }
+        } else if (x6) {
+          // A operand: L; B operand: U' (LU) or L again (Cholesky)
+          K(pla_k_pack_split_ex(rest, b, at(k + b, k), 1, ld, Lp, ku, 6, kSplitA6, 0, stream()));
+          if (F.kind == 0)
+            K(pla_k_pack_split_ex(rest, b, at(k, k + b), ld, 1, Up, ku, 6, kSplitB6, 0,
+                                  stream()));
+          else
+            K(pla_k_pack_split_ex(rest, b, at(k + b, k), 1, ld, Up, ku, 6, kSplitB6, 0,
+                                  stream()));
+          Uop = (const char *)Up;
         } else {
           K(pla_k_pack_rows(kprec, rest, b, at(k + b, k), ld, Lp, nb, stream()));
           if (F.kind == 0) {
@@ -313,8 +362,8 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
                                             Uop + off * nb * esz, nb, n - off, su + off / 128,
                                             F.a, ld, ld, n, k2, c0, F.kind == 1, cap, &st[0],
                                             stream())
-                   : pla_k_tc_update_ex(kprec, rest, nc, b, -1.0f, Lp, nb, n,
-                                        Uop + off * nb * esz, nb, n - off, F.a, ld, ld, n, k2, c0,
+                   : pla_k_tc_update_ex(kprec, rest, nc, nseg * b, -1.0f, Lp, ku, n,
+                                        Uop + off * ku * esz, ku, n - off, F.a, ld, ld, n, k2, c0,
                                         F.kind == 1, cap, &st[0], stream());
         if (t.on) ph.update_launches++;
         return r;
@@ -370,6 +419,19 @@ int factor_fp64(Factor &F, const double *A, long lda, int *info) {
 int precond(const Factor &F, const double *v, long ldv, double *out, long ldo, int nrhs,
             float *t32) {
   const int n = F.n;
+  if (F.dinv1d) {  // bf16 x 6 factors: P, then both solves in FP64 through `out`
+    if (F.kind == 0 && F.perm)
+      K(pla_k_gather_rows(MPI_DOUBLE, n, nrhs, F.perm, v, ldv, out, ldo, stream()));
+    else
+      K(pla_k_copy(MPI_DOUBLE, PLA_NO_TRANSPOSE, n, nrhs, v, ldv, out, ldo, stream()));
+    if (F.kind == 0 && !F.perm) K(pla_k_laswp_rows(MPI_DOUBLE, out, ldo, nrhs, n, F.piv, stream()));
+    const char u2 = F.kind == 0 ? 'U' : 'L', t2 = F.kind == 0 ? 'N' : 'T';
+    K(pla_k_trsv_ticket_multi_f64('L', 'N', n, nrhs, F.a, F.ld, F.dinv1d, F.ldd, out, ldo, out,
+                                  ldo, F.status, stream()));
+    K(pla_k_trsv_ticket_multi_f64(u2, t2, n, nrhs, F.a, F.ld, F.dinv2d, F.ldd, out, ldo, out, ldo,
+                                  F.status, stream()));
+    return PLA_SUCCESS;
+  }
   if (F.prec == PLA_B200_PREC_FP64) {
     if (F.kind == 0 && F.perm)
       K(pla_k_gather_rows(MPI_DOUBLE, n, nrhs, F.perm, v, ldv, out, ldo, stream()));
@@ -880,21 +942,41 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
 }
 
 // the next precision up when the refinement stagnates (0: none left).  BF16
-// and FP16 go straight to FP64: fp32 has no tensor-core path of fp32
-// accuracy, and the FP64 factorization on the DMMA pipe is the faster of the
-// two here (n = 32768 LU: 0.8 s FP64 against 1.1 s fp32; n = 49152
-// Cholesky: 1.6 s against 1.7 s), besides needing a step or two of
-// refinement where fp32 factors at kappa = 1e10 needed over a hundred GMRES
-// iterations.  FP32 factors stay available on request.
+// and FP16 go to bf16 x 6 factors (fp32 accuracy from the tensor cores at
+// about six times the bf16 tensor work), then to FP64.  Plain fp32 factors
+// (the SIMT update) are slower than either: at n = 32768 the fp32 LU took
+// 1.1 s against 0.8 s for the FP64 LU on the DMMA pipe; they stay available
+// on request and go to FP64.
 int escalated(int prec) {
   switch (prec) {
     case PLA_B200_PREC_FP8: return PLA_B200_PREC_BF16;
     case PLA_B200_PREC_BF16:
-    case PLA_B200_PREC_FP16:
+    case PLA_B200_PREC_FP16: return PLA_B200_PREC_BF16X6;
+    case PLA_B200_PREC_BF16X6:
     case PLA_B200_PREC_FP32: return PLA_B200_PREC_FP64;
     default: return 0;
   }
 }
+
+// unit roundoff of the trailing update's operands at each precision
+double unit_roundoff(int prec) {
+  switch (prec) {
+    case PLA_B200_PREC_FP8: return std::ldexp(1.0, -4);
+    case PLA_B200_PREC_BF16: return std::ldexp(1.0, -8);
+    case PLA_B200_PREC_FP16: return std::ldexp(1.0, -11);
+    case PLA_B200_PREC_BF16X6:
+    case PLA_B200_PREC_FP32: return std::ldexp(1.0, -24);
+    default: return std::ldexp(1.0, -53);
+  }
+}
+
+// Early escalation: factors whose diagonal range (max / min |u_ii|, a lower
+// bound on their condition number; squared for a Cholesky factor) times the
+// precision's unit roundoff exceeds this have been refactored one precision
+// up at once.  Measured on the n = 32768 C3 family: fp16 at kappa = 1e6 is
+// about 500 (17 GMRES iterations), at kappa = 1e10 about 5e6 (no convergence
+// within a restart cycle).
+constexpr double kEarlyEscalate = 1e4;
 
 // Ah: when not null, A's values are in host memory (column-major, ldh) and are
 // copied into the device object A during the call
@@ -908,7 +990,7 @@ int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
   if (pin) p = *pin;
   if (p.max_iterations <= 0) p.max_iterations = 50;
   if (p.gmres_restart <= 0) p.gmres_restart = 30;
-  if (p.precision < PLA_B200_PREC_BF16 || p.precision > PLA_B200_PREC_FP8)
+  if (p.precision < PLA_B200_PREC_BF16 || p.precision > PLA_B200_PREC_BF16X6)
     PLA_FAIL("unknown precision");
   if (p.panel_pivoting != PLA_B200_PIVOT_PARTIAL && p.panel_pivoting != PLA_B200_PIVOT_TOURNAMENT)
     PLA_FAIL("unknown panel pivoting");
@@ -1025,6 +1107,20 @@ int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
       if (!p.escalate || !escalated(prec)) break;
       prec = escalated(prec);
       continue;
+    }
+    if (prec != PLA_B200_PREC_FP64 && p.escalate && escalated(prec)) {
+      // the factors' diagonal range says whether to refine them at all; one
+      // level up at a time, since low-precision factors of an
+      // ill-conditioned matrix can show a range far beyond its condition
+      float dr[2];
+      K(pla_k_diag_range(n, F.a, F.ld, (float *)tmp, stream()));
+      PLA_CUDA(d2h(dr, tmp, sizeof dr));
+      double ratio = (double)dr[0] / (double)dr[1];
+      if (kind == 1) ratio *= ratio;
+      if (!(ratio * unit_roundoff(prec) <= kEarlyEscalate)) {
+        prec = escalated(prec);
+        continue;
+      }
     }
 
     // ---- refinement ----

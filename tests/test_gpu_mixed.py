@@ -237,12 +237,24 @@ def solve_mixed_params(s, pla, A, B, kind, **kw):
     return rc, X, rep
 
 
+def haar_matrix(n, kappa, seed):
+    """A = Q1 diag(sigma) Q2' with Q1, Q2 dense orthogonal (QR of Gaussian
+    matrices): unlike the C3 family, its LU factors' diagonal spreads over
+    only about sqrt(kappa), so the diagonal-range rule does not fire."""
+    rng = np.random.default_rng(seed)
+    q1 = np.linalg.qr(rng.standard_normal((n, n)))[0]
+    q2 = np.linalg.qr(rng.standard_normal((n, n)))[0]
+    sigma = kappa ** (-np.arange(n) / (n - 1))
+    return np.asfortranarray((q1 * sigma) @ q2.T)
+
+
 @pytest.mark.parametrize("prec", [1, 2])
-def test_kappa_1e10_escalates_to_fp64_backward_error(env, prec):
-    """kappa = 1e10 is out of reach of bf16/fp16 factors (kappa * u_f >> 1):
-    the refinement stagnates and the solver refactors in FP64, ending at FP64
-    backward error; the forward error is checked against the FP64 LAPACK
-    solution."""
+def test_kappa_1e10_escalates_to_split_factors(env, prec):
+    """kappa = 1e10 is out of reach of bf16/fp16 factors (kappa * u_f >> 1).
+    The C3 family's factors show it on their diagonal (range about kappa), so
+    the solver refactors with bf16 x 6 operands at once, without refining
+    the first factors, and ends at FP64 backward error; the forward error is
+    checked against the FP64 LAPACK solution."""
     s, torch, pla = env
     n = 2048
     A = c3_matrix(n, 1e10, 11)
@@ -250,8 +262,9 @@ def test_kappa_1e10_escalates_to_fp64_backward_error(env, prec):
     B = A @ x_true
     rc, X, rep = solve_mixed_params(s, pla, A, B, "lu", precision=prec, refinement=2)
     assert rc == 0 and rep.converged == 1, (rep.iterations, rep.backward_error)
-    # bf16 / fp16 escalate straight to FP64 (the faster of FP32 and FP64 here)
-    assert rep.precision_used == pla.PLA_B200_PREC_FP64 and rep.factorizations == 2
+    assert (rep.precision_used, rep.factorizations) == (pla.PLA_B200_PREC_BF16X6, 2), \
+        (rep.precision_used, rep.factorizations, rep.iterations, rep.inner_iterations)
+    assert rep.inner_iterations <= 60, rep.inner_iterations
     assert backward_error(A, X, B) <= n * 2.0 ** -53
     Xr = np.linalg.solve(A, B)
     fwd = np.abs(X - Xr).max() / np.abs(Xr).max()
@@ -261,21 +274,109 @@ def test_kappa_1e10_escalates_to_fp64_backward_error(env, prec):
 @pytest.mark.parametrize("refinement,max_steps", [(1, 2), (2, 1)])
 def test_stagnation_rule_per_refinement(env, refinement, max_steps):
     """How many non-halving steps escalate: one GMRES-IR step (a whole restart
-    cycle), two classic LU-IR steps.  kappa = 1e10 stagnates at once with fp16
-    factors, so the fp16 attempt ends after max_steps corrections and FP64
-    factors finish the solve."""
+    cycle), two classic LU-IR steps.  A dense-orthogonal kappa = 1e10 matrix
+    passes the diagonal-range rule with fp16 factors but stagnates at once,
+    so the fp16 attempt ends after max_steps corrections and higher
+    factors (bf16 x 6, then FP64 if those stagnate too) finish the solve."""
     s, torch, pla = env
     n = 1024
-    A = c3_matrix(n, 1e10, 17)
+    A = haar_matrix(n, 1e10, 17)
     B = A @ np.random.default_rng(18).standard_normal((n, 1))
     rc, X, rep = solve_mixed_params(s, pla, A, B, "lu", precision=2, refinement=refinement)
     assert rc == 0 and rep.converged == 1
-    assert rep.precision_used == pla.PLA_B200_PREC_FP64 and rep.factorizations == 2
-    # the fp16 attempt takes at most max_steps corrections, FP64 factors a few
-    assert rep.iterations <= max_steps + 3, rep.iterations
-    if refinement == 2:  # one restart cycle of fp16 GMRES (30), then short FP64 cycles
-        assert rep.inner_iterations <= 30 + 10, rep.inner_iterations
+    assert rep.factorizations >= 2
+    assert rep.precision_used in (pla.PLA_B200_PREC_BF16X6, pla.PLA_B200_PREC_FP64)
+    # the fp16 attempt takes at most max_steps corrections, the later ones a few
+    assert rep.iterations <= max_steps + 2 * 3, rep.iterations
+    if refinement == 2:  # one restart cycle of fp16 GMRES (30), then short cycles
+        assert rep.inner_iterations <= 30 + 40, rep.inner_iterations
     assert backward_error(A, X, B) <= n * 2.0 ** -53
+
+
+def test_bf16x6_factors(env):
+    """bf16 x 6 factors requested: fp32-level preconditioner, a few GMRES
+    iterations at kappa = 1e6 where fp16 factors need a dozen or more."""
+    s, torch, pla = env
+    n = 3000
+    A = c3_matrix(n, 1e6, 21)
+    B = A @ np.random.default_rng(22).standard_normal((n, 2))
+    rc, X, rep = solve_mixed_params(s, pla, A, B, "lu", precision=pla.PLA_B200_PREC_BF16X6,
+                                    refinement=2, nb=256)
+    assert rc == 0 and rep.converged == 1 and rep.factorizations == 1
+    assert rep.precision_used == pla.PLA_B200_PREC_BF16X6
+    assert rep.inner_iterations <= 2 * 6, rep.inner_iterations
+    assert backward_error(A, X, B) <= n * 2.0 ** -53
+
+
+@pytest.mark.parametrize("kappa", [1e3, 1e7])
+def test_bf16x6_cholesky(env, kappa):
+    s, torch, pla = env
+    n = 2048
+    A = spd_family(n, kappa, 33)
+    B = np.asfortranarray(A @ np.random.default_rng(34).standard_normal((n, 4)))
+    rc, X, rep = solve_mixed_params(s, pla, A, B, "chol", precision=pla.PLA_B200_PREC_BF16X6,
+                                    refinement=2)
+    assert rc == 0 and rep.converged == 1, (rep.iterations, rep.backward_error)
+    assert rep.precision_used in (pla.PLA_B200_PREC_BF16X6, pla.PLA_B200_PREC_FP64)
+    if kappa == 1e3:
+        assert rep.precision_used == pla.PLA_B200_PREC_BF16X6
+    assert backward_error(A, X, B) <= n * 2.0 ** -53
+
+
+def pack_split(lib, torch, X, nseg, code):
+    """pla_k_pack_split_ex of the column-major m x k float32 tensor X (stored
+    as X' row-major), rows of nseg k-wide segments."""
+    fn = lib.pla_k_pack_split_ex
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_long, ctypes.c_long,
+                   ctypes.c_void_p, ctypes.c_long, ctypes.c_int, ctypes.c_uint, ctypes.c_int,
+                   ctypes.c_void_p]
+    k, m = X.shape
+    out = torch.zeros(m, nseg * k, dtype=torch.bfloat16, device="cuda")
+    assert fn(m, k, X.data_ptr(), 1, m, out.data_ptr(), nseg * k, nseg, code, 0, None) == 0
+    torch.cuda.synchronize()
+    return out
+
+
+def test_pack_split_three_parts(env):
+    """x = p0 + p1 + p2 in bf16 parts, to within fp32 rounding; segment codes
+    place the parts."""
+    s, torch, pla = env
+    g = torch.Generator(device="cuda").manual_seed(5)
+    m, k = 300, 70
+    X = (torch.randn(k, m, device="cuda", generator=g) *
+         torch.exp(torch.randn(k, m, device="cuda", generator=g) * 4))
+    out = pack_split(s.lib, torch, X, 3, 0 | (1 << 2) | (2 << 4)).float()
+    x = X.t()                                                  # m x k, element (i, kk)
+    p0, p1, p2 = out[:, :k], out[:, k:2 * k], out[:, 2 * k:]
+    assert torch.equal(p0, x.to(torch.bfloat16).float())
+    assert torch.equal(p1, (x - p0).to(torch.bfloat16).float())
+    rec = (p0.double() + p1.double()) + p2.double()
+    assert ((rec - x.double()).abs() <= x.double().abs() * 2.0 ** -24).all()
+    six = pack_split(s.lib, torch, X, 6, 0x910).float()       # [0 0 1 0 1 2]
+    for seg, part in enumerate([p0, p0, p1, p0, p1, p2]):
+        assert torch.equal(six[:, seg * k:(seg + 1) * k], part)
+
+
+def test_tc_update_bf16x6_is_fp32_accurate(env):
+    """One K = 6b tensor-core product of bf16 x 6 split operands against the
+    float64 product of the fp32 operands: within a few fp32 roundings, far
+    inside what bf16 operands alone give."""
+    s, torch, pla = env
+    g = torch.Generator(device="cuda").manual_seed(7)
+    M, N, b = 1000, 900, 256
+    Lf = torch.randn(b, M, device="cuda", generator=g)          # column-major M x b
+    Uf = torch.randn(b, N, device="cuda", generator=g)          # U' column-major N x b
+    La = pack_split(s.lib, torch, Lf, 6, 0x124)                # [0 1 2 0 1 0]
+    Ub = pack_split(s.lib, torch, Uf, 6, 0x46)                 # [2 1 0 1 0 0]
+    ld = (M + 31) // 32 * 32
+    Cc = torch.zeros(N, ld, device="cuda")
+    tc_update(s.lib, torch, 1001, M, N, 6 * b, La, Ub, Cc, 0, 0)
+    ref = -(Lf.t().double() @ Uf.double())                     # M x N
+    err = (Cc[:, :M].t().double() - ref).abs().max().item()
+    assert err <= 8 * b * 2.0 ** -24 * (Lf.abs().max() * Uf.abs().max()).item(), err
+    lo = -(Lf.t().to(torch.bfloat16).double() @ Uf.to(torch.bfloat16).double())
+    assert err < 0.01 * (lo - ref).abs().max().item()
 
 
 def test_no_escalation_reports_stagnation(env):
@@ -408,7 +509,7 @@ def test_fp8_cholesky_ir(env, kappa):
     rc, X, rep = solve_mixed_params(s, pla, A, B, "chol", precision=pla.PLA_B200_PREC_FP8,
                                     refinement=2)
     assert rc == 0 and rep.converged == 1, (rep.iterations, rep.backward_error)
-    assert rep.precision_used in (pla.PLA_B200_PREC_FP8, 1, 3, 4)
+    assert rep.precision_used in (pla.PLA_B200_PREC_FP8, 1, 3, 4, pla.PLA_B200_PREC_BF16X6)
     assert backward_error(A, X, B) <= n * 2.0 ** -53
     Xr = np.linalg.solve(A, B)
     assert np.abs(X - Xr).max() / np.abs(Xr).max() <= kappa * n * 2.0 ** -53
@@ -527,3 +628,54 @@ def test_trsv_ticket_multi(env, uplo, trans, diag, n, ld, nrhs):
     ref = torch.linalg.solve_triangular(op, B.double().t(), upper=(uplo == "U") != (trans == "T"))
     err = (X.double().t() - ref).abs().max().item()
     assert err <= 64 * n * np.finfo(np.float32).eps * ref.abs().max().item(), err
+
+
+@pytest.mark.parametrize("uplo,trans,diag", [("L", "N", "U"), ("U", "N", "N"), ("L", "N", "N"),
+                                             ("L", "T", "N")])
+@pytest.mark.parametrize("n,ld,nrhs", [(1000, 1000, 1), (4096, 4096, 8), (777, 781, 16)])
+def test_trsv_ticket_multi_f64(env, uplo, trans, diag, n, ld, nrhs):
+    """The FP64 form on an fp32 triangle (the preconditioner of bf16 x 6
+    factors): FP64 right-hand sides, FP64 inverse diagonal blocks and
+    arithmetic, so the result matches an FP64 solve with the same fp32 values
+    to FP64 rounding, not fp32."""
+    s, torch, pla = env
+    lib = s.lib
+    for name, args in (("pla_k_trsv_inv_blocks_f64", [ctypes.c_char, ctypes.c_char, ctypes.c_char,
+                                                      ctypes.c_int, ctypes.c_void_p, ctypes.c_long,
+                                                      ctypes.c_void_p, ctypes.c_long,
+                                                      ctypes.c_void_p]),
+                       ("pla_k_trsv_ticket_multi_f64", [ctypes.c_char, ctypes.c_char, ctypes.c_int,
+                                                        ctypes.c_int, ctypes.c_void_p,
+                                                        ctypes.c_long, ctypes.c_void_p,
+                                                        ctypes.c_long, ctypes.c_void_p,
+                                                        ctypes.c_long, ctypes.c_void_p,
+                                                        ctypes.c_long, ctypes.c_void_p,
+                                                        ctypes.c_void_p])):
+        getattr(lib, name).argtypes = args
+        getattr(lib, name).restype = ctypes.c_int
+    g = torch.Generator(device="cuda").manual_seed(n + nrhs + 1)
+    M = torch.randn(n, n, device="cuda", generator=g, dtype=torch.float64) * (0.5 / n ** 0.5)
+    T = torch.tril(M, -1) if uplo == "L" else torch.triu(M, 1)
+    T.diagonal().copy_(1.0 + torch.rand(n, device="cuda", generator=g, dtype=torch.float64))
+    T32 = T.float()
+    Acm = torch.zeros(n, ld, device="cuda", dtype=torch.float32)
+    Acm[:, :n] = T32.t()
+    ldd = (n + 127) // 128 * 128
+    dinv = torch.zeros(128, ldd, device="cuda", dtype=torch.float64)
+    st = torch.zeros(4, dtype=torch.int32, device="cuda")
+    assert lib.pla_k_trsv_inv_blocks_f64(uplo.encode(), trans.encode(), diag.encode(), n,
+                                         Acm.data_ptr(), ld, dinv.data_ptr(), ldd, None) == 0
+    B = torch.randn(nrhs, n, device="cuda", generator=g, dtype=torch.float64)
+    X = B.clone()
+    assert lib.pla_k_trsv_ticket_multi_f64(uplo.encode(), trans.encode(), n, nrhs, Acm.data_ptr(),
+                                           ld, dinv.data_ptr(), ldd, X.data_ptr(), n, X.data_ptr(),
+                                           n, st.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    assert st[0].item() == 0
+    Td = T32.double()
+    if diag == "U":
+        Td.diagonal().fill_(1.0)
+    op = Td.t() if trans == "T" else Td
+    ref = torch.linalg.solve_triangular(op, B.t(), upper=(uplo == "U") != (trans == "T"))
+    err = (X.t() - ref).abs().max().item()
+    assert err <= 64 * n * np.finfo(np.float64).eps * ref.abs().max().item(), err
