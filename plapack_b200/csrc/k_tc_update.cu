@@ -10,7 +10,9 @@
 // HBM busy: one persistent CTA per SM walks 128 x 128 tiles of C with three
 // roles that overlap one tile's epilogue with the next tile's loads and MMAs:
 //   warp 0 (one thread): TMA loads of 64-wide K chunks of L and U (128-byte
-//            swizzle) into a ring of kStages shared-memory stages;
+//            swizzle) into a ring of STAGES shared-memory stages (4, or 5 for
+//            K > 512, where the chunks of a tile outnumber the stages and
+//            the load latency from L2 must be covered);
 //   warp 1 (one thread): tcgen05.mma (kind::f16, fp32 accumulate) into one of
 //            two TMEM accumulators; tcgen05.commit frees each stage and, after
 //            the last chunk, hands the accumulator to the epilogue;
@@ -33,13 +35,14 @@ namespace {
 
 constexpr int TM = 128, TN = 128, KBOX = 64;
 constexpr int BOX_BYTES = TM * KBOX * 2;      // 16 KB: 128 rows x 128 bytes
-constexpr int kStages = 4;                    // operand ring: (L box, U box) per stage
 constexpr int STAGE_BYTES = 2 * BOX_BYTES;    // 32 KB
 constexpr int CW = 32;                        // epilogue chunk: 32 columns of a tile
 constexpr int kChunks = 4;                    // staging buffers for the reduce-adds
 constexpr int CHUNK_BYTES = TM * CW * 4;      // 16 KB of fp32
 constexpr int THREADS = 192;                  // TMA warp, MMA warp, 4 epilogue warps
-constexpr int SMEM_BYTES = kStages * STAGE_BYTES + kChunks * CHUNK_BYTES + 1024;
+// dynamic shared memory with `stages` operand stages (the ring, then the
+// reduce-add staging buffers, 1 KB of alignment slack)
+constexpr int smem_bytes(int stages) { return stages * STAGE_BYTES + kChunks * CHUNK_BYTES + 1024; }
 constexpr long kSpin = 20000000;              // bounded polling (~1-2 s)
 
 __device__ __forceinline__ uint32_t su32(const void *p) {
@@ -189,7 +192,7 @@ __device__ __forceinline__ void tile_coords(int t, int tiles_m, int tiles_n, int
 
 // F8: E4M3 operands with one power-of-two scale per 128-row tile of L and of
 // U (inv_l, inv_u); a K chunk is then 128 elements (still 128 bytes per row)
-template <bool F8>
+template <bool F8, int STAGES>
 __global__ void __launch_bounds__(THREADS, 1)
 tc_update_k(const __grid_constant__ CUtensorMap mapL, const __grid_constant__ CUtensorMap mapU,
             const __grid_constant__ CUtensorMap mapC, int M, int N, int kchunks, int row0,
@@ -197,6 +200,7 @@ tc_update_k(const __grid_constant__ CUtensorMap mapL, const __grid_constant__ CU
             const float *inv_u, int *status) {
   constexpr int KE = F8 ? 128 : KBOX;  // elements per K chunk
   extern __shared__ uint8_t smem_raw[];
+  constexpr int kStages = STAGES;
   __shared__ __align__(8) uint64_t full[kStages], empty[kStages], acc_full[2], acc_empty[2],
       bar_drain;
   __shared__ uint32_t tmem_s;
@@ -400,7 +404,7 @@ int encode(CUtensorMap *map, CUtensorMapDataType dt, int esize, const void *ptr,
 
 int g_sms = 0;
 
-template <bool F8>
+template <bool F8, int STAGES>
 int launch(const CUtensorMap &mL, const CUtensorMap &mU, const CUtensorMap &mC, int M, int N,
            int kchunks, int row0, int col0, float alpha, uint32_t idesc, int lower, int band,
            const float *inv_l, const float *inv_u, int max_ctas, int *status, cudaStream_t s) {
@@ -409,14 +413,17 @@ int launch(const CUtensorMap &mL, const CUtensorMap &mU, const CUtensorMap &mC, 
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
   }
-  cudaFuncSetAttribute(tc_update_k<F8>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  constexpr int kSmem = smem_bytes(STAGES);
+  cudaFuncSetAttribute(tc_update_k<F8, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       kSmem);
   const long tiles = (long)((M + TM - 1) / TM) * ((N + TN - 1) / TN);
   const int cap = max_ctas > 0 && max_ctas < g_sms ? max_ctas : g_sms;
   const int grid = (int)(tiles < cap ? tiles : cap);
   const int tiles_m = (M + TM - 1) / TM;
   if (band <= 0 || band > tiles_m) band = tiles_m;
-  tc_update_k<F8><<<grid, THREADS, SMEM_BYTES, s>>>(mL, mU, mC, M, N, kchunks, row0, col0, alpha,
-                                                    idesc, lower, band, inv_l, inv_u, status);
+  tc_update_k<F8, STAGES><<<grid, THREADS, kSmem, s>>>(mL, mU, mC, M, N, kchunks, row0, col0,
+                                                       alpha, idesc, lower, band, inv_l, inv_u,
+                                                       status);
   pla_k_count(1);
   return (int)cudaGetLastError();
 }
@@ -453,8 +460,12 @@ extern "C" int pla_k_tc_update_ex(int prec, int M, int N, int K, float alpha, co
   // K past 512 (split operands): bands of 32 tile rows, so that the L rows
   // in flight (32 x 128 rows x 2K bytes) stay in L2 across the band's columns
   const int band = K > 512 ? 32 : 0;
-  return launch<false>(mL, mU, mC, M, N, K / KBOX, row0, col0, alpha, idesc, lower, band, nullptr,
-                       nullptr, max_ctas, status, s);
+  // a fifth stage for the long K: 8 % faster at K = 1536 (16384^2), 2 % slower at K = 256
+  if (K > 512)
+    return launch<false, 5>(mL, mU, mC, M, N, K / KBOX, row0, col0, alpha, idesc, lower, band,
+                            nullptr, nullptr, max_ctas, status, s);
+  return launch<false, 4>(mL, mU, mC, M, N, K / KBOX, row0, col0, alpha, idesc, lower, band,
+                          nullptr, nullptr, max_ctas, status, s);
 }
 
 extern "C" int pla_k_tc_update(int prec, int M, int N, int K, float alpha, const void *L,
@@ -492,8 +503,8 @@ extern "C" int pla_k_tc_update_fp8_ex(int M, int N, int K, float alpha, const vo
   // instruction descriptor, kind::f8f6f4: fp32 accumulate, A and B both E4M3
   // (format 0), both K-major, N = 128, M = 128
   const uint32_t idesc = (1u << 4) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
-  return launch<true>(mL, mU, mC, M, N, K / 128, row0, col0, alpha, idesc, lower, 0, inv_l, inv_u,
-                      max_ctas, status, s);
+  return launch<true, 4>(mL, mU, mC, M, N, K / 128, row0, col0, alpha, idesc, lower, 0, inv_l,
+                         inv_u, max_ctas, status, s);
 }
 
 extern "C" int pla_k_tc_update_fp8(int M, int N, int K, float alpha, const void *L, long ldl,

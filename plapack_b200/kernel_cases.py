@@ -226,26 +226,39 @@ def case_trsv(torch, lib, a):
 
 
 def case_trsv_multi(torch, lib, a):
-    """pla_k_trsv_ticket_multi: --k right-hand sides (at most 16) in one launch."""
+    """pla_k_trsv_ticket_multi: --k right-hand sides (at most 16) in one launch,
+    on an fp32 factor; with --dtype f64 the FP64 form (pla_k_trsv_ticket_multi_f64:
+    FP64 right-hand sides and arithmetic, the bf16 x 6 preconditioner)."""
     n, nrhs = a.n, min(a.k, 16)
+    f64 = a.dtype == "f64"
+    vt = torch.float64 if f64 else torch.float32
     ld = (n + 31) // 32 * 32
     M = torch.randn(n, ld, device="cuda") * 0.01
     M.diagonal()[:n] += 1.0
     ldd = (n + 127) // 128 * 128
-    Dinv = torch.zeros(128, ldd, device="cuda")
-    B = torch.randn(nrhs, n, device="cuda")
+    Dinv = torch.zeros(128, ldd, device="cuda", dtype=vt)
+    B = torch.randn(nrhs, n, device="cuda", dtype=vt)
     X = torch.empty_like(B)
     st = torch.zeros(4, dtype=torch.int32, device="cuda")
-    inv = _fn(lib, "pla_k_trsv_inv_blocks", [i32, ch, ch, ch, i32, vp, lg, vp, lg, vp])
-    assert inv(pla.MPI_FLOAT, b"L", b"N", b"U", n, M.data_ptr(), ld, Dinv.data_ptr(), ldd, None) == 0
-    g = _fn(lib, "pla_k_trsv_ticket_multi", [ch, ch, i32, i32, vp, lg, vp, lg, vp, lg, vp, lg, vp,
-                                             vp])
+    if f64:
+        inv = _fn(lib, "pla_k_trsv_inv_blocks_f64", [ch, ch, ch, i32, vp, lg, vp, lg, vp])
+        assert inv(b"L", b"N", b"U", n, M.data_ptr(), ld, Dinv.data_ptr(), ldd, None) == 0
+        g = _fn(lib, "pla_k_trsv_ticket_multi_f64", [ch, ch, i32, i32, vp, lg, vp, lg, vp, lg, vp,
+                                                     lg, vp, vp])
+    else:
+        inv = _fn(lib, "pla_k_trsv_inv_blocks", [i32, ch, ch, ch, i32, vp, lg, vp, lg, vp])
+        assert inv(pla.MPI_FLOAT, b"L", b"N", b"U", n, M.data_ptr(), ld, Dinv.data_ptr(), ldd,
+                   None) == 0
+        g = _fn(lib, "pla_k_trsv_ticket_multi", [ch, ch, i32, i32, vp, lg, vp, lg, vp, lg, vp, lg,
+                                                 vp, vp])
     t = _time(torch, lambda: g(b"L", b"N", n, nrhs, M.data_ptr(), ld, Dinv.data_ptr(), ldd,
                                B.data_ptr(), n, X.data_ptr(), n, st.data_ptr(), None),
               a.warmup, a.reps)
     assert st[0].item() == 0
-    byt = 4.0 * n * n / 2 + 2 * 4.0 * n * nrhs
-    return {"case": f"single-launch unit-lower triangular solve, n={n}, {nrhs} rhs (fp32 factor)",
+    es = 8 if f64 else 4
+    byt = 4.0 * n * n / 2 + 2 * es * n * nrhs
+    return {"case": f"single-launch unit-lower triangular solve, n={n}, {nrhs} rhs (fp32 factor, "
+                    f"{'FP64' if f64 else 'fp32'} right-hand sides and arithmetic)",
             "s": t, "algorithmic_bytes": byt, "gbs": byt / t / 1e9,
             "gflops": 2.0 * n * n / 2 * nrhs / t / 1e9}
 
