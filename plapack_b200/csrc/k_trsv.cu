@@ -226,6 +226,206 @@ trsv_ticket_k(int n, int nblk, const T *A, long lda, bool lower_op, bool trans, 
   }
 }
 
+// The link blocks of the fp32 single-column solve: for every block row i
+// that has a predecessor p in the solve order (p = i - 1 going forward, i + 1
+// going backward), G_i = op(A)(i, p) inv(D_p), element (r, c) at
+// G[i TB + r + c ldd] (the layout of Dinv).  One CTA per link, the two
+// 128 x 128 factors in shared memory.
+__global__ void __launch_bounds__(THREADS)
+link_blocks_k(int n, int nblk, const float *A, long lda, bool lower_op, bool trans,
+              const float *Dinv, long ldd, float *G) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  float *As = reinterpret_cast<float *>(sm);  // op(A)(i, p), column-major, ld TB + 1
+  float *Ds = As + TB * (TB + 1);             // inv(D_p), column-major, ld TB + 1
+  constexpr int L = TB + 1;
+  const int i = lower_op ? blockIdx.x + 1 : blockIdx.x, p = lower_op ? i - 1 : i + 1;
+  const long r0 = (long)i * TB, c0 = (long)p * TB;
+  const int nbi = min(TB, n - (int)r0), nbp = min(TB, n - (int)c0);
+  for (int e = threadIdx.x; e < TB * TB; e += THREADS) {
+    const int r = e % TB, c = e / TB;
+    As[r + c * L] = r < nbi && c < nbp ? (trans ? A[(c0 + c) + (r0 + r) * lda]
+                                                 : A[(r0 + r) + (c0 + c) * lda])
+                                       : 0.f;
+    Ds[r + c * L] = Dinv[(c0 + r) + (long)c * ldd];
+  }
+  __syncthreads();
+  // thread (r, cg): row r, columns cg, cg + 2, ... (64 of them)
+  const int r = threadIdx.x % TB, cg = threadIdx.x / TB;
+  for (int c = cg; c < TB; c += 2) {
+    float acc = 0.f;
+    for (int k = 0; k < TB; k++) acc = fmaf(As[r + k * L], Ds[k + c * L], acc);
+    G[r0 + r + (long)c * ldd] = acc;
+  }
+}
+
+// The single-column fp32 solve with link blocks.  Block row i publishes y_i =
+// b_i - sum_{j before i} op(A)(i, j) x_j before it forms x_i = inv(D_i) y_i;
+// its successor s reads y_i and multiplies it by G_s = op(A)(s, i) inv(D_i)
+// in place of op(A)(s, i) x_i.  y carries its own readiness: the buffer is
+// filled with the bit pattern kEmpty before the launch, the producer stores
+// plain values (a value with that pattern, a NaN, is stored as another NaN),
+// and each consumer thread polls its own element until it changes -- no
+// fence, flag or second load on the chain from one block to the next.  x_i
+// is then published behind a flag (fx) for the blocks further on; every other
+// detail is trsv_ticket_k's.
+constexpr unsigned kEmpty = 0xffffffffu;
+
+__device__ __forceinline__ unsigned ld_relaxed_u32(const float *p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__global__ void __launch_bounds__(THREADS)
+trsv_link_k(int n, int nblk, const float *A, long lda, bool lower_op, bool trans,
+            const float *Dinv, long ldd, const float *G, const float *b, float *x, float *ybuf,
+            int *ticket, int *fx, int *status, bool vec_ok, bool g_ok) {
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  float *Ds = reinterpret_cast<float *>(dyn_smem);  // TB x TB inverse diagonal block
+  __shared__ float xs[TB];
+  __shared__ float part[2][TB];
+  __shared__ float red[8][TB];
+  __shared__ int s_blk, s_bad;
+  const int r = threadIdx.x % TB, half = threadIdx.x / TB;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_blk = atomicAdd(ticket, 1);
+      s_bad = 0;
+    }
+    __syncthreads();
+    const int q = s_blk;
+    if (q >= nblk) return;
+    const int i = lower_op ? q : nblk - 1 - q;
+    const long r0 = (long)i * TB;
+    const int nbi = min(TB, n - (int)r0);
+    const int rg = threadIdx.x & 31, cg = threadIdx.x >> 5;
+    float acc4[4] = {0.f, 0.f, 0.f, 0.f};
+    float acc = 0.f;
+    for (int u = threadIdx.x; u < TB * TB / 4; u += THREADS) {
+      const int c = u / (TB / 4), r4 = (u % (TB / 4)) * 4;
+      cp_async16(&Ds[c * TB + r4], Dinv + (r0 + r4) + (long)c * ldd);
+    }
+    cp_async_commit();
+    for (int s = 0; s < q; s++) {
+      const int j = lower_op ? s : nblk - 1 - s;
+      const bool link = s == q - 1;  // the block solved just before i: G_i and y_j
+      const long c0 = (long)j * TB;
+      const int nbj = min(TB, n - (int)c0);
+      const bool full = nbi == TB && nbj == TB && (link ? g_ok : vec_ok);
+      const bool ntr = link || !trans;  // G is stored untransposed
+      float4 v[16];
+      if (full) {
+        const float *base = link ? G + (r0 + 4 * rg) + (long)(16 * cg) * ldd
+                            : trans ? A + (r0 + r) * lda + c0 + 64 * half
+                                    : A + (r0 + 4 * rg) + (c0 + 16 * cg) * lda;
+        const long step = link ? ldd : trans ? 4 : lda;
+#pragma unroll
+        for (int u = 0; u < 16; u++) v[u] = *reinterpret_cast<const float4 *>(base + u * step);
+      }
+      if (link) {  // each thread waits for its own element of y_j
+        if (threadIdx.x < nbj) {
+          long spins = 0;
+          unsigned u;
+          while ((u = ld_relaxed_u32(&ybuf[c0 + threadIdx.x])) == kEmpty) {
+            if (++spins > kSpin || *(volatile int *)status != PLA_K_OK) {
+              atomicCAS(status, PLA_K_OK, PLA_K_TIMEOUT);
+              s_bad = 1;
+              break;
+            }
+            __nanosleep(32);
+          }
+          xs[threadIdx.x] = __uint_as_float(u);
+        }
+        __syncthreads();
+        if (s_bad) return;
+      } else {
+        if (threadIdx.x == 0) {
+          long spins = 0;
+          while (ld_acquire(&fx[j]) == 0) {
+            if (++spins > kSpin || *(volatile int *)status != PLA_K_OK) {
+              atomicCAS(status, PLA_K_OK, PLA_K_TIMEOUT);
+              s_bad = 1;
+              break;
+            }
+            __nanosleep(32);
+          }
+        }
+        __syncthreads();
+        if (s_bad) return;
+        if (threadIdx.x < nbj) xs[threadIdx.x] = __ldcg(&x[c0 + threadIdx.x]);
+        __syncthreads();
+      }
+      if (full && ntr) {
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+          const float xv = xs[16 * cg + u];
+          acc4[0] += v[u].x * xv;
+          acc4[1] += v[u].y * xv;
+          acc4[2] += v[u].z * xv;
+          acc4[3] += v[u].w * xv;
+        }
+      } else if (full) {
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+          const int c = 64 * half + 4 * u;
+          acc += v[u].x * xs[c] + v[u].y * xs[c + 1] + v[u].z * xs[c + 2] + v[u].w * xs[c + 3];
+        }
+      } else if (r < nbi) {
+        if (link) {
+          for (int c = half; c < nbj; c += 2) acc += G[(r0 + r) + (long)c * ldd] * xs[c];
+        } else if (!trans) {
+          for (int c = half; c < nbj; c += 2) acc += A[(r0 + r) + (c0 + c) * lda] * xs[c];
+        } else {
+          const int cb = half * (TB / 2), ce = min(cb + TB / 2, nbj);
+          const float *col = A + (r0 + r) * lda + c0;
+          for (int c = cb; c < ce; c++) acc += col[c] * xs[c];
+        }
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int e = 0; e < 4; e++) red[cg][4 * rg + e] = acc4[e];
+    part[half][r] = acc;
+    __syncthreads();
+    if (threadIdx.x < TB) {
+      float sacc = part[0][r] + part[1][r];
+#pragma unroll
+      for (int g = 0; g < 8; g++) sacc += red[g][r];
+      const float y = r < nbi ? b[r0 + r] - sacc : 0.f;
+      xs[threadIdx.x] = y;
+      if (r < nbi)  // the successor may start
+        ybuf[r0 + r] = __float_as_uint(y) == kEmpty ? __uint_as_float(0x7fffffffu) : y;
+    }
+    __syncthreads();
+    // x_i = inv(D_i) y_i, for the blocks further on
+    cp_async_wait_all();
+    __syncthreads();
+    {
+      float y4[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int u = 0; u < 16; u++) {
+        const float4 d = *reinterpret_cast<const float4 *>(&Ds[(16 * cg + u) * TB + 4 * rg]);
+        const float xv = xs[16 * cg + u];
+        y4[0] += d.x * xv;
+        y4[1] += d.y * xv;
+        y4[2] += d.z * xv;
+        y4[3] += d.w * xv;
+      }
+#pragma unroll
+      for (int e = 0; e < 4; e++) red[cg][4 * rg + e] = y4[e];
+    }
+    __syncthreads();
+    if (threadIdx.x < nbi) {
+      float y = 0.f;
+#pragma unroll
+      for (int g = 0; g < 8; g++) y += red[g][threadIdx.x];
+      x[r0 + threadIdx.x] = y;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) st_release(&fx[i], 1);
+  }
+}
+
 // The same solve for several right-hand sides (fp32): X := inv(op(A)) B, B
 // and X n x nrhs.  The columns form groups of NR (blockIdx.y); each group is
 // an independent ticket chain with its own counter and flags, and the groups'
@@ -670,6 +870,49 @@ int ticket_solve64(char uplo, char trans, int n, const void *A, long lda, const 
   return (int)cudaGetLastError();
 }
 
+int link_blocks(char uplo, char trans, int n, const float *A, long lda, const float *Dinv,
+                long ldd, float *G, cudaStream_t s) {
+  const bool tr = trans != 'N', lower_op = (uplo == 'L') != tr;
+  const int nblk = (n + TB - 1) / TB;
+  if (nblk < 2) return 0;
+  if (ldd % TB) return (int)cudaErrorMisalignedAddress;
+  const size_t sm = (size_t)2 * TB * (TB + 1) * sizeof(float);
+  cudaFuncSetAttribute(link_blocks_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  link_blocks_k<<<nblk - 1, THREADS, sm, s>>>(n, nblk, A, lda, lower_op, tr, Dinv, ldd, G);
+  pla_k_count(1);
+  return (int)cudaGetLastError();
+}
+
+int ticket_solve_link(char uplo, char trans, int n, const float *A, long lda, const float *Dinv,
+                      long ldd, const float *G, const float *b, float *x, int *status,
+                      cudaStream_t s) {
+  const bool tr = trans != 'N', lower_op = (uplo == 'L') != tr;
+  const int nblk = (n + TB - 1) / TB;
+  // fx, the ticket, then y (n floats, filled with the bit pattern kEmpty)
+  const int nflags = nblk + 8;
+  int *fl = flags_for(nflags + n);
+  if (!fl) return (int)cudaErrorMemoryAllocation;
+  cudaError_t e = cudaMemsetAsync(fl, 0, (size_t)nflags * sizeof(int), s);
+  if (e) return (int)e;
+  e = cudaMemsetAsync(fl + nflags, 0xff, (size_t)n * sizeof(float), s);
+  if (e) return (int)e;
+  if (!g_sms) {
+    int d;
+    cudaGetDevice(&d);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, d);
+  }
+  if (ldd % TB || (uintptr_t)Dinv % 16 || (uintptr_t)G % 16) return (int)cudaErrorMisalignedAddress;
+  const bool vec_ok = lda % 4 == 0 && (uintptr_t)A % 16 == 0;
+  int grid = nblk < 3 * g_sms ? nblk : 3 * g_sms;
+  const size_t dyn = (size_t)TB * TB * sizeof(float);
+  cudaFuncSetAttribute(trsv_link_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+  trsv_link_k<<<grid, THREADS, dyn, s>>>(n, nblk, A, lda, lower_op, tr, Dinv, ldd, G, b, x,
+                                         reinterpret_cast<float *>(fl + nflags), fl + nblk, fl,
+                                         status, vec_ok, true);
+  pla_k_count(1);
+  return (int)cudaGetLastError();
+}
+
 }  // namespace
 
 // Dinv must hold ldd x TB elements with ldd >= n rounded up to TB (TB = 128
@@ -727,6 +970,24 @@ extern "C" int pla_k_trsv_ticket_multi_f64(char uplo, char trans, int n, int nrh
   if (nrhs > 16) return (int)cudaErrorInvalidValue;
   return ticket_solve_nr<4, double>(uplo, trans, n, nrhs, A, lda, Dinv, ldd, B, ldb, X, ldx,
                                     status, s);
+}
+
+// The link blocks G of an fp32 triangle (ldd x TB floats, the layout of its
+// Dinv), for pla_k_trsv_ticket_link
+extern "C" int pla_k_trsv_link_blocks(char uplo, char trans, int n, const float *A, long lda,
+                                      const float *Dinv, long ldd, float *G, cudaStream_t s) {
+  if (n <= 0) return 0;
+  return link_blocks(uplo, trans, n, A, lda, Dinv, ldd, G, s);
+}
+
+// x := inv(op(A)) b (fp32, one column, b and x may be the same array) with the
+// link blocks: the chain between consecutive blocks skips the inverse-block
+// product
+extern "C" int pla_k_trsv_ticket_link(char uplo, char trans, int n, const float *A, long lda,
+                                      const float *Dinv, long ldd, const float *G,
+                                      const float *b, float *x, int *status, cudaStream_t s) {
+  if (n <= 0) return 0;
+  return ticket_solve_link(uplo, trans, n, A, lda, Dinv, ldd, G, b, x, status, s);
 }
 
 extern "C" void pla_trsv_release(void) {

@@ -204,6 +204,14 @@ int pla_k_trsv_inv_blocks_f64(char uplo, char trans, char diag, int n, const flo
 int pla_k_trsv_ticket_multi_f64(char uplo, char trans, int n, int nrhs, const float *A, long lda,
                                 const double *Dinv, long ldd, const double *B, long ldb,
                                 double *X, long ldx, int *status, cudaStream_t s);
+/* single-column fp32 solve with link blocks G_i = op(A)(i, p) inv(D_p) (p the
+ * block solved just before i; ldd x 128 floats, the layout of Dinv): the chain
+ * between blocks skips the inverse-block product */
+int pla_k_trsv_link_blocks(char uplo, char trans, int n, const float *A, long lda,
+                           const float *Dinv, long ldd, float *G, cudaStream_t s);
+int pla_k_trsv_ticket_link(char uplo, char trans, int n, const float *A, long lda,
+                           const float *Dinv, long ldd, const float *G, const float *b, float *x,
+                           int *status, cudaStream_t s);
 void pla_trsv_release(void);
 /* out (dt_out = MPI_FLOAT or MPI_DOUBLE, n x nrhs, ldo) := rows perm[0..n) of
  * the FP64 in (ldi): a composed row permutation and a conversion in one pass */

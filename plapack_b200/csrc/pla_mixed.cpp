@@ -69,8 +69,10 @@ struct Factor {
   int *piv = nullptr;
   int *perm = nullptr;    // LU: row i of P v is v[perm[i]] (the pivots composed)
   int *status = nullptr;  // [status, info, zero_info]
-  // inverses of the 128 x 128 diagonal blocks of the two triangular factors
+  // inverses of the 128 x 128 diagonal blocks of the two triangular factors,
+  // and their link blocks (op(T)(i, p) inv(D_p), p the block solved before i)
   float *dinv1 = nullptr, *dinv2 = nullptr;
+  float *link1 = nullptr, *link2 = nullptr;
   // BF16X6: the same inverses in FP64, the solves with the fp32 factors then
   // carried out in FP64 (fp32-level factors serve up to kappa near 2^24 times
   // the refinement's reach, and an fp32 solve would round that away)
@@ -80,6 +82,7 @@ struct Factor {
 
 constexpr int kSlotDinv = 13;
 constexpr int kSlotDinv64 = 12;
+constexpr int kSlotLink = 28;
 constexpr int kSlotPerm = 30;
 
 // The row interchanges of an LU composed into one permutation, once per
@@ -122,16 +125,18 @@ int prepare_solves(Factor &F) {
     return PLA_SUCCESS;
   }
   float *d = (float *)scratch(kSlotDinv, (size_t)2 * F.ldd * 128 * sizeof(float));
-  if (!d) PLA_FAIL("cannot allocate the inverse diagonal blocks");
+  float *g = (float *)scratch(kSlotLink, (size_t)2 * F.ldd * 128 * sizeof(float));
+  if (!d || !g) PLA_FAIL("cannot allocate the inverse diagonal blocks");
   F.dinv1 = d;
   F.dinv2 = d + F.ldd * 128;
-  if (F.kind == 0) {
-    K(pla_k_trsv_inv_blocks(MPI_FLOAT, 'L', 'N', 'U', F.n, F.a, F.ld, F.dinv1, F.ldd, stream()));
-    K(pla_k_trsv_inv_blocks(MPI_FLOAT, 'U', 'N', 'N', F.n, F.a, F.ld, F.dinv2, F.ldd, stream()));
-  } else {
-    K(pla_k_trsv_inv_blocks(MPI_FLOAT, 'L', 'N', 'N', F.n, F.a, F.ld, F.dinv1, F.ldd, stream()));
-    K(pla_k_trsv_inv_blocks(MPI_FLOAT, 'L', 'T', 'N', F.n, F.a, F.ld, F.dinv2, F.ldd, stream()));
-  }
+  F.link1 = g;
+  F.link2 = g + F.ldd * 128;
+  const char u1 = 'L', t1 = 'N', d1 = F.kind == 0 ? 'U' : 'N';
+  const char u2 = F.kind == 0 ? 'U' : 'L', t2 = F.kind == 0 ? 'N' : 'T';
+  K(pla_k_trsv_inv_blocks(MPI_FLOAT, u1, t1, d1, F.n, F.a, F.ld, F.dinv1, F.ldd, stream()));
+  K(pla_k_trsv_inv_blocks(MPI_FLOAT, u2, t2, 'N', F.n, F.a, F.ld, F.dinv2, F.ldd, stream()));
+  K(pla_k_trsv_link_blocks(u1, t1, F.n, F.a, F.ld, F.dinv1, F.ldd, F.link1, stream()));
+  K(pla_k_trsv_link_blocks(u2, t2, F.n, F.a, F.ld, F.dinv2, F.ldd, F.link2, stream()));
   return PLA_SUCCESS;
 }
 
@@ -462,12 +467,14 @@ int precond(const Factor &F, const double *v, long ldv, double *out, long ldo, i
   const char u1 = 'L', t1 = 'N', d1 = F.kind == 0 ? 'U' : 'N';
   const char u2 = F.kind == 0 ? 'U' : 'L', t2 = F.kind == 0 ? 'N' : 'T', d2 = 'N';
   if (nrhs <= 2 && F.dinv1) {
+    // the single-column solves with link blocks: the successor of a block
+    // starts from its y, before the inverse-block product
     for (int j = 0; j < nrhs; j++) {
       float *col = t32 + (long)j * n;
-      K(pla_k_trsv_ticket(MPI_FLOAT, u1, t1, n, F.a, F.ld, F.dinv1, F.ldd, col, col, F.status,
-                          stream()));
-      K(pla_k_trsv_ticket(MPI_FLOAT, u2, t2, n, F.a, F.ld, F.dinv2, F.ldd, col, col, F.status,
-                          stream()));
+      K(pla_k_trsv_ticket_link(u1, t1, n, F.a, F.ld, F.dinv1, F.ldd, F.link1, col, col,
+                               F.status, stream()));
+      K(pla_k_trsv_ticket_link(u2, t2, n, F.a, F.ld, F.dinv2, F.ldd, F.link2, col, col,
+                               F.status, stream()));
     }
   } else if (nrhs <= 16 && F.dinv1) {
     // all the columns in one launch per triangle: the factors are read once

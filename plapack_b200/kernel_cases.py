@@ -224,6 +224,32 @@ def case_trsv(torch, lib, a):
     return {"case": f"single-launch unit-lower triangular solve, n={n} (fp32 factor)", "s": t,
             "algorithmic_bytes": byt, "gbs": byt / t / 1e9}
 
+def case_trsv_link(torch, lib, a):
+    """The single-column solve with link blocks (pla_k_trsv_ticket_link), the
+    link blocks formed once beforehand as the refinement does per factor."""
+    n = a.n
+    ld = (n + 31) // 32 * 32
+    M = torch.randn(n, ld, device="cuda") * 0.01
+    M.diagonal()[:n] += 1.0
+    ldd = (n + 127) // 128 * 128
+    Dinv = torch.zeros(128, ldd, device="cuda")
+    G = torch.zeros(128, ldd, device="cuda")
+    b = torch.randn(n, device="cuda")
+    x = torch.empty_like(b)
+    st = torch.zeros(4, dtype=torch.int32, device="cuda")
+    inv = _fn(lib, "pla_k_trsv_inv_blocks", [i32, ch, ch, ch, i32, vp, lg, vp, lg, vp])
+    assert inv(pla.MPI_FLOAT, b"L", b"N", b"U", n, M.data_ptr(), ld, Dinv.data_ptr(), ldd, None) == 0
+    lk = _fn(lib, "pla_k_trsv_link_blocks", [ch, ch, i32, vp, lg, vp, lg, vp, vp])
+    assert lk(b"L", b"N", n, M.data_ptr(), ld, Dinv.data_ptr(), ldd, G.data_ptr(), None) == 0
+    g = _fn(lib, "pla_k_trsv_ticket_link", [ch, ch, i32, vp, lg, vp, lg, vp, vp, vp, vp, vp])
+    t = _time(torch, lambda: g(b"L", b"N", n, M.data_ptr(), ld, Dinv.data_ptr(), ldd,
+                               G.data_ptr(), b.data_ptr(), x.data_ptr(), st.data_ptr(), None),
+              a.warmup, a.reps)
+    assert st[0].item() == 0
+    byt = 4.0 * n * n / 2
+    return {"case": f"single-launch unit-lower triangular solve with link blocks, n={n} "
+                    f"(fp32 factor)", "s": t, "algorithmic_bytes": byt, "gbs": byt / t / 1e9}
+
 
 def case_trsv_multi(torch, lib, a):
     """pla_k_trsv_ticket_multi: --k right-hand sides (at most 16) in one launch,

@@ -122,6 +122,54 @@ def test_single_launch_trsv(env, uplo, trans, diag, n):
     assert err <= 1e-4 * max(1.0, ref.abs().max().item())
 
 
+@pytest.mark.parametrize("uplo,trans,diag", [("L", "N", "U"), ("U", "N", "N"), ("L", "N", "N"),
+                                             ("L", "T", "N")])
+@pytest.mark.parametrize("n", [1, 100, 128, 1000, 3001, 8192])
+def test_single_launch_trsv_link_blocks(env, uplo, trans, diag, n):
+    """The solve with link blocks (G_i = op(A)(i, p) inv(D_p): the successor of a
+    block reads its y before the inverse-block product) against an FP64 solve,
+    in place, every triangle and transpose the preconditioner uses."""
+    s, torch, pla = env
+    lib = s.lib
+    g = torch.Generator(device="cuda").manual_seed(n + 7)
+    ld = (n + 31) // 32 * 32
+    M = torch.randn(n, ld, device="cuda", generator=g) * (0.5 / max(n, 1) ** 0.5)
+    M[:, :n] += 2.0 * torch.eye(n, device="cuda")
+    Acm = M[:, :n].t()
+    ldd = (n + 127) // 128 * 128
+    Dinv = torch.zeros(128, ldd, device="cuda")
+    G = torch.full((128, ldd), float("nan"), device="cuda")
+    b = torch.randn(n, device="cuda", generator=g)
+    x = b.clone()
+    status = torch.zeros(4, dtype=torch.int32, device="cuda")
+    c = ctypes.c_char
+    vp = ctypes.c_void_p
+    lg = ctypes.c_long
+    lib.pla_k_trsv_inv_blocks.argtypes = [ctypes.c_int, c, c, c, ctypes.c_int, vp, lg, vp, lg, vp]
+    lib.pla_k_trsv_link_blocks.argtypes = [c, c, ctypes.c_int, vp, lg, vp, lg, vp, vp]
+    lib.pla_k_trsv_ticket_link.argtypes = [c, c, ctypes.c_int, vp, lg, vp, lg, vp, vp, vp, vp, vp]
+    assert lib.pla_k_trsv_inv_blocks(pla.MPI_FLOAT, uplo.encode(), trans.encode(), diag.encode(),
+                                     n, M.data_ptr(), ld, Dinv.data_ptr(), ldd, None) == 0
+    assert lib.pla_k_trsv_link_blocks(uplo.encode(), trans.encode(), n, M.data_ptr(), ld,
+                                      Dinv.data_ptr(), ldd, G.data_ptr(), None) == 0
+    for _ in range(2):   # twice: the second solve reuses the flags and the y buffer
+        x.copy_(b)
+        assert lib.pla_k_trsv_ticket_link(uplo.encode(), trans.encode(), n, M.data_ptr(), ld,
+                                          Dinv.data_ptr(), ldd, G.data_ptr(), x.data_ptr(),
+                                          x.data_ptr(), status.data_ptr(), None) == 0
+        torch.cuda.synchronize()
+        assert status[0].item() == 0
+    T = torch.tril(Acm) if uplo == "L" else torch.triu(Acm)
+    if diag == "U":
+        T = T - torch.diag(torch.diag(T)) + torch.eye(n, device="cuda")
+    if trans == "T":
+        T = T.t()
+    ref = torch.linalg.solve_triangular(T.double(), b.double()[:, None],
+                                        upper=(uplo == "U") != (trans == "T"))[:, 0]
+    err = (x.double() - ref).abs().max().item()
+    assert err <= 1e-4 * max(1.0, ref.abs().max().item())
+
+
 def solve_mixed(s, pla, A, B, kind, prec, ref, nb=0):
     n = A.shape[0]
     a = s.matrix(n, n)
