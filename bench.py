@@ -57,7 +57,7 @@ TC_UPDATE_TRAFFIC_RATIO = 486.5 / 545.3
 PANEL_TRAFFIC_PER_STEP = None
 
 # PLA_B200_PREC_* codes as the JSON line names them
-PREC_NAMES = {1: "bf16", 2: "fp16", 3: "fp32", 4: "fp64", 5: "fp8", 6: "bf16x6"}
+PREC_NAMES = {1: "bf16", 2: "fp16", 3: "fp32", 4: "fp64", 5: "fp8", 6: "bf16x6", 7: "bf16x3"}
 
 
 def parse():
@@ -68,7 +68,8 @@ def parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--n", type=int, default=32768)
     p.add_argument("--kappa", type=float, default=1e6)
-    p.add_argument("--precision", choices=["fp16", "bf16", "bf16x6", "fp32"], default="fp16")
+    p.add_argument("--precision", choices=["fp16", "bf16", "bf16x3", "bf16x6", "fp32"],
+                   default="fp16")
     p.add_argument("--refinement", choices=["gmres", "lu"], default="gmres")
     p.add_argument("--nb", type=int, default=256, help="block size of the mixed factorization")
     p.add_argument("--panel-pivoting", choices=["tournament", "partial"], default="tournament",
@@ -354,13 +355,22 @@ def run_batched(torch, pla, lib, device, stream, dtype, steps, warmup, dist, cou
 def run_mixed_sweep(torch, pla, lib, s, device, stream, a, n, args, params):
     """The C3 configurations beside the headline one, each solved once after a
     warm-up solve: kappa 1e2 and 1e10 with one right-hand side (1e10 makes the
-    refinement escalate the factor precision), kappa 1e6 with 16 right-hand
-    sides, and the FP64 PLA_General_solve of the 16-rhs system.  Reports the
+    solver escalate the factor precision), kappa 1e6 with 16 right-hand sides
+    (with the headline's precision, and with bf16 x 3 factors, whose fewer
+    GMRES iterations pay off over many columns), and the FP64
+    PLA_General_solve of the 16-rhs system.  Reports the
     time, the precision that finished, iterations and the largest normwise
     backward error over the right-hand sides."""
     out = []
-    for kappa, nrhs, fp64 in ((1e2, 1, False), (1e10, 1, False), (1e6, 16, False),
-                              (1e6, 16, True)):
+    for kappa, nrhs, fp64, prec in ((1e2, 1, False, None), (1e10, 1, False, None),
+                                    (1e6, 16, False, None),
+                                    (1e6, 16, False, pla.PLA_B200_PREC_BF16X3),
+                                    (1e6, 16, True, None)):
+        prm = params
+        if prec is not None:
+            prm = pla.MixedParams()
+            ctypes.memmove(ctypes.byref(prm), ctypes.byref(params), ctypes.sizeof(prm))
+            prm.precision = prec
         T, x_true, _ = c3_device(n, kappa, 2000 + int(np.log10(kappa)), torch, device)
         g = torch.Generator(device=device).manual_seed(77)
         X = torch.randn(n, nrhs, dtype=torch.float64, device=device, generator=g)
@@ -379,7 +389,7 @@ def run_mixed_sweep(torch, pla, lib, s, device, stream, a, n, args, params):
             if fp64:
                 pla.check(lib.PLA_General_solve(a, piv, bo), "PLA_General_solve")
             else:
-                pla.check(lib.PLA_General_solve_mixed(a, bo, ctypes.byref(params),
+                pla.check(lib.PLA_General_solve_mixed(a, bo, ctypes.byref(prm),
                                                       ctypes.byref(rep)), "solve_mixed")
 
         solve()
@@ -397,8 +407,9 @@ def run_mixed_sweep(torch, pla, lib, s, device, stream, a, n, args, params):
         a_inf = T.abs().sum(dim=0).max().item()
         eta = (R.abs().amax(dim=0) / (a_inf * Xs.abs().amax(dim=0) + Bm.abs().amax(dim=0))).max().item()
         fwd = ((Xs[:, 0] - x_true[:, 0]).abs().max() / x_true.abs().max()).item()
+        pname = PREC_NAMES.get(prec) if prec is not None else args.precision
         entry = {"kappa": kappa, "nrhs": nrhs, "solver": "PLA_General_solve (FP64)" if fp64 else
-                 f"PLA_General_solve_mixed ({args.precision}, {args.refinement.upper()}-IR)",
+                 f"PLA_General_solve_mixed ({pname}, {args.refinement.upper()}-IR)",
                  "solve_s": t, "backward_error_max": eta, "forward_error_rhs0": fwd}
         if not fp64:
             entry.update({"precision_used": PREC_NAMES.get(rep.precision_used),
@@ -584,7 +595,8 @@ def run_ours(args):
     check(lib.PLA_Obj_set_local_contents_device(ctypes.c_void_p(T.data_ptr()), n, a), "fill A")
 
     prec = {"fp16": pla.PLA_B200_PREC_FP16, "bf16": pla.PLA_B200_PREC_BF16,
-            "bf16x6": pla.PLA_B200_PREC_BF16X6, "fp32": pla.PLA_B200_PREC_FP32}[args.precision]
+            "bf16x6": pla.PLA_B200_PREC_BF16X6, "bf16x3": pla.PLA_B200_PREC_BF16X3,
+            "fp32": pla.PLA_B200_PREC_FP32}[args.precision]
     params = pla.MixedParams()
     lib.PLA_Mixed_params_default(ctypes.byref(params))
     params.precision = prec

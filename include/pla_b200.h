@@ -81,6 +81,10 @@ long PLA_B200_kernel_launches(void);
                                     p1 + p2) and six of the nine part products
                                     summed in fp32: fp32-level factors at about
                                     six times the bf16 tensor work */
+#define PLA_B200_PREC_BF16X3 7   /* the same split, two ways (x = p0 + p1, about 16
+                                    significant bits) and three part products: the
+                                    trailing update and U12 at three times the bf16
+                                    tensor work, factors about 2^-16 accurate */
 #define PLA_B200_IR_LU       1   /* classic iterative refinement             */
 #define PLA_B200_IR_GMRES    2   /* GMRES-IR                                 */
 /* pivoting of the low-precision LU's fp32 panels (the FP64 PLA_LU always uses
@@ -102,8 +106,8 @@ typedef struct {
                            the backward error; a non-finite iterate;
                            max_iterations reached) or the low-precision
                            Cholesky breaks down, refactor one precision higher
-                           (FP8 -> BF16 -> BF16X6 -> FP64; FP16 -> BF16X6 ->
-                           FP64; FP32 -> FP64) and continue from the current
+                           (FP8 -> BF16 -> BF16X6 -> FP64; FP16, BF16X3 ->
+                           BF16X6 -> FP64; FP32 -> FP64) and continue from the current
                            iterate.  Right after a low-precision factorization,
                            a diagonal range of its factors (max / min |u_ii|,
                            squared for a Cholesky factor) above 1e4 over the

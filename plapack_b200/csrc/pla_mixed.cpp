@@ -251,11 +251,12 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
   const bool lowp = F.prec != PLA_B200_PREC_FP32;
   const bool f8 = F.prec == PLA_B200_PREC_FP8;
   // bf16 x 6: each operand of the update split three ways into bf16, six
-  // K-wide segments per packed row, one K = 6b product of fp32 accuracy
-  const bool x6 = F.prec == PLA_B200_PREC_BF16X6;
-  const int nseg = x6 ? 6 : 1;
+  // K-wide segments per packed row, one K = 6b product of fp32 accuracy;
+  // bf16 x 3: split two ways, three segments, K = 3b
+  const bool x6 = F.prec == PLA_B200_PREC_BF16X6, x3 = F.prec == PLA_B200_PREC_BF16X3;
+  const int nseg = x6 ? 6 : x3 ? 3 : 1;
   const int kprec =
-      F.prec == PLA_B200_PREC_BF16 || x6 ? PLA_K_BF16 : PLA_K_FP16;
+      F.prec == PLA_B200_PREC_BF16 || x6 || x3 ? PLA_K_BF16 : PLA_K_FP16;
   const int kmult = f8 ? 128 : 64;  // K granularity of the tensor-core update
   const long ku = (long)nseg * nb;  // elements per packed operand row
   void *Lp = nullptr, *Up = nullptr;
@@ -290,7 +291,7 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
   // fp32 factorization keeps the fp32 solve)
   const bool split = F.kind == 0 && lowp && nb % 64 == 0 && nb <= 256;
   SplitU12 S;
-  if (split) PK(split_alloc(S, n, nb, x6 ? 6 : 3));
+  if (split) PK(split_alloc(S, n, nb, x6 ? 6 : 3));  // bf16 x 3 below fp32-level factors
   int ready = -1;
   for (int k = 0; k < n; k += nb) {
     const int b = std::min(nb, n - k), rest = n - k - b, k2 = k + b;
@@ -341,15 +342,14 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
             Uop = (const char *)Up;
             su = inv_u;
           }
-        } else if (x6) {
+        } else if (x6 || x3) {
           // A operand: L; B operand: U' (LU) or L again (Cholesky)
-          K(pla_k_pack_split_ex(rest, b, at(k + b, k), 1, ld, Lp, ku, 6, kSplitA6, 0, stream()));
+          const unsigned ca = x6 ? kSplitA6 : kSplitA3, cb = x6 ? kSplitB6 : kSplitB3;
+          K(pla_k_pack_split_ex(rest, b, at(k + b, k), 1, ld, Lp, ku, nseg, ca, 0, stream()));
           if (F.kind == 0)
-            K(pla_k_pack_split_ex(rest, b, at(k, k + b), ld, 1, Up, ku, 6, kSplitB6, 0,
-                                  stream()));
+            K(pla_k_pack_split_ex(rest, b, at(k, k + b), ld, 1, Up, ku, nseg, cb, 0, stream()));
           else
-            K(pla_k_pack_split_ex(rest, b, at(k + b, k), 1, ld, Up, ku, 6, kSplitB6, 0,
-                                  stream()));
+            K(pla_k_pack_split_ex(rest, b, at(k + b, k), 1, ld, Up, ku, nseg, cb, 0, stream()));
           Uop = (const char *)Up;
         } else {
           K(pla_k_pack_rows(kprec, rest, b, at(k + b, k), ld, Lp, nb, stream()));
@@ -958,7 +958,8 @@ int escalated(int prec) {
   switch (prec) {
     case PLA_B200_PREC_FP8: return PLA_B200_PREC_BF16;
     case PLA_B200_PREC_BF16:
-    case PLA_B200_PREC_FP16: return PLA_B200_PREC_BF16X6;
+    case PLA_B200_PREC_FP16:
+    case PLA_B200_PREC_BF16X3: return PLA_B200_PREC_BF16X6;
     case PLA_B200_PREC_BF16X6:
     case PLA_B200_PREC_FP32: return PLA_B200_PREC_FP64;
     default: return 0;
@@ -971,6 +972,7 @@ double unit_roundoff(int prec) {
     case PLA_B200_PREC_FP8: return std::ldexp(1.0, -4);
     case PLA_B200_PREC_BF16: return std::ldexp(1.0, -8);
     case PLA_B200_PREC_FP16: return std::ldexp(1.0, -11);
+    case PLA_B200_PREC_BF16X3: return std::ldexp(1.0, -16);
     case PLA_B200_PREC_BF16X6:
     case PLA_B200_PREC_FP32: return std::ldexp(1.0, -24);
     default: return std::ldexp(1.0, -53);
@@ -997,7 +999,7 @@ int solve_mixed(int kind, PLA_Obj A, PLA_Obj B, const PLA_Mixed_params *pin,
   if (pin) p = *pin;
   if (p.max_iterations <= 0) p.max_iterations = 50;
   if (p.gmres_restart <= 0) p.gmres_restart = 30;
-  if (p.precision < PLA_B200_PREC_BF16 || p.precision > PLA_B200_PREC_BF16X6)
+  if (p.precision < PLA_B200_PREC_BF16 || p.precision > PLA_B200_PREC_BF16X3)
     PLA_FAIL("unknown precision");
   if (p.panel_pivoting != PLA_B200_PIVOT_PARTIAL && p.panel_pivoting != PLA_B200_PIVOT_TOURNAMENT)
     PLA_FAIL("unknown panel pivoting");

@@ -37,6 +37,7 @@ PLA_ERROR = -1000
 PLA_B200_PREC_BF16, PLA_B200_PREC_FP16, PLA_B200_PREC_FP32, PLA_B200_PREC_FP64 = 1, 2, 3, 4
 PLA_B200_PREC_FP8 = 5
 PLA_B200_PREC_BF16X6 = 6
+PLA_B200_PREC_BF16X3 = 7
 PLA_B200_IR_LU, PLA_B200_IR_GMRES = 1, 2
 PLA_B200_PIVOT_PARTIAL, PLA_B200_PIVOT_TOURNAMENT = 0, 1
 

@@ -356,6 +356,24 @@ def test_bf16x6_factors(env):
     assert backward_error(A, X, B) <= n * 2.0 ** -53
 
 
+@pytest.mark.parametrize("kind", ["lu", "chol"])
+def test_bf16x3_factors(env, kind):
+    """bf16 x 3 factors (operands split two ways, three part products): FP64
+    backward error with fewer GMRES iterations than fp16 factors need."""
+    s, torch, pla = env
+    n = 3000
+    A = c3_matrix(n, 1e6, 23) if kind == "lu" else spd_family(n, 1e5, 24)
+    B = np.asfortranarray(A @ np.random.default_rng(24).standard_normal((n, 2)))
+    its = {}
+    for prec in (pla.PLA_B200_PREC_FP16, pla.PLA_B200_PREC_BF16X3):
+        rc, X, rep = solve_mixed_params(s, pla, A, B, kind, precision=prec, refinement=2)
+        assert rc == 0 and rep.converged == 1, (prec, rep.iterations, rep.backward_error)
+        assert rep.precision_used == prec and rep.factorizations == 1
+        assert backward_error(A, X, B) <= n * 2.0 ** -53
+        its[prec] = rep.inner_iterations
+    assert its[pla.PLA_B200_PREC_BF16X3] < its[pla.PLA_B200_PREC_FP16], its
+
+
 @pytest.mark.parametrize("kappa", [1e3, 1e7])
 def test_bf16x6_cholesky(env, kappa):
     s, torch, pla = env
