@@ -374,6 +374,11 @@ int factor_mixed(Factor &F, const double *A, long lda, int nb) {
         return r;
       };
       const int b2 = std::min(nb, rest);
+      // The next panel's columns must end on a 128-column tile boundary: the
+      // update walks whole 128 x 128 tiles, so a partial last tile would also
+      // fold its product into the columns the second launch updates (and
+      // fp8's U' scales are per 128 rows).  nb = 192 with the split that
+      // allows measured slower anyway (factorization 167 against 154 ms).
       if (la && b2 % 128 == 0 && rest > b2) {
         K(upd(k2, b2, 0));  // the next panel's columns first
         PLA_CUDA(cudaEventRecord(ev_next, s0));
