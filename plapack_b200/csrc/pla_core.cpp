@@ -102,6 +102,16 @@ cudaStream_t copy_stream() {
   return s.copy_stream;
 }
 
+cudaStream_t replay_stream() {
+  State &s = state();
+  if (!s.replay_stream) {
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    cudaStreamCreateWithPriority(&s.replay_stream, cudaStreamNonBlocking, lo);
+  }
+  return s.replay_stream;
+}
+
 cudaEvent_t lookahead_event(int i) {
   State &s = state();
   if (!s.la_events[i]) cudaEventCreateWithFlags(&s.la_events[i], cudaEventDisableTiming);
@@ -416,7 +426,7 @@ int PLA_Finalize(void) {
   release_ooc();
   release_interchange_counter();
   pla_kernels_release();
-  for (cudaStream_t *st : {&s.la_stream, &s.copy_stream})
+  for (cudaStream_t *st : {&s.la_stream, &s.copy_stream, &s.replay_stream})
     if (*st) {
       cudaStreamSynchronize(*st);
       cudaStreamDestroy(*st);

@@ -70,6 +70,7 @@ struct State {
   cudaStream_t override_stream = nullptr;  // set by OnStream while a scope queues elsewhere
   cudaStream_t la_stream = nullptr;        // high-priority stream of the lookahead panels
   cudaStream_t copy_stream = nullptr;      // host-to-device copies of a streamed solve
+  cudaStream_t replay_stream = nullptr;    // a streamed solve's catch-up of arrived columns
   cudaEvent_t la_events[2] = {nullptr, nullptr};
   int phase_timing = 0;
   PLA_Phase_times phases{};
@@ -100,6 +101,7 @@ int lookahead_ctas(int dt);
 cudaStream_t lookahead_stream();
 cudaEvent_t lookahead_event(int i);
 cudaStream_t copy_stream();
+cudaStream_t replay_stream();
 // while alive, stream() returns `s` (host code is sequential, so the switch
 // only affects the calls made inside the scope)
 struct OnStream {

@@ -56,7 +56,7 @@ namespace {
 enum Slots { kSlotA32 = 4, kSlotL = 5, kSlotU = 6, kSlotPiv = 7, kSlotVec = 8, kSlotWork = 9,
              kSlotV = 10, kSlotSt = 11, kSlotA64 = 16, kSlotScales = 18, kSlotDiag = 19,
              kSlotLbig = 24, kSlotDinvSteps = 25, kSlotSclSteps = 26, kSlotTmp = 27,
-             kSlotSplitL = 31, kSlotSplitU = 32 };
+             kSlotSplitL = 31, kSlotSplitU = 32, kSlotUr = 33, kSlotSplitUr = 34 };
 
 long round_up(long v, long m) { return (v + m - 1) / m * m; }
 
@@ -776,16 +776,20 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
   }
   char *Lbig = (char *)scratch(kSlotLbig, lbytes + 256);
   float *dinv = (float *)scratch(kSlotDinvSteps, (size_t)nsteps * nb * nb * sizeof(float));
-  float *scl = (float *)scratch(kSlotSclSteps, ((size_t)nsteps + 1) * tiles * sizeof(float));
+  float *scl = (float *)scratch(kSlotSclSteps, ((size_t)nsteps + 2) * tiles * sizeof(float));
   void *Ub = scratch(kSlotU, (size_t)n * nb * 2 + 256);
+  void *Ub_r = scratch(kSlotUr, (size_t)n * nb * 2 + 256);  // the replay stream's U'
+  __nv_bfloat16 *usplit_r =
+      (__nv_bfloat16 *)scratch(kSlotSplitUr, (size_t)n * 3 * nb * 2 + 256);
   // per step: the split of inv(L11) for the tensor-core U12 solves (replays
   // of late column groups use old steps' splits)
   __nv_bfloat16 *lsplit =
       (__nv_bfloat16 *)scratch(kSlotSplitL, (size_t)nsteps * nb * 3 * nb * 2 + 256);
   __nv_bfloat16 *usplit = (__nv_bfloat16 *)scratch(kSlotSplitU, (size_t)n * 3 * nb * 2 + 256);
-  if (!Lbig || !dinv || !scl || !Ub || !lsplit || !usplit)
+  if (!Lbig || !dinv || !scl || !Ub || !lsplit || !usplit || !Ub_r || !usplit_r)
     PLA_FAIL("cannot allocate the streamed-solve buffers");
   float *inv_u = scl + (size_t)nsteps * tiles;  // the U' scales of the launch in flight
+  float *inv_u_r = inv_u + tiles;               // ... of the replay stream's
   int *st = F.status;
   PLA_Phase_times &ph = state().phases;
   cudaStream_t s0 = stream(), s1 = lookahead_stream(), sc = copy_stream();
@@ -796,16 +800,20 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   }
   const int side_ctas = std::max(1, sms - lookahead_ctas(MPI_FLOAT));
-  std::vector<cudaEvent_t> arr(ngroups), thr(4);
+  std::vector<cudaEvent_t> arr(ngroups), thr(4), rep(ngroups + 1);
   for (auto &e : arr) PLA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   for (auto &e : thr) PLA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  for (auto &e : rep) PLA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   struct Events {  // destroyed on every return path
-    std::vector<cudaEvent_t> *a, *b;
+    std::vector<cudaEvent_t> *a, *b, *c;
     ~Events() {
       for (auto e : *a) cudaEventDestroy(e);
       for (auto e : *b) cudaEventDestroy(e);
+      for (auto e : *c) cudaEventDestroy(e);
     }
-  } guard{&arr, &thr};
+  } guard{&arr, &thr, &rep};
+  cudaEvent_t ev_post0 = rep[ngroups];  // step 0's panel and its packed L, on s0
+  cudaStream_t sr = replay_stream();
   cudaEvent_t ev_next = lookahead_event(0), ev_panel = lookahead_event(1);
 
   // 1. the copies and conversions, group by group, on the copy stream
@@ -849,8 +857,9 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
       K(pla_k_pack_rows(kprec, rest, b, at(k0 + b, k0), ld, Lbig + loff[s], nb, stream()));
     return 0;
   };
-  // step s on columns [c0, c1): interchanges, U rows, packed U'
-  auto prep = [&](int s, int c0, int c1) -> int {
+  // step s on columns [c0, c1): interchanges, U rows, packed U' (into ub,
+  // with the split operand us and the fp8 scales iu of the stream it runs on)
+  auto prep = [&](int s, int c0, int c1, void *ub, __nv_bfloat16 *us, float *iu) -> int {
     const int k0 = s * nb, b = std::min(nb, n - k0), nc = c1 - c0;
     if (nc <= 0) return 0;
     {
@@ -861,31 +870,60 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
       // U rows := inv(L11) block on the tensor cores, bf16 hi/lo split (see
       // split_solve): the block is split and cleared, then accumulated into
       PhaseTimer t(&ph.trsm_ms);
-      K(pla_k_pack_split(nc, b, at(k0, c0), ld, 1, usplit, 3L * b, 0b010, 1, stream()));
+      K(pla_k_pack_split(nc, b, at(k0, c0), ld, 1, us, 3L * b, 0b010, 1, stream()));
       K(pla_k_tc_update_ex(PLA_K_BF16, b, nc, 3 * b, 1.0f, lsplit + (size_t)s * nb * 3 * nb,
-                           3L * b, b, usplit, 3L * b, nc, F.a, ld, ld, n, k0, c0, 0, 0, &st[0],
+                           3L * b, b, us, 3L * b, nc, F.a, ld, ld, n, k0, c0, 0, 0, &st[0],
                            stream()));
     }
     if (n - k0 - b <= 0) return 0;
     PhaseTimer t(&ph.convert_ms);
-    if (f8) K(pla_k_pack_fp8(nc, b, at(k0, c0), ld, 1, Ub, nb, inv_u, stream()));
-    else K(pla_k_convert(MPI_FLOAT, at(k0, c0), ld, kprec, Ub, nb, b, nc, stream()));
+    if (f8) K(pla_k_pack_fp8(nc, b, at(k0, c0), ld, 1, ub, nb, iu, stream()));
+    else K(pla_k_convert(MPI_FLOAT, at(k0, c0), ld, kprec, ub, nb, b, nc, stream()));
     return 0;
   };
-  // step s's update of columns [c0, c1), whose U' was packed from column p0
-  auto upd = [&](int s, int c0, int c1, int p0, int cap) -> int {
+  // step s's update of columns [c0, c1), whose U' (in ub, fp8 scales iu) was
+  // packed from column p0
+  auto upd = [&](int s, int c0, int c1, int p0, int cap, void *ub, float *iu) -> int {
     const int k0 = s * nb, b = std::min(nb, n - k0), rest = n - k0 - b, nc = c1 - c0;
     if (nc <= 0 || rest <= 0) return 0;
     const long off = c0 - p0;  // columns of U' skipped (a multiple of 128)
     PhaseTimer t(&ph.update_ms);
     K(f8 ? pla_k_tc_update_fp8_ex(rest, nc, b, -1.0f, Lbig + loff[s], nb, rest,
-                                  scl + (size_t)s * tiles, (char *)Ub + off * nb * esz, nb, nc,
-                                  inv_u + off / 128, F.a, ld, ld, n, k0 + b, c0, 0, cap, &st[0],
+                                  scl + (size_t)s * tiles, (char *)ub + off * nb * esz, nb, nc,
+                                  iu + off / 128, F.a, ld, ld, n, k0 + b, c0, 0, cap, &st[0],
                                   stream())
          : pla_k_tc_update_ex(kprec, rest, nc, b, -1.0f, Lbig + loff[s], nb, rest,
-                              (char *)Ub + off * nb * esz, nb, nc, F.a, ld, ld, n, k0 + b, c0, 0,
+                              (char *)ub + off * nb * esz, nb, nc, F.a, ld, ld, n, k0 + b, c0, 0,
                               cap, &st[0], stream()));
     if (t.on) ph.update_launches++;
+    return 0;
+  };
+  // Group g's catch-up on the replay stream: the steps [applied[g], upto) it
+  // missed, once it has arrived and those steps' panels are packed.  It runs
+  // beside the panel chain and the main update (they work on other
+  // columns), from the group's arrival on, so that when the chain reaches the
+  // group only the steps since the last call remain.  Every column receives
+  // the operations of the in-HBM factorization, in its order.
+  std::vector<int> applied(ngroups, 0);  // steps already applied to each group
+  std::vector<char> started(ngroups, 0);
+  auto replay = [&](int g, int upto) -> int {
+    OnStream on(sr);
+    if (!started[g]) {
+      PLA_CUDA(cudaStreamWaitEvent(sr, arr[g], 0));
+      PLA_CUDA(cudaStreamWaitEvent(sr, ev_post0, 0));
+      started[g] = 1;
+    }
+    if (applied[g] < upto) {
+      // the panels of steps < upto (upto - 1 <= the chain's step) and their L
+      if (upto > 1) PLA_CUDA(cudaStreamWaitEvent(sr, ev_panel, 0));
+      for (int s2 = applied[g]; s2 < upto; s2++) {
+        const int c0 = std::max(gb[g], (s2 + 1) * nb);
+        PK(prep(s2, c0, gb[g + 1], Ub_r, usplit_r, inv_u_r));
+        PK(upd(s2, c0, gb[g + 1], c0, side_ctas, Ub_r, inv_u_r));
+      }
+      applied[g] = upto;
+    }
+    PLA_CUDA(cudaEventRecord(rep[g], sr));
     return 0;
   };
 
@@ -897,7 +935,8 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
                F.pivoting));
   }
   PK(post_panel(0));
-  std::vector<int> applied(ngroups, 0);  // steps already applied to each group
+  PLA_CUDA(cudaEventRecord(ev_post0, s0));
+  int arrived = known;  // groups [known, arrived) have arrived and catch up on sr
   for (int k = 0; k < nsteps; k++) {
     const int k0 = k * nb, b = std::min(nb, n - k0), rest = n - k0 - b;
     if (k > 0) PLA_CUDA(cudaStreamWaitEvent(s0, ev_panel, 0));
@@ -906,23 +945,23 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
     const int upto = (int)std::min<long>(n, (long)(k + 2) * nb);
     int need = 0;
     while (gb[need] < upto) need++;
-    const int was = known;
-    PK(poll(need));
-    for (int g = was; g < known; g++) {  // replay the steps a new group missed
-      const int g0 = gb[g], g1 = gb[g + 1];
-      for (int s2 = applied[g]; s2 < k; s2++) {
-        const int c0 = std::max(g0, (s2 + 1) * nb);
-        PK(prep(s2, c0, g1));
-        PK(upd(s2, c0, g1, c0, 0));
-      }
-      applied[g] = k;
+    // the groups that have arrived catch up (through step k - 1) on sr; the
+    // needed ones then join the main update, which takes them from step k on
+    while (arrived < ngroups) {
+      cudaError_t q = cudaEventQuery(arr[arrived]);
+      cudaGetLastError();  // a "not ready" answer is not an error
+      if (q != cudaSuccess) break;
+      arrived++;
     }
+    for (int g = known; g < std::max(arrived, need); g++) PK(replay(g, k));
+    for (; known < need; known++) PLA_CUDA(cudaStreamWaitEvent(s0, rep[known], 0));
+    arrived = std::max(arrived, known);
     const int kc = gb[known];  // columns that take part
     if (rest > 0) {
-      PK(prep(k, k0 + b, kc));
+      PK(prep(k, k0 + b, kc, Ub, usplit, inv_u));
       const int b2 = std::min(nb, rest);
       if (k + 1 < nsteps) {
-        PK(upd(k, k0 + b, k0 + b + b2, k0 + b, 0));  // the next panel's columns first
+        PK(upd(k, k0 + b, k0 + b + b2, k0 + b, 0, Ub, inv_u));  // the next panel's columns first
         PLA_CUDA(cudaEventRecord(ev_next, s0));
         PLA_CUDA(cudaStreamWaitEvent(s1, ev_next, 0));
         {
@@ -935,13 +974,18 @@ int factor_mixed_streamed(Factor &F, const double *Ah, long ldh, double *Ad, lon
           PK(post_panel(k + 1));
         }
         PLA_CUDA(cudaEventRecord(ev_panel, s1));
-        PK(upd(k, k0 + b + b2, kc, k0 + b, side_ctas));
+        PK(upd(k, k0 + b + b2, kc, k0 + b, side_ctas, Ub, inv_u));
       }
     }
     for (int g = 0; g < known; g++) applied[g] = k + 1;
     PLA_CUDA(cudaEventRecord(thr[k % 4], s0));
   }
-  PK(poll(ngroups));  // the refinement reads all of A
+  // every group has joined (the last step needs them all); the refinement
+  // reads all of A
+  for (; known < ngroups; known++) {
+    PK(replay(known, nsteps));
+    PLA_CUDA(cudaStreamWaitEvent(s0, rep[known], 0));
+  }
   // 3. the interchanges of every step on the columns to its left
   for (int k = 1; k < nsteps; k++) {
     const int k0 = k * nb, b = std::min(nb, n - k0);
