@@ -693,7 +693,8 @@ def run_ours(args):
           "swap": ph.swap_ms / args.steps, "refine": report.refine_ms}
     kernels = {
         "panel": "tslu_select_k + tslu_apply_k (tournament-pivoted fp32 sub-panels), laswp_k, "
-                 "trsm_left_k, sgemm_k (updates inside the panel); on the lookahead stream",
+                 "panel_update_k (U12 solve + rank-32 update inside the panel); on the "
+                 "lookahead stream",
         "update": "tc_update_k (tcgen05 fp16 trailing update, TMA reduce-add into fp32)",
         "trsm": "trsm_left_k / sgemm_k (U12 = inv(L11) A12)",
         "convert": "pack_rows_k, convert_k (fp32 -> fp16 operand packs)",

@@ -30,6 +30,9 @@
 // in registers, shifted one column left per step so every index is static.
 #include <climits>
 #include <cstdint>
+#include <mutex>
+#include <utility>
+#include <vector>
 
 #include "pla_internal.h"
 #include "pla_kernels.h"
@@ -401,6 +404,94 @@ tslu_apply_k(float *__restrict__ A, long lda, int r, int w, const float *__restr
   }
 }
 
+// The rest of a sub-panel's step inside the panel, after its interchanges:
+// U12 = inv(L11) A12 and A22 -= L21 U12, in one launch.  P is the sub-panel's
+// top-left corner (m rows, w <= 32 columns, then ncols more columns of the
+// panel to its right).  CTA (x, y) takes rows x kPU + w .. of the kPG columns
+// of group y.  It stages the group's A12 and L11 in shared memory (coalesced
+// loads), forms the group's U12 there (forward substitution, a column per
+// thread, u_j -= L(j, k) u_k for k = 0 .. j-1 in order), then each thread
+// updates one row of the group (a_c -= l_k U12(k, c) for k = 0 .. w-1 in
+// order, U12 read back by columns in 16-byte pieces).  A12 is only read; the
+// last CTA of a group to finish (an atomic counter per group, no CTA waits)
+// writes the group's U12 over it.  W32 compiles the common w = 32.
+constexpr int kPU = 256;  // threads (rows) of a panel_update_k CTA
+constexpr int kPG = 16;   // columns of a panel_update_k group
+
+template <bool W32>
+__global__ void __launch_bounds__(kPU)
+panel_update_k(int m, int w_, int ncols, float *__restrict__ P, long lda, unsigned *counters) {
+  const int w = W32 ? kW : w_;
+  __shared__ __align__(16) float ut[kPG][kW];  // the group's U12, by columns
+  __shared__ float a12[kPG][kW + 1];
+  __shared__ float l11[kW][kW + 1];
+  __shared__ int s_last;
+  const int tid = threadIdx.x;
+  const int c0 = blockIdx.y * kPG, nc = min(kPG, ncols - c0);
+  float *A12 = P + (long)(w + c0) * lda;
+  for (int e = tid; e < kW * kW; e += kPU) {
+    const int j = e % kW, k = e / kW;
+    l11[j][k] = k < j && j < w ? P[j + (long)k * lda] : 0.f;
+  }
+  for (int e = tid; e < kPG * kW; e += kPU) {
+    const int j = e % kW, c = e / kW;
+    a12[c][j] = j < w && c < nc ? A12[j + (long)c * lda] : 0.f;
+  }
+  __syncthreads();
+  if (tid < kPG) {
+    float u[kW];
+#pragma unroll
+    for (int j = 0; j < kW; j++) u[j] = a12[tid][j];
+#pragma unroll
+    for (int k = 0; k < kW - 1; k++) {
+      asm volatile("" ::: "memory");  // one column step's L11 loads at a time
+#pragma unroll
+      for (int j = k + 1; j < kW; j++) u[j] = fmaf(-l11[j][k], u[k], u[j]);
+    }
+#pragma unroll
+    for (int q = 0; q < kW / 4; q++)
+      *reinterpret_cast<float4 *>(&ut[tid][4 * q]) =
+          make_float4(u[4 * q], u[4 * q + 1], u[4 * q + 2], u[4 * q + 3]);
+  }
+  __syncthreads();
+  const long i = (long)blockIdx.x * kPU + tid + w;
+  if (i < m) {
+    float l[kW], a[kPG];
+#pragma unroll
+    for (int k = 0; k < kW; k++) l[k] = k < w ? P[i + (long)k * lda] : 0.f;
+#pragma unroll
+    for (int c = 0; c < kPG; c++) a[c] = c < nc ? A12[i + (long)c * lda] : 0.f;
+#pragma unroll
+    for (int c = 0; c < kPG; c++) {
+#pragma unroll
+      for (int q = 0; q < kW / 4; q++) {
+        const float4 f = *reinterpret_cast<const float4 *>(&ut[c][4 * q]);
+        if (W32 || 4 * q < w) a[c] = fmaf(-l[4 * q], f.x, a[c]);
+        if (W32 || 4 * q + 1 < w) a[c] = fmaf(-l[4 * q + 1], f.y, a[c]);
+        if (W32 || 4 * q + 2 < w) a[c] = fmaf(-l[4 * q + 2], f.z, a[c]);
+        if (W32 || 4 * q + 3 < w) a[c] = fmaf(-l[4 * q + 3], f.w, a[c]);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < kPG; c++)
+      if (c < nc) A12[i + (long)c * lda] = a[c];
+  }
+  // the group's last CTA writes its U12 (every CTA of the group has read A12
+  // before it counts)
+  __syncthreads();
+  if (tid == 0) {
+    const unsigned prev = atomicAdd(&counters[blockIdx.y], 1u);
+    s_last = prev == gridDim.x - 1;
+    if (s_last) counters[blockIdx.y] = 0;  // ready for the next launch
+  }
+  __syncthreads();
+  if (s_last)
+    for (int e = tid; e < w * nc; e += kPU) {
+      const int k = e % w, c = e / w;
+      A12[k + (long)c * lda] = ut[c][k];
+    }
+}
+
 struct Ws {
   void *ptr = nullptr;
   size_t bytes = 0;
@@ -476,6 +567,38 @@ extern "C" int pla_k_lu_panel_tslu(int r, int w, float *A, long lda, int *piv, i
   if (Pa > 2 * g_tsms) Pa = 2 * g_tsms;
   tslu_apply_k<<<Pa, kThreads, 0, s>>>(A, lda, r, w, lu11, uinv, stage, disp);
   pla_k_count(2);
+  return (int)cudaGetLastError();
+}
+
+// U12 = inv(L11) A12 and A22 -= L21 U12 for the m x w sub-panel at P (w <= 32)
+// and the ncols columns right of it (ncols <= PLA_K_PANEL_UPDATE_MAX), one
+// launch.  Each stream has its own group counters (launches on one stream run
+// in order; launches on different streams may overlap).
+extern "C" int pla_k_panel_update(int m, int w, int ncols, float *P, long lda, cudaStream_t s) {
+  if (m <= 0 || w <= 0 || ncols <= 0) return 0;
+  if (w > kW || w > m || ncols > PLA_K_PANEL_UPDATE_MAX) return (int)cudaErrorInvalidValue;
+  constexpr int kGroups = (PLA_K_PANEL_UPDATE_MAX + kPG - 1) / kPG;
+  static std::mutex mu;
+  static std::vector<std::pair<cudaStream_t, unsigned *>> table;
+  unsigned *counters = nullptr;
+  {
+    std::lock_guard<std::mutex> g(mu);
+    for (auto &pr : table)
+      if (pr.first == s) counters = pr.second;
+    if (!counters) {
+      cudaError_t e = cudaMalloc(&counters, kGroups * sizeof(unsigned));
+      if (e != cudaSuccess) return (int)e;
+      e = cudaMemsetAsync(counters, 0, kGroups * sizeof(unsigned), s);  // before the first launch
+      if (e != cudaSuccess) return (int)e;
+      table.emplace_back(s, counters);
+    }
+  }
+  dim3 grid(std::max(1, (m - w + kPU - 1) / kPU), (ncols + kPG - 1) / kPG);
+  if (w == kW)
+    panel_update_k<true><<<grid, kPU, 0, s>>>(m, w, ncols, P, lda, counters);
+  else
+    panel_update_k<false><<<grid, kPU, 0, s>>>(m, w, ncols, P, lda, counters);
+  pla_k_count(1);
   return (int)cudaGetLastError();
 }
 

@@ -52,6 +52,10 @@ int pla_k_lu_panel(int dt, int r, int w, void *A, long lda, int *piv, int *statu
 int pla_k_lu_panel_tslu(int r, int w, float *A, long lda, int *piv, int *zero_info,
                         int row_base, int max_ctas, cudaStream_t s);
 void pla_tslu_release(void);
+/* U12 = inv(L11) A12 and A22 -= L21 U12 for the m x w fp32 sub-panel at P (w <= 32,
+ * unit-lower L11 at its top) and the ncols columns right of it, one launch */
+#define PLA_K_PANEL_UPDATE_MAX 480
+int pla_k_panel_update(int m, int w, int ncols, float *P, long lda, cudaStream_t s);
 /* the mixed / FP64 LU's blocked r x b panel factorization (32-column
  * sub-panels, pivoting PLA_B200_PIVOT_*) on stream s (0: the library stream) */
 int pla_k_panel_lu_blocked(int dt, int r, int b, void *P, long lda, int *piv, int *zero_info,

@@ -149,8 +149,9 @@ namespace pla {
 // cooperative kernel on sub-panels of kSub columns, whose rows stay in shared
 // memory; after each sub-panel its pivots are applied to the panel's other
 // columns and the columns to its right get the unit-lower solve and the
-// rank-kSub update.  Pivot choices are those of the column-by-column loop;
-// only the rounding order of the panel's trailing columns differs.  (Tournament
+// rank-kSub update (for fp32 both in one launch, pla_k_panel_update).  Pivot
+// choices are those of the column-by-column loop; only the rounding order of
+// the panel's trailing columns differs.  (Tournament
 // pivoting of the sub-panels with their interchanges and U12 solve done in
 // the tournament kernels themselves, two launches fewer per sub-panel, was
 // measured slower inside the solve: 233 against 225 ms at n = 32768, that
@@ -178,6 +179,11 @@ int panel_lu(int dt, int r, int b, char *P, long lda, int *piv, int *status, int
     e = pla_k_laswp(dt, at(s, 0), lda, sb, piv + s, 0, s, s + sb, b, stream());
     if (e) return e;
     if (rest <= 0) continue;
+    if (dt == MPI_FLOAT && rest <= PLA_K_PANEL_UPDATE_MAX) {  // U12 solve and update, one launch
+      e = pla_k_panel_update(r - s, sb, rest, (float *)at(s, s), lda, stream());
+      if (e) return e;
+      continue;
+    }
     e = pla_k_trsm_small(dt, 'L', 'L', 'N', 'U', sb, rest, 1.0, at(s, s), lda, at(s, s + sb), lda,
                          status, stream());
     if (e) return e;

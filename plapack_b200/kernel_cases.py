@@ -16,6 +16,7 @@ bytes or flops and the rate they imply.
     python -m plapack_b200.kernel_cases trsm_small --side R --m 32768 --k 128 --dtype f64
     python -m plapack_b200.kernel_cases sgemm --m 32768 --n 224 --k 32
     python -m plapack_b200.kernel_cases panel_blocked --m 32768 --n 256 --ctas 72
+    python -m plapack_b200.kernel_cases panel_update --m 32768 --n 224 --k 32
     python -m plapack_b200.kernel_cases trtri --m 32768 --k 256
 
 The cases mirror the calls the solvers make (the trailing update of one LU
@@ -414,6 +415,26 @@ def case_sgemm(torch, lib, a):
     byt = 4.0 * (2.0 * m * n + m * k + k * n)
     return {"case": f"fp32 update C -= A B, {m} x {n} x {k}", "s": t,
             "tflops": flops / t / 1e12, "algorithmic_bytes": byt, "gbs": byt / t / 1e9}
+
+
+def case_panel_update(torch, lib, a):
+    """pla_k_panel_update as the fp32 panel calls it after a sub-panel's
+    interchanges: U12 = inv(L11) A12 and A22 -= L21 U12 for the --m x --k
+    sub-panel (k <= 32) and --n columns right of it, one launch."""
+    m, n, w = a.m, a.n, a.k
+    P0 = torch.randn(w + n, m, device="cuda")
+    P0[:w, :w] = torch.eye(w, device="cuda") + 0.1 * torch.randn(w, w, device="cuda").tril(-1).t()
+    P = P0.clone()
+    g = _fn(lib, "pla_k_panel_update", [i32, i32, i32, vp, lg, vp])
+
+    def launch():
+        return g(m, w, n, P.data_ptr(), m, None)
+
+    t = _time(torch, launch, a.warmup, a.reps)
+    flops = 2.0 * (m - w) * n * w + float(w) * w * n
+    byt = 4.0 * (2.0 * m * n + m * w)
+    return {"case": f"fp32 sub-panel step: U12 solve and A22 -= L21 U12, {m} x {n} x {w}",
+            "s": t, "tflops": flops / t / 1e12, "algorithmic_bytes": byt, "gbs": byt / t / 1e9}
 
 
 def case_batched(torch, lib, a):

@@ -158,3 +158,72 @@ def test_unit_lower_inverse(env, n):
     assert np.all(np.triu(D, 1) == 0.0) and np.all(np.diag(D) == 1.0)
     Dref = np.linalg.inv(L.astype(np.float32).astype(np.float64))
     assert np.abs(D - Dref).max() <= 64 * n * 2.0 ** -24 * np.abs(Dref).max()
+
+
+@pytest.mark.parametrize("m,w,ncols", [(32768, 32, 224), (1000, 20, 37), (32, 32, 100),
+                                       (33, 32, 480), (5000, 32, 16), (300, 7, 1)])
+def test_panel_update(env, m, w, ncols):
+    """The fp32 panel's sub-panel step after its interchanges (pla_k_panel_update):
+    U12 = inv(L11) A12 over A12 and A22 -= L21 U12, one launch, to fp32 rounding;
+    the sub-panel itself and the rows past m untouched.  Launched twice so the
+    per-group counters are seen reset."""
+    import scipy.linalg as sl
+    s, torch, pla, _ = env
+    lib = s.lib
+    lib.pla_k_panel_update.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                       ctypes.c_long, ctypes.c_void_p]
+    lib.pla_k_panel_update.restype = ctypes.c_int
+    ld = m + 3
+    for rep in range(2):
+        rng = np.random.default_rng(m + w + ncols + rep)
+        buf = rng.standard_normal((w + ncols, ld)).astype(np.float32)   # column-major, ld
+        buf[:w, :w] = (np.tril(rng.uniform(-1, 1, (w, w)), -1) + np.triu(np.full((w, w), 9.0))).T
+        t = torch.from_numpy(buf).cuda()
+        assert lib.pla_k_panel_update(m, w, ncols, t.data_ptr(), ld, None) == 0
+        torch.cuda.synchronize()
+        out = t.cpu().numpy()
+        A = buf[:, :m].T.astype(np.float64)                             # m x (w + ncols)
+        L11 = np.tril(A[:w, :w], -1) + np.eye(w)
+        U12 = sl.solve_triangular(L11, A[:w, w:], lower=True, unit_diagonal=True)
+        A22 = A[w:, w:] - A[w:, :w] @ U12
+        got = out[:, :m].T.astype(np.float64)
+        assert np.array_equal(out[:w], buf[:w])                          # the sub-panel
+        assert np.array_equal(out[:, m:], buf[:, m:])                    # rows past m
+        tol = 8 * w * 2.0 ** -24
+        assert np.abs(got[:w, w:] - U12).max() <= tol * max(1.0, np.abs(U12).max())
+        if m > w:
+            scale = np.abs(A[w:, w:]).max() + np.abs(A[w:, :w]).max() * np.abs(U12).max() * w
+            assert np.abs(got[w:, w:] - A22).max() <= tol * scale
+
+
+@pytest.mark.parametrize("r,b,pivoting", [(4096, 256, 1), (4096, 256, 0), (700, 96, 1),
+                                          (256, 256, 1)])
+def test_blocked_panel_is_an_lu_factorization(env, r, b, pivoting):
+    """The mixed LU's whole r x b fp32 panel (pla_k_panel_lu_blocked: 32-column
+    sub-panels, each followed by its interchanges and pla_k_panel_update):
+    P A = L U to fp32 rounding, with tournament (1) and partial (0) pivoting."""
+    s, torch, pla, _ = env
+    lib = s.lib
+    lib.pla_k_panel_lu_blocked.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_void_p]
+    lib.pla_k_panel_lu_blocked.restype = ctypes.c_int
+    A = np.random.default_rng(r + b + pivoting).standard_normal((r, b)).astype(np.float32)
+    t = torch.from_numpy(np.ascontiguousarray(A.T)).cuda()
+    piv = torch.full((b,), -7, dtype=torch.int32, device="cuda")
+    zinfo = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert lib.pla_k_panel_lu_blocked(pla.MPI_FLOAT, r, b, t.data_ptr(), r, piv.data_ptr(),
+                                      zinfo.data_ptr(), 72, pivoting, None) == 0
+    torch.cuda.synchronize()
+    LU = t.cpu().numpy().T.astype(np.float64)
+    p = piv.cpu().numpy()
+    assert np.all(p >= 0) and np.all(np.arange(b) + p < r) and int(zinfo.item()) == 0
+    perm = np.arange(r)
+    for j in range(b):
+        q = j + p[j]
+        perm[[j, q]] = perm[[q, j]]
+    L = np.tril(LU, -1)[:, :b] + np.eye(r, b)
+    U = np.triu(LU[:b])
+    res = np.abs(A[perm].astype(np.float64) - L @ U).max() / np.abs(A).max()
+    assert res < 4 * b * 2.0 ** -24
