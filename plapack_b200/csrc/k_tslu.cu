@@ -496,6 +496,17 @@ struct Ws {
   void *ptr = nullptr;
   size_t bytes = 0;
 };
+
+// panel_update_k's group counters, one set per (device, stream): launches on
+// one stream run in order and leave them at zero; launches on different
+// streams may overlap, so they do not share a set.  Freed by pla_tslu_release.
+struct PuCounters {
+  int dev;
+  cudaStream_t stream;
+  unsigned *ptr;
+};
+std::mutex g_pu_mu;
+std::vector<PuCounters> g_pu;
 Ws g_tws;
 int g_tsms = 0;
 
@@ -578,19 +589,23 @@ extern "C" int pla_k_panel_update(int m, int w, int ncols, float *P, long lda, c
   if (m <= 0 || w <= 0 || ncols <= 0) return 0;
   if (w > kW || w > m || ncols > PLA_K_PANEL_UPDATE_MAX) return (int)cudaErrorInvalidValue;
   constexpr int kGroups = (PLA_K_PANEL_UPDATE_MAX + kPG - 1) / kPG;
-  static std::mutex mu;
-  static std::vector<std::pair<cudaStream_t, unsigned *>> table;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
   unsigned *counters = nullptr;
   {
-    std::lock_guard<std::mutex> g(mu);
-    for (auto &pr : table)
-      if (pr.first == s) counters = pr.second;
+    std::lock_guard<std::mutex> g(g_pu_mu);
+    for (const PuCounters &pc : g_pu)
+      if (pc.dev == dev && pc.stream == s) counters = pc.ptr;
     if (!counters) {
-      cudaError_t e = cudaMalloc(&counters, kGroups * sizeof(unsigned));
+      e = cudaMalloc(&counters, kGroups * sizeof(unsigned));
       if (e != cudaSuccess) return (int)e;
       e = cudaMemsetAsync(counters, 0, kGroups * sizeof(unsigned), s);  // before the first launch
-      if (e != cudaSuccess) return (int)e;
-      table.emplace_back(s, counters);
+      if (e != cudaSuccess) {
+        cudaFree(counters);
+        return (int)e;
+      }
+      g_pu.push_back({dev, s, counters});
     }
   }
   dim3 grid(std::max(1, (m - w + kPU - 1) / kPU), (ncols + kPG - 1) / kPG);
@@ -606,4 +621,7 @@ extern "C" void pla_tslu_release(void) {
   if (g_tws.ptr) cudaFree(g_tws.ptr);
   g_tws.ptr = nullptr;
   g_tws.bytes = 0;
+  std::lock_guard<std::mutex> g(g_pu_mu);
+  for (const PuCounters &pc : g_pu) cudaFree(pc.ptr);
+  g_pu.clear();
 }
